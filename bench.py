@@ -1,0 +1,386 @@
+"""Benchmark of the hot path on B200: stiffness assembly throughput (elements/s)
+on the Q8 512x512 workload, plus the time to solve it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config q8_512]
+  python bench.py --impl reference ...     # the reference's CPU path on host cores
+
+One JSON line on rank 0.  `value` = elements assembled per second with inputs
+resident in HBM (device time of gf_assemble: K zero-fill + colour-scheduled fused
+integration/scatter kernels, FP32), L2 flushed between steps.  `e2e` = the same
+metric through the public C-ABI from pinned host buffers: mesh upload, pattern,
+colouring, assembly and download of the ELL matrix, every step.  For N > 1 each
+rank assembles its own replica of the workload (weak scaling; the assembly needs
+no exchange) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "elems/s assembled"
+UNIT = "elements/s"
+WORKLOADS = {
+    # name: (description, dtype of the timed assembly)
+    "q8_512": "Q8 512x512 plane stress, jitter 0.15h, 3x3 Gauss, log-normal E (sigma 0.5), "
+              "FP32 colour-scheduled assembly into ELL",
+    "q4_64": "Q4 64x64 plane stress, jitter 0.2h, 2x2 Gauss, FP64 assembly",
+    "brick8_128": "Brick8 128^3, jitter 0.1h, 2x2x2 Gauss, FP32 assembly",
+    "brick20_64": "Brick20 64^3, jitter 0.05h, 3x3x3 Gauss, correlated log-normal E, FP32",
+}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.fh = None
+
+    def __enter__(self):
+        try:
+            self.fh = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.fh is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.fh.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.fh.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU assembly on a bounded sample
+# ---------------------------------------------------------------------------
+def reference_sample(config: str, steps: int, warmup: int):
+    """Time the reference's StiffAlgoCPU (naive, OpenMP critical scatter, FP32 as
+    shipped) on a down-scaled copy of the workload; elements/s per step.  Falls
+    back to the single-threaded C oracle port when the reference build is absent."""
+    from gpufem_b200 import meshgen as mg
+    from oracle.oracle import Oracle, Reference
+    scale = {"q8_512": 1 / 4, "q4_64": 1.0, "brick8_128": 1 / 4, "brick20_64": 1 / 4}[config]
+    m = mg.workload(config, scale=scale)
+    cores = os.cpu_count() or 1
+    times = []
+    if Reference.available("fp32"):
+        kind = "reference"
+        R = Reference("fp32")
+        s = R.open_mesh(m)
+        for i in range(warmup + steps):
+            t = s.assemble(coloring=False, nthreads=cores)
+            if i >= warmup:
+                times.append(t)
+        s.close()
+        sample = (f"{mg.NAMES[m.elem_type]} {'x'.join(map(str, m.n))} ({m.nelem} elements, "
+                  f"scalar E): reference StiffAlgoCPU naive, FP32, {cores} OpenMP threads")
+    else:
+        kind = "port"
+        cores = 1
+        O = Oracle()
+        pat = O.pattern(m.elem_type, m.nnodes, m.conn)
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            O.assemble(m.elem_type, m.ngauss, m.coords, m.conn, m.E0, m.nu, E_elem=m.E, pattern=pat)
+            if i >= warmup:
+                times.append(time.perf_counter() - t0)
+        sample = (f"{mg.NAMES[m.elem_type]} {'x'.join(map(str, m.n))} ({m.nelem} elements): "
+                  f"C oracle port, FP64, 1 thread")
+    t = float(np.median(times))
+    return {"value": m.nelem / t, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+            "cpu": cpu_model(), "seconds_per_step": t}
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 5))
+    warm = max(1, min(args.warmup, 2))
+    cb = reference_sample(args.config, steps, warm)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": cb["seconds_per_step"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "description": WORKLOADS[args.config]},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu_arm(args):
+    import torch
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from gpufem_b200 import _lib
+    from gpufem_b200 import meshgen as mg
+    from gpufem_b200.fem import Context
+
+    cfg = args.config
+    m = mg.workload(cfg)
+    dtype = _lib.GF_F64 if cfg == "q4_64" else _lib.GF_F32
+    esize = 8 if dtype == _lib.GF_F64 else 4
+    ctx = Context(local)
+    ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+    n, W, nnz = ctx.build_pattern()
+    ctx.color(None)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        ctx.assemble(dtype, _lib.GF_SCATTER_COLOR)
+    barrier()
+    launches0 = ctx.launches()
+    dev_s = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            dev_s.append(ctx.assemble(dtype, _lib.GF_SCATTER_COLOR))
+        barrier()
+    launches = ctx.launches() - launches0
+    total = float(sum(dev_s))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    per_step = total / args.steps
+    value = world * m.nelem / per_step
+
+    # atomic scatter variant (measured against the colour schedule)
+    at = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        at.append(ctx.assemble(dtype, _lib.GF_SCATTER_ATOMIC))
+    atomic_eps = m.nelem / float(np.median(at))
+
+    # roofline of the assembly phase: algorithmic bytes = K values written once +
+    # node coordinates, connectivity and moduli read once
+    hbm, peak_kind = peaks()
+    alg_bytes = nnz * esize + m.nnodes * m.dim * esize + m.nelem * (m.nen * 4 + esize)
+    achieved = alg_bytes / per_step / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "ncu_traffic.json"
+    if tfile.exists():
+        tr = json.loads(tfile.read_text()).get(f"{cfg}/assemble")
+        traffic = None if tr is None else tr.get("bytes_per_assembly")
+
+    # SpMV roofline (FP32 values + int32 columns + x gather + y write)
+    ctx.assemble(dtype, _lib.GF_SCATTER_COLOR)
+    xs = torch.randn(n, device="cuda", dtype=torch.float32 if esize == 4 else torch.float64)
+    ys = torch.empty_like(xs)
+    sp = []
+    for _ in range(10):
+        flush.zero_()
+        torch.cuda.synchronize()
+        _lib.check(_lib.lib.gf_spmv(ctx.h, dtype, xs.data_ptr(), ys.data_ptr()), ctx.h)
+        sp.append(_lib.lib.gf_last_device_seconds(ctx.h))
+    t_spmv = float(np.median(sp))
+    spmv_bytes = nnz * (esize + 4) + n * (4 + 2 * esize)
+
+    # e2e through the public API from pinned host buffers, every step
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    h_coords, h_conn = pin(m.coords), pin(m.conn)
+    h_E = pin(m.E) if m.E is not None else None
+    h_rownnz = torch.empty(n, dtype=torch.int32).pin_memory()
+    h_colidx = torch.empty(n * W, dtype=torch.int32).pin_memory()
+    h_vals = torch.empty(n * W, dtype=torch.float32 if esize == 4 else torch.float64).pin_memory()
+    import ctypes as C
+    lib = _lib.lib
+
+    def e2e_step():
+        _lib.check(lib.gf_mesh_create(ctx.h, m.elem_type, m.nnodes, C.c_void_p(h_coords.data_ptr()),
+                                      m.nelem, C.c_void_p(h_conn.data_ptr()), m.ngauss, m.E0,
+                                      None if h_E is None else C.c_void_p(h_E.data_ptr()), m.nu, 0),
+                   ctx.h)
+        _lib.check(lib.gf_assemble(ctx.h, dtype, _lib.GF_SCATTER_COLOR, 0), ctx.h)
+        _lib.check(lib.gf_ell_download(ctx.h, dtype, C.c_void_p(h_rownnz.data_ptr()),
+                                       C.c_void_p(h_colidx.data_ptr()),
+                                       C.c_void_p(h_vals.data_ptr())), ctx.h)
+
+    e2e_step()
+    barrier()
+    e2e_t = []
+    for _ in range(max(2, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_per = float(np.median(e2e_t))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_per], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_per = float(t.item())
+    h2d = m.coords.nbytes + m.conn.nbytes + (m.E.nbytes if m.E is not None else 0)
+    d2h = n * 4 + n * W * 4 + n * W * esize
+
+    # solve: FP64 Jacobi-PCG vs FP32/FP64 mixed refinement on the same problem
+    solve = None
+    if not args.no_solve:
+        ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+        ctx.set_supports(m.supports)
+        ctx.set_force(m.f)
+        ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_COLOR)
+        ctx.assemble(_lib.GF_F32, _lib.GF_SCATTER_COLOR)
+        ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
+        ref = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-13, max_iter=400000,
+                        raise_on_error=False)
+        ustar = ctx.solution()
+        p64 = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-10, max_iter=400000,
+                        raise_on_error=False)
+        u64 = ctx.solution()
+        mix = ctx.solve(_lib.GF_SOLVER_MIXED_PCG, tol=1e-10, max_iter=400000, inner_tol=1e-4,
+                        raise_on_error=False)
+        umix = ctx.solution()
+        nrm = np.linalg.norm(ustar)
+        solve = {"oracle": {"solver": "FP64 Jacobi-PCG", "rel_residual": ref.rel_residual,
+                            "iterations": ref.iterations, "seconds": ref.seconds},
+                 "pcg_fp64": {"seconds": p64.seconds, "iterations": p64.iterations,
+                              "rel_residual": p64.rel_residual,
+                              "rel_err_vs_oracle": float(np.linalg.norm(u64 - ustar) / nrm)},
+                 "mixed_pcg": {"seconds": mix.seconds, "iterations": mix.iterations,
+                               "outer": mix.outer, "rel_residual": mix.rel_residual,
+                               "rel_err_vs_oracle": float(np.linalg.norm(umix - ustar) / nrm)},
+                 "tol": 1e-10}
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = reference_sample(cfg, steps=2, warmup=1)
+        cpu_baseline = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if esize == 4 else "f64", "data": "synthetic",
+            "config": {"workload": cfg, "description": WORKLOADS[cfg], "elements": m.nelem,
+                       "dofs": n, "nnz": nnz, "ell_width": W, "l2": "flushed (256 MB write) "
+                       "between timed steps", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "k_assemble (colour passes) + K zero-fill",
+                         "algorithmic_bytes": alg_bytes, "peak_source": peak_kind},
+            "roofline_spmv": {"bound": "hbm", "achieved": spmv_bytes / t_spmv / 1e9, "peak": hbm,
+                              "unit": "GB/s", "frac": spmv_bytes / t_spmv / 1e9 / hbm,
+                              "us_per_launch": t_spmv * 1e6, "algorithmic_bytes": spmv_bytes},
+            "atomic_scatter": {"value": atomic_eps, "unit": UNIT},
+            "e2e": {"value": world * m.nelem / e2e_per, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "includes": "mesh upload, pattern, colouring, assembly, ELL download"},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "solve": solve,
+            "cpu_baseline": cpu_baseline,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="q8_512", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,356 @@
+// Numeric assembly: Ke = sum_gp B^T D B detJ w for every element, scattered
+// straight into the column-major ELL values (Ke never touches HBM).
+//
+// Reference: StiffAlgoCPU::CalcGlobalStiffnessNaive / CalcStiffnessColoring
+// (src/FEM/StiffAlgoCPU.cc:58-284) with StiffAlgo::GetdShapeFunctNatCoord,
+// GetJacobianMatrix, BuildBMatrix (src/FEM/StiffAlgo.cc:47-278), det/matInverse
+// (src/LAops/LAops.cc:80-117) and AssembleK/AssembleKcol (StiffAlgo.cc:304-401).
+//
+// Formulation.  For isotropic D the node-pair block of B^T D B is
+//   Ke[i,a ; j,b] = sum_gp w detJ E ( lam1 g_i[a] g_j[b] + mu1 g_i[b] g_j[a]
+//                                     + mu1 delta_ab g_i . g_j )
+// with g_i = dN_i/dx and (lam1, mu1) the reference's D per unit modulus
+// (plane stress: lam1 = nu/(1-nu^2), mu1 = 1/(2(1+nu)); 3-D and plane strain:
+// the Lame constants per unit E).  This is B^T D B entry by entry, without the
+// zero entries of B: 2*dim^2 FMAs per node pair and Gauss point instead of the
+// dense (s x m) products.  Ke is symmetric, so only pairs i <= j are formed and
+// each writes block (i,j) and its transpose (j,i).
+//
+// CTA = a tile of TE elements of one colour (or any elements for the atomic
+// scatter), 256 threads:
+//   phase 1  thread per (element, Gauss point): J, detJ, J^-1, g = J^-1 dN/dxi
+//            into shared memory G[gp][node][comp][elem]; for the FP32 path an
+//            element whose max/min |detJ| over its Gauss points exceeds 10 gets
+//            J, J^-1 and g in FP64.
+//   phase 2  thread per (element, node pair i <= j): the dim x dim block, then
+//            read-modify-write into K (colour schedule: no two elements of a
+//            colour share a node, so plain RMW is race-free) or red.global.add
+//            (atomic schedule).  The slot of each block comes from the slot map
+//            built with the pattern.
+#include <cmath>
+#include <algorithm>
+
+#include "gf_internal.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct AsmTables {
+  // dN/dxi at each Gauss point: [gp][a][i], and weights, both precisions
+  double dN64[GF_MAX_GP * 3 * GF_MAX_NEN];
+  float dN32[GF_MAX_GP * 3 * GF_MAX_NEN];
+  double w64[GF_MAX_GP];
+  float w32[GF_MAX_GP];
+};
+
+template <int DIM, typename R>
+__device__ inline R det_inv(const R (&J)[3][3], R (&Ji)[3][3]) {
+  if (DIM == 2) {
+    R d = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    R id = R(1) / d;
+    Ji[0][0] = J[1][1] * id;
+    Ji[0][1] = -J[0][1] * id;
+    Ji[1][0] = -J[1][0] * id;
+    Ji[1][1] = J[0][0] * id;
+    return d;
+  } else {
+    R c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    R c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    R c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    R d = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    R id = R(1) / d;
+    Ji[0][0] = c00 * id;
+    Ji[1][0] = c01 * id;
+    Ji[2][0] = c02 * id;
+    Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+    Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+    Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+    Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    return d;
+  }
+}
+
+// Jacobian J[a][b] = sum_i dN_i/dxi_a * x_i[b] (rows natural, columns x,y,z),
+// as StiffAlgo::GetJacobianMatrix (StiffAlgo.cc:207-244).
+template <int NEN, int DIM, typename R, typename TC>
+__device__ inline void jacobian(const TC* dN /*[DIM][NEN]*/, const TC* X /*[NEN][DIM]*/,
+                                R (&J)[3][3]) {
+#pragma unroll
+  for (int a = 0; a < DIM; ++a)
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) {
+      R s = R(0);
+#pragma unroll 4
+      for (int i = 0; i < NEN; ++i) s += R(dN[a * NEN + i]) * R(X[i * DIM + b]);
+      J[a][b] = s;
+    }
+}
+
+template <typename T>
+__device__ inline void k_add(T* p, T v, bool atomic) {
+  if (atomic) {
+    atomicAdd(p, v);
+  } else {
+    *p += v;
+  }
+}
+
+template <int ET, typename TC, bool ATOMIC>
+__global__ void __launch_bounds__(kThreads)
+k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
+           const int32_t* __restrict__ conn, const TC* __restrict__ coords,
+           const TC* __restrict__ Eel, const uint16_t* __restrict__ slotmap, int nelem, int n,
+           const AsmTables* __restrict__ tab, TC lam1, TC mu1, TC* __restrict__ K) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  constexpr int NEN = info.nen, DIM = info.dim;
+  constexpr int NPAIR = NEN * (NEN + 1) / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TC* sdN = reinterpret_cast<TC*>(smem_raw);                 // ngp*DIM*NEN
+  TC* sw = sdN + ngp * DIM * NEN;                            // ngp
+  TC* sX = sw + ngp;                                         // TE*NEN*DIM
+  TC* sG = sX + TE * NEN * DIM;                              // ngp*NEN*DIM*TE
+  TC* swd = sG + ngp * NEN * DIM * TE;                       // ngp*TE
+  int* sconn = reinterpret_cast<int*>(swd + ngp * TE);       // TE*NEN
+  int* sel = sconn + TE * NEN;                               // TE
+  int* sflag = sel + TE;                                     // TE
+
+  const int tile0 = blockIdx.x * TE;
+  const int nt = min(TE, count - tile0);
+  const bool f64 = sizeof(TC) == 8;
+
+  for (int k = threadIdx.x; k < ngp * DIM * NEN; k += kThreads)
+    sdN[k] = f64 ? TC(tab->dN64[k]) : TC(tab->dN32[k]);
+  for (int k = threadIdx.x; k < ngp; k += kThreads) sw[k] = f64 ? TC(tab->w64[k]) : TC(tab->w32[k]);
+  for (int e = threadIdx.x; e < TE; e += kThreads) {
+    sel[e] = e < nt ? elems[tile0 + e] : -1;
+    sflag[e] = 0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nt * NEN; k += kThreads) {
+    const int e = k / NEN, i = k % NEN;
+    const int node = conn[(int64_t)sel[e] * NEN + i];
+    sconn[k] = node;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) sX[k * DIM + c] = coords[(int64_t)node * DIM + c];
+  }
+  __syncthreads();
+
+  // phase 1a (FP32 path only): flag elements with a large detJ spread
+  if (!f64) {
+    for (int e = threadIdx.x; e < nt; e += kThreads) {
+      float dmin = 3.4e38f, dmax = 0.f;
+      for (int g = 0; g < ngp; ++g) {
+        float J[3][3], Ji[3][3];
+        jacobian<NEN, DIM, float, TC>(sdN + g * DIM * NEN, sX + e * NEN * DIM, J);
+        float d = fabsf(det_inv<DIM, float>(J, Ji));
+        dmin = fminf(dmin, d);
+        dmax = fmaxf(dmax, d);
+      }
+      sflag[e] = (dmax > 10.f * dmin) ? 1 : 0;
+    }
+    __syncthreads();
+  }
+
+  // phase 1: gradients at Gauss points
+  for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
+    const int e = t % TE, g = t / TE;
+    if (e >= nt) continue;
+    const TC* dN = sdN + g * DIM * NEN;
+    const TC* X = sX + e * NEN * DIM;
+    TC detJ;
+    if (f64 || sflag[e]) {
+      double J[3][3], Ji[3][3];
+      jacobian<NEN, DIM, double, TC>(dN, X, J);
+      detJ = TC(det_inv<DIM, double>(J, Ji));
+#pragma unroll 4
+      for (int i = 0; i < NEN; ++i) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          double s = 0.0;
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) s += Ji[c][a] * double(dN[a * NEN + i]);
+          sG[((g * NEN + i) * DIM + c) * TE + e] = TC(s);
+        }
+      }
+    } else {
+      TC J[3][3], Ji[3][3];
+      jacobian<NEN, DIM, TC, TC>(dN, X, J);
+      detJ = det_inv<DIM, TC>(J, Ji);
+#pragma unroll 4
+      for (int i = 0; i < NEN; ++i) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          TC s = TC(0);
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i];
+          sG[((g * NEN + i) * DIM + c) * TE + e] = s;
+        }
+      }
+    }
+    swd[g * TE + e] = sw[g] * detJ * Eel[sel[e]];
+  }
+  __syncthreads();
+
+  // phase 2: node-pair blocks and scatter
+  for (int t = threadIdx.x; t < TE * NPAIR; t += kThreads) {
+    const int e = t % TE;
+    if (e >= nt) continue;
+    int p = t / TE;
+    // pair index -> (i, j), i <= j, row-major upper triangle
+    int i = 0;
+    while (p >= NEN - i) { p -= NEN - i; ++i; }
+    const int j = i + p;
+    TC H[DIM][DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) H[a][b] = TC(0);
+    for (int g = 0; g < ngp; ++g) {
+      const TC w = swd[g * TE + e];
+      TC gi[DIM], gj[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        gi[c] = sG[((g * NEN + i) * DIM + c) * TE + e] * w;
+        gj[c] = sG[((g * NEN + j) * DIM + c) * TE + e];
+      }
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) H[a][b] += gi[a] * gj[b];
+    }
+    TC tr = TC(0);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) tr += H[a][a];
+    const int el = sel[e];
+    const int ni = sconn[e * NEN + i], nj = sconn[e * NEN + j];
+    const int sij = slotmap[(int64_t)(i * NEN + j) * nelem + el] * DIM;
+    const int sji = slotmap[(int64_t)(j * NEN + i) * nelem + el] * DIM;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        TC v = lam1 * H[a][b] + mu1 * H[b][a];
+        if (a == b) v += mu1 * tr;
+        k_add(&K[(int64_t)(sij + b) * n + (ni * DIM + a)], v, ATOMIC);
+        if (i != j) k_add(&K[(int64_t)(sji + a) * n + (nj * DIM + b)], v, ATOMIC);
+      }
+  }
+}
+
+template <int ET, typename TC>
+size_t smem_bytes(int TE, int ngp) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  size_t nTC = (size_t)ngp * info.dim * info.nen + ngp + (size_t)TE * info.nen * info.dim +
+               (size_t)ngp * info.nen * info.dim * TE + (size_t)ngp * TE;
+  return nTC * sizeof(TC) + sizeof(int) * ((size_t)TE * info.nen + 2 * TE) + 16;
+}
+
+template <int ET, typename TC>
+int pick_tile(int ngp) {
+  // largest power of two <= 128 whose working set fits ~100 KB (2 CTAs per SM)
+  int TE = 128;
+  while (TE > 4 && smem_bytes<ET, TC>(TE, ngp) > 100 * 1024) TE >>= 1;
+  return TE;
+}
+
+template <int ET, typename TC>
+gf_status launch_et(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* K) {
+  const int TE = pick_tile<ET, TC>(ctx->ngp);
+  const size_t sm = smem_bytes<ET, TC>(TE, ctx->ngp);
+  const TC* coords = sizeof(TC) == 8 ? (const TC*)ctx->d_coords64 : (const TC*)ctx->d_coords32;
+  const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
+  auto kc = k_assemble<ET, TC, false>;
+  auto ka = k_assemble<ET, TC, true>;
+  GF_CUDA(ctx, cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  if (scatter == GF_SCATTER_ATOMIC) {
+    const int count = ctx->nelem;
+    ka<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
+        ctx->d_allperm, count, TE, ctx->ngp, ctx->d_conn, coords, Eel, ctx->d_slotmap,
+        ctx->nelem, ctx->n, d_tab, TC(ctx->lam1), TC(ctx->mu1), K);
+    GF_LAUNCH_CHECK(ctx, "k_assemble(atomic)");
+  } else {
+    for (int c = 0; c < ctx->ncolors; ++c) {
+      const int c0 = ctx->color_off[c], count = ctx->color_off[c + 1] - c0;
+      if (count == 0) continue;
+      kc<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
+          ctx->d_perm + c0, count, TE, ctx->ngp, ctx->d_conn, coords, Eel, ctx->d_slotmap,
+          ctx->nelem, ctx->n, d_tab, TC(ctx->lam1), TC(ctx->mu1), K);
+      GF_LAUNCH_CHECK(ctx, "k_assemble(colour)");
+    }
+  }
+  return GF_OK;
+}
+
+template <typename TC>
+gf_status launch_dispatch(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* K) {
+  switch (ctx->elem_type) {
+    case GF_Q4: return launch_et<GF_Q4, TC>(ctx, scatter, d_tab, K);
+    case GF_Q8: return launch_et<GF_Q8, TC>(ctx, scatter, d_tab, K);
+    case GF_BRICK8: return launch_et<GF_BRICK8, TC>(ctx, scatter, d_tab, K);
+    default: return launch_et<GF_BRICK20, TC>(ctx, scatter, d_tab, K);
+  }
+}
+
+}  // namespace
+
+// Shape-derivative tables for the context's element type and Gauss rule, kept
+// in a small device buffer owned by the context (built once per mesh).
+static gf_status ensure_tables(gf_ctx* ctx) {
+  if (ctx->d_asmtab) return GF_OK;
+  AsmTables h{};
+  std::vector<double> pts, w;
+  gf_gauss_rule<double>(ctx->dim, ctx->ngauss, pts, w);
+  std::vector<double> dN(ctx->dim * ctx->nen);
+  for (int g = 0; g < ctx->ngp; ++g) {
+    gf_dshape<double>(ctx->elem_type, gf_node_nat_host[ctx->elem_type], &pts[g * ctx->dim],
+                      dN.data());
+    for (int k = 0; k < ctx->dim * ctx->nen; ++k) {
+      h.dN64[g * ctx->dim * ctx->nen + k] = dN[k];
+      h.dN32[g * ctx->dim * ctx->nen + k] = (float)dN[k];
+    }
+    h.w64[g] = w[g];
+    h.w32[g] = (float)w[g];
+  }
+  AsmTables* d = nullptr;
+  gf_status st = gf_alloc(ctx, &d, 1);
+  if (st != GF_OK) return st;
+  GF_CUDA(ctx, cudaMemcpy(d, &h, sizeof(AsmTables), cudaMemcpyHostToDevice));
+  ctx->d_asmtab = d;
+  return GF_OK;
+}
+
+gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
+  if (engine != GF_ENGINE_CUDA_CORE)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "tensor-core engine not available in this build");
+  gf_status st;
+  if ((st = ensure_tables(ctx)) != GF_OK) return st;
+  const AsmTables* d_tab = (const AsmTables*)ctx->d_asmtab;
+  const int64_t total = (int64_t)ctx->n * ctx->W;
+  if (dtype == GF_F64) {
+    if (!ctx->d_K64 && (st = gf_alloc(ctx, &ctx->d_K64, (size_t)total)) != GF_OK) return st;
+  } else {
+    if (!ctx->d_K32 && (st = gf_alloc(ctx, &ctx->d_K32, (size_t)total)) != GF_OK) return st;
+  }
+  cudaEventRecord(ctx->ev0, ctx->stream);
+  if (dtype == GF_F64) {
+    cudaMemsetAsync(ctx->d_K64, 0, sizeof(double) * total, ctx->stream);
+    st = launch_dispatch<double>(ctx, scatter, d_tab, ctx->d_K64);
+  } else {
+    cudaMemsetAsync(ctx->d_K32, 0, sizeof(float) * total, ctx->stream);
+    st = launch_dispatch<float>(ctx, scatter, d_tab, ctx->d_K32);
+  }
+  cudaEventRecord(ctx->ev1, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (st != GF_OK) return st;
+  if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "assembly");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->last_seconds = ms * 1e-3;
+  if (dtype == GF_F64) ctx->has64 = true; else ctx->has32 = true;
+  ctx->bc_mode_applied = -1;
+  return GF_OK;
+}

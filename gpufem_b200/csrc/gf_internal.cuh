@@ -1,0 +1,254 @@
+// Internal declarations shared by the gpufem_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "gpufem_b200.h"
+
+// ---------------------------------------------------------------------------
+// Element families.  Node natural coordinates follow the reference's node order
+// (src/FEM/StiffAlgo.cc:47-202):
+//   Q4      (-1,-1) (1,-1) (1,1) (-1,1)
+//   Q8      (-1,-1) (0,-1) (1,-1) (1,0) (1,1) (0,1) (-1,1) (-1,0)
+//   Brick8  (1,-1,-1) (1,1,-1) (1,1,1) (1,-1,1) (-1,-1,-1) (-1,1,-1) (-1,1,1) (-1,-1,1)
+//   Brick20 corners at 0,2,4,6 (r=+1) and 12,14,16,18 (r=-1) in Brick8's (s,t) order;
+//           mid-side nodes 1,3,5,7 on r=+1, 8..11 on r=0, 13,15,17,19 on r=-1.
+// Shape functions are the standard bilinear/trilinear Lagrange and quadratic
+// serendipity families written from their definitions; derivatives are taken
+// analytically below.
+// ---------------------------------------------------------------------------
+constexpr int GF_MAX_NEN = 20;
+constexpr int GF_MAX_GP = 27;
+
+struct ElemInfo {
+  int nen, dim, serendipity;
+};
+
+__host__ __device__ constexpr ElemInfo gf_elem_info(int et) {
+  return et == GF_Q4 ? ElemInfo{4, 2, 0}
+       : et == GF_Q8 ? ElemInfo{8, 2, 1}
+       : et == GF_BRICK8 ? ElemInfo{8, 3, 0}
+                         : ElemInfo{20, 3, 1};
+}
+
+// natural coordinates (xi, eta, zeta) of element nodes, [et][node][3]
+extern const signed char gf_node_nat_host[4][GF_MAX_NEN][3];
+
+// Derivatives dN_i/dxi_a at natural point p (host and device), written from:
+//   Lagrange:     N = prod_a (1 + xi_a p_a) / 2^dim
+//   Serendipity corner:   N = prod(1 + xi_a p_a)/2^dim * (sum_a xi_a p_a - (dim-1))
+//   Serendipity mid-side (one xi_c = 0):
+//                 N = (1 - p_c^2) * prod_{a != c} (1 + xi_a p_a) / 2^(dim-1)
+template <typename R>
+__host__ __device__ inline void gf_dshape(int et, const signed char (*nat)[3], const R* p,
+                                          R* dN /* [dim][nen] */) {
+  const ElemInfo info = gf_elem_info(et);
+  const int dim = info.dim, nen = info.nen;
+  for (int i = 0; i < nen; ++i) {
+    R xi[3] = {R(nat[i][0]), R(nat[i][1]), R(nat[i][2])};
+    R f[3];    // linear factors (1 + xi_a p_a)
+    for (int a = 0; a < dim; ++a) f[a] = R(1) + xi[a] * p[a];
+    if (!info.serendipity) {
+      const R scale = dim == 2 ? R(0.25) : R(0.125);
+      for (int a = 0; a < dim; ++a) {
+        R d = scale * xi[a];
+        for (int b = 0; b < dim; ++b)
+          if (b != a) d *= f[b];
+        dN[a * nen + i] = d;
+      }
+    } else {
+      int c = -1;  // zero natural coordinate (mid-side node)
+      for (int a = 0; a < dim; ++a)
+        if (nat[i][a] == 0) c = a;
+      if (c < 0) {
+        const R scale = dim == 2 ? R(0.25) : R(0.125);
+        R lin = R(1);
+        for (int a = 0; a < dim; ++a) lin *= f[a];
+        R s = -R(dim - 1);
+        for (int a = 0; a < dim; ++a) s += xi[a] * p[a];
+        for (int a = 0; a < dim; ++a) {
+          // d/dp_a [ scale * prod f * s ] = scale * (xi_a prod_{b!=a} f_b * s + prod f * xi_a)
+          R pr = R(1);
+          for (int b = 0; b < dim; ++b)
+            if (b != a) pr *= f[b];
+          dN[a * nen + i] = scale * xi[a] * (pr * s + lin);
+        }
+      } else {
+        const R scale = dim == 2 ? R(0.5) : R(0.25);
+        R q = R(1) - p[c] * p[c];
+        for (int a = 0; a < dim; ++a) {
+          R d;
+          if (a == c) {
+            d = scale * (R(-2) * p[c]);
+            for (int b = 0; b < dim; ++b)
+              if (b != c) d *= f[b];
+          } else {
+            d = scale * q * xi[a];
+            for (int b = 0; b < dim; ++b)
+              if (b != c && b != a) d *= f[b];
+          }
+          dN[a * nen + i] = d;
+        }
+      }
+    }
+  }
+}
+
+// Gauss rule in the reference's tensor order (FemData::CalcGaussVectors,
+// src/FEM/FemData.cc:226-316): index s runs i (first coordinate) outermost,
+// last coordinate innermost; weight = product of 1-D weights.
+template <typename R>
+inline void gf_gauss_rule(int dim, int ng1, std::vector<R>& pts, std::vector<R>& w) {
+  R x[3], wt[3];
+  if (ng1 == 2) {
+    x[0] = -R(1) / std::sqrt(R(3)); x[1] = -x[0];
+    wt[0] = wt[1] = R(1);
+  } else {
+    x[0] = -std::sqrt(R(3) / R(5)); x[1] = R(0); x[2] = -x[0];
+    wt[0] = R(5) / R(9); wt[1] = R(8) / R(9); wt[2] = wt[0];
+  }
+  pts.clear(); w.clear();
+  if (dim == 2) {
+    for (int i = 0; i < ng1; ++i)
+      for (int j = 0; j < ng1; ++j) {
+        pts.push_back(x[i]); pts.push_back(x[j]);
+        w.push_back(wt[i] * wt[j]);
+      }
+  } else {
+    for (int i = 0; i < ng1; ++i)
+      for (int j = 0; j < ng1; ++j)
+        for (int k = 0; k < ng1; ++k) {
+          pts.push_back(x[i]); pts.push_back(x[j]); pts.push_back(x[k]);
+          w.push_back(wt[i] * wt[j] * wt[k]);
+        }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct SolveScalars;  // device-side solver scalars (gf_solve.cu)
+
+struct gf_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  double last_seconds = 0.0;
+  int64_t launches = 0;
+  int sm_count = 148;
+
+  // mesh
+  bool has_mesh = false;
+  int elem_type = 0, dim = 0, nen = 0, ngauss = 0, ngp = 0;
+  int nnodes = 0, nelem = 0, analysis = 0;
+  double E = 0.0, nu = 0.0;
+  double lam1 = 0.0, mu1 = 0.0;  // Lame-type factors per unit modulus
+  std::vector<int32_t> h_conn;   // 0-based, host copy (colouring)
+  double* d_coords64 = nullptr;
+  float* d_coords32 = nullptr;
+  int32_t* d_conn = nullptr;     // 0-based node ids
+  double* d_Eel = nullptr;       // per-element modulus
+  float* d_Eel32 = nullptr;
+  void* d_asmtab = nullptr;      // shape-derivative tables (gf_assemble.cu)
+
+  // colouring
+  int ncolors = 0;
+  std::vector<int32_t> h_color;      // per element
+  std::vector<int32_t> color_off;    // ncolors + 1
+  int32_t* d_perm = nullptr;         // elements sorted by colour
+  int32_t* d_allperm = nullptr;      // identity (atomic scatter)
+
+  // pattern
+  bool has_pattern = false;
+  int n = 0, W = 0;
+  int64_t nnz = 0;
+  int32_t* d_rownnz = nullptr;
+  int32_t* d_colidx = nullptr;
+  uint16_t* d_slotmap = nullptr;  // [nen*nen][nelem]: neighbour position of node j in node i's list
+  int32_t* d_adj_off = nullptr;   // node adjacency CSR
+  int32_t* d_adj = nullptr;
+  int32_t* d_diagpos = nullptr;   // per node: own position in its adjacency list
+
+  // values
+  bool has64 = false, has32 = false;
+  double* d_K64 = nullptr;
+  float* d_K32 = nullptr;
+
+  // loads / constraints
+  double* d_f = nullptr;
+  std::vector<double> h_f;
+  std::vector<int32_t> h_supports;  // nsup*(dim+1)
+  int nsup = 0;
+  uint8_t* d_fixed = nullptr;       // per dof
+  int bc_mode_applied = -1;
+
+  // solver state
+  double* d_u = nullptr;
+  void* d_work = nullptr;  // solver work vectors
+  size_t work_bytes = 0;
+  SolveScalars* d_scal = nullptr;
+  void* h_pinned = nullptr;  // pinned scalars readback
+  double* d_red = nullptr;   // reduction scratch
+};
+
+// ---------------------------------------------------------------------------
+// Error helpers
+// ---------------------------------------------------------------------------
+gf_status gf_fail(gf_ctx* ctx, gf_status st, const char* fmt, ...);
+gf_status gf_cuda_fail(gf_ctx* ctx, cudaError_t e, const char* where);
+
+#define GF_CUDA(ctx, call)                                   \
+  do {                                                       \
+    cudaError_t e__ = (call);                                \
+    if (e__ != cudaSuccess) return gf_cuda_fail(ctx, e__, #call); \
+  } while (0)
+
+#define GF_LAUNCH_CHECK(ctx, name)                                    \
+  do {                                                                \
+    (ctx)->launches++;                                                \
+    cudaError_t e__ = cudaGetLastError();                             \
+    if (e__ != cudaSuccess) return gf_cuda_fail(ctx, e__, name);      \
+  } while (0)
+
+template <typename T>
+gf_status gf_alloc(gf_ctx* ctx, T** p, size_t count) {
+  if (*p) { cudaFree(*p); *p = nullptr; }
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return gf_fail(ctx, e == cudaErrorMemoryAllocation ? GF_ERR_OOM : GF_ERR_CUDA,
+                   "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
+                   cudaGetErrorString(e));
+  }
+  return GF_OK;
+}
+
+template <typename T>
+void gf_free(T*& p) {
+  if (p) { cudaFree(p); p = nullptr; }
+}
+
+inline int gf_blocks(int64_t work, int threads) {
+  int64_t b = (work + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > (1LL << 30)) b = (1LL << 30);
+  return (int)b;
+}
+
+// internal entry points across translation units
+gf_status gf_pattern_build(gf_ctx* ctx);
+gf_status gf_color_build(gf_ctx* ctx, const int32_t* user_colors);
+gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine);
+gf_status gf_constraints_apply(gf_ctx* ctx, int mode);
+gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y);
+gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info);
+void gf_solver_free(gf_ctx* ctx);
+void gf_mesh_free(gf_ctx* ctx);
+void gf_pattern_free(gf_ctx* ctx);

@@ -1,0 +1,342 @@
+// Symbolic phase: the topological ELL pattern (built on the device) and the
+// element colour schedule (built on the host).
+//
+// Pattern.  The reference discovers its pattern entry by entry while adding
+// values (ELLmatrix::AddElem/InsertElem, src/SPRmatrix/ELLmatrix.cc:91-138),
+// so its row lengths depend on which contributions are exactly 0.0 and its
+// padded width grows 32 -> +64 (ELLmatrix.cc:486-529).  Here the pattern is
+// topological: row r (component c of node a) holds every dof of every node
+// that shares an element with a, in increasing column order, stored
+// column-major (entry (row, slot) at slot*n + row; ELLmatrix.h:35-44).
+// width W = max row length; slots past rownnz hold col = row and value 0.
+//
+// Steps (all on the device):
+//   1. node -> element incidence (count, scan, fill)
+//   2. per node, the sorted set of adjacent nodes (warp per node, candidates in
+//      shared memory, rank of each distinct candidate = its position)
+//   3. rownnz / colidx
+//   4. slot map: for element e and local nodes (i, j), the position of node_j in
+//      node_i's adjacency list, so the numeric scatter never searches.
+//
+// Colouring.  Greedy first-fit over elements in index order where elements
+// sharing at least one node conflict: the rule of femColor::MakeGreedyColoring
+// over METIS_MeshToDual(ncommon = 1) (src/FEM/femColor.cc:79-191).
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <numeric>
+
+#include "gf_internal.cuh"
+
+namespace {
+
+constexpr int kWarpsPerBlock = 8;
+constexpr int kCandCap = 1024;  // candidate nodes per node (valence * nen)
+
+__global__ void k_count_incidence(int64_t total, const int32_t* __restrict__ conn,
+                                  int32_t* __restrict__ cnt) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < total) atomicAdd(&cnt[conn[i]], 1);
+}
+
+__global__ void k_fill_incidence(int64_t total, int nen, const int32_t* __restrict__ conn,
+                                 int32_t* __restrict__ fillptr, int32_t* __restrict__ inc) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < total) {
+    int pos = atomicAdd(&fillptr[conn[i]], 1);
+    inc[pos] = (int32_t)(i / nen);
+  }
+}
+
+// Warp per node: collect the nodes of all incident elements, then for each
+// first occurrence compute its rank among distinct values.  mode 0 counts,
+// mode 1 writes adj[adj_off[node] + rank].
+template <int MODE>
+__global__ void k_node_adjacency(int nnodes, int nen, const int32_t* __restrict__ conn,
+                                 const int32_t* __restrict__ inc_off,
+                                 const int32_t* __restrict__ inc,
+                                 int32_t* __restrict__ nadj, const int32_t* __restrict__ adj_off,
+                                 int32_t* __restrict__ adj, int32_t* __restrict__ errflag) {
+  __shared__ int32_t cand[kWarpsPerBlock][kCandCap];
+  __shared__ uint8_t firstf[kWarpsPerBlock][kCandCap];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int node = blockIdx.x * kWarpsPerBlock + warp;
+  if (node >= nnodes) return;
+  int32_t* c = cand[warp];
+  uint8_t* fl = firstf[warp];
+  const int e0 = inc_off[node], e1 = inc_off[node + 1];
+  const int C = (e1 - e0) * nen;
+  if (C > kCandCap) {
+    if (lane == 0) atomicExch(errflag, 1);
+    return;
+  }
+  for (int k = lane; k < C; k += 32) {
+    int e = inc[e0 + k / nen];
+    c[k] = conn[(int64_t)e * nen + (k % nen)];
+  }
+  __syncwarp();
+  // first-occurrence flags
+  for (int k = lane; k < C; k += 32) {
+    const int v = c[k];
+    uint8_t first = 1;
+    for (int q = 0; q < k; ++q)
+      if (c[q] == v) { first = 0; break; }
+    fl[k] = first;
+  }
+  __syncwarp();
+  int count = 0;
+  for (int k = lane; k < C; k += 32) {
+    if (!fl[k]) continue;
+    if (MODE == 0) {
+      ++count;
+    } else {
+      const int v = c[k];
+      int rank = 0;
+      for (int q = 0; q < C; ++q) rank += (fl[q] && c[q] < v) ? 1 : 0;
+      adj[adj_off[node] + rank] = v;
+    }
+  }
+  if (MODE == 0) {
+    for (int o = 16; o > 0; o >>= 1) count += __shfl_down_sync(0xffffffffu, count, o);
+    if (lane == 0) nadj[node] = count;
+  }
+}
+
+__global__ void k_rownnz(int nnodes, int dim, const int32_t* __restrict__ nadj,
+                         int32_t* __restrict__ rownnz) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < nnodes)
+    for (int c = 0; c < dim; ++c) rownnz[a * dim + c] = nadj[a] * dim;
+}
+
+__global__ void k_colidx(int n, int W, int dim, const int32_t* __restrict__ rownnz,
+                         const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
+                         int32_t* __restrict__ colidx) {
+  const int64_t total = (int64_t)n * W;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int row = (int)(i % n);
+    const int slot = (int)(i / n);
+    int col = row;
+    if (slot < rownnz[row]) {
+      const int node = row / dim;
+      col = adj[adj_off[node] + slot / dim] * dim + slot % dim;
+    }
+    colidx[i] = col;
+  }
+}
+
+// thread per (element, local node i); e fastest so slot-map writes coalesce.
+__global__ void k_slotmap(int nelem, int nen, const int32_t* __restrict__ conn,
+                          const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
+                          uint16_t* __restrict__ slotmap, int32_t* __restrict__ errflag) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nelem * nen) return;
+  const int e = (int)(t % nelem);
+  const int i = (int)(t / nelem);
+  const int a = conn[(int64_t)e * nen + i];
+  const int lo0 = adj_off[a], hi0 = adj_off[a + 1];
+  for (int j = 0; j < nen; ++j) {
+    const int b = conn[(int64_t)e * nen + j];
+    int lo = lo0, hi = hi0;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (adj[mid] < b) lo = mid + 1; else hi = mid;
+    }
+    if (lo >= hi0 || adj[lo] != b) atomicExch(errflag, 2);
+    slotmap[(int64_t)(i * nen + j) * nelem + e] = (uint16_t)(lo - lo0);
+  }
+}
+
+__global__ void k_diagpos(int nnodes, const int32_t* __restrict__ adj_off,
+                          const int32_t* __restrict__ adj, int32_t* __restrict__ diagpos) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= nnodes) return;
+  int lo = adj_off[a], hi = adj_off[a + 1];
+  const int lo0 = lo;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (adj[mid] < a) lo = mid + 1; else hi = mid;
+  }
+  diagpos[a] = lo - lo0;
+}
+
+}  // namespace
+
+gf_status gf_pattern_build(gf_ctx* ctx) {
+  const int nnodes = ctx->nnodes, nelem = ctx->nelem, nen = ctx->nen, dim = ctx->dim;
+  const int64_t total = (int64_t)nelem * nen;
+  cudaStream_t s = ctx->stream;
+  gf_pattern_free(ctx);
+  gf_status st;
+
+  int32_t *d_cnt = nullptr, *d_inc_off = nullptr, *d_fill = nullptr, *d_inc = nullptr;
+  int32_t *d_nadj = nullptr, *d_err = nullptr, *d_max = nullptr;
+  void* d_tmp = nullptr;
+  size_t tmp_bytes = 0, b1 = 0, b2 = 0, b3 = 0;
+  auto cleanup = [&]() {
+    gf_free(d_cnt); gf_free(d_inc_off); gf_free(d_fill); gf_free(d_inc);
+    gf_free(d_nadj); gf_free(d_err); gf_free(d_max);
+    if (d_tmp) cudaFree(d_tmp);
+  };
+#define GF_TRY(x)             \
+  do {                        \
+    if ((st = (x)) != GF_OK) { cleanup(); return st; } \
+  } while (0)
+#define GF_TRYC(call)                                                  \
+  do {                                                                 \
+    cudaError_t e__ = (call);                                          \
+    if (e__ != cudaSuccess) { cleanup(); return gf_cuda_fail(ctx, e__, #call); } \
+  } while (0)
+
+  GF_TRY(gf_alloc(ctx, &d_cnt, (size_t)nnodes + 1));
+  GF_TRY(gf_alloc(ctx, &d_inc_off, (size_t)nnodes + 1));
+  GF_TRY(gf_alloc(ctx, &d_fill, (size_t)nnodes + 1));
+  GF_TRY(gf_alloc(ctx, &d_inc, (size_t)total));
+  GF_TRY(gf_alloc(ctx, &d_nadj, (size_t)nnodes + 1));
+  GF_TRY(gf_alloc(ctx, &d_err, 1));
+  GF_TRY(gf_alloc(ctx, &d_max, 1));
+  GF_TRY(gf_alloc(ctx, &ctx->d_adj_off, (size_t)nnodes + 1));
+  GF_TRYC(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (nnodes + 1), s));
+  GF_TRYC(cudaMemsetAsync(d_nadj, 0, sizeof(int32_t) * (nnodes + 1), s));
+  GF_TRYC(cudaMemsetAsync(d_err, 0, sizeof(int32_t), s));
+
+  cub::DeviceScan::ExclusiveSum(nullptr, b1, d_cnt, d_inc_off, nnodes + 1, s);
+  cub::DeviceReduce::Max(nullptr, b2, d_nadj, d_max, nnodes, s);
+  b3 = b1;
+  tmp_bytes = std::max(b1, std::max(b2, b3));
+  GF_TRYC(cudaMalloc(&d_tmp, tmp_bytes));
+
+  k_count_incidence<<<gf_blocks(total, 256), 256, 0, s>>>(total, ctx->d_conn, d_cnt);
+  ctx->launches++;
+  GF_TRYC(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_cnt, d_inc_off, nnodes + 1, s));
+  GF_TRYC(cudaMemcpyAsync(d_fill, d_inc_off, sizeof(int32_t) * (nnodes + 1),
+                          cudaMemcpyDeviceToDevice, s));
+  k_fill_incidence<<<gf_blocks(total, 256), 256, 0, s>>>(total, nen, ctx->d_conn, d_fill, d_inc);
+  ctx->launches++;
+  const int ablocks = (nnodes + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  k_node_adjacency<0><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
+      nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, nullptr, nullptr, d_err);
+  ctx->launches++;
+  GF_TRYC(cudaGetLastError());
+  GF_TRYC(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_nadj, ctx->d_adj_off, nnodes + 1, s));
+  GF_TRYC(cub::DeviceReduce::Max(d_tmp, tmp_bytes, d_nadj, d_max, nnodes, s));
+  int32_t h_err = 0, h_max = 0, h_tot = 0;
+  GF_TRYC(cudaMemcpyAsync(&h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GF_TRYC(cudaMemcpyAsync(&h_max, d_max, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GF_TRYC(cudaMemcpyAsync(&h_tot, ctx->d_adj_off + nnodes, sizeof(int32_t),
+                          cudaMemcpyDeviceToHost, s));
+  GF_TRYC(cudaStreamSynchronize(s));
+  if (h_err) {
+    cleanup();
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED,
+                   "a node is shared by more than %d element-node slots (valence * nen)",
+                   kCandCap);
+  }
+  if (h_max * dim > 65535) {
+    cleanup();
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "row width %d exceeds 65535", h_max * dim);
+  }
+  ctx->W = h_max * dim;
+  ctx->nnz = (int64_t)h_tot * dim * dim;
+  const int n = ctx->n;
+  const int64_t slots = (int64_t)n * ctx->W;
+  GF_TRY(gf_alloc(ctx, &ctx->d_adj, (size_t)h_tot));
+  GF_TRY(gf_alloc(ctx, &ctx->d_rownnz, (size_t)n));
+  GF_TRY(gf_alloc(ctx, &ctx->d_colidx, (size_t)slots));
+  GF_TRY(gf_alloc(ctx, &ctx->d_slotmap, (size_t)nelem * nen * nen));
+  GF_TRY(gf_alloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
+  k_node_adjacency<1><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
+      nnodes, nen, ctx->d_conn, d_inc_off, d_inc, nullptr, ctx->d_adj_off, ctx->d_adj, d_err);
+  ctx->launches++;
+  k_rownnz<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, dim, d_nadj, ctx->d_rownnz);
+  ctx->launches++;
+  k_colidx<<<ctx->sm_count * 16, 256, 0, s>>>(n, ctx->W, dim, ctx->d_rownnz, ctx->d_adj_off,
+                                              ctx->d_adj, ctx->d_colidx);
+  ctx->launches++;
+  k_slotmap<<<gf_blocks(total, 256), 256, 0, s>>>(nelem, nen, ctx->d_conn, ctx->d_adj_off,
+                                                  ctx->d_adj, ctx->d_slotmap, d_err);
+  ctx->launches++;
+  k_diagpos<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_adj_off, ctx->d_adj,
+                                                   ctx->d_diagpos);
+  ctx->launches++;
+  GF_TRYC(cudaGetLastError());
+  GF_TRYC(cudaMemcpyAsync(&h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GF_TRYC(cudaStreamSynchronize(s));
+  if (h_err) {
+    cleanup();
+    return gf_fail(ctx, GF_ERR_CUDA, "pattern build: slot map lookup failed (%d)", h_err);
+  }
+  cleanup();
+  ctx->has_pattern = true;
+  return GF_OK;
+#undef GF_TRY
+#undef GF_TRYC
+}
+
+// ---------------------------------------------------------------------------
+// Colouring (host)
+// ---------------------------------------------------------------------------
+gf_status gf_color_build(gf_ctx* ctx, const int32_t* user_colors) {
+  const int nelem = ctx->nelem, nen = ctx->nen, nnodes = ctx->nnodes;
+  const std::vector<int32_t>& conn = ctx->h_conn;
+  // node -> element incidence
+  std::vector<int32_t> off(nnodes + 1, 0), inc((size_t)nelem * nen);
+  for (size_t k = 0; k < conn.size(); ++k) off[conn[k] + 1]++;
+  for (int i = 0; i < nnodes; ++i) off[i + 1] += off[i];
+  {
+    std::vector<int32_t> fill(off.begin(), off.end() - 1);
+    for (size_t k = 0; k < conn.size(); ++k) inc[fill[conn[k]]++] = (int32_t)(k / nen);
+  }
+  std::vector<int32_t> color(nelem, -1);
+  if (user_colors) {
+    for (int e = 0; e < nelem; ++e) {
+      if (user_colors[e] < 0 || user_colors[e] > 4095)
+        return gf_fail(ctx, GF_ERR_INVALID_ARG, "colour of element %d is %d", e, user_colors[e]);
+      color[e] = user_colors[e];
+    }
+    // validate: the elements around each node have pairwise distinct colours
+    std::vector<int32_t> seen;
+    for (int a = 0; a < nnodes; ++a) {
+      seen.clear();
+      for (int q = off[a]; q < off[a + 1]; ++q) seen.push_back(color[inc[q]]);
+      std::sort(seen.begin(), seen.end());
+      if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
+        return gf_fail(ctx, GF_ERR_INVALID_ARG,
+                       "invalid colouring: two elements of one colour share node %d", a + 1);
+    }
+  } else {
+    // greedy first-fit in element order; uncoloured neighbours do not constrain
+    std::vector<int32_t> stamp(4096, -1);
+    for (int e = 0; e < nelem; ++e) {
+      for (int i = 0; i < nen; ++i) {
+        const int a = conn[(size_t)e * nen + i];
+        for (int q = off[a]; q < off[a + 1]; ++q) {
+          const int c = color[inc[q]];
+          if (c >= 0) stamp[c] = e;
+        }
+      }
+      int c = 0;
+      while (c < 4096 && stamp[c] == e) ++c;
+      if (c == 4096) return gf_fail(ctx, GF_ERR_UNSUPPORTED, "more than 4096 colours");
+      color[e] = c;
+    }
+  }
+  int ncol = 0;
+  for (int e = 0; e < nelem; ++e) ncol = std::max(ncol, color[e] + 1);
+  std::vector<int32_t> coff(ncol + 1, 0), perm(nelem);
+  for (int e = 0; e < nelem; ++e) coff[color[e] + 1]++;
+  for (int c = 0; c < ncol; ++c) coff[c + 1] += coff[c];
+  {
+    std::vector<int32_t> fill(coff.begin(), coff.end() - 1);
+    for (int e = 0; e < nelem; ++e) perm[fill[color[e]]++] = e;  // stable: ascending ids
+  }
+  gf_status st;
+  if ((st = gf_alloc(ctx, &ctx->d_perm, (size_t)nelem)) != GF_OK) return st;
+  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_perm, perm.data(), sizeof(int32_t) * nelem,
+                               cudaMemcpyHostToDevice, ctx->stream));
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->h_color = color;
+  ctx->color_off = coff;
+  ctx->ncolors = ncol;
+  return GF_OK;
+}

@@ -1,0 +1,641 @@
+// ELL SpMV, constraints and the CG family, all device-resident.
+//
+// Reference: ELLmatrix::Axy (src/SPRmatrix/ELLmatrix.cc:194-204), the OpenCL
+// SpMV variants (src/OpenCL/clKernels/LAopsEll.cl), SPRmatrix::CPU_CG
+// (src/SPRmatrix/SPRmatrix.cc:405-480), ELLmatrix::SolveCgGpu
+// (ELLmatrix.cc:315-459), LAops dot/axpy (src/LAops/LAops.cc:54-61,178-203) and
+// FEM::ApplyConstraint (src/FEM/fem.cc:112-167).
+//
+// The reference crosses PCIe twice per CG iteration (SolveCgGpu).  Here every
+// vector and scalar stays on the device: one iteration is three kernels
+//   K1  q = K p, p.q                      (SpMV with fused dot)
+//   K2  alpha; x += alpha p; r -= alpha q; z = M r; r.z; r.r   (fused axpy/precond/dots)
+//   K3  beta; p = z + beta p; convergence flag
+// with the scalars in device memory.  Chunks of iterations are captured once
+// into a CUDA graph; the host reads the convergence flag after each chunk, and
+// kernels of a finished solve return immediately.
+#include <chrono>
+#include <cmath>
+#include <algorithm>
+
+#include "gf_internal.cuh"
+
+struct SolveScalars {
+  double pq;    // p . A p (accumulated by K1)
+  double rz;    // r . z of the current iteration
+  double rzn;   // r . z of the next iteration (accumulated by K2)
+  double rr;    // r . r after the update (accumulated by K2)
+  double rr0;   // initial r . r
+  double tol2;  // stop when rr <= tol2
+  int iter;
+  int done;     // 0 running, 1 converged, 2 breakdown, 3 iteration cap
+  int maxit;
+  int pad;
+};
+
+namespace {
+
+constexpr int kT = 256;
+
+template <typename T>
+__device__ inline double block_sum(T v, double* sh) {
+  double x = (double)v;
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = x;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  return s;  // valid in thread 0
+}
+
+// Row dot of the column-major ELL: sum_{slot < rownnz} val[slot*n+row] * x[col].
+template <typename TK, typename TX>
+__device__ inline double ell_row(int row, int n, int nz, const int32_t* __restrict__ col,
+                                 const TK* __restrict__ val, const TX* __restrict__ x) {
+  using Acc = typename std::conditional<sizeof(TK) == 8 || sizeof(TX) == 8, double, float>::type;
+  Acc a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  int64_t o = row;
+  int s = 0;
+  for (; s + 4 <= nz; s += 4, o += 4 * (int64_t)n) {
+    const int c0 = __ldg(col + o), c1 = __ldg(col + o + n), c2 = __ldg(col + o + 2 * (int64_t)n),
+              c3 = __ldg(col + o + 3 * (int64_t)n);
+    const TK v0 = __ldg(val + o), v1 = __ldg(val + o + n), v2 = __ldg(val + o + 2 * (int64_t)n),
+             v3 = __ldg(val + o + 3 * (int64_t)n);
+    a0 += (Acc)v0 * (Acc)__ldg(x + c0);
+    a1 += (Acc)v1 * (Acc)__ldg(x + c1);
+    a2 += (Acc)v2 * (Acc)__ldg(x + c2);
+    a3 += (Acc)v3 * (Acc)__ldg(x + c3);
+  }
+  for (; s < nz; ++s, o += n) a0 += (Acc)__ldg(val + o) * (Acc)__ldg(x + __ldg(col + o));
+  return (double)((a0 + a1) + (a2 + a3));
+}
+
+template <typename TK, typename TX, typename TY>
+__global__ void __launch_bounds__(kT)
+k_spmv(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
+       const TK* __restrict__ val, const TX* __restrict__ x, TY* __restrict__ y) {
+  const int row = blockIdx.x * kT + threadIdx.x;
+  if (row < n) y[row] = (TY)ell_row(row, n, rownnz[row], col, val, x);
+}
+
+// r = f - K u (FP64), and r.r
+__global__ void __launch_bounds__(kT)
+k_residual64(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
+             const double* __restrict__ val, const double* __restrict__ u,
+             const double* __restrict__ f, double* __restrict__ r, double* __restrict__ acc) {
+  __shared__ double sh[32];
+  const int row = blockIdx.x * kT + threadIdx.x;
+  double rr = 0.0;
+  if (row < n) {
+    double v = f[row] - ell_row(row, n, rownnz[row], col, val, u);
+    r[row] = v;
+    rr = v * v;
+  }
+  double s = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(acc, s);
+}
+
+// ---- CG kernels ------------------------------------------------------------
+template <typename V>
+__global__ void __launch_bounds__(kT)
+k_cg_init(int n, const V* __restrict__ b, const V* __restrict__ dinv, V* __restrict__ x,
+          V* __restrict__ r, V* __restrict__ z, V* __restrict__ p, SolveScalars* sc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kT + threadIdx.x;
+  double rz = 0.0, rr = 0.0;
+  if (i < n) {
+    V bi = b[i];
+    x[i] = V(0);
+    r[i] = bi;
+    V zi = dinv ? bi * dinv[i] : bi;
+    z[i] = zi;
+    p[i] = zi;
+    rz = (double)bi * (double)zi;
+    rr = (double)bi * (double)bi;
+  }
+  double s1 = block_sum(rz, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
+  double s2 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
+__global__ void k_cg_init_fin(SolveScalars* sc, double eps, int maxit) {
+  sc->rr0 = sc->rr;
+  sc->tol2 = eps * eps * sc->rr;
+  sc->iter = 0;
+  sc->maxit = maxit;
+  sc->pq = 0.0;
+  sc->done = (sc->rr <= 0.0 || sc->rr <= sc->tol2) ? 1 : (maxit <= 0 ? 3 : 0);
+}
+
+template <typename TK, typename V>
+__global__ void __launch_bounds__(kT)
+k_cg_spmv_dot(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
+              const TK* __restrict__ val, const V* __restrict__ p, V* __restrict__ q,
+              SolveScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->rz = sc->rzn;
+    sc->rzn = 0.0;
+    sc->rr = 0.0;
+  }
+  const int row = blockIdx.x * kT + threadIdx.x;
+  double pq = 0.0;
+  if (row < n) {
+    double v = ell_row(row, n, rownnz[row], col, val, p);
+    q[row] = (V)v;
+    pq = (double)p[row] * (double)(V)v;
+  }
+  double s = block_sum(pq, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->pq, s);
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kT)
+k_cg_update(int n, V* __restrict__ x, V* __restrict__ r, V* __restrict__ z,
+            const V* __restrict__ p, const V* __restrict__ q, const V* __restrict__ dinv,
+            SolveScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const double pq = sc->pq;
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 2;
+    return;
+  }
+  const V alpha = (V)(sc->rz / pq);
+  const int i = blockIdx.x * kT + threadIdx.x;
+  double rz = 0.0, rr = 0.0;
+  if (i < n) {
+    x[i] += alpha * p[i];
+    V ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    V zi = ri;
+    if (dinv) {
+      zi = ri * dinv[i];
+      z[i] = zi;
+    }
+    rz = (double)ri * (double)zi;
+    rr = (double)ri * (double)ri;
+  }
+  double s1 = block_sum(rz, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
+  double s2 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kT)
+k_cg_direction(int n, const V* __restrict__ z, V* __restrict__ p, SolveScalars* sc) {
+  if (sc->done) return;
+  const V beta = (V)(sc->rzn / sc->rz);
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) p[i] = z[i] + beta * p[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->pq = 0.0;
+    sc->iter += 1;
+    if (sc->rr <= sc->tol2) sc->done = 1;
+    else if (sc->iter >= sc->maxit) sc->done = 3;
+  }
+}
+
+// Jacobi: 1 / K_rr (0 for an empty or zero diagonal -> identity row)
+template <typename TK, typename V>
+__global__ void k_diag_inv(int n, const int32_t* __restrict__ rownnz,
+                           const int32_t* __restrict__ col, const TK* __restrict__ val,
+                           V* __restrict__ dinv) {
+  const int row = blockIdx.x * kT + threadIdx.x;
+  if (row >= n) return;
+  const int nz = rownnz[row];
+  double d = 0.0;
+  for (int s = 0; s < nz; ++s) {
+    int64_t o = (int64_t)s * n + row;
+    if (col[o] == row) { d = (double)val[o]; break; }
+  }
+  dinv[row] = (d != 0.0) ? (V)(1.0 / d) : V(1);
+}
+
+__global__ void k_scale_to_f32(int n, const double* __restrict__ a, double s,
+                               float* __restrict__ b) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) b[i] = (float)(a[i] * s);
+}
+
+__global__ void k_axpy_f32_into_f64(int n, double alpha, const float* __restrict__ d,
+                                    double* __restrict__ u) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) u[i] += alpha * (double)d[i];
+}
+
+template <typename V>
+__global__ void k_copy_to_f64(int n, const V* __restrict__ a, double* __restrict__ b) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+
+template <typename V>
+__global__ void k_copy_from_f64(int n, const double* __restrict__ a, V* __restrict__ b) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) b[i] = (V)a[i];
+}
+
+// ---- constraints -----------------------------------------------------------
+template <typename T>
+__global__ void k_diag_max(int nnodes, int dim, int n, const int32_t* __restrict__ diagpos,
+                           const T* __restrict__ K, double* __restrict__ blockmax) {
+  __shared__ double sh[32];
+  double m = -INFINITY;
+  for (int row = blockIdx.x * kT + threadIdx.x; row < n; row += gridDim.x * kT) {
+    const int a = row / dim, c = row % dim;
+    m = fmax(m, (double)K[(int64_t)(diagpos[a] * dim + c) * n + row]);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = sh[0];
+    for (int k = 1; k < (kT >> 5); ++k) r = fmax(r, sh[k]);
+    blockmax[blockIdx.x] = r;
+  }
+}
+
+// K_dd <- (1e4 * max_i K_ii) * K_dd in the matrix precision (fem.cc:119-143).
+template <typename T>
+__global__ void k_penalty(int nblocks, const double* __restrict__ blockmax, int dim, int n,
+                          const int32_t* __restrict__ diagpos, const uint8_t* __restrict__ fixed,
+                          T* __restrict__ K) {
+  __shared__ T pen;
+  if (threadIdx.x == 0) {
+    double m = blockmax[0];
+    for (int b = 1; b < nblocks; ++b) m = fmax(m, blockmax[b]);
+    pen = (T)m * (T)10000;
+  }
+  __syncthreads();
+  for (int row = blockIdx.x * kT + threadIdx.x; row < n; row += gridDim.x * kT) {
+    if (!fixed[row]) continue;
+    const int a = row / dim, c = row % dim;
+    T* d = &K[(int64_t)(diagpos[a] * dim + c) * n + row];
+    *d = pen * *d;
+  }
+}
+
+template <typename T>
+__global__ void k_eliminate(int n, int W, const int32_t* __restrict__ rownnz,
+                            const int32_t* __restrict__ col, const uint8_t* __restrict__ fixed,
+                            T* __restrict__ K) {
+  const int64_t total = (int64_t)n * W;
+  for (int64_t i = blockIdx.x * (int64_t)kT + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * kT) {
+    const int row = (int)(i % n), slot = (int)(i / n);
+    if (slot >= rownnz[row]) continue;
+    const int c = col[i];
+    if (fixed[row] || fixed[c]) K[i] = (c == row) ? T(1) : T(0);
+  }
+}
+
+__global__ void k_zero_fixed(int n, const uint8_t* __restrict__ fixed, double* __restrict__ f) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n && fixed[i]) f[i] = 0.0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y) {
+  cudaEventRecord(ctx->ev0, ctx->stream);
+  if (dtype == GF_F64)
+    k_spmv<double, double, double><<<gf_blocks(ctx->n, kT), kT, 0, ctx->stream>>>(
+        ctx->n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, (const double*)x, (double*)y);
+  else
+    k_spmv<float, float, float><<<gf_blocks(ctx->n, kT), kT, 0, ctx->stream>>>(
+        ctx->n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32, (const float*)x, (float*)y);
+  GF_LAUNCH_CHECK(ctx, "k_spmv");
+  cudaEventRecord(ctx->ev1, ctx->stream);
+  GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->last_seconds = ms * 1e-3;
+  return GF_OK;
+}
+
+gf_status gf_constraints_apply(gf_ctx* ctx, int mode) {
+  const int n = ctx->n;
+  if (mode == GF_BC_PENALTY) {
+    if (!ctx->d_diagpos)
+      return gf_fail(ctx, GF_ERR_STATE, "penalty needs a mesh-built pattern");
+    const int nb = std::min(gf_blocks(n, kT), 1024);
+    double* d_bmax = nullptr;
+    gf_status st = gf_alloc(ctx, &d_bmax, (size_t)nb);
+    if (st != GF_OK) return st;
+    if (ctx->has64) {
+      k_diag_max<double><<<nb, kT, 0, ctx->stream>>>(ctx->nnodes, ctx->dim, n, ctx->d_diagpos,
+                                                     ctx->d_K64, d_bmax);
+      ctx->launches++;
+      k_penalty<double><<<nb, kT, 0, ctx->stream>>>(nb, d_bmax, ctx->dim, n, ctx->d_diagpos,
+                                                    ctx->d_fixed, ctx->d_K64);
+      ctx->launches++;
+    }
+    if (ctx->has32) {
+      k_diag_max<float><<<nb, kT, 0, ctx->stream>>>(ctx->nnodes, ctx->dim, n, ctx->d_diagpos,
+                                                    ctx->d_K32, d_bmax);
+      ctx->launches++;
+      k_penalty<float><<<nb, kT, 0, ctx->stream>>>(nb, d_bmax, ctx->dim, n, ctx->d_diagpos,
+                                                   ctx->d_fixed, ctx->d_K32);
+      ctx->launches++;
+    }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_bmax);
+    if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "penalty");
+  } else {
+    const int nb = ctx->sm_count * 8;
+    if (ctx->has64) {
+      k_eliminate<double><<<nb, kT, 0, ctx->stream>>>(n, ctx->W, ctx->d_rownnz, ctx->d_colidx,
+                                                      ctx->d_fixed, ctx->d_K64);
+      ctx->launches++;
+    }
+    if (ctx->has32) {
+      k_eliminate<float><<<nb, kT, 0, ctx->stream>>>(n, ctx->W, ctx->d_rownnz, ctx->d_colidx,
+                                                     ctx->d_fixed, ctx->d_K32);
+      ctx->launches++;
+    }
+    k_zero_fixed<<<gf_blocks(n, kT), kT, 0, ctx->stream>>>(n, ctx->d_fixed, ctx->d_f);
+    ctx->launches++;
+    GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  GF_CUDA(ctx, cudaGetLastError());
+  ctx->bc_mode_applied = mode;
+  return GF_OK;
+}
+
+void gf_solver_free(gf_ctx* ctx) {
+  gf_free(ctx->d_u);
+  if (ctx->d_work) { cudaFree(ctx->d_work); ctx->d_work = nullptr; }
+  ctx->work_bytes = 0;
+  gf_free(ctx->d_scal);
+  gf_free(ctx->d_red);
+  if (ctx->h_pinned) { cudaFreeHost(ctx->h_pinned); ctx->h_pinned = nullptr; }
+}
+
+namespace {
+
+struct CgVecs {
+  void *x, *r, *z, *p, *q, *dinv;
+};
+
+// Runs (P)CG on matrix values `val` (TK) with vectors of type V until the
+// device flag says done.  b must already be in vecs.r's type (copied into x's
+// buffer by the caller as `b`).  Returns iterations and final done code.
+template <typename TK, typename V>
+gf_status run_cg(gf_ctx* ctx, const TK* val, const V* b, CgVecs vv, bool precond, double eps,
+                 int maxit, int check_every, double max_seconds,
+                 std::chrono::steady_clock::time_point t0, int* iters, int* done_code,
+                 double* rr_final, double* rr0_out) {
+  const int n = ctx->n;
+  const int nb = gf_blocks(n, kT);
+  cudaStream_t s = ctx->stream;
+  SolveScalars* sc = ctx->d_scal;
+  V *x = (V*)vv.x, *r = (V*)vv.r, *z = (V*)vv.z, *p = (V*)vv.p, *q = (V*)vv.q;
+  const V* dinv = precond ? (const V*)vv.dinv : nullptr;
+  V* zz = precond ? z : r;  // without a preconditioner z aliases r
+  GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
+  k_cg_init<V><<<nb, kT, 0, s>>>(n, b, dinv, x, r, zz, p, sc);
+  GF_LAUNCH_CHECK(ctx, "k_cg_init");
+  k_cg_init_fin<<<1, 1, 0, s>>>(sc, eps, maxit);
+  GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
+
+  // capture one chunk of iterations as a graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < check_every; ++k) {
+    k_cg_spmv_dot<TK, V><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, val, p, q, sc);
+    k_cg_update<V><<<nb, kT, 0, s>>>(n, x, r, zz, p, q, dinv, sc);
+    k_cg_direction<V><<<nb, kT, 0, s>>>(n, zz, p, sc);
+  }
+  cudaError_t ce = cudaStreamEndCapture(s, &graph);
+  if (ce != cudaSuccess) return gf_cuda_fail(ctx, ce, "graph capture");
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  if (ce != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return gf_cuda_fail(ctx, ce, "graph instantiate");
+  }
+  SolveScalars* hs = (SolveScalars*)ctx->h_pinned;
+  gf_status st = GF_OK;
+  for (;;) {
+    ce = cudaGraphLaunch(exec, s);
+    if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "graph launch"); break; }
+    ctx->launches += 3 * check_every;
+    ce = cudaMemcpyAsync(hs, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "cg chunk"); break; }
+    if (hs->done) break;
+    if (max_seconds > 0.0) {
+      double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (el > max_seconds) break;
+    }
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  if (st != GF_OK) return st;
+  *iters = hs->iter;
+  *done_code = hs->done;
+  *rr_final = hs->rr;
+  *rr0_out = hs->rr0;
+  return GF_OK;
+}
+
+gf_status ensure_work(gf_ctx* ctx) {
+  const size_t need = (size_t)ctx->n * 8 * 10 + 256;
+  gf_status st;
+  if (ctx->work_bytes < need) {
+    if (ctx->d_work) cudaFree(ctx->d_work);
+    ctx->d_work = nullptr;
+    ctx->work_bytes = 0;
+    if (cudaMalloc(&ctx->d_work, need) != cudaSuccess) {
+      cudaGetLastError();
+      return gf_fail(ctx, GF_ERR_OOM, "solver work vectors (%zu bytes)", need);
+    }
+    ctx->work_bytes = need;
+  }
+  if (!ctx->d_u && (st = gf_alloc(ctx, &ctx->d_u, (size_t)ctx->n)) != GF_OK) return st;
+  if (!ctx->d_scal && (st = gf_alloc(ctx, &ctx->d_scal, 1)) != GF_OK) return st;
+  if (!ctx->d_red && (st = gf_alloc(ctx, &ctx->d_red, 4)) != GF_OK) return st;
+  if (!ctx->h_pinned) {
+    if (cudaMallocHost(&ctx->h_pinned, 256) != cudaSuccess) {
+      cudaGetLastError();
+      return gf_fail(ctx, GF_ERR_OOM, "pinned scalars");
+    }
+  }
+  return GF_OK;
+}
+
+// ||f - K64 u|| in FP64 into r64; returns r.r
+gf_status residual64(gf_ctx* ctx, double* r64, double* rr) {
+  cudaStream_t s = ctx->stream;
+  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_red, 0, sizeof(double), s));
+  k_residual64<<<gf_blocks(ctx->n, kT), kT, 0, s>>>(ctx->n, ctx->d_rownnz, ctx->d_colidx,
+                                                    ctx->d_K64, ctx->d_u, ctx->d_f, r64,
+                                                    ctx->d_red);
+  GF_LAUNCH_CHECK(ctx, "k_residual64");
+  double* h = (double*)ctx->h_pinned + 16;
+  GF_CUDA(ctx, cudaMemcpyAsync(h, ctx->d_red, sizeof(double), cudaMemcpyDeviceToHost, s));
+  GF_CUDA(ctx, cudaStreamSynchronize(s));
+  *rr = *h;
+  return GF_OK;
+}
+
+gf_status status_of(int done) {
+  return done == 1 ? GF_OK : done == 2 ? GF_ERR_STALLED : GF_ERR_NOT_CONVERGED;
+}
+
+}  // namespace
+
+gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info) {
+  *info = gf_solve_info{};
+  const int solver = o->solver;
+  if (solver < GF_SOLVER_CG || solver > GF_SOLVER_LEARNED_FCG)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown solver %d", solver);
+  if (solver == GF_SOLVER_LEARNED_FCG)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "learned preconditioner not available in this build");
+  if (!(o->tol > 0.0)) return gf_fail(ctx, GF_ERR_INVALID_ARG, "tol must be > 0");
+  const int maxit = o->max_iter > 0 ? o->max_iter : 10000;
+  const int check = o->check_every > 0 ? std::min(o->check_every, 256) : 16;
+  const int max_outer = o->max_outer > 0 ? o->max_outer : 50;
+  const double inner_tol = o->inner_tol > 0.0 ? o->inner_tol : 1e-4;
+  const int n = ctx->n;
+  gf_status st;
+  if ((st = ensure_work(ctx)) != GF_OK) return st;
+  cudaStream_t s = ctx->stream;
+  const int nb = gf_blocks(n, kT);
+  char* w = (char*)ctx->d_work;
+  auto t0 = std::chrono::steady_clock::now();
+  cudaEventRecord(ctx->ev0, s);
+
+  if (solver == GF_SOLVER_CG || solver == GF_SOLVER_PCG) {
+    const bool pre = solver == GF_SOLVER_PCG;
+    const int dt = o->matrix;
+    if ((dt == GF_F64 && !ctx->has64) || (dt == GF_F32 && !ctx->has32) ||
+        (dt != GF_F64 && dt != GF_F32))
+      return gf_fail(ctx, GF_ERR_STATE, "matrix dtype %d not assembled", dt);
+    int iters = 0, done = 0;
+    double rr = 0.0, rr0 = 0.0;
+    if (dt == GF_F64) {
+      double* v = (double*)w;
+      CgVecs vv{v, v + n, v + 2 * (size_t)n, v + 3 * (size_t)n, v + 4 * (size_t)n, v + 5 * (size_t)n};
+      if (pre) {
+        k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
+                                                     (double*)vv.dinv);
+        GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+      }
+      st = run_cg<double, double>(ctx, ctx->d_K64, ctx->d_f, vv, pre, o->tol, maxit, check,
+                                  o->max_seconds, t0, &iters, &done, &rr, &rr0);
+      if (st != GF_OK) return st;
+      GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_u, vv.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+      float* v = (float*)w;
+      CgVecs vv{v, v + n, v + 2 * (size_t)n, v + 3 * (size_t)n, v + 4 * (size_t)n, v + 5 * (size_t)n};
+      float* b32 = v + 6 * (size_t)n;
+      k_copy_from_f64<float><<<nb, kT, 0, s>>>(n, ctx->d_f, b32);
+      GF_LAUNCH_CHECK(ctx, "k_copy_from_f64");
+      if (pre) {
+        k_diag_inv<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32,
+                                                   (float*)vv.dinv);
+        GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+      }
+      st = run_cg<float, float>(ctx, ctx->d_K32, b32, vv, pre, o->tol, maxit, check,
+                                o->max_seconds, t0, &iters, &done, &rr, &rr0);
+      if (st != GF_OK) return st;
+      k_copy_to_f64<float><<<nb, kT, 0, s>>>(n, (const float*)vv.x, ctx->d_u);
+      GF_LAUNCH_CHECK(ctx, "k_copy_to_f64");
+    }
+    cudaEventRecord(ctx->ev1, s);
+    GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    info->seconds = ctx->last_seconds = ms * 1e-3;
+    info->iterations = iters;
+    info->outer = 1;
+    info->rel_residual = rr0 > 0.0 ? std::sqrt(rr / rr0) : 0.0;
+    if (ctx->has64) {
+      // report the true FP64 residual ||f - K64 u|| / ||f|| when an FP64 matrix exists
+      double* r64 = (double*)w + 7 * (size_t)n;
+      double rrt = 0.0, ff = 0.0;
+      if ((st = residual64(ctx, r64, &rrt)) != GF_OK) return st;
+      std::vector<double> f(n);
+      GF_CUDA(ctx, cudaMemcpy(f.data(), ctx->d_f, sizeof(double) * n, cudaMemcpyDeviceToHost));
+      for (double v : f) ff += v * v;
+      info->rel_residual = ff > 0.0 ? std::sqrt(rrt / ff) : 0.0;
+    }
+    info->status = status_of(done);
+    if (done != 1)
+      gf_fail(ctx, (gf_status)info->status, "solver stopped with code %d after %d iterations",
+              done, iters);
+    return (gf_status)info->status;
+  }
+
+  // MIXED_PCG: FP64 refinement around FP32 Jacobi-PCG on K32
+  if (!ctx->has64 || !ctx->has32)
+    return gf_fail(ctx, GF_ERR_STATE, "mixed solve needs both FP64 and FP32 matrices");
+  double* r64 = (double*)w;                  // n doubles
+  float* v = (float*)((double*)w + n);       // f32 vectors after it
+  CgVecs vv{v, v + n, v + 2 * (size_t)n, v + 3 * (size_t)n, v + 4 * (size_t)n, v + 5 * (size_t)n};
+  float* b32 = v + 6 * (size_t)n;
+  k_diag_inv<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32,
+                                             (float*)vv.dinv);
+  GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u, 0, sizeof(double) * n, s));
+  double ff = 0.0;
+  {
+    std::vector<double> f(n);
+    GF_CUDA(ctx, cudaMemcpyAsync(f.data(), ctx->d_f, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    GF_CUDA(ctx, cudaStreamSynchronize(s));
+    for (double x : f) ff += x * x;
+  }
+  int total_it = 0, outer = 0, last_done = 1;
+  double rr = 0.0;
+  if ((st = residual64(ctx, r64, &rr)) != GF_OK) return st;
+  while (true) {
+    if (ff == 0.0 || std::sqrt(rr / ff) <= o->tol) { last_done = 1; break; }
+    if (outer >= max_outer || total_it >= maxit) { last_done = 3; break; }
+    if (o->max_seconds > 0.0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds) {
+      last_done = 3;
+      break;
+    }
+    const double rn = std::sqrt(rr);
+    k_scale_to_f32<<<nb, kT, 0, s>>>(n, r64, 1.0 / rn, b32);
+    GF_LAUNCH_CHECK(ctx, "k_scale_to_f32");
+    int iters = 0, done = 0;
+    double rri = 0.0, rr0 = 0.0;
+    st = run_cg<float, float>(ctx, ctx->d_K32, b32, vv, true, inner_tol, maxit - total_it, check,
+                              o->max_seconds, t0, &iters, &done, &rri, &rr0);
+    if (st != GF_OK) return st;
+    total_it += iters;
+    ++outer;
+    k_axpy_f32_into_f64<<<nb, kT, 0, s>>>(n, rn, (const float*)vv.x, ctx->d_u);
+    GF_LAUNCH_CHECK(ctx, "k_axpy_f32_into_f64");
+    double rr_new = 0.0;
+    if ((st = residual64(ctx, r64, &rr_new)) != GF_OK) return st;
+    if (done == 2 && !(rr_new < rr)) { last_done = 2; rr = rr_new; break; }
+    rr = rr_new;
+  }
+  cudaEventRecord(ctx->ev1, s);
+  GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  info->seconds = ctx->last_seconds = ms * 1e-3;
+  info->iterations = total_it;
+  info->outer = outer;
+  info->rel_residual = ff > 0.0 ? std::sqrt(rr / ff) : 0.0;
+  info->status = status_of(last_done);
+  if (last_done != 1)
+    gf_fail(ctx, (gf_status)info->status, "mixed solve stopped with code %d (%d iterations)",
+            last_done, total_it);
+  return (gf_status)info->status;
+}

@@ -1,0 +1,350 @@
+"""Host-side mirror of the reference's FEM / StiffAlgo / SPRmatrix interface for
+the hot path, over the C-ABI (include/gpufem_b200.h).
+
+Reference interface mirrored (fpaboim/gpufem):
+  FEM            src/FEM/fem.h:34-86      Init, CalcStiffnessMat, ApplyConstraint,
+                                           SetDeviceMode, SetUseColoring, GetFemData
+  FemData        src/FEM/FemData.h:43-105 Init(format, n_gpts, E, Nu, fileIO) -> here
+                                           Init from arrays (coords, connectivity,
+                                           supports, loads)
+  StiffAlgo      src/FEM/StiffAlgo.h:40-84 CalcGlobalStiffness(femdata) -> seconds,
+                                           SetParallelColoring, SetMakeAssembly
+  SPRmatrix/ELL  src/SPRmatrix/SPRmatrix.h:71-89, ELLmatrix.h:46-72
+                                           GetElem, GetNNZ, GetMatSize, Axy, CG
+
+Everything computes on the GPU through libgpufem_b200.so.  `Context` is the thin
+owner of one gf_ctx; the reference-named classes sit on top of it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One gf_ctx: a CUDA stream plus all device memory of one problem."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        st = lib.gf_create(C.byref(h), device)
+        if st != _lib.GF_OK:
+            raise _lib.GpufemError(st, f"gf_create(device={device}) failed")
+        self.h = h
+        self.dim = 0
+        self.n = 0
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib.gf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _c(self, st: int) -> None:
+        check(st, self.h)
+
+    # ---- mesh -----------------------------------------------------------
+    def mesh_create(self, elem_type: int, coords: np.ndarray, conn: np.ndarray, ngauss: int,
+                    E: float, E_elem: Optional[np.ndarray] = None, nu: float = 0.3,
+                    analysis: int = _lib.GF_PLANE_STRESS) -> None:
+        coords = np.ascontiguousarray(coords, np.float64)
+        conn = np.ascontiguousarray(conn, np.int32)
+        E_elem = None if E_elem is None else np.ascontiguousarray(E_elem, np.float64)
+        nnodes = coords.shape[0]
+        self._c(lib.gf_mesh_create(self.h, elem_type, nnodes, _ptr(coords), conn.shape[0],
+                                   _ptr(conn), ngauss, float(E), _ptr(E_elem), float(nu),
+                                   analysis))
+        self.dim = coords.shape[1] if coords.ndim == 2 else (2 if elem_type < 2 else 3)
+        self.n = nnodes * self.dim
+
+    def set_modulus(self, E: float, E_elem: Optional[np.ndarray] = None) -> None:
+        E_elem = None if E_elem is None else np.ascontiguousarray(E_elem, np.float64)
+        self._c(lib.gf_mesh_set_modulus(self.h, float(E), _ptr(E_elem)))
+
+    def color(self, colors: Optional[np.ndarray] = None) -> int:
+        colors = None if colors is None else np.ascontiguousarray(colors, np.int32)
+        nc = C.c_int32()
+        self._c(lib.gf_mesh_color(self.h, _ptr(colors), C.byref(nc)))
+        return nc.value
+
+    def colors(self, nelem: int) -> np.ndarray:
+        out = np.empty(nelem, np.int32)
+        self._c(lib.gf_mesh_get_colors(self.h, _ptr(out)))
+        return out
+
+    def build_pattern(self):
+        n, w, nnz = C.c_int32(), C.c_int32(), C.c_int64()
+        self._c(lib.gf_ell_build_pattern(self.h, C.byref(n), C.byref(w), C.byref(nnz)))
+        self.n = n.value
+        return n.value, w.value, nnz.value
+
+    def assemble(self, dtype: int = _lib.GF_F64, scatter: int = _lib.GF_SCATTER_COLOR,
+                 engine: int = _lib.GF_ENGINE_CUDA_CORE) -> float:
+        self._c(lib.gf_assemble(self.h, dtype, scatter, engine))
+        return lib.gf_last_device_seconds(self.h)
+
+    def convert_f64_to_f32(self) -> None:
+        self._c(lib.gf_ell_convert_f64_to_f32(self.h))
+
+    def ell_shape(self):
+        n, w = C.c_int32(), C.c_int32()
+        self._c(lib.gf_ell_view(self.h, _lib.GF_F64, C.byref(n), C.byref(w), None, None, None))
+        return n.value, w.value
+
+    def ell_download(self, dtype: int = _lib.GF_F64):
+        n, w = self.ell_shape()
+        rownnz = np.empty(n, np.int32)
+        colidx = np.empty(n * w, np.int32)
+        vals = np.empty(n * w, np.float64 if dtype == _lib.GF_F64 else np.float32)
+        self._c(lib.gf_ell_download(self.h, dtype, _ptr(rownnz), _ptr(colidx), _ptr(vals)))
+        return rownnz, colidx.reshape(w, n), vals.reshape(w, n)
+
+    def ell_upload(self, rownnz: np.ndarray, colidx: np.ndarray, vals: np.ndarray) -> None:
+        """colidx / vals: (width, n) column-major ELL as the reference stores it."""
+        rownnz = np.ascontiguousarray(rownnz, np.int32)
+        colidx = np.ascontiguousarray(colidx, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        w, n = colidx.shape
+        self._c(lib.gf_ell_upload(self.h, n, w, _ptr(rownnz), _ptr(colidx), _ptr(vals)))
+        self.n = n
+
+    # ---- loads / constraints -------------------------------------------
+    def set_supports(self, supports: np.ndarray) -> None:
+        supports = np.ascontiguousarray(supports, np.int32)
+        self._c(lib.gf_set_supports(self.h, supports.shape[0], _ptr(supports)))
+
+    def set_nodal_loads(self, loads: np.ndarray) -> None:
+        loads = np.ascontiguousarray(loads, np.float64)
+        self._c(lib.gf_set_nodal_loads(self.h, loads.shape[0], _ptr(loads)))
+
+    def set_force(self, f: np.ndarray) -> None:
+        f = np.ascontiguousarray(f, np.float64)
+        self._c(lib.gf_set_force(self.h, _ptr(f)))
+
+    def get_force(self) -> np.ndarray:
+        f = np.empty(self.n, np.float64)
+        self._c(lib.gf_get_force(self.h, _ptr(f)))
+        return f
+
+    def apply_constraints(self, mode: int) -> None:
+        self._c(lib.gf_apply_constraints(self.h, mode))
+
+    # ---- solve ----------------------------------------------------------
+    def spmv(self, x: np.ndarray, dtype: int = _lib.GF_F64) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        self._c(lib.gf_spmv_host(self.h, dtype, _ptr(x), _ptr(y)))
+        return y
+
+    def solve(self, solver: int = _lib.GF_SOLVER_PCG, matrix: int = _lib.GF_F64,
+              tol: float = 1e-10, max_iter: int = 10000, inner_tol: float = 0.0,
+              max_outer: int = 0, check_every: int = 0, max_seconds: float = 0.0,
+              raise_on_error: bool = True) -> _lib.SolveInfo:
+        o = _lib.SolveOpts(solver=solver, matrix=matrix, max_iter=max_iter, tol=tol,
+                           inner_tol=inner_tol, max_outer=max_outer, check_every=check_every,
+                           max_seconds=max_seconds)
+        info = _lib.SolveInfo()
+        st = lib.gf_solve(self.h, C.byref(o), C.byref(info))
+        if raise_on_error:
+            self._c(st)
+        return info
+
+    def solution(self) -> np.ndarray:
+        u = np.empty(self.n, np.float64)
+        self._c(lib.gf_get_solution(self.h, _ptr(u)))
+        return u
+
+    def launches(self) -> int:
+        return int(lib.gf_kernel_launches(self.h))
+
+    def sync(self) -> None:
+        self._c(lib.gf_sync(self.h))
+
+
+# ---------------------------------------------------------------------------
+# Reference-named mirror
+# ---------------------------------------------------------------------------
+class FemData:
+    """Mesh, material, Gauss rule, supports and loads (FemData::Init,
+    src/FEM/FemData.cc:122-194), from arrays instead of a FileIO."""
+
+    def Init(self, elem_type: int, coords, conn, n_gpts: int, E: float, Nu: float,
+             supports=None, nodal_loads=None, E_elem=None,
+             analysis: int = _lib.GF_PLANE_STRESS) -> None:
+        self.elem_type = elem_type
+        self.coords = np.ascontiguousarray(coords, np.float64)
+        self.conn = np.ascontiguousarray(conn, np.int32)
+        self.n_gpts = n_gpts
+        self.E = E
+        self.Nu = Nu
+        self.E_elem = E_elem
+        self.analysis = analysis
+        self.supports = supports
+        self.nodal_loads = nodal_loads
+        self.stiffness: Optional[ELLmatrixCUDA] = None
+        self.displacements: Optional[np.ndarray] = None
+
+    def GetStiffnessMatrix(self) -> "ELLmatrixCUDA":
+        return self.stiffness
+
+    def GetDisplVector(self) -> Optional[np.ndarray]:
+        return self.displacements
+
+
+class ELLmatrixCUDA:
+    """Device-resident ELL matrix (SPRmatrix interface, ELLmatrix.h:46-72)."""
+
+    def __init__(self, ctx: Context, dtype: int = _lib.GF_F64):
+        self.ctx = ctx
+        self.dtype = dtype
+        self._host = None
+
+    def _download(self):
+        if self._host is None:
+            self._host = self.ctx.ell_download(self.dtype)
+        return self._host
+
+    def invalidate(self) -> None:
+        self._host = None
+
+    def GetMatDim(self) -> int:
+        return self.ctx.ell_shape()[0]
+
+    def GetElem(self, row: int, col: int) -> float:
+        n, w = self.ctx.ell_shape()
+        if row < 0 or row >= n or col < 0 or col >= n:
+            return 0.0
+        rownnz, colidx, vals = self._download()
+        for s in range(rownnz[row]):
+            if colidx[s, row] == col:
+                return float(vals[s, row])
+        return 0.0
+
+    def GetNNZ(self) -> int:
+        rownnz, colidx, vals = self._download()
+        mask = np.arange(colidx.shape[0])[:, None] < rownnz[None, :]
+        return int(np.count_nonzero(vals[mask]))
+
+    def GetMatSize(self) -> int:
+        n, w = self.ctx.ell_shape()
+        return n * w * (8 if self.dtype == _lib.GF_F64 else 4) + n * w * 4
+
+    def Axy(self, x: np.ndarray) -> np.ndarray:
+        return self.ctx.spmv(x, self.dtype)
+
+    def CG(self, vector_B: np.ndarray, n_iterations: int = 10000, epsilon: float = 1e-4,
+           preconditioned: bool = False) -> np.ndarray:
+        """Plain CG from x0 = 0, stop at ||r|| <= eps ||b|| (SPRmatrix::CPU_CG,
+        SPRmatrix.cc:405-480); Jacobi-preconditioned when asked."""
+        self.ctx.set_force(np.asarray(vector_B, np.float64))
+        solver = _lib.GF_SOLVER_PCG if preconditioned else _lib.GF_SOLVER_CG
+        info = self.ctx.solve(solver=solver, matrix=self.dtype, tol=epsilon,
+                              max_iter=n_iterations, raise_on_error=False)
+        if info.status not in (_lib.GF_OK, _lib.GF_ERR_NOT_CONVERGED):
+            check(info.status, self.ctx.h)
+        self.last_info = info
+        return self.ctx.solution()
+
+
+class StiffAlgoCUDA:
+    """StiffAlgo strategy that assembles on the GPU (StiffAlgo.h:40-84)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.m_assemble = True
+        self.m_usecoloring = True
+        self.dtype = _lib.GF_F64
+
+    def SetParallelColoring(self, usecoloring: bool) -> None:
+        self.m_usecoloring = bool(usecoloring)
+
+    def GetParallelColoring(self) -> bool:
+        return self.m_usecoloring
+
+    def SetMakeAssembly(self, assemble: bool) -> None:
+        self.m_assemble = bool(assemble)
+
+    def GetMakeAssembly(self) -> bool:
+        return self.m_assemble
+
+    def CalcGlobalStiffness(self, femdata: FemData) -> float:
+        scatter = _lib.GF_SCATTER_COLOR if self.m_usecoloring else _lib.GF_SCATTER_ATOMIC
+        secs = self.ctx.assemble(self.dtype, scatter)
+        femdata.stiffness = ELLmatrixCUDA(self.ctx, self.dtype)
+        return secs
+
+
+class FEM:
+    """FEM facade (src/FEM/fem.h:34-86).  DeviceMode GPU maps to StiffAlgoCUDA."""
+    CPU, OMP, GPUOMP, GPU = 0, 1, 2, 3
+    PEN, SUB = 0, 1
+
+    def __init__(self, device: int = 0):
+        self.ctx = Context(device)
+        self.m_femdata: Optional[FemData] = None
+        self.m_stiffnessalgo: Optional[StiffAlgoCUDA] = None
+
+    def Init(self, assemble: bool = True, devicemode: int = 3) -> None:
+        if devicemode != FEM.GPU:
+            raise ValueError("this implementation provides only the GPU strategy; the CPU "
+                             "strategies are the reference's own code")
+        self.m_femdata = FemData()
+        self.m_stiffnessalgo = StiffAlgoCUDA(self.ctx)
+        self.m_stiffnessalgo.SetMakeAssembly(assemble)
+
+    def GetFemData(self) -> FemData:
+        return self.m_femdata
+
+    def SetUseColoring(self, usecolor: bool) -> None:
+        self.m_stiffnessalgo.SetParallelColoring(usecolor)
+
+    def SetPrecision(self, dtype: int) -> None:
+        self.m_stiffnessalgo.dtype = dtype
+
+    def _upload(self) -> None:
+        fd = self.m_femdata
+        self.ctx.mesh_create(fd.elem_type, fd.coords, fd.conn, fd.n_gpts, fd.E, fd.E_elem,
+                             fd.Nu, fd.analysis)
+        if fd.supports is not None:
+            self.ctx.set_supports(fd.supports)
+        if fd.nodal_loads is not None:
+            self.ctx.set_nodal_loads(fd.nodal_loads)
+        self._uploaded = True
+
+    def CalcStiffnessMat(self) -> float:
+        if not getattr(self, "_uploaded", False):
+            self._upload()
+        return self.m_stiffnessalgo.CalcGlobalStiffness(self.m_femdata)
+
+    def ApplyConstraint(self, conmode: int) -> None:
+        mode = _lib.GF_BC_PENALTY if conmode == FEM.PEN else _lib.GF_BC_ELIMINATION
+        self.ctx.apply_constraints(mode)
+        if self.m_femdata.stiffness is not None:
+            self.m_femdata.stiffness.invalidate()
+
+    def Solve(self, n_iterations: int = 3000, epsilon: float = 1e-3,
+              preconditioned: bool = False) -> np.ndarray:
+        """CG on the assembled matrix with the force vector (interface.cpp:304-328)."""
+        f = self.ctx.get_force()
+        u = self.m_femdata.stiffness.CG(f, n_iterations, epsilon, preconditioned)
+        self.m_femdata.displacements = u
+        return u

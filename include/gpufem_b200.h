@@ -1,0 +1,204 @@
+/*
+ * gpufem_b200 — C-ABI of the B200 (sm_100a) implementation of gpufem's hot path:
+ * per-element stiffness integration (Q4, Q8, Brick8, Brick20), scatter of Ke into a
+ * column-major ELL matrix, and the ELL SpMV / dot / axpy loop of (preconditioned) CG.
+ *
+ * Every entry point takes plain pointers and sizes, returns a gf_status, never aborts
+ * and never exits.  gf_last_error() gives the message of the last failure on a context.
+ * One context owns one CUDA stream and all device memory it allocates; contexts are
+ * independent (no global state) and a context must be driven by one host thread at a
+ * time.  Calls are synchronous unless the name says otherwise.
+ *
+ * Reference interfaces replaced (paths within fpaboim/gpufem):
+ *   FemData::Init                    src/FEM/FemData.cc:122-194      -> gf_mesh_create
+ *   femColor (METIS dual + greedy)   src/FEM/femColor.cc:79-191      -> gf_mesh_color
+ *   StiffAlgo::CalcGlobalStiffness   src/FEM/StiffAlgo.h:46          -> gf_assemble
+ *     (StiffAlgoCPU.cc:58-284, StiffAlgoGpuOmp.cc:49-323, gpuFEM_*.cl)
+ *   ELLmatrix storage                src/SPRmatrix/ELLmatrix.h:35-89 -> gf_ell_view / gf_ell_download
+ *   FEM::ApplyConstraint             src/FEM/fem.cc:112-167          -> gf_apply_constraints
+ *   FemData::CalcForceVector         src/FEM/FemData.cc:370-385      -> gf_set_nodal_loads
+ *   ELLmatrix::Axy / AxyGPU          src/SPRmatrix/ELLmatrix.cc:194-285 -> gf_spmv
+ *   SPRmatrix::CG / CPU_CG / SolveCgGpu  SPRmatrix.cc:374-480, ELLmatrix.cc:289-459 -> gf_solve
+ *   SPRmatrix::SetElem/AddElem/GetElem   SPRmatrix.h:71-73           -> gf_ell_upload (host-built ELL)
+ */
+#ifndef GPUFEM_B200_H_
+#define GPUFEM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GF_API __attribute__((visibility("default")))
+#else
+#define GF_API
+#endif
+
+typedef enum gf_status {
+  GF_OK = 0,
+  GF_ERR_INVALID_ARG = 1,   /* bad pointer, size, enum or mesh data            */
+  GF_ERR_OOM = 2,           /* device or pinned allocation failed               */
+  GF_ERR_NOT_CONVERGED = 3, /* iteration or time cap reached before tolerance   */
+  GF_ERR_STALLED = 4,       /* solver made no progress / breakdown (p.Ap <= 0)  */
+  GF_ERR_CUDA = 5,          /* a CUDA runtime call failed                       */
+  GF_ERR_STATE = 6,         /* call out of order (e.g. assemble before mesh)    */
+  GF_ERR_UNSUPPORTED = 7    /* mesh outside the kernels' limits                 */
+} gf_status;
+
+/* Element families, same numbering idea as FileIO::ElemType (src/Utils/fileIO.h:40-46)
+ * but 0-based.  Node order within an element is the reference's natural-coordinate
+ * order (src/FEM/StiffAlgo.cc:47-202); connectivity is 1-based as in FileIO/FemData. */
+typedef enum gf_elem_type { GF_Q4 = 0, GF_Q8 = 1, GF_BRICK8 = 2, GF_BRICK20 = 3 } gf_elem_type;
+
+/* 2-D constitutive law (FemData::CalcConstituitiveData, src/FEM/FemData.cc:322-365).
+ * Ignored for 3-D elements. */
+typedef enum gf_analysis { GF_PLANE_STRESS = 0, GF_PLANE_STRAIN = 1 } gf_analysis;
+
+/* Value type of an assembled matrix / vector. */
+typedef enum gf_dtype { GF_F64 = 0, GF_F32 = 1 } gf_dtype;
+
+/* Scatter schedule of gf_assemble. */
+typedef enum gf_scatter {
+  GF_SCATTER_COLOR = 0,  /* colour classes in turn, plain read-modify-write (no atomics) */
+  GF_SCATTER_ATOMIC = 1  /* all elements at once, red.global.add into K               */
+} gf_scatter;
+
+/* Element-integration engine of gf_assemble (FP32 only; FP64 always uses CUDA cores). */
+typedef enum gf_engine {
+  GF_ENGINE_CUDA_CORE = 0, /* FP32/FP64 FMA                                             */
+  GF_ENGINE_TF32_MMA = 1   /* per-element Gram contraction G.G^T on tensor cores (TF32,
+                              FP32 accumulate); tolerance is TF32's, not FP32's        */
+} gf_engine;
+
+/* Constraint treatment (FEM::ConstraintMode, src/FEM/fem.h:51-54). */
+typedef enum gf_bc_mode {
+  GF_BC_PENALTY = 0,     /* reference PEN: K_dd <- (1e4 * max_i K_ii) * K_dd, f unchanged */
+  GF_BC_ELIMINATION = 1  /* symmetric elimination: zero row+column, K_dd = 1, f_d = 0     */
+} gf_bc_mode;
+
+typedef enum gf_solver {
+  GF_SOLVER_CG = 0,          /* reference CPU_CG semantics: plain CG, x0 = 0, stop on
+                                r.r <= eps^2 * r0.r0; runs in the dtype of `matrix`      */
+  GF_SOLVER_PCG = 1,         /* Jacobi-preconditioned CG in the dtype of `matrix`        */
+  GF_SOLVER_MIXED_PCG = 2,   /* FP64 iterative refinement (r = f - K64 u in FP64) around
+                                an FP32 Jacobi-PCG inner solve on K32                     */
+  GF_SOLVER_LEARNED_FCG = 3  /* as MIXED_PCG, inner solve = FP32 flexible CG with the
+                                learned (message-passing) preconditioner, falling back to
+                                Jacobi-PCG when it stalls                                */
+} gf_solver;
+
+typedef struct gf_solve_opts {
+  int32_t solver;        /* gf_solver                                              */
+  int32_t matrix;        /* gf_dtype used by CG / PCG                              */
+  int32_t max_iter;      /* total inner iterations cap (0 -> 10000)                */
+  double tol;            /* relative residual target ||f - K u|| / ||f||           */
+  double inner_tol;      /* MIXED/LEARNED: inner relative reduction per refinement
+                            step (0 -> 1e-4)                                        */
+  int32_t max_outer;     /* MIXED/LEARNED: refinement steps cap (0 -> 50)          */
+  int32_t check_every;   /* iterations between host convergence checks (0 -> 16)   */
+  double max_seconds;    /* wall-time cap (0 -> none)                               */
+} gf_solve_opts;
+
+typedef struct gf_solve_info {
+  int32_t iterations;    /* inner iterations performed (all refinement steps)      */
+  int32_t outer;         /* refinement steps (MIXED/LEARNED), else 1               */
+  int32_t fallback;      /* LEARNED: 1 if Jacobi-PCG took over                      */
+  int32_t status;        /* gf_status of the solve                                  */
+  double rel_residual;   /* final ||f - K u|| / ||f|| in FP64 on the FP64 matrix
+                            (in the matrix dtype for CG / PCG on FP32)              */
+  double seconds;        /* device time of the solve                                */
+} gf_solve_info;
+
+typedef struct gf_ctx gf_ctx;
+
+/* ---- context ------------------------------------------------------------------ */
+GF_API gf_status gf_create(gf_ctx** ctx, int32_t device);
+GF_API gf_status gf_destroy(gf_ctx* ctx);
+GF_API const char* gf_last_error(const gf_ctx* ctx);
+GF_API const char* gf_version(void);
+/* Device time (seconds) of the last timed phase: assemble, spmv or solve. */
+GF_API double gf_last_device_seconds(const gf_ctx* ctx);
+/* Kernel launches issued by this context since creation (for accounting). */
+GF_API int64_t gf_kernel_launches(const gf_ctx* ctx);
+/* Synchronise the context's stream. */
+GF_API gf_status gf_sync(gf_ctx* ctx);
+
+/* ---- mesh (FemData::Init) --------------------------------------------------------
+ * coords: nnodes*dim doubles, packed xy / xyz (dim = 2 for Q4/Q8, 3 for bricks).
+ * connect: nelem*nen int32, 1-based node ids, element-major.
+ * ngauss: Gauss points per direction, 2 or 3 (FemData::CalcGaussVectors).
+ * E_elem: nelem Young's moduli, or NULL for the scalar E.  Replaces any previous mesh. */
+GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
+                                const double* coords, int32_t nelem,
+                                const int32_t* connect, int32_t ngauss, double E,
+                                const double* E_elem, double nu, int32_t analysis);
+/* Update per-element moduli (or the scalar E when E_elem is NULL) without
+ * rebuilding the pattern. */
+GF_API gf_status gf_mesh_set_modulus(gf_ctx* ctx, double E, const double* E_elem);
+
+/* Colour schedule for GF_SCATTER_COLOR.  elem_color: nelem colours (0-based) from the
+ * caller, or NULL to compute the reference's greedy first-fit colouring of the element
+ * dual graph (elements sharing >= 1 node are adjacent; femColor.cc:103-191).  Returns
+ * the number of colours.  A caller colouring is validated (no two elements of a colour
+ * share a node) and rejected with GF_ERR_INVALID_ARG otherwise. */
+GF_API gf_status gf_mesh_color(gf_ctx* ctx, const int32_t* elem_color, int32_t* ncolors);
+/* Copy the colour of each element (0-based) to host. */
+GF_API gf_status gf_mesh_get_colors(gf_ctx* ctx, int32_t* elem_color);
+
+/* ---- ELL pattern (symbolic) --------------------------------------------------------
+ * Topological pattern: row r (dof of node a) holds every dof of every node sharing an
+ * element with a, columns strictly increasing.  Column-major: entry (row, slot) at
+ * slot*n + row.  width = max row length.  Slots past rownnz hold col = row, value 0.  */
+GF_API gf_status gf_ell_build_pattern(gf_ctx* ctx, int32_t* n, int32_t* width,
+                                      int64_t* nnz);
+
+/* ---- numeric assembly (StiffAlgo::CalcGlobalStiffness) ------------------------------
+ * Computes Ke = sum_gp B^T D B detJ w for every element and scatters it into the ELL
+ * values of dtype `dtype`.  Builds the pattern and the colouring on first use.  */
+GF_API gf_status gf_assemble(gf_ctx* ctx, int32_t dtype, int32_t scatter, int32_t engine);
+/* Round the FP64 matrix into the FP32 matrix (same pattern). */
+GF_API gf_status gf_ell_convert_f64_to_f32(gf_ctx* ctx);
+
+/* Device pointers of the assembled matrix (owned by the context). */
+GF_API gf_status gf_ell_view(gf_ctx* ctx, int32_t dtype, int32_t* n, int32_t* width,
+                             const int32_t** rownnz, const int32_t** colidx,
+                             const void** values);
+/* Copy to host: rownnz[n], colidx[n*width], values[n*width] (dtype-sized). */
+GF_API gf_status gf_ell_download(gf_ctx* ctx, int32_t dtype, int32_t* rownnz,
+                                 int32_t* colidx, void* values);
+/* Replace the matrix with a host-built ELL (n, width, rownnz, colidx, FP64 values);
+ * fills both the FP64 and FP32 matrices.  Slots past rownnz are ignored. */
+GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width,
+                               const int32_t* rownnz, const int32_t* colidx,
+                               const double* values);
+
+/* ---- loads and constraints ----------------------------------------------------------
+ * supports: nsup rows of (dim+1) int32: node id (1-based), then 1 = fixed per component
+ * (FileIO::extractNodeSupports layout).  loads: nload rows of (dim+1) doubles: node id,
+ * then force components; a nonzero component SETS f[dof] (CalcForceVector semantics). */
+GF_API gf_status gf_set_supports(gf_ctx* ctx, int32_t nsup, const int32_t* supports);
+GF_API gf_status gf_set_nodal_loads(gf_ctx* ctx, int32_t nload, const double* loads);
+/* Full right-hand side (n doubles), replacing the nodal loads. */
+GF_API gf_status gf_set_force(gf_ctx* ctx, const double* f);
+GF_API gf_status gf_get_force(gf_ctx* ctx, double* f);
+/* Apply the supports to the assembled matrices present (FP64 and/or FP32). */
+GF_API gf_status gf_apply_constraints(gf_ctx* ctx, int32_t mode);
+
+/* ---- solve --------------------------------------------------------------------------- */
+/* y = K x on device pointers of dtype `dtype` (x, y: n entries). */
+GF_API gf_status gf_spmv(gf_ctx* ctx, int32_t dtype, const void* x, void* y);
+/* Host-buffer SpMV (n doubles in, n doubles out), computed in `dtype`. */
+GF_API gf_status gf_spmv_host(gf_ctx* ctx, int32_t dtype, const double* x, double* y);
+GF_API gf_status gf_solve(gf_ctx* ctx, const gf_solve_opts* opts, gf_solve_info* info);
+/* Solution of the last solve (n doubles). */
+GF_API gf_status gf_get_solution(gf_ctx* ctx, double* u);
+/* Device pointer of the FP64 solution. */
+GF_API gf_status gf_solution_view(gf_ctx* ctx, const double** u);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUFEM_B200_H_ */

@@ -1,0 +1,204 @@
+"""Parity of the CUDA assembly (through the C-ABI) with the reference's golden
+vectors and with the oracle.  Tolerances (row-relative: max|A-B| / max|A_row|):
+FP64 1e-12, FP32 1e-6; ELL column indices and row lengths bit-exact against the
+topological pattern."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from ellutil import ell_to_dense, row_rel_err
+from gpufem_b200 import _lib
+from gpufem_b200 import meshgen as mg
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-6
+
+
+@pytest.fixture(scope="module")
+def fem():
+    from gpufem_b200.fem import Context
+    return Context
+
+
+def make_ctx(Context, g=None, mesh=None, E_elem=None):
+    ctx = Context(0)
+    if g is not None:
+        ctx.mesh_create(int(g["elem_type"]), g["coords"], g["conn"], int(g["ngauss"]),
+                        float(g["E"]), None, float(g["nu"]))
+    else:
+        ctx.mesh_create(mesh.elem_type, mesh.coords, mesh.conn, mesh.ngauss, mesh.E0,
+                        mesh.E if E_elem is None else E_elem, mesh.nu)
+    return ctx
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("scatter", [_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC])
+def test_fp64_assembly_matches_reference(fem, oracle, name, scatter):
+    g = load_golden(name)
+    ctx = make_ctx(fem, g)
+    ctx.assemble(_lib.GF_F64, scatter)
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    # pattern: bit-exact against the topological oracle pattern
+    orn, oci = oracle.pattern(int(g["elem_type"]), g["coords"].shape[0], g["conn"])
+    assert np.array_equal(rn, orn)
+    assert np.array_equal(ci, oci)
+    # reference rows are subsets of ours (value-dependent pattern, zeros dropped)
+    for r in range(rn.size):
+        assert set(g["colidx_fp64"][: g["rownnz_fp64"][r], r]) <= set(ci[: rn[r], r])
+    n = rn.size
+    A = ell_to_dense(g["rownnz_fp64"], g["colidx_fp64"], g["vals_fp64"], n)
+    B = ell_to_dense(rn, ci, v, n)
+    assert row_rel_err(A, B) <= TOL64
+    # padding slots hold col = row and value 0
+    W = ci.shape[0]
+    pad = np.arange(W)[:, None] >= rn[None, :]
+    assert np.all(v[pad] == 0) and np.all(ci[pad] == np.broadcast_to(np.arange(n), (W, n))[pad])
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("scatter", [_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC])
+def test_fp32_assembly_matches_reference(fem, name, scatter):
+    g = load_golden(name)
+    ctx = make_ctx(fem, g)
+    ctx.assemble(_lib.GF_F32, scatter)
+    rn, ci, v = ctx.ell_download(_lib.GF_F32)
+    n = rn.size
+    A = ell_to_dense(g["rownnz_fp32"], g["colidx_fp32"], g["vals_fp32"].astype(np.float64), n)
+    B = ell_to_dense(rn, ci, v.astype(np.float64), n)
+    assert row_rel_err(A, B) <= TOL32
+    A64 = ell_to_dense(g["rownnz_fp64"], g["colidx_fp64"], g["vals_fp64"], n)
+    assert row_rel_err(A64, B) <= TOL32
+
+
+@pytest.mark.parametrize("et,n,ng", [(mg.Q4, (9, 7), 2), (mg.Q8, (6, 5), 3), (mg.Q8, (5, 4), 2),
+                                     (mg.BRICK8, (5, 4, 3), 2), (mg.BRICK8, (3, 3, 3), 3),
+                                     (mg.BRICK20, (3, 3, 2), 3), (mg.BRICK20, (3, 2, 2), 2)])
+def test_per_element_modulus_matches_oracle(fem, oracle, et, n, ng):
+    m = mg.structured(et, n, jitter=0.2, seed=31, ngauss=ng)
+    E = mg.lognormal_iid(m, 1.0, seed=5)
+    ctx = make_ctx(fem, mesh=m, E_elem=E)
+    ro, co, vo = oracle.assemble(et, ng, m.coords, m.conn, 210e3, m.nu, E_elem=E)
+    A = ell_to_dense(ro, co, vo)
+    for dtype, tol in ((_lib.GF_F64, TOL64), (_lib.GF_F32, TOL32)):
+        for scatter in (_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC):
+            ctx.assemble(dtype, scatter)
+            rn, ci, v = ctx.ell_download(dtype)
+            assert np.array_equal(ci, co)
+            assert row_rel_err(A, ell_to_dense(rn, ci, v.astype(np.float64))) <= tol
+
+
+def test_colour_and_atomic_agree_and_parity_colouring(fem):
+    m = mg.workload("brick20_64", scale=1 / 8)
+    ctx = make_ctx(fem, mesh=m)
+    nc = ctx.color(m.colors)
+    assert nc == 8
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_COLOR)
+    _, _, v1 = ctx.ell_download(_lib.GF_F64)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_ATOMIC)
+    _, _, v2 = ctx.ell_download(_lib.GF_F64)
+    assert np.abs(v1 - v2).max() <= 1e-13 * np.abs(v1).max()
+    # library greedy colouring equals the oracle's (reference femColor rule)
+    ctx2 = make_ctx(fem, mesh=m)
+    nc2 = ctx2.color(None)
+    from oracle.oracle import Oracle
+    col, ncol = Oracle().greedy_color(m.elem_type, m.nnodes, m.conn)
+    assert nc2 == ncol
+    assert np.array_equal(ctx2.colors(m.nelem), col)
+
+
+def test_invalid_colouring_rejected(fem):
+    m = mg.structured(mg.Q4, (4, 4))
+    ctx = make_ctx(fem, mesh=m)
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.color(np.zeros(m.nelem, np.int32))
+    assert ei.value.status == _lib.GF_ERR_INVALID_ARG
+
+
+def test_distorted_element_fp32_uses_fp64_jacobian(fem, oracle):
+    """An element with max/min detJ > 10 over its Gauss points: FP32 stays within
+    tolerance of the FP64 oracle (the FP32 path switches J, J^-1 to FP64)."""
+    m = mg.structured(mg.BRICK20, (1, 1, 1), ngauss=3)
+    # taper: the cross-section shrinks linearly with z to 5% at the top face; the
+    # map is linear along every edge, so mid-side nodes stay at edge midpoints
+    X = m.coords.copy()
+    s = 1.0 - 0.95 * X[:, 2]
+    X[:, 0] = (X[:, 0] - 0.5) * s + 0.5
+    X[:, 1] = (X[:, 1] - 0.5) * s + 0.5
+    m.coords = X
+    e = m.conn[0] - 1
+    ctx = make_ctx(fem, mesh=m)
+    ro, co, vo = oracle.assemble(mg.BRICK20, 3, X, m.conn, 210e3, 0.3)
+    pts, _ = oracle.gauss(3, 3)
+    dets = [np.linalg.det(oracle.dshape(mg.BRICK20, p) @ X[e]) for p in pts]
+    assert min(dets) > 0 and max(dets) / min(dets) > 10
+    ctx.assemble(_lib.GF_F32, _lib.GF_SCATTER_COLOR)
+    rn, ci, v = ctx.ell_download(_lib.GF_F32)
+    assert row_rel_err(ell_to_dense(ro, co, vo), ell_to_dense(rn, ci, v.astype(np.float64))) <= TOL32
+
+
+def test_single_element_and_isolated_node(fem, oracle):
+    m = mg.structured(mg.Q8, (1, 1), ngauss=3)
+    coords = np.vstack([m.coords, [[5.0, 5.0]]])      # node 9 belongs to no element
+    ctx = fem(0)
+    ctx.mesh_create(mg.Q8, coords, m.conn, 3, 210e3, None, 0.3)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_COLOR)
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    assert rn[-1] == 0 and rn[-2] == 0
+    ro, co, vo = oracle.assemble(mg.Q8, 3, m.coords, m.conn, 210e3, 0.3)
+    A = ell_to_dense(ro, co, vo)
+    B = ell_to_dense(rn, ci, v)[:16, :16]
+    assert row_rel_err(A, B) <= TOL64
+
+
+@pytest.mark.parametrize("bad", ["zero_id", "too_big", "repeat", "ngauss", "nu", "modulus"])
+def test_invalid_mesh_rejected(fem, bad):
+    m = mg.structured(mg.Q4, (2, 2))
+    conn = m.conn.copy()
+    ng, nu, E = 2, 0.3, 210e3
+    if bad == "zero_id":
+        conn[0, 0] = 0
+    elif bad == "too_big":
+        conn[0, 0] = m.nnodes + 1
+    elif bad == "repeat":
+        conn[0, 1] = conn[0, 0]
+    elif bad == "ngauss":
+        ng = 4
+    elif bad == "nu":
+        nu = 0.5
+    elif bad == "modulus":
+        E = -1.0
+    ctx = fem(0)
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.mesh_create(mg.Q4, m.coords, conn, ng, E, None, nu)
+    assert ei.value.status == _lib.GF_ERR_INVALID_ARG
+
+
+def test_state_errors(fem):
+    ctx = fem(0)
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.assemble()
+    assert ei.value.status == _lib.GF_ERR_STATE
+
+
+@pytest.mark.parametrize("name", ["q8_512", "brick20_64"])
+def test_full_size_rigid_translation(fem, name):
+    """Size-independent property at the full workload size: K annihilates rigid
+    translations (before constraints), checked with the device SpMV."""
+    m = mg.workload(name)
+    ctx = make_ctx(fem, mesh=m)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_COLOR)
+    n = m.ndof
+    rn, ci, v = None, None, None
+    for c in range(m.dim):
+        u = np.zeros((m.nnodes, m.dim))
+        u[:, c] = 1.0
+        y = ctx.spmv(u.ravel(), _lib.GF_F64)
+        diag_scale = 210e3 * (20.0 if m.dim == 3 else 5.0)
+        assert np.abs(y).max() <= 1e-9 * diag_scale * (np.exp(3) if m.E is not None else 1)
+    ctx.assemble(_lib.GF_F32, _lib.GF_SCATTER_COLOR)
+    x = np.random.default_rng(0).standard_normal(n)
+    y32 = ctx.spmv(x, _lib.GF_F32)
+    y64 = ctx.spmv(x, _lib.GF_F64)
+    assert np.linalg.norm(y32 - y64) <= 1e-5 * np.linalg.norm(y64)
