@@ -119,8 +119,9 @@ void gf_pattern_free(gf_ctx* ctx) {
   gf_free(ctx->d_diagpos);
   gf_free(ctx->d_K64);
   gf_free(ctx->d_K32);
+  // n (the dof count) belongs to the mesh and survives; width and nnz do not
   ctx->has_pattern = ctx->has64 = ctx->has32 = false;
-  ctx->n = ctx->W = 0;
+  ctx->W = 0;
   ctx->nnz = 0;
 }
 
@@ -407,13 +408,16 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
       }
     }
   }
+  // the uploaded matrix replaces any mesh-derived system (mesh, pattern, loads)
   cudaStreamSynchronize(ctx->stream);
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
-  if (!ctx->has_mesh) {
-    gf_free(ctx->d_f);
-    gf_free(ctx->d_fixed);
-  }
+  gf_mesh_free(ctx);
+  gf_free(ctx->d_f);
+  gf_free(ctx->d_fixed);
+  ctx->h_supports.clear();
+  ctx->nsup = 0;
+  ctx->bc_mode_applied = -1;
   gf_status st;
   ctx->n = n;
   ctx->W = width;
@@ -422,13 +426,11 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
   if ((st = gf_alloc(ctx, &ctx->d_colidx, total)) != GF_OK) return st;
   if ((st = gf_alloc(ctx, &ctx->d_K64, total)) != GF_OK) return st;
   if ((st = gf_alloc(ctx, &ctx->d_K32, total)) != GF_OK) return st;
-  if (!ctx->d_f && (st = gf_alloc(ctx, &ctx->d_f, (size_t)n)) != GF_OK) return st;
-  if (!ctx->d_fixed && (st = gf_alloc(ctx, &ctx->d_fixed, (size_t)n)) != GF_OK) return st;
-  if ((int)ctx->h_f.size() != n) {
-    ctx->h_f.assign(n, 0.0);
-    GF_CUDA(ctx, cudaMemsetAsync(ctx->d_f, 0, sizeof(double) * n, ctx->stream));
-    GF_CUDA(ctx, cudaMemsetAsync(ctx->d_fixed, 0, n, ctx->stream));
-  }
+  if ((st = gf_alloc(ctx, &ctx->d_f, (size_t)n)) != GF_OK) return st;
+  if ((st = gf_alloc(ctx, &ctx->d_fixed, (size_t)n)) != GF_OK) return st;
+  ctx->h_f.assign(n, 0.0);
+  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_f, 0, sizeof(double) * n, ctx->stream));
+  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_fixed, 0, n, ctx->stream));
   GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_rownnz, rownnz, sizeof(int32_t) * n,
                                cudaMemcpyHostToDevice, ctx->stream));
   GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_colidx, col.data(), sizeof(int32_t) * total,

@@ -101,7 +101,7 @@ __device__ inline void k_add(T* p, T v, bool atomic) {
 template <int ET, typename TC, bool ATOMIC>
 __global__ void __launch_bounds__(kThreads)
 k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
-           const int32_t* __restrict__ conn, const TC* __restrict__ coords,
+           const int32_t* __restrict__ conn, const double* __restrict__ coords,
            const TC* __restrict__ Eel, const uint16_t* __restrict__ slotmap, int nelem, int n,
            const AsmTables* __restrict__ tab, TC lam1, TC mu1, TC* __restrict__ K) {
   constexpr ElemInfo info = gf_elem_info(ET);
@@ -129,12 +129,17 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
     sflag[e] = 0;
   }
   __syncthreads();
+  // Element-local coordinates x_i - x_0, formed in FP64 before rounding: J depends
+  // only on coordinate differences, so the FP32 path keeps full relative precision
+  // in J however small the element is against its distance from the origin.
   for (int k = threadIdx.x; k < nt * NEN; k += kThreads) {
     const int e = k / NEN, i = k % NEN;
     const int node = conn[(int64_t)sel[e] * NEN + i];
+    const int node0 = conn[(int64_t)sel[e] * NEN];
     sconn[k] = node;
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) sX[k * DIM + c] = coords[(int64_t)node * DIM + c];
+    for (int c = 0; c < DIM; ++c)
+      sX[k * DIM + c] = TC(coords[(int64_t)node * DIM + c] - coords[(int64_t)node0 * DIM + c]);
   }
   __syncthreads();
 
@@ -260,7 +265,7 @@ template <int ET, typename TC>
 gf_status launch_et(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* K) {
   const int TE = pick_tile<ET, TC>(ctx->ngp);
   const size_t sm = smem_bytes<ET, TC>(TE, ctx->ngp);
-  const TC* coords = sizeof(TC) == 8 ? (const TC*)ctx->d_coords64 : (const TC*)ctx->d_coords32;
+  const double* coords = ctx->d_coords64;
   const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
   auto kc = k_assemble<ET, TC, false>;
   auto ka = k_assemble<ET, TC, true>;

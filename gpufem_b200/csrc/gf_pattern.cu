@@ -167,6 +167,9 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   const int64_t total = (int64_t)nelem * nen;
   cudaStream_t s = ctx->stream;
   gf_pattern_free(ctx);
+  if (ctx->n != nnodes * dim)
+    return gf_fail(ctx, GF_ERR_STATE, "dof count %d does not match the mesh (%d)", ctx->n,
+                   nnodes * dim);
   gf_status st;
 
   int32_t *d_cnt = nullptr, *d_inc_off = nullptr, *d_fill = nullptr, *d_inc = nullptr;
