@@ -72,7 +72,10 @@ SIGNATURES = {
     "gf_solve": (I32, [P, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     "gf_get_solution": (I32, [P, P]),
     "gf_solution_view": (I32, [P, C.POINTER(P)]),
+    "gf_pcg_noalloc": (I32, [I32, I32, P, P, P, P, P, D, I32, P, C.POINTER(I32),
+                             C.POINTER(D)]),
 }
+GF_PCG_NOALLOC_MAX_N = 262144
 
 
 def _load() -> C.CDLL:

@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <algorithm>
+#include <mutex>
 
 #include "gf_internal.cuh"
 
@@ -638,4 +639,115 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
     gf_fail(ctx, (gf_status)info->status, "mixed solve stopped with code %d (%d iterations)",
             last_done, total_it);
   return (gf_status)info->status;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free Jacobi-PCG (gf_pcg_noalloc).
+//
+// For callers that may not allocate device memory themselves or through this
+// library: a host framework that owns every device byte through its own arena,
+// or a time-stepping loop where a cudaMalloc/cudaFree (which can synchronise the
+// device) is not allowed.  The caller passes the ELL matrix, right-hand side and
+// solution buffers; the solver's work vectors and scalars live in one file-scope
+// __device__ array of fixed size, held by every GPU that loads this library until
+// the process exits.  It never calls cudaMalloc, cudaFree or cudaMallocHost.
+//
+// Shared-state rules: all calls share that array and it keeps the previous call's
+// contents (every word a call reads is written or cleared by the same call first),
+// so two calls whose GPU work overlaps — on two streams, or from two host threads —
+// race and corrupt each other.  The first call on a device looks up the array's
+// device address with cudaGetSymbolAddress (which may load the module onto that
+// device); make that first call before any stream capture.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocVecs = 5;           // r, z, p, q, 1/diag
+constexpr int kNoAllocScalarDoubles = 32; // SolveScalars + residual accumulator
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(GF_PCG_NOALLOC_MAX_N > 0, "max size");
+static_assert(sizeof(SolveScalars) <= 16 * sizeof(double), "scalar block");
+}  // namespace
+
+static __device__ __align__(256) double
+    g_pcg_noalloc_scratch[(size_t)kNoAllocVecs * GF_PCG_NOALLOC_MAX_N + kNoAllocScalarDoubles];
+
+static std::mutex g_pcg_noalloc_mu;
+static double* g_pcg_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up once per
+// device, with that device current).
+static gf_status pcg_noalloc_scratch(double** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return GF_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return GF_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_pcg_noalloc_mu);
+  if (!g_pcg_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_pcg_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return GF_ERR_CUDA;
+    }
+    g_pcg_noalloc_addr[dev] = static_cast<double*>(p);
+  }
+  *out = g_pcg_noalloc_addr[dev];
+  return GF_OK;
+}
+
+extern "C" GF_API gf_status gf_pcg_noalloc(int32_t n, int32_t width, const int32_t* rownnz,
+                                           const int32_t* colidx, const double* values,
+                                           const double* b, double* x, double tol,
+                                           int32_t max_iter, void* stream, int32_t* iterations,
+                                           double* rel_residual) {
+  if (n <= 0 || n > GF_PCG_NOALLOC_MAX_N) return GF_ERR_INVALID_ARG;
+  if (width <= 0 || !rownnz || !colidx || !values || !b || !x) return GF_ERR_INVALID_ARG;
+  if (!(tol > 0.0) || max_iter <= 0) return GF_ERR_INVALID_ARG;
+  double* S = nullptr;
+  gf_status st = pcg_noalloc_scratch(&S);
+  if (st != GF_OK) return st;
+  const size_t M = GF_PCG_NOALLOC_MAX_N;
+  double *r = S, *z = S + M, *p = S + 2 * M, *q = S + 3 * M, *dinv = S + 4 * M;
+  SolveScalars* sc = reinterpret_cast<SolveScalars*>(S + kNoAllocVecs * M);
+  double* acc = S + kNoAllocVecs * M + 16;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int nb = gf_blocks(n, kT);
+  const int chunk = 16;
+  auto fail = [](cudaError_t e) {
+    cudaGetLastError();
+    return e == cudaSuccess ? GF_OK : GF_ERR_CUDA;
+  };
+  cudaError_t e = cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s);
+  if (e != cudaSuccess) return fail(e);
+  k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, rownnz, colidx, values, dinv);
+  k_cg_init<double><<<nb, kT, 0, s>>>(n, b, dinv, x, r, z, p, sc);
+  k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, max_iter);
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+  SolveScalars hs{};  // pageable host copy: no pinned allocation
+  for (;;) {
+    for (int k = 0; k < chunk; ++k) {
+      k_cg_spmv_dot<double, double><<<nb, kT, 0, s>>>(n, rownnz, colidx, values, p, q, sc);
+      k_cg_update<double><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+      k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+    e = cudaMemcpyAsync(&hs, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(e);
+    if (hs.done) break;
+  }
+  // true residual ||b - K x|| / ||b|| in FP64 (r0 = b since x0 = 0)
+  double rr = 0.0;
+  e = cudaMemsetAsync(acc, 0, sizeof(double), s);
+  if (e != cudaSuccess) return fail(e);
+  k_residual64<<<nb, kT, 0, s>>>(n, rownnz, colidx, values, x, b, r, acc);
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+  e = cudaMemcpyAsync(&rr, acc, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(e);
+  if (iterations) *iterations = hs.iter;
+  if (rel_residual) *rel_residual = hs.rr0 > 0.0 ? std::sqrt(rr / hs.rr0) : 0.0;
+  return status_of(hs.done);
 }

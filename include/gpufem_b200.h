@@ -198,6 +198,27 @@ GF_API gf_status gf_get_solution(gf_ctx* ctx, double* u);
 /* Device pointer of the FP64 solution. */
 GF_API gf_status gf_solution_view(gf_ctx* ctx, const double** u);
 
+/* ---- allocation-free solve -------------------------------------------------------------
+ * No counterpart in the reference.  FP64 Jacobi-PCG (x0 = 0, stop when the recursive
+ * residual satisfies r.r <= tol^2 b.b, or after max_iter iterations) for callers that
+ * cannot allocate GPU memory: applications whose framework hands out every device byte
+ * from its own arena, or loops in which a cudaMalloc/cudaFree and the device-wide
+ * synchronisation it can cause are not allowed.  It allocates nothing and takes no
+ * context: every pointer is a caller-owned DEVICE buffer (the column-major ELL matrix as
+ * gf_ell_view describes it, b and x of n doubles) and `stream` is the caller's CUDA stream
+ * (NULL = legacy default stream).  Its work vectors live in one fixed __device__ array
+ * sized for n <= GF_PCG_NOALLOC_MAX_N (about 10.5 MB, held by every GPU that loads the
+ * library until the process exits); larger n returns GF_ERR_INVALID_ARG.  All calls share
+ * that array: calls whose GPU work overlaps (other streams, other threads) race.  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  Returns when done; *iterations and *rel_residual (true FP64
+ * ||b - K x|| / ||b||) may be NULL. */
+#define GF_PCG_NOALLOC_MAX_N 262144
+GF_API gf_status gf_pcg_noalloc(int32_t n, int32_t width, const int32_t* rownnz,
+                                const int32_t* colidx, const double* values, const double* b,
+                                double* x, double tol, int32_t max_iter, void* stream,
+                                int32_t* iterations, double* rel_residual);
+
 #ifdef __cplusplus
 }
 #endif
