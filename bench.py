@@ -55,57 +55,67 @@ def dist_info():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every 5 ms while the timed
+    region runs (read-only queries; nothing about the GPU is changed)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.fh = None
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+        self.error = None
 
     def __enter__(self):
+        import threading
         try:
-            self.fh = tempfile.TemporaryFile(mode="w+")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=self.fh, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            dev_index = self.device
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            if vis:
+                try:
+                    dev_index = int(vis.split(",")[self.device])
+                except ValueError:
+                    pass
+            h = pynvml.nvmlDeviceGetHandleByIndex(dev_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        except Exception as exc:  # NVML unavailable: report it, keep benchmarking
+            self.error = str(exc)
+            return self
+        self._stop = threading.Event()
+
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for nm, bit in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(nm)
+                except Exception:
+                    pass
+                self._stop.wait(0.005)
+
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self):
-        if self.proc is None or self.fh is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.fh.seek(0)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.fh.read().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.error:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"nvml: {self.error}"]}
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
 
 
 def cpu_model():
@@ -208,8 +218,10 @@ def run_gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    scatter = {"owner": _lib.GF_SCATTER_OWNER, "colour": _lib.GF_SCATTER_COLOR,
+               "atomic": _lib.GF_SCATTER_ATOMIC}[args.scatter]
     for _ in range(args.warmup):
-        ctx.assemble(dtype, _lib.GF_SCATTER_COLOR)
+        ctx.assemble(dtype, scatter)
     barrier()
     launches0 = ctx.launches()
     dev_s = []
@@ -217,7 +229,7 @@ def run_gpu_arm(args):
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            dev_s.append(ctx.assemble(dtype, _lib.GF_SCATTER_COLOR))
+            dev_s.append(ctx.assemble(dtype, scatter))
         barrier()
     launches = ctx.launches() - launches0
     total = float(sum(dev_s))
@@ -229,13 +241,17 @@ def run_gpu_arm(args):
     per_step = total / args.steps
     value = world * m.nelem / per_step
 
-    # atomic scatter variant (measured against the colour schedule)
-    at = []
-    for _ in range(max(3, args.steps // 2)):
-        flush.zero_()
-        torch.cuda.synchronize()
-        at.append(ctx.assemble(dtype, _lib.GF_SCATTER_ATOMIC))
-    atomic_eps = m.nelem / float(np.median(at))
+    # the three scatter schedules side by side (median of a few steps each)
+    variants = {}
+    for name, sc in (("owner", _lib.GF_SCATTER_OWNER), ("colour", _lib.GF_SCATTER_COLOR),
+                     ("atomic", _lib.GF_SCATTER_ATOMIC)):
+        ts = []
+        for _ in range(max(3, min(args.steps, 10))):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ts.append(ctx.assemble(dtype, sc))
+        variants[name] = {"value": m.nelem / float(np.median(ts)), "unit": UNIT,
+                          "ms": float(np.median(ts)) * 1e3}
 
     # roofline of the assembly phase: algorithmic bytes = K values written once +
     # node coordinates, connectivity and moduli read once
@@ -249,7 +265,7 @@ def run_gpu_arm(args):
         traffic = None if tr is None else tr.get("bytes_per_assembly")
 
     # SpMV roofline (FP32 values + int32 columns + x gather + y write)
-    ctx.assemble(dtype, _lib.GF_SCATTER_COLOR)
+    ctx.assemble(dtype, scatter)
     xs = torch.randn(n, device="cuda", dtype=torch.float32 if esize == 4 else torch.float64)
     ys = torch.empty_like(xs)
     sp = []
@@ -276,7 +292,7 @@ def run_gpu_arm(args):
                                       m.nelem, C.c_void_p(h_conn.data_ptr()), m.ngauss, m.E0,
                                       None if h_E is None else C.c_void_p(h_E.data_ptr()), m.nu, 0),
                    ctx.h)
-        _lib.check(lib.gf_assemble(ctx.h, dtype, _lib.GF_SCATTER_COLOR, 0), ctx.h)
+        _lib.check(lib.gf_assemble(ctx.h, dtype, scatter, 0), ctx.h)
         _lib.check(lib.gf_ell_download(ctx.h, dtype, C.c_void_p(h_rownnz.data_ptr()),
                                        C.c_void_p(h_colidx.data_ptr()),
                                        C.c_void_p(h_vals.data_ptr())), ctx.h)
@@ -303,8 +319,8 @@ def run_gpu_arm(args):
         ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
         ctx.set_supports(m.supports)
         ctx.set_force(m.f)
-        ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_COLOR)
-        ctx.assemble(_lib.GF_F32, _lib.GF_SCATTER_COLOR)
+        ctx.assemble(_lib.GF_F64, scatter)
+        ctx.convert_f64_to_f32()     # symmetric FP32 copy for the mixed solver
         ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
         ref = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-13, max_iter=400000,
                         raise_on_error=False)
@@ -342,15 +358,18 @@ def run_gpu_arm(args):
                        "between timed steps", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "kernel": "k_assemble (colour passes) + K zero-fill",
+                         "kernel": {"owner": "k_assemble_owner (one launch)",
+                                    "colour": "k_assemble colour passes + K zero-fill",
+                                    "atomic": "k_assemble atomic + K zero-fill"}[args.scatter],
                          "algorithmic_bytes": alg_bytes, "peak_source": peak_kind},
             "roofline_spmv": {"bound": "hbm", "achieved": spmv_bytes / t_spmv / 1e9, "peak": hbm,
                               "unit": "GB/s", "frac": spmv_bytes / t_spmv / 1e9 / hbm,
                               "us_per_launch": t_spmv * 1e6, "algorithmic_bytes": spmv_bytes},
-            "atomic_scatter": {"value": atomic_eps, "unit": UNIT},
+            "scatter": args.scatter,
+            "scatter_variants": variants,
             "e2e": {"value": world * m.nelem / e2e_per, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "includes": "mesh upload, pattern, colouring, assembly, ELL download"},
+                    "includes": "mesh upload, pattern, assembly, ELL download"},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "solve": solve,
@@ -373,6 +392,7 @@ def main():
     ap.add_argument("--config", default="q8_512", choices=sorted(WORKLOADS))
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scatter", default="owner", choices=["owner", "colour", "atomic"])
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -117,6 +117,14 @@ void gf_pattern_free(gf_ctx* ctx) {
   gf_free(ctx->d_adj_off);
   gf_free(ctx->d_adj);
   gf_free(ctx->d_diagpos);
+  gf_free(ctx->d_inc_off);
+  gf_free(ctx->d_inc);
+  gf_free(ctx->d_inc_loc);
+  gf_free(ctx->d_inc_slot);
+  if (ctx->d_geo) cudaFree(ctx->d_geo);
+  ctx->d_geo = nullptr;
+  ctx->geo_bytes = 0;
+  ctx->maxval = 0;
   gf_free(ctx->d_K64);
   gf_free(ctx->d_K32);
   // n (the dof count) belongs to the mesh and survives; width and nnz do not
@@ -296,7 +304,7 @@ GF_API gf_status gf_assemble(gf_ctx* ctx, int32_t dtype, int32_t scatter, int32_
   if (!ctx->has_mesh) return gf_fail(ctx, GF_ERR_STATE, "no mesh");
   if (dtype != GF_F64 && dtype != GF_F32)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown dtype %d", dtype);
-  if (scatter != GF_SCATTER_COLOR && scatter != GF_SCATTER_ATOMIC)
+  if (scatter != GF_SCATTER_COLOR && scatter != GF_SCATTER_ATOMIC && scatter != GF_SCATTER_OWNER)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown scatter %d", scatter);
   if (engine != GF_ENGINE_CUDA_CORE && engine != GF_ENGINE_TF32_MMA)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown engine %d", engine);

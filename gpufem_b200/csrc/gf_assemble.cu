@@ -30,64 +30,11 @@
 #include <cmath>
 #include <algorithm>
 
-#include "gf_internal.cuh"
+#include "gf_elem.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-
-struct AsmTables {
-  // dN/dxi at each Gauss point: [gp][a][i], and weights, both precisions
-  double dN64[GF_MAX_GP * 3 * GF_MAX_NEN];
-  float dN32[GF_MAX_GP * 3 * GF_MAX_NEN];
-  double w64[GF_MAX_GP];
-  float w32[GF_MAX_GP];
-};
-
-template <int DIM, typename R>
-__device__ inline R det_inv(const R (&J)[3][3], R (&Ji)[3][3]) {
-  if (DIM == 2) {
-    R d = J[0][0] * J[1][1] - J[0][1] * J[1][0];
-    R id = R(1) / d;
-    Ji[0][0] = J[1][1] * id;
-    Ji[0][1] = -J[0][1] * id;
-    Ji[1][0] = -J[1][0] * id;
-    Ji[1][1] = J[0][0] * id;
-    return d;
-  } else {
-    R c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
-    R c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
-    R c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-    R d = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
-    R id = R(1) / d;
-    Ji[0][0] = c00 * id;
-    Ji[1][0] = c01 * id;
-    Ji[2][0] = c02 * id;
-    Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
-    Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
-    Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
-    Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
-    Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
-    Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
-    return d;
-  }
-}
-
-// Jacobian J[a][b] = sum_i dN_i/dxi_a * x_i[b] (rows natural, columns x,y,z),
-// as StiffAlgo::GetJacobianMatrix (StiffAlgo.cc:207-244).
-template <int NEN, int DIM, typename R, typename TC>
-__device__ inline void jacobian(const TC* dN /*[DIM][NEN]*/, const TC* X /*[NEN][DIM]*/,
-                                R (&J)[3][3]) {
-#pragma unroll
-  for (int a = 0; a < DIM; ++a)
-#pragma unroll
-    for (int b = 0; b < DIM; ++b) {
-      R s = R(0);
-#pragma unroll 4
-      for (int i = 0; i < NEN; ++i) s += R(dN[a * NEN + i]) * R(X[i * DIM + b]);
-      J[a][b] = s;
-    }
-}
 
 template <typename T>
 __device__ inline void k_add(T* p, T v, bool atomic) {
@@ -145,17 +92,8 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
 
   // phase 1a (FP32 path only): flag elements with a large detJ spread
   if (!f64) {
-    for (int e = threadIdx.x; e < nt; e += kThreads) {
-      float dmin = 3.4e38f, dmax = 0.f;
-      for (int g = 0; g < ngp; ++g) {
-        float J[3][3], Ji[3][3];
-        jacobian<NEN, DIM, float, TC>(sdN + g * DIM * NEN, sX + e * NEN * DIM, J);
-        float d = fabsf(det_inv<DIM, float>(J, Ji));
-        dmin = fminf(dmin, d);
-        dmax = fmaxf(dmax, d);
-      }
-      sflag[e] = (dmax > 10.f * dmin) ? 1 : 0;
-    }
+    for (int e = threadIdx.x; e < nt; e += kThreads)
+      sflag[e] = gf_distorted<NEN, DIM, TC>(sdN, ngp, sX + e * NEN * DIM);
     __syncthreads();
   }
 
@@ -163,38 +101,9 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
     const int e = t % TE, g = t / TE;
     if (e >= nt) continue;
-    const TC* dN = sdN + g * DIM * NEN;
-    const TC* X = sX + e * NEN * DIM;
-    TC detJ;
-    if (f64 || sflag[e]) {
-      double J[3][3], Ji[3][3];
-      jacobian<NEN, DIM, double, TC>(dN, X, J);
-      detJ = TC(det_inv<DIM, double>(J, Ji));
-#pragma unroll 4
-      for (int i = 0; i < NEN; ++i) {
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          double s = 0.0;
-#pragma unroll
-          for (int a = 0; a < DIM; ++a) s += Ji[c][a] * double(dN[a * NEN + i]);
-          sG[((g * NEN + i) * DIM + c) * TE + e] = TC(s);
-        }
-      }
-    } else {
-      TC J[3][3], Ji[3][3];
-      jacobian<NEN, DIM, TC, TC>(dN, X, J);
-      detJ = det_inv<DIM, TC>(J, Ji);
-#pragma unroll 4
-      for (int i = 0; i < NEN; ++i) {
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          TC s = TC(0);
-#pragma unroll
-          for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i];
-          sG[((g * NEN + i) * DIM + c) * TE + e] = s;
-        }
-      }
-    }
+    const TC detJ = gf_gradients<NEN, DIM, TC>(sdN + g * DIM * NEN, sX + e * NEN * DIM,
+                                               f64 || sflag[e], sG + (g * NEN * DIM) * TE + e,
+                                               TE);
     swd[g * TE + e] = sw[g] * detJ * Eel[sel[e]];
   }
   __syncthreads();
@@ -302,10 +211,14 @@ gf_status launch_dispatch(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* 
 
 }  // namespace
 
-// Shape-derivative tables for the context's element type and Gauss rule, kept
-// in a small device buffer owned by the context (built once per mesh).
-static gf_status ensure_tables(gf_ctx* ctx) {
-  if (ctx->d_asmtab) return GF_OK;
+gf_status gf_assemble_owner(gf_ctx* ctx, int dtype, const AsmTables* d_tab);
+gf_status gf_assemble_owner_check(gf_ctx* ctx);
+
+gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out) {
+  if (ctx->d_asmtab) {
+    *out = (const AsmTables*)ctx->d_asmtab;
+    return GF_OK;
+  }
   AsmTables h{};
   std::vector<double> pts, w;
   gf_gauss_rule<double>(ctx->dim, ctx->ngauss, pts, w);
@@ -325,6 +238,7 @@ static gf_status ensure_tables(gf_ctx* ctx) {
   if (st != GF_OK) return st;
   GF_CUDA(ctx, cudaMemcpy(d, &h, sizeof(AsmTables), cudaMemcpyHostToDevice));
   ctx->d_asmtab = d;
+  *out = d;
   return GF_OK;
 }
 
@@ -332,8 +246,8 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   if (engine != GF_ENGINE_CUDA_CORE)
     return gf_fail(ctx, GF_ERR_UNSUPPORTED, "tensor-core engine not available in this build");
   gf_status st;
-  if ((st = ensure_tables(ctx)) != GF_OK) return st;
-  const AsmTables* d_tab = (const AsmTables*)ctx->d_asmtab;
+  const AsmTables* d_tab = nullptr;
+  if ((st = gf_asm_tables(ctx, &d_tab)) != GF_OK) return st;
   const int64_t total = (int64_t)ctx->n * ctx->W;
   if (dtype == GF_F64) {
     if (!ctx->d_K64 && (st = gf_alloc(ctx, &ctx->d_K64, (size_t)total)) != GF_OK) return st;
@@ -341,7 +255,10 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
     if (!ctx->d_K32 && (st = gf_alloc(ctx, &ctx->d_K32, (size_t)total)) != GF_OK) return st;
   }
   cudaEventRecord(ctx->ev0, ctx->stream);
-  if (dtype == GF_F64) {
+  if (scatter == GF_SCATTER_OWNER) {
+    // owner-computes: every K entry (padding included) is written exactly once
+    st = gf_assemble_owner(ctx, dtype, d_tab);
+  } else if (dtype == GF_F64) {
     cudaMemsetAsync(ctx->d_K64, 0, sizeof(double) * total, ctx->stream);
     st = launch_dispatch<double>(ctx, scatter, d_tab, ctx->d_K64);
   } else {
@@ -352,6 +269,7 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (st != GF_OK) return st;
   if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "assembly");
+  if (scatter == GF_SCATTER_OWNER && (st = gf_assemble_owner_check(ctx)) != GF_OK) return st;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   ctx->last_seconds = ms * 1e-3;

@@ -1,0 +1,304 @@
+// Owner-computes assembly (GF_SCATTER_OWNER): every ELL entry of K is written
+// exactly once, with coalesced stores, and no global atomics, colouring or
+// zero-fill are needed.
+//
+// Same arithmetic as gf_assemble.cu (node-pair blocks lam1 g_i g_j^T +
+// mu1 g_j g_i^T + mu1 (g_i . g_j) I, weighted by w detJ E), organised by rows:
+//
+//   k_elem_geometry  element-parallel, thread per (element, Gauss point): J^-1 and
+//                    w*detJ.  Element-local coordinates x_i - x_0 are formed in
+//                    FP64; J, J^-1 are FP64 for the FP64 path and for FP32 elements
+//                    whose max/min |detJ| over the Gauss points exceeds 10.
+//                    Layout GEO[element][gp][dim*dim + 1].
+//   k_assemble_owner a CTA owns NB consecutive nodes = NB*dim consecutive ELL rows,
+//                    with a shared-memory tile of those rows ([slot][row], W slots).
+//                    One task per (owned node a, incident element e) accumulates
+//                    H_j = sum_gp (w detJ E) g_i g_j^T, g = J^-1 dN, for the block
+//                    row i_a of Ke(e) and adds each block into the tile at the
+//                    neighbour slot of node j (shared-memory atomics: two elements
+//                    around a can hit the same slot).  The tile is then written to
+//                    K: for each slot the CTA's rows are contiguous in the
+//                    column-major ELL, so the stores coalesce, and padding slots
+//                    get their zeros.
+// Storing J^-1 (dim^2 + 1 values per Gauss point) instead of all node gradients
+// (nen*dim values) keeps the per-element buffer small: each element is re-read
+// once per owner node, so its size, not the extra FMAs, sets the cost.
+// Each element's block rows are formed by the owners of its nodes (no symmetry
+// saving), in exchange for K — the dominant traffic — being written once instead
+// of zero-filled and read-modified-written per contribution.  Reference: the
+// scatter of StiffAlgo::AssembleK (src/FEM/StiffAlgo.cc:304-401), by rows.
+#include <algorithm>
+#include <cmath>
+
+#include "gf_elem.cuh"
+
+namespace {
+
+constexpr int kOT = 256;
+constexpr size_t kOwnerSmemLimit = 60 * 1024;
+
+// ---------------------------------------------------------------------------
+template <int ET, typename TC>
+__global__ void __launch_bounds__(kOT)
+k_elem_geometry(int nelem, int ngp, int EB, const int32_t* __restrict__ conn,
+                const double* __restrict__ coords, const AsmTables* __restrict__ tab,
+                TC* __restrict__ geo) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  constexpr int NEN = info.nen, DIM = info.dim, GS = DIM * DIM + 1;
+  const bool f64 = sizeof(TC) == 8;
+  __shared__ double sX64[kOT / 4 * GF_MAX_NEN * 3];  // EB * NEN * DIM (EB <= 64)
+  __shared__ float sdet[kOT];
+  __shared__ int sflag[kOT / 4];
+  const int e0 = blockIdx.x * EB;
+  const int ne = min(EB, nelem - e0);
+  for (int k = threadIdx.x; k < ne * NEN; k += kOT) {
+    const int e = k / NEN, i = k % NEN;
+    const int node = conn[(int64_t)(e0 + e) * NEN + i];
+    const int node0 = conn[(int64_t)(e0 + e) * NEN];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c)
+      sX64[k * DIM + c] = coords[(int64_t)node * DIM + c] - coords[(int64_t)node0 * DIM + c];
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int el = t / ngp, g = t % ngp;
+  const bool active = t < ne * ngp;
+  const double* X = sX64 + el * NEN * DIM;
+  float Jf[3][3], Jif[3][3];
+  float detf = 0.f;
+  if (active) {
+    const float* dN = tab->dN32 + g * DIM * NEN;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        float s = 0.f;
+#pragma unroll
+        for (int i = 0; i < NEN; ++i) s += dN[a * NEN + i] * (float)X[i * DIM + b];
+        Jf[a][b] = s;
+      }
+    detf = gf_det_inv<DIM, float>(Jf, Jif);
+    sdet[t] = fabsf(detf);
+  }
+  __syncthreads();
+  if (t < ne) {
+    float dmin = 3.4e38f, dmax = 0.f;
+    for (int k = 0; k < ngp; ++k) {
+      dmin = fminf(dmin, sdet[t * ngp + k]);
+      dmax = fmaxf(dmax, sdet[t * ngp + k]);
+    }
+    sflag[t] = dmax > 10.f * dmin ? 1 : 0;
+  }
+  __syncthreads();
+  if (!active) return;
+  TC* out = geo + ((int64_t)(e0 + el) * ngp + g) * GS;
+  if (f64 || sflag[el]) {
+    const double* dN = tab->dN64 + g * DIM * NEN;
+    double J[3][3], Ji[3][3];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < NEN; ++i) s += dN[a * NEN + i] * X[i * DIM + b];
+        J[a][b] = s;
+      }
+    const double d = gf_det_inv<DIM, double>(J, Ji);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) out[a * DIM + b] = TC(Ji[a][b]);
+    out[DIM * DIM] = TC(tab->w64[g] * d);
+  } else {
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) out[a * DIM + b] = TC(Jif[a][b]);
+    out[DIM * DIM] = TC(tab->w32[g] * detf);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// JG element nodes per pass (register budget: JG * dim^2 accumulators).
+template <int ET, typename TC, int JG>
+__global__ void __launch_bounds__(kOT)
+k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
+                 const int32_t* __restrict__ inc_off, const int32_t* __restrict__ inc,
+                 const uint8_t* __restrict__ inc_loc, const uint16_t* __restrict__ inc_slot,
+                 const TC* __restrict__ geo, const TC* __restrict__ Eel,
+                 const AsmTables* __restrict__ tab, TC lam1, TC mu1, TC* __restrict__ K) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  constexpr int NEN = info.nen, DIM = info.dim, GS = DIM * DIM + 1;
+  static_assert(NEN % JG == 0, "node groups must tile the element");
+  const bool f64 = sizeof(TC) == 8;
+  const int RB = NB * DIM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TC* tile = reinterpret_cast<TC*>(smem_raw);       // [W][RB]
+  TC* sdN = tile + (size_t)W * RB;                  // [ngp][DIM][NEN]
+  int* soff = reinterpret_cast<int*>(sdN + ngp * DIM * NEN);  // [NB + 1]
+
+  const int a0 = blockIdx.x * NB;
+  const int a1 = min(a0 + NB, nnodes);
+  for (int k = threadIdx.x; k < W * RB; k += kOT) tile[k] = TC(0);
+  for (int k = threadIdx.x; k < ngp * DIM * NEN; k += kOT)
+    sdN[k] = f64 ? TC(tab->dN64[k]) : TC(tab->dN32[k]);
+  for (int k = threadIdx.x; k <= a1 - a0; k += kOT) soff[k] = inc_off[a0 + k];
+  __syncthreads();
+  const int q0 = soff[0];
+  const int T = soff[a1 - a0] - q0;
+
+  for (int t = threadIdx.x; t < T; t += kOT) {
+    int lo = 0, hi = a1 - a0;  // owned node of this incidence entry
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (soff[mid] - q0 <= t) lo = mid; else hi = mid;
+    }
+    const int al = lo;
+    const int q = q0 + t;
+    const int e = inc[q];
+    const int i = inc_loc[q];
+    const TC Ee = Eel[e];
+    const TC* ge = geo + (int64_t)e * ngp * GS;
+    const uint16_t* slots = inc_slot + (int64_t)q * NEN;
+#pragma unroll 1
+    for (int j0 = 0; j0 < NEN; j0 += JG) {
+      TC H[JG][DIM][DIM];
+#pragma unroll
+      for (int jj = 0; jj < JG; ++jj)
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) H[jj][a][b] = TC(0);
+#pragma unroll 1
+      for (int g = 0; g < ngp; ++g) {
+        TC Ji[DIM][DIM];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) Ji[a][b] = __ldg(ge + g * GS + a * DIM + b);
+        const TC wd = __ldg(ge + g * GS + DIM * DIM) * Ee;
+        const TC* dN = sdN + g * DIM * NEN;
+        TC gi[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          TC s = TC(0);
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i];
+          gi[c] = s * wd;
+        }
+#pragma unroll
+        for (int jj = 0; jj < JG; ++jj) {
+          const int j = j0 + jj;
+          TC gj[DIM];
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) {
+            TC s = TC(0);
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + j];
+            gj[c] = s;
+          }
+#pragma unroll
+          for (int a = 0; a < DIM; ++a)
+#pragma unroll
+            for (int b = 0; b < DIM; ++b) H[jj][a][b] += gi[a] * gj[b];
+        }
+      }
+#pragma unroll
+      for (int jj = 0; jj < JG; ++jj) {
+        const int p = slots[j0 + jj];
+        TC tr = TC(0);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) tr += H[jj][a][a];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) {
+            TC v = lam1 * H[jj][a][b] + mu1 * H[jj][b][a];
+            if (a == b) v += mu1 * tr;
+            atomicAdd(&tile[(size_t)(p * DIM + b) * RB + al * DIM + a], v);
+          }
+      }
+    }
+  }
+  __syncthreads();
+  const int rows = (a1 - a0) * DIM;
+  const int64_t row0 = (int64_t)a0 * DIM;
+  for (int idx = threadIdx.x; idx < W * RB; idx += kOT) {
+    const int s = idx / RB, r = idx % RB;
+    if (r < rows) K[(int64_t)s * n + row0 + r] = tile[idx];
+  }
+}
+
+template <int ET, typename TC>
+size_t owner_smem_bytes(int NB, int W, int ngp) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  return sizeof(TC) * ((size_t)W * NB * info.dim + (size_t)ngp * info.dim * info.nen) +
+         sizeof(int) * (NB + 1) + 16;
+}
+
+template <int ET>
+constexpr int owner_jgroup() {
+  return gf_elem_info(ET).nen <= 8 ? gf_elem_info(ET).nen : 5;
+}
+
+template <int ET, typename TC>
+gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  const int W = ctx->W, ngp = ctx->ngp;
+  const size_t need = (size_t)ctx->nelem * ngp * (info.dim * info.dim + 1) * sizeof(TC);
+  if (ctx->geo_bytes < need) {
+    if (ctx->d_geo) cudaFree(ctx->d_geo);
+    ctx->d_geo = nullptr;
+    ctx->geo_bytes = 0;
+    if (cudaMalloc(&ctx->d_geo, need) != cudaSuccess) {
+      cudaGetLastError();
+      return gf_fail(ctx, GF_ERR_OOM, "geometry buffer (%zu bytes)", need);
+    }
+    ctx->geo_bytes = need;
+  }
+  TC* geo = static_cast<TC*>(ctx->d_geo);
+  const int EB = kOT / ngp;
+  k_elem_geometry<ET, TC><<<(ctx->nelem + EB - 1) / EB, kOT, 0, ctx->stream>>>(
+      ctx->nelem, ngp, EB, ctx->d_conn, ctx->d_coords64, d_tab, geo);
+  GF_LAUNCH_CHECK(ctx, "k_elem_geometry");
+  int NB = 256;  // largest node block whose tile keeps several CTAs per SM
+  while (NB > 1 && owner_smem_bytes<ET, TC>(NB, W, ngp) > kOwnerSmemLimit) NB >>= 1;
+  const size_t sm = owner_smem_bytes<ET, TC>(NB, W, ngp);
+  if (sm > kOwnerSmemLimit)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "owner scatter: a row block does not fit");
+  constexpr int JG = owner_jgroup<ET>();
+  auto kern = k_assemble_owner<ET, TC, JG>;
+  GF_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
+  kern<<<(ctx->nnodes + NB - 1) / NB, kOT, sm, ctx->stream>>>(
+      ctx->nnodes, ctx->n, W, NB, ngp, ctx->d_inc_off, ctx->d_inc, ctx->d_inc_loc,
+      ctx->d_inc_slot, geo, Eel, d_tab, TC(ctx->lam1), TC(ctx->mu1), K);
+  GF_LAUNCH_CHECK(ctx, "k_assemble_owner");
+  return GF_OK;
+}
+
+template <typename TC>
+gf_status owner_dispatch(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
+  switch (ctx->elem_type) {
+    case GF_Q4: return launch_owner<GF_Q4, TC>(ctx, K, d_tab);
+    case GF_Q8: return launch_owner<GF_Q8, TC>(ctx, K, d_tab);
+    case GF_BRICK8: return launch_owner<GF_BRICK8, TC>(ctx, K, d_tab);
+    default: return launch_owner<GF_BRICK20, TC>(ctx, K, d_tab);
+  }
+}
+
+}  // namespace
+
+// Launches the owner-computes assembly on the context's stream (no sync).
+gf_status gf_assemble_owner(gf_ctx* ctx, int dtype, const AsmTables* d_tab) {
+  if (ctx->ngp < 4 || ctx->ngp > GF_MAX_GP)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "Gauss rule size %d", ctx->ngp);
+  if (dtype == GF_F64) return owner_dispatch<double>(ctx, ctx->d_K64, d_tab);
+  return owner_dispatch<float>(ctx, ctx->d_K32, d_tab);
+}
+
+gf_status gf_assemble_owner_check(gf_ctx* ctx) {
+  (void)ctx;
+  return GF_OK;
+}

@@ -1,0 +1,113 @@
+// Element-level device helpers shared by the assembly kernels: shape-derivative
+// tables, Jacobian, determinant/inverse and the Cartesian gradients at a Gauss
+// point (StiffAlgo::GetJacobianMatrix / BuildBMatrix, src/FEM/StiffAlgo.cc:207-278;
+// det / matInverse, src/LAops/LAops.cc:80-117).
+#pragma once
+
+#include "gf_internal.cuh"
+
+struct AsmTables {
+  // dN/dxi at each Gauss point: [gp][a][i], and weights, both precisions
+  double dN64[GF_MAX_GP * 3 * GF_MAX_NEN];
+  float dN32[GF_MAX_GP * 3 * GF_MAX_NEN];
+  double w64[GF_MAX_GP];
+  float w32[GF_MAX_GP];
+};
+
+template <int DIM, typename R>
+__device__ inline R gf_det_inv(const R (&J)[3][3], R (&Ji)[3][3]) {
+  if (DIM == 2) {
+    R d = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    R id = R(1) / d;
+    Ji[0][0] = J[1][1] * id;
+    Ji[0][1] = -J[0][1] * id;
+    Ji[1][0] = -J[1][0] * id;
+    Ji[1][1] = J[0][0] * id;
+    return d;
+  } else {
+    R c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    R c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    R c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    R d = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    R id = R(1) / d;
+    Ji[0][0] = c00 * id;
+    Ji[1][0] = c01 * id;
+    Ji[2][0] = c02 * id;
+    Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+    Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+    Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+    Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    return d;
+  }
+}
+
+// J[a][b] = sum_i dN_i/dxi_a * x_i[b] (rows natural, columns x, y, z).
+template <int NEN, int DIM, typename R, typename TC>
+__device__ inline void gf_jacobian(const TC* dN /*[DIM][NEN]*/, const TC* X /*[NEN][DIM]*/,
+                                   R (&J)[3][3]) {
+#pragma unroll
+  for (int a = 0; a < DIM; ++a)
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) {
+      R s = R(0);
+#pragma unroll 4
+      for (int i = 0; i < NEN; ++i) s += R(dN[a * NEN + i]) * R(X[i * DIM + b]);
+      J[a][b] = s;
+    }
+}
+
+// Element with max/min |detJ| over its Gauss points above 10: the FP32 path then
+// forms J, J^-1 and the gradients in FP64.
+template <int NEN, int DIM, typename TC>
+__device__ inline int gf_distorted(const TC* sdN, int ngp, const TC* X) {
+  float dmin = 3.4e38f, dmax = 0.f;
+  for (int g = 0; g < ngp; ++g) {
+    float J[3][3], Ji[3][3];
+    gf_jacobian<NEN, DIM, float, TC>(sdN + g * DIM * NEN, X, J);
+    float d = fabsf(gf_det_inv<DIM, float>(J, Ji));
+    dmin = fminf(dmin, d);
+    dmax = fmaxf(dmax, d);
+  }
+  return dmax > 10.f * dmin ? 1 : 0;
+}
+
+// Gradients g_i = J^-1 dN_i/dxi at one Gauss point, written to
+// G[(i*DIM + c) * stride]; returns detJ.  `use64` selects FP64 arithmetic.
+template <int NEN, int DIM, typename TC>
+__device__ inline TC gf_gradients(const TC* dN, const TC* X, bool use64, TC* G, int stride) {
+  if (use64) {
+    double J[3][3], Ji[3][3];
+    gf_jacobian<NEN, DIM, double, TC>(dN, X, J);
+    const double d = gf_det_inv<DIM, double>(J, Ji);
+#pragma unroll 4
+    for (int i = 0; i < NEN; ++i)
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) s += Ji[c][a] * double(dN[a * NEN + i]);
+        G[(i * DIM + c) * stride] = TC(s);
+      }
+    return TC(d);
+  } else {
+    TC J[3][3], Ji[3][3];
+    gf_jacobian<NEN, DIM, TC, TC>(dN, X, J);
+    const TC d = gf_det_inv<DIM, TC>(J, Ji);
+#pragma unroll 4
+    for (int i = 0; i < NEN; ++i)
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        TC s = TC(0);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i];
+        G[(i * DIM + c) * stride] = s;
+      }
+    return d;
+  }
+}
+
+// Shape-derivative tables for the context's element type and Gauss rule (device
+// buffer owned by the context, built once per mesh).
+gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out);

@@ -173,6 +173,13 @@ struct gf_ctx {
   int32_t* d_adj_off = nullptr;   // node adjacency CSR
   int32_t* d_adj = nullptr;
   int32_t* d_diagpos = nullptr;   // per node: own position in its adjacency list
+  int32_t* d_inc_off = nullptr;   // node -> element incidence CSR, element ids ascending
+  int32_t* d_inc = nullptr;
+  uint8_t* d_inc_loc = nullptr;   // local index of the node within each incident element
+  uint16_t* d_inc_slot = nullptr; // [incidence][nen]: neighbour position of each element node
+  int maxval = 0;                 // max elements sharing one node
+  void* d_geo = nullptr;          // owner scatter: J^-1, w detJ per (element, Gauss point)
+  size_t geo_bytes = 0;
 
   // values
   bool has64 = false, has32 = false;

@@ -160,6 +160,48 @@ __global__ void k_diagpos(int nnodes, const int32_t* __restrict__ adj_off,
   diagpos[a] = lo - lo0;
 }
 
+// Thread per node: sort its incident elements ascending, then record the node's
+// local index in each of them and, for every node of each incident element, that
+// node's position in this node's adjacency list (the owner-computes scatter
+// writes row blocks of this node without searching).
+__global__ void k_incidence_finish(int nnodes, int nen, const int32_t* __restrict__ conn,
+                                   const int32_t* __restrict__ inc_off, int32_t* __restrict__ inc,
+                                   const int32_t* __restrict__ adj_off,
+                                   const int32_t* __restrict__ adj, uint8_t* __restrict__ inc_loc,
+                                   uint16_t* __restrict__ inc_slot, int32_t* __restrict__ errflag) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= nnodes) return;
+  const int q0 = inc_off[a], q1 = inc_off[a + 1];
+  for (int q = q0 + 1; q < q1; ++q) {  // insertion sort (lists are short)
+    const int v = inc[q];
+    int k = q - 1;
+    while (k >= q0 && inc[k] > v) {
+      inc[k + 1] = inc[k];
+      --k;
+    }
+    inc[k + 1] = v;
+  }
+  const int lo0 = adj_off[a], hi0 = adj_off[a + 1];
+  for (int q = q0; q < q1; ++q) {
+    const int e = inc[q];
+    int loc = -1;
+    for (int i = 0; i < nen; ++i)
+      if (conn[(int64_t)e * nen + i] == a) loc = i;
+    if (loc < 0) atomicExch(errflag, 3);
+    inc_loc[q] = (uint8_t)(loc < 0 ? 0 : loc);
+    for (int j = 0; j < nen; ++j) {
+      const int b = conn[(int64_t)e * nen + j];
+      int lo = lo0, hi = hi0;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (adj[mid] < b) lo = mid + 1; else hi = mid;
+      }
+      if (lo >= hi0 || adj[lo] != b) atomicExch(errflag, 4);
+      inc_slot[(int64_t)q * nen + j] = (uint16_t)(lo - lo0);
+    }
+  }
+}
+
 }  // namespace
 
 gf_status gf_pattern_build(gf_ctx* ctx) {
@@ -262,6 +304,16 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   k_diagpos<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_adj_off, ctx->d_adj,
                                                    ctx->d_diagpos);
   ctx->launches++;
+  // incidence kept for the owner-computes scatter
+  GF_TRY(gf_alloc(ctx, &ctx->d_inc_loc, (size_t)total));
+  GF_TRY(gf_alloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
+  k_incidence_finish<<<gf_blocks(nnodes, 128), 128, 0, s>>>(
+      nnodes, nen, ctx->d_conn, d_inc_off, d_inc, ctx->d_adj_off, ctx->d_adj, ctx->d_inc_loc,
+      ctx->d_inc_slot, d_err);
+  ctx->launches++;
+  GF_TRYC(cub::DeviceReduce::Max(d_tmp, tmp_bytes, d_cnt, d_max, nnodes, s));
+  int32_t h_maxval = 0;
+  GF_TRYC(cudaMemcpyAsync(&h_maxval, d_max, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_TRYC(cudaGetLastError());
   GF_TRYC(cudaMemcpyAsync(&h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_TRYC(cudaStreamSynchronize(s));
@@ -269,6 +321,11 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
     cleanup();
     return gf_fail(ctx, GF_ERR_CUDA, "pattern build: slot map lookup failed (%d)", h_err);
   }
+  ctx->d_inc_off = d_inc_off;  // ownership moves to the context
+  ctx->d_inc = d_inc;
+  d_inc_off = nullptr;
+  d_inc = nullptr;
+  ctx->maxval = h_maxval;
   cleanup();
   ctx->has_pattern = true;
   return GF_OK;

@@ -497,6 +497,163 @@ gf_status status_of(int done) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Mixed precision: FP32 Jacobi-PCG whose residual is recomputed in FP64
+// ("reliable updates").  Vectors x, r, z, p, q are FP32 and scaled by the norm
+// sigma of the FP64 residual at the last update; the solution accumulates in
+// FP64 (u += sigma x).  When the FP32 residual has dropped by 10x since the last
+// update (or the recursion reports convergence / breakdown / the iteration cap),
+// the host triggers an update: u += sigma x, r64 = f - K64 u in FP64, and the
+// FP32 residual restarts from r64 / ||r64|| with the search direction rescaled and
+// kept, so the Krylov process continues instead of restarting.  Convergence is
+// decided on the true FP64 residual only.
+namespace {
+
+__global__ void k_mixed_accumulate(int n, double sigma, float* __restrict__ x,
+                                   double* __restrict__ u) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) {
+    u[i] += sigma * (double)x[i];
+    x[i] = 0.f;
+  }
+}
+
+__global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv, float pscale,
+                              int restart, const float* __restrict__ dinv, float* __restrict__ r,
+                              float* __restrict__ z, float* __restrict__ p, SolveScalars* sc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kT + threadIdx.x;
+  double rz = 0.0, rr = 0.0;
+  if (i < n) {
+    const float ri = (float)(r64[i] * inv);
+    const float zi = ri * dinv[i];
+    r[i] = ri;
+    z[i] = zi;
+    p[i] = restart ? zi : p[i] * pscale;
+    rz = (double)ri * (double)zi;
+    rr = (double)ri * (double)ri;
+  }
+  double s1 = block_sum(rz, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
+  double s2 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
+__global__ void k_mixed_scalars(SolveScalars* sc, double tol2) {
+  sc->tol2 = tol2;
+  sc->pq = 0.0;
+  sc->done = sc->iter >= sc->maxit ? 3 : 0;
+}
+
+gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
+                    std::chrono::steady_clock::time_point t0, gf_solve_info* info) {
+  const int n = ctx->n;
+  const int nb = gf_blocks(n, kT);
+  cudaStream_t s = ctx->stream;
+  SolveScalars* sc = ctx->d_scal;
+  SolveScalars* hs = (SolveScalars*)ctx->h_pinned;
+  double* r64 = (double*)ctx->d_work;
+  float* v = (float*)(r64 + n);
+  float *x = v, *r = v + n, *z = v + 2 * (size_t)n, *p = v + 3 * (size_t)n, *q = v + 4 * (size_t)n;
+  float* dinv = v + 5 * (size_t)n;
+  const double tol = o->tol;
+  const double delta2 = 0.01;  // update when ||r|| fell 10x since the last update
+  gf_status st;
+  k_diag_inv<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32, dinv);
+  GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u, 0, sizeof(double) * n, s));
+  double ff = 0.0;
+  if ((st = residual64(ctx, r64, &ff)) != GF_OK) return st;  // u = 0: r64 = f
+  double rr64 = ff;
+  int updates = 0, done_code = 1;
+  if (ff > 0.0) {
+    double sigma = std::sqrt(ff);
+    k_scale_to_f32<<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
+    GF_LAUNCH_CHECK(ctx, "k_scale_to_f32");
+    GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
+    k_cg_init<float><<<nb, kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
+    GF_LAUNCH_CHECK(ctx, "k_cg_init");
+    k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
+    GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < check; ++k) {
+      k_cg_spmv_dot<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32,
+                                                     p, q, sc);
+      k_cg_update<float><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+      k_cg_direction<float><<<nb, kT, 0, s>>>(n, z, p, sc);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) return gf_cuda_fail(ctx, ce, "graph capture");
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return gf_cuda_fail(ctx, ce, "graph instantiate");
+    }
+    double rr_max = 1.0;
+    int breakdowns = 0;
+    done_code = 3;
+    for (;;) {
+      ce = cudaGraphLaunch(exec, s);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(hs, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s);
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+      if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "mixed chunk"); break; }
+      ctx->launches += 3 * check;
+      const bool timeout = o->max_seconds > 0.0 &&
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds;
+      // growth of the FP32 residual by 100x over its value at the last update means
+      // the FP32 recursion is diverging (K32 nearly indefinite for very ill-conditioned
+      // systems): update and restart the direction
+      const bool diverging = hs->done == 0 && hs->rr > 1e4;
+      if (hs->done == 0 && hs->rr > delta2 * rr_max && !timeout && !diverging) {
+        rr_max = std::max(rr_max, hs->rr);
+        continue;
+      }
+      // reliable update
+      k_mixed_accumulate<<<nb, kT, 0, s>>>(n, sigma, x, ctx->d_u);
+      ce = cudaGetLastError();
+      if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "k_mixed_accumulate"); break; }
+      ctx->launches++;
+      if ((st = residual64(ctx, r64, &rr64)) != GF_OK) break;
+      ++updates;
+      if (std::sqrt(rr64 / ff) <= tol) { done_code = 1; break; }
+      if (hs->done == 3 || timeout) { done_code = 3; break; }
+      const bool restart = hs->done == 2 || diverging;
+      if (restart && ++breakdowns > 50) { done_code = 2; break; }
+      const double sigma_new = std::sqrt(rr64);
+      ce = cudaMemsetAsync(&sc->rzn, 0, 2 * sizeof(double), s);  // rzn, rr
+      if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "reset"); break; }
+      k_mixed_reset<<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma_new, (float)(sigma / sigma_new),
+                                      restart ? 1 : 0, dinv, r, z, p, sc);
+      k_mixed_scalars<<<1, 1, 0, s>>>(sc, tol * tol * ff / rr64);
+      ce = cudaGetLastError();
+      if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "k_mixed_reset"); break; }
+      ctx->launches += 2;
+      sigma = sigma_new;
+      rr_max = 1.0;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (st != GF_OK) return st;
+  }
+  cudaEventRecord(ctx->ev1, s);
+  GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  info->seconds = ctx->last_seconds = ms * 1e-3;
+  info->iterations = ff > 0.0 ? hs->iter : 0;
+  info->outer = updates;
+  info->rel_residual = ff > 0.0 ? std::sqrt(rr64 / ff) : 0.0;
+  info->status = status_of(done_code);
+  if (done_code != 1)
+    gf_fail(ctx, (gf_status)info->status, "mixed solve stopped with code %d (%d iterations)",
+            done_code, info->iterations);
+  return (gf_status)info->status;
+}
+
+}  // namespace
+
 gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info) {
   *info = gf_solve_info{};
   const int solver = o->solver;
@@ -580,65 +737,10 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
     return (gf_status)info->status;
   }
 
-  // MIXED_PCG: FP64 refinement around FP32 Jacobi-PCG on K32
+  // MIXED_PCG: FP32 Jacobi-PCG on K32 with FP64 reliable updates on K64
   if (!ctx->has64 || !ctx->has32)
     return gf_fail(ctx, GF_ERR_STATE, "mixed solve needs both FP64 and FP32 matrices");
-  double* r64 = (double*)w;                  // n doubles
-  float* v = (float*)((double*)w + n);       // f32 vectors after it
-  CgVecs vv{v, v + n, v + 2 * (size_t)n, v + 3 * (size_t)n, v + 4 * (size_t)n, v + 5 * (size_t)n};
-  float* b32 = v + 6 * (size_t)n;
-  k_diag_inv<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32,
-                                             (float*)vv.dinv);
-  GF_LAUNCH_CHECK(ctx, "k_diag_inv");
-  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u, 0, sizeof(double) * n, s));
-  double ff = 0.0;
-  {
-    std::vector<double> f(n);
-    GF_CUDA(ctx, cudaMemcpyAsync(f.data(), ctx->d_f, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-    GF_CUDA(ctx, cudaStreamSynchronize(s));
-    for (double x : f) ff += x * x;
-  }
-  int total_it = 0, outer = 0, last_done = 1;
-  double rr = 0.0;
-  if ((st = residual64(ctx, r64, &rr)) != GF_OK) return st;
-  while (true) {
-    if (ff == 0.0 || std::sqrt(rr / ff) <= o->tol) { last_done = 1; break; }
-    if (outer >= max_outer || total_it >= maxit) { last_done = 3; break; }
-    if (o->max_seconds > 0.0 &&
-        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds) {
-      last_done = 3;
-      break;
-    }
-    const double rn = std::sqrt(rr);
-    k_scale_to_f32<<<nb, kT, 0, s>>>(n, r64, 1.0 / rn, b32);
-    GF_LAUNCH_CHECK(ctx, "k_scale_to_f32");
-    int iters = 0, done = 0;
-    double rri = 0.0, rr0 = 0.0;
-    st = run_cg<float, float>(ctx, ctx->d_K32, b32, vv, true, inner_tol, maxit - total_it, check,
-                              o->max_seconds, t0, &iters, &done, &rri, &rr0);
-    if (st != GF_OK) return st;
-    total_it += iters;
-    ++outer;
-    k_axpy_f32_into_f64<<<nb, kT, 0, s>>>(n, rn, (const float*)vv.x, ctx->d_u);
-    GF_LAUNCH_CHECK(ctx, "k_axpy_f32_into_f64");
-    double rr_new = 0.0;
-    if ((st = residual64(ctx, r64, &rr_new)) != GF_OK) return st;
-    if (done == 2 && !(rr_new < rr)) { last_done = 2; rr = rr_new; break; }
-    rr = rr_new;
-  }
-  cudaEventRecord(ctx->ev1, s);
-  GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  info->seconds = ctx->last_seconds = ms * 1e-3;
-  info->iterations = total_it;
-  info->outer = outer;
-  info->rel_residual = ff > 0.0 ? std::sqrt(rr / ff) : 0.0;
-  info->status = status_of(last_done);
-  if (last_done != 1)
-    gf_fail(ctx, (gf_status)info->status, "mixed solve stopped with code %d (%d iterations)",
-            last_done, total_it);
-  return (gf_status)info->status;
+  return run_mixed(ctx, o, maxit, check, t0, info);
 }
 
 // ---------------------------------------------------------------------------

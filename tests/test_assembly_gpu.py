@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
 TOL32 = 1e-6
+SCATTERS = [_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC, _lib.GF_SCATTER_OWNER]
 
 
 @pytest.fixture(scope="module")
@@ -34,7 +35,7 @@ def make_ctx(Context, g=None, mesh=None, E_elem=None):
 
 
 @pytest.mark.parametrize("name", golden_names())
-@pytest.mark.parametrize("scatter", [_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC])
+@pytest.mark.parametrize("scatter", SCATTERS)
 def test_fp64_assembly_matches_reference(fem, oracle, name, scatter):
     g = load_golden(name)
     ctx = make_ctx(fem, g)
@@ -58,7 +59,7 @@ def test_fp64_assembly_matches_reference(fem, oracle, name, scatter):
 
 
 @pytest.mark.parametrize("name", golden_names())
-@pytest.mark.parametrize("scatter", [_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC])
+@pytest.mark.parametrize("scatter", SCATTERS)
 def test_fp32_assembly_matches_reference(fem, name, scatter):
     g = load_golden(name)
     ctx = make_ctx(fem, g)
@@ -82,7 +83,7 @@ def test_per_element_modulus_matches_oracle(fem, oracle, et, n, ng):
     ro, co, vo = oracle.assemble(et, ng, m.coords, m.conn, 210e3, m.nu, E_elem=E)
     A = ell_to_dense(ro, co, vo)
     for dtype, tol in ((_lib.GF_F64, TOL64), (_lib.GF_F32, TOL32)):
-        for scatter in (_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC):
+        for scatter in SCATTERS:
             ctx.assemble(dtype, scatter)
             rn, ci, v = ctx.ell_download(dtype)
             assert np.array_equal(ci, co)
@@ -99,6 +100,9 @@ def test_colour_and_atomic_agree_and_parity_colouring(fem):
     ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_ATOMIC)
     _, _, v2 = ctx.ell_download(_lib.GF_F64)
     assert np.abs(v1 - v2).max() <= 1e-13 * np.abs(v1).max()
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+    _, _, v3 = ctx.ell_download(_lib.GF_F64)
+    assert np.abs(v1 - v3).max() <= 1e-13 * np.abs(v1).max()
     # library greedy colouring equals the oracle's (reference femColor rule)
     ctx2 = make_ctx(fem, mesh=m)
     nc2 = ctx2.color(None)
@@ -133,9 +137,11 @@ def test_distorted_element_fp32_uses_fp64_jacobian(fem, oracle):
     pts, _ = oracle.gauss(3, 3)
     dets = [np.linalg.det(oracle.dshape(mg.BRICK20, p) @ X[e]) for p in pts]
     assert min(dets) > 0 and max(dets) / min(dets) > 10
-    ctx.assemble(_lib.GF_F32, _lib.GF_SCATTER_COLOR)
-    rn, ci, v = ctx.ell_download(_lib.GF_F32)
-    assert row_rel_err(ell_to_dense(ro, co, vo), ell_to_dense(rn, ci, v.astype(np.float64))) <= TOL32
+    for scatter in SCATTERS:
+        ctx.assemble(_lib.GF_F32, scatter)
+        rn, ci, v = ctx.ell_download(_lib.GF_F32)
+        B = ell_to_dense(rn, ci, v.astype(np.float64))
+        assert row_rel_err(ell_to_dense(ro, co, vo), B) <= TOL32
 
 
 def test_single_element_and_isolated_node(fem, oracle):
@@ -143,13 +149,15 @@ def test_single_element_and_isolated_node(fem, oracle):
     coords = np.vstack([m.coords, [[5.0, 5.0]]])      # node 9 belongs to no element
     ctx = fem(0)
     ctx.mesh_create(mg.Q8, coords, m.conn, 3, 210e3, None, 0.3)
-    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_COLOR)
-    rn, ci, v = ctx.ell_download(_lib.GF_F64)
-    assert rn[-1] == 0 and rn[-2] == 0
     ro, co, vo = oracle.assemble(mg.Q8, 3, m.coords, m.conn, 210e3, 0.3)
     A = ell_to_dense(ro, co, vo)
-    B = ell_to_dense(rn, ci, v)[:16, :16]
-    assert row_rel_err(A, B) <= TOL64
+    for scatter in SCATTERS:
+        ctx.assemble(_lib.GF_F64, scatter)
+        rn, ci, v = ctx.ell_download(_lib.GF_F64)
+        assert rn[-1] == 0 and rn[-2] == 0
+        assert np.all(v[:, -2:] == 0)
+        B = ell_to_dense(rn, ci, v)[:16, :16]
+        assert row_rel_err(A, B) <= TOL64
 
 
 @pytest.mark.parametrize("bad", ["zero_id", "too_big", "repeat", "ngauss", "nu", "modulus"])
