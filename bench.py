@@ -188,6 +188,69 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# learned preconditioner vs plain Jacobi-PCG (multi-mesh Brick8 workload)
+# ---------------------------------------------------------------------------
+def learned_comparison(seed_base: int = 20260105, n_train: int = 6):
+    """Brick8 cubes with correlated log-normal E (sigma U(0.5, 2), correlation length
+    U(0.05, 0.3)) and nu U(0.2, 0.4), z = 0 clamped, pressure on z = 1.  The network is
+    trained on small seeded cubes (edge 12..20) and evaluated on held-out cubes (edge
+    24, 32, 40): time and iterations to reach FP64-oracle relative error 1e-6, for FP64
+    Jacobi-PCG, mixed-precision PCG and learned FCG (with its Jacobi fallback)."""
+    from gpufem_b200 import _lib
+    from gpufem_b200 import meshgen as mg
+    from gpufem_b200.fem import Context
+
+    def make(nn, seed):
+        m = mg.clamp_and_load(mg.structured(mg.BRICK8, (nn,) * 3, jitter=0.1, seed=seed))
+        rs = np.random.default_rng(seed)
+        m.E = mg.lognormal_correlated(m, rs.uniform(0.5, 2.0), rs.uniform(0.05, 0.3), seed)
+        m.nu = float(rs.uniform(0.2, 0.4))
+        return m
+
+    def setup(ctx, m):
+        ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+        ctx.set_supports(m.supports)
+        ctx.set_force(m.f)
+        ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+        ctx.convert_f64_to_f32()
+        ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
+
+    ctx = Context(0)
+    ctx.lp_init(3, seed=seed_base)
+    rng = np.random.default_rng(seed_base)
+    t0 = time.perf_counter()
+    losses = []
+    for epoch in range(2):
+        for k in range(n_train):
+            nn = int(rng.integers(12, 21))
+            m = make(nn, seed_base + 100 + k)
+            setup(ctx, m)
+            ctx.lp_collect(npairs=32, every=8, tol=1e-8)
+            losses.append(ctx.lp_train(steps=60, batch=8, lr=1e-3, seed=seed_base + epoch * 97 + k))
+    train_s = time.perf_counter() - t0
+    results = []
+    for nn, seed in ((24, seed_base + 901), (32, seed_base + 902), (40, seed_base + 903)):
+        m = make(nn, seed)
+        setup(ctx, m)
+        ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-12, max_iter=400000, raise_on_error=False)
+        ustar = ctx.solution()
+        nrm = np.linalg.norm(ustar)
+        row = {"edge": nn, "dofs": m.ndof}
+        for name, solver in (("pcg_fp64", _lib.GF_SOLVER_PCG), ("mixed_pcg", _lib.GF_SOLVER_MIXED_PCG),
+                             ("learned_fcg", _lib.GF_SOLVER_LEARNED_FCG)):
+            info = ctx.solve(solver, _lib.GF_F64, tol=1e-8, max_iter=400000, raise_on_error=False)
+            err = float(np.linalg.norm(ctx.solution() - ustar) / nrm)
+            row[name] = {"seconds": info.seconds, "iterations": info.iterations,
+                         "rel_err_vs_oracle": err, "status": info.status,
+                         **({"fallback": info.fallback} if name == "learned_fcg" else {})}
+        results.append(row)
+    ctx.close()
+    return {"train_meshes": 2 * n_train, "train_seconds": train_s,
+            "final_train_loss": losses[-1], "first_train_loss": losses[0],
+            "tol_rel_residual": 1e-8, "held_out": results}
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args):
@@ -342,6 +405,10 @@ def run_gpu_arm(args):
                                "rel_err_vs_oracle": float(np.linalg.norm(umix - ustar) / nrm)},
                  "tol": 1e-10}
 
+    learned = None
+    if not args.no_solve and rank == 0:
+        learned = learned_comparison()
+
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = reference_sample(cfg, steps=2, warmup=1)
@@ -373,6 +440,7 @@ def run_gpu_arm(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "solve": solve,
+            "learned": learned,
             "cpu_baseline": cpu_baseline,
         }
         print(json.dumps(line), flush=True)

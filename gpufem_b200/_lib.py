@@ -72,6 +72,14 @@ SIGNATURES = {
     "gf_solve": (I32, [P, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     "gf_get_solution": (I32, [P, P]),
     "gf_solution_view": (I32, [P, C.POINTER(P)]),
+    "gf_lp_num_params": (I64, [I32]),
+    "gf_lp_init": (I32, [P, I32, C.c_uint64]),
+    "gf_lp_get_weights": (I32, [P, P]),
+    "gf_lp_set_weights": (I32, [P, P]),
+    "gf_lp_collect": (I32, [P, I32, I32, D, I32]),
+    "gf_lp_train": (I32, [P, I32, I32, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "gf_lp_apply": (I32, [P, P, P]),
+    "gf_lp_loss_grad": (I32, [P, P, P, C.POINTER(C.c_float), P]),
     "gf_pcg_noalloc": (I32, [I32, I32, P, P, P, P, P, D, I32, P, C.POINTER(I32),
                              C.POINTER(D)]),
 }

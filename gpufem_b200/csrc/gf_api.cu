@@ -70,6 +70,7 @@ GF_API gf_status gf_destroy(gf_ctx* ctx) {
   if (!ctx) return GF_ERR_INVALID_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  gf_lp_free(ctx);
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
@@ -127,6 +128,7 @@ void gf_pattern_free(gf_ctx* ctx) {
   ctx->maxval = 0;
   gf_free(ctx->d_K64);
   gf_free(ctx->d_K32);
+  gf_sell_free(ctx);
   // n (the dof count) belongs to the mesh and survives; width and nnz do not
   ctx->has_pattern = ctx->has64 = ctx->has32 = false;
   ctx->W = 0;
@@ -206,6 +208,7 @@ GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
+  gf_lp_mesh_changed(ctx);
   gf_free(ctx->d_f);
   gf_free(ctx->d_fixed);
   ctx->h_supports.clear();
@@ -329,6 +332,7 @@ GF_API gf_status gf_ell_convert_f64_to_f32(gf_ctx* ctx) {
   k_f64_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(total, ctx->d_K64, ctx->d_K32);
   GF_LAUNCH_CHECK(ctx, "k_f64_to_f32");
   ctx->has32 = true;
+  ctx->kver32++;
   return GF_OK;
 }
 
@@ -421,6 +425,7 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
+  gf_lp_mesh_changed(ctx);
   gf_free(ctx->d_f);
   gf_free(ctx->d_fixed);
   ctx->h_supports.clear();
@@ -450,6 +455,8 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
   GF_LAUNCH_CHECK(ctx, "k_f64_to_f32");
   GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->has_pattern = ctx->has64 = ctx->has32 = true;
+  ctx->kver64++;
+  ctx->kver32++;
   return GF_OK;
 }
 

@@ -273,7 +273,7 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   ctx->last_seconds = ms * 1e-3;
-  if (dtype == GF_F64) ctx->has64 = true; else ctx->has32 = true;
+  if (dtype == GF_F64) { ctx->has64 = true; ctx->kver64++; } else { ctx->has32 = true; ctx->kver32++; }
   ctx->bc_mode_applied = -1;
   return GF_OK;
 }

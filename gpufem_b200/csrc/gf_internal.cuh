@@ -132,6 +132,7 @@ inline void gf_gauss_rule(int dim, int ng1, std::vector<R>& pts, std::vector<R>&
 // Context
 // ---------------------------------------------------------------------------
 struct SolveScalars;  // device-side solver scalars (gf_solve.cu)
+struct LpState;       // learned preconditioner (gf_learned.cu)
 
 struct gf_ctx {
   int device = 0;
@@ -185,6 +186,19 @@ struct gf_ctx {
   bool has64 = false, has32 = false;
   double* d_K64 = nullptr;
   float* d_K32 = nullptr;
+  int64_t kver64 = 0, kver32 = 0;  // bumped whenever the values change
+
+  // sliced-ELL copy for the solver's SpMVs (gf_sell.cu)
+  bool sell_ready = false;
+  int sell_nslice = 0, sell_nslots = 0;
+  int64_t sell_total = 0;
+  int64_t sell_ver64 = -1, sell_ver32 = -1;
+  int32_t* d_sell_perm = nullptr;  // [nslots] row of each slot, -1 = padding
+  int64_t* d_sell_off = nullptr;   // [nslice + 1]
+  int32_t* d_sell_w = nullptr;     // [nslice]
+  int32_t* d_sell_col = nullptr;   // [total]
+  double* d_sell_v64 = nullptr;
+  float* d_sell_v32 = nullptr;
 
   // loads / constraints
   double* d_f = nullptr;
@@ -201,6 +215,10 @@ struct gf_ctx {
   SolveScalars* d_scal = nullptr;
   void* h_pinned = nullptr;  // pinned scalars readback
   double* d_red = nullptr;   // reduction scratch
+  void* d_fcg = nullptr;     // flexible-CG scalars
+
+  // learned preconditioner
+  LpState* lp = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -259,3 +277,19 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
 void gf_solver_free(gf_ctx* ctx);
 void gf_mesh_free(gf_ctx* ctx);
 void gf_pattern_free(gf_ctx* ctx);
+
+// sliced-ELL copy (gf_sell.cu)
+gf_status gf_sell_prepare(gf_ctx* ctx, int dtype);
+void gf_sell_free(gf_ctx* ctx);
+
+// learned preconditioner (gf_learned.cu)
+void gf_lp_free(gf_ctx* ctx);
+void gf_lp_mesh_changed(gf_ctx* ctx);
+gf_status gf_lp_prepare(gf_ctx* ctx);
+bool gf_lp_ready(const gf_ctx* ctx);
+// z = M(r): FP64 residual in, FP64 preconditioned vector out (r32: n floats of scratch)
+gf_status gf_lp_apply64(gf_ctx* ctx, const double* r64, float* r32_scratch, double* z);
+// Jacobi-PCG on the FP64 matrix recording (float(r_k), float(ustar - x_k)) every
+// `every` iterations into r_out / e_out (npairs slots of n floats); *recorded set.
+gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every, double tol,
+                        int maxit, float* r_out, float* e_out, int* recorded);

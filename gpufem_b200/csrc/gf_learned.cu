@@ -1,0 +1,754 @@
+// Learned preconditioner: a message-passing network over the node graph of K,
+// trained on the GPU by the kernels below, used inside flexible CG.
+// No counterpart in the reference (its CG is unpreconditioned,
+// src/SPRmatrix/SPRmatrix.cc:405-480).
+//
+// M(r) = D^-1 r + c * y(r),   rho = D^-1 r (Jacobi), c = rms(rho),
+// y = network(features) with per-node features [rho_a / c (dim), log(d_a / mean d) (dim)]:
+//   h0 = relu(W0 f + b0)                                   (2 dim -> 64)
+//   h_{l+1} = relu(Ws_l h_l + Wn_l mean_{b in N(a)} h_l[b] + b_l),  l = 0, 1, 2   (64 -> 64)
+//   y = Wout h3 + bout                                     (64 -> dim)
+// N(a) = nodes sharing an element with a (the ELL node adjacency, self included).
+// Weights are kept in FP32 (Adam master copy) and used as BF16; activations and
+// accumulation are FP32.  Wout starts at zero, so an untrained network is Jacobi.
+// The output scale c makes M(s r) = s M(r).
+//
+// Training pairs (r_k, e_k = u* - x_k) come from Jacobi-PCG runs on the context's
+// matrix (u* = a tighter PCG solution).  Loss per pair, with t = e - rho:
+//   L = sum_dofs d (c y - t)^2 / sum_dofs d e^2        (D-weighted relative error)
+#include <cuda_bf16.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "gf_internal.cuh"
+
+namespace {
+
+constexpr int H = 64;       // hidden width
+constexpr int kLT = 256;    // threads per block
+constexpr int kLayers = 3;  // message-passing layers
+
+struct LpOffsets {
+  int64_t W0, b0, Ws[kLayers], Wn[kLayers], bl[kLayers], Wout, bout, total;
+};
+
+LpOffsets lp_offsets(int dim) {
+  LpOffsets o{};
+  const int F = 2 * dim;
+  int64_t p = 0;
+  o.W0 = p; p += (int64_t)H * F;
+  o.b0 = p; p += H;
+  for (int l = 0; l < kLayers; ++l) {
+    o.Ws[l] = p; p += (int64_t)H * H;
+    o.Wn[l] = p; p += (int64_t)H * H;
+    o.bl[l] = p; p += H;
+  }
+  o.Wout = p; p += (int64_t)dim * H;
+  o.bout = p; p += dim;
+  o.total = p;
+  return o;
+}
+
+struct LpScalars {
+  double sumsq;   // sum rho^2
+  double c;       // rms(rho)
+  double loss;    // accumulated loss
+  double dsum;    // sum d e^2 (loss normaliser)
+};
+
+}  // namespace
+
+// Per-context learned-preconditioner state.
+struct LpState {
+  int dim = 0, N = 0, n = 0;
+  LpOffsets off{};
+  float* w = nullptr;       // FP32 master weights
+  __nv_bfloat16* wb = nullptr;  // BF16 copy used by the network
+  float* g = nullptr;       // gradients
+  float* m = nullptr;       // Adam moments
+  float* v = nullptr;
+  int64_t adam_t = 0;
+  // node graph
+  float* deg_inv = nullptr;  // 1 / |N(a)|
+  // per-dof
+  float* dinv = nullptr;     // 1 / K_rr (FP32)
+  double* dinv64 = nullptr;
+  float* dlog = nullptr;     // log(d / mean d)
+  float* dvec = nullptr;     // d (loss weight)
+  // activations [N][H] (pre-activations kept for the ReLU masks)
+  float* feat = nullptr;     // [N][2 dim]
+  float* pre[kLayers + 1] = {};
+  float* h[kLayers + 1] = {};
+  float* agg[kLayers] = {};
+  float* y = nullptr;        // [N][dim] == n
+  float* dy = nullptr;       // [n] loss gradient w.r.t. y
+  float* rho = nullptr;      // [n]
+  float* dh = nullptr;       // [N][H]
+  float* dpre = nullptr;     // [N][H]
+  float* tmp = nullptr;      // [N][H]
+  LpScalars* sc = nullptr;
+  // training pairs
+  int npairs = 0;
+  float* pr = nullptr;       // [npairs][n]
+  float* pe = nullptr;       // [npairs][n]
+  bool ready = false;        // diag / graph set up for the current matrix
+};
+
+namespace {
+
+template <typename T>
+gf_status lp_alloc(gf_ctx* ctx, T** p, size_t count) {
+  return gf_alloc(ctx, p, count);
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__device__ inline double lp_block_sum(double x, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = x;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  return s;
+}
+
+// rho = dinv * r, sum rho^2
+__global__ void k_lp_prep(int n, const float* __restrict__ r, const float* __restrict__ dinv,
+                          float* __restrict__ rho, LpScalars* sc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  double s = 0.0;
+  if (i < n) {
+    const float v = r[i] * dinv[i];
+    rho[i] = v;
+    s = (double)v * v;
+  }
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->sumsq, s);
+}
+
+__global__ void k_lp_features(int N, int dim, const float* __restrict__ rho,
+                              const float* __restrict__ dlog, float* __restrict__ feat,
+                              LpScalars* sc) {
+  const int a = blockIdx.x * kLT + threadIdx.x;
+  const double n = (double)N * dim;
+  const double c = sqrt(sc->sumsq / n) + 1e-30;
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->c = c;
+  if (a >= N) return;
+  const float ic = (float)(1.0 / c);
+  for (int k = 0; k < dim; ++k) {
+    feat[(int64_t)a * 2 * dim + k] = rho[a * dim + k] * ic;
+    feat[(int64_t)a * 2 * dim + dim + k] = dlog[a * dim + k];
+  }
+}
+
+// out[a][o] = act(b[o] + sum_k W1[o][k] A[a][k] (+ sum_k W2[o][k] B[a][k]))
+// Thread per (node, output channel); weights staged in shared memory as FP32.
+template <int CIN, int COUT, bool TWO>
+__global__ void __launch_bounds__(kLT)
+k_lp_dense(int N, const float* __restrict__ A, const float* __restrict__ B,
+           const __nv_bfloat16* __restrict__ W1, const __nv_bfloat16* __restrict__ W2,
+           const __nv_bfloat16* __restrict__ bias, float* __restrict__ pre,
+           float* __restrict__ out, int relu) {
+  __shared__ float sW1[COUT][CIN + 1];
+  __shared__ float sW2[TWO ? COUT : 1][TWO ? CIN + 1 : 1];
+  __shared__ float sb[COUT];
+  for (int k = threadIdx.x; k < COUT * CIN; k += kLT) {
+    sW1[k / CIN][k % CIN] = __bfloat162float(W1[k]);
+    if (TWO) sW2[k / CIN][k % CIN] = __bfloat162float(W2[k]);
+  }
+  for (int k = threadIdx.x; k < COUT; k += kLT) sb[k] = __bfloat162float(bias[k]);
+  __syncthreads();
+  const int64_t total = (int64_t)N * COUT;
+  for (int64_t t = blockIdx.x * (int64_t)kLT + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * kLT) {
+    const int a = (int)(t / COUT), o = (int)(t % COUT);
+    const float* Aa = A + (int64_t)a * CIN;
+    float acc = sb[o];
+#pragma unroll 16
+    for (int k = 0; k < CIN; ++k) acc += sW1[o][k] * __ldg(Aa + k);
+    if (TWO) {
+      const float* Ba = B + (int64_t)a * CIN;
+#pragma unroll 16
+      for (int k = 0; k < CIN; ++k) acc += sW2[o][k] * __ldg(Ba + k);
+    }
+    if (pre) pre[t] = acc;
+    out[t] = (relu && acc < 0.f) ? 0.f : acc;
+  }
+}
+
+// out[a][k] (+)= sum_o W[o][k] G[a][o]   (transpose of the dense layer, data gradient)
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kLT)
+k_lp_dense_t(int N, const float* __restrict__ G, const __nv_bfloat16* __restrict__ W,
+             float* __restrict__ out, int accumulate) {
+  __shared__ float sW[COUT][CIN + 1];
+  for (int k = threadIdx.x; k < COUT * CIN; k += kLT) sW[k / CIN][k % CIN] = __bfloat162float(W[k]);
+  __syncthreads();
+  const int64_t total = (int64_t)N * CIN;
+  for (int64_t t = blockIdx.x * (int64_t)kLT + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * kLT) {
+    const int a = (int)(t / CIN), k = (int)(t % CIN);
+    const float* Ga = G + (int64_t)a * COUT;
+    float acc = 0.f;
+#pragma unroll 16
+    for (int o = 0; o < COUT; ++o) acc += sW[o][k] * __ldg(Ga + o);
+    out[t] = accumulate ? out[t] + acc : acc;
+  }
+}
+
+// Weight gradient: dW[o][k] += sum_a G[a][o] A[a][k]; db[o] += sum_a G[a][o].
+// Block handles a chunk of nodes staged in shared memory.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kLT)
+k_lp_wgrad(int N, const float* __restrict__ G, const float* __restrict__ A,
+           float* __restrict__ dW, float* __restrict__ db) {
+  constexpr int CHUNK = 32;
+  __shared__ float sG[CHUNK][COUT + 1];
+  __shared__ float sA[CHUNK][CIN + 1];
+  constexpr int PAIRS = COUT * CIN;
+  constexpr int PER = (PAIRS + kLT - 1) / kLT;
+  float acc[PER];
+  float accb = 0.f;
+#pragma unroll
+  for (int k = 0; k < PER; ++k) acc[k] = 0.f;
+  for (int a0 = blockIdx.x * CHUNK; a0 < N; a0 += gridDim.x * CHUNK) {
+    const int na = min(CHUNK, N - a0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < CHUNK * COUT; k += kLT) {
+      const int r = k / COUT, c = k % COUT;
+      sG[r][c] = r < na ? G[(int64_t)(a0 + r) * COUT + c] : 0.f;
+    }
+    for (int k = threadIdx.x; k < CHUNK * CIN; k += kLT) {
+      const int r = k / CIN, c = k % CIN;
+      sA[r][c] = r < na ? A[(int64_t)(a0 + r) * CIN + c] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int pidx = threadIdx.x + k * kLT;
+      if (pidx < PAIRS) {
+        const int o = pidx / CIN, c = pidx % CIN;
+        float s = 0.f;
+#pragma unroll 8
+        for (int r = 0; r < CHUNK; ++r) s += sG[r][o] * sA[r][c];
+        acc[k] += s;
+      }
+    }
+    if (threadIdx.x < COUT) {
+      float s = 0.f;
+      for (int r = 0; r < CHUNK; ++r) s += sG[r][threadIdx.x];
+      accb += s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int pidx = threadIdx.x + k * kLT;
+    if (pidx < PAIRS) atomicAdd(&dW[pidx], acc[k]);
+  }
+  if (threadIdx.x < COUT) atomicAdd(&db[threadIdx.x], accb);
+}
+
+// forward:  out[a] = deg_inv[a] * sum_{b in N(a)} h[b]
+// backward: out[b] = sum_{a in N(b)} deg_inv[a] * g[a]   (the node graph is symmetric)
+// Thread per (node, channel); channel fastest so a warp reads 128 contiguous bytes.
+__global__ void __launch_bounds__(kLT)
+k_lp_aggregate(int N, const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
+               const float* __restrict__ deg_inv, const float* __restrict__ h,
+               float* __restrict__ out, int backward) {
+  const int64_t total = (int64_t)N * H;
+  for (int64_t t = blockIdx.x * (int64_t)kLT + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * kLT) {
+    const int a = (int)(t / H), c = (int)(t % H);
+    float s = 0.f;
+    const int q1 = adj_off[a + 1];
+    for (int q = adj_off[a]; q < q1; ++q) {
+      const int b = __ldg(adj + q);
+      const float v = __ldg(h + (int64_t)b * H + c);
+      s += backward ? v * __ldg(deg_inv + b) : v;
+    }
+    out[t] = backward ? s : s * deg_inv[a];
+  }
+}
+
+__global__ void k_lp_relu_grad(int64_t total, const float* __restrict__ dh,
+                               const float* __restrict__ pre, float* __restrict__ dpre) {
+  for (int64_t t = blockIdx.x * (int64_t)kLT + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * kLT)
+    dpre[t] = pre[t] > 0.f ? dh[t] : 0.f;
+}
+
+// z = rho + c y, in FP32 or FP64
+template <typename V>
+__global__ void k_lp_output(int n, const float* __restrict__ rho, const float* __restrict__ y,
+                            const LpScalars* __restrict__ sc, V* __restrict__ z) {
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  if (i < n) z[i] = (V)rho[i] + (V)sc->c * (V)y[i];
+}
+
+// Loss for one pair: t = e - rho; L = sum d (c y - t)^2 / sum d e^2; dy = dL/dy
+__global__ void k_lp_loss_sums(int n, const float* __restrict__ e, const float* __restrict__ d,
+                               LpScalars* sc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  double s = 0.0;
+  if (i < n) s = (double)d[i] * e[i] * e[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->dsum, s);
+}
+
+__global__ void k_lp_loss_grad(int n, const float* __restrict__ e, const float* __restrict__ rho,
+                               const float* __restrict__ y, const float* __restrict__ d,
+                               float* __restrict__ dy, LpScalars* sc, double* loss_acc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  const double c = sc->c, S = sc->dsum > 0 ? sc->dsum : 1.0;
+  double l = 0.0;
+  if (i < n) {
+    const double diff = c * y[i] - ((double)e[i] - rho[i]);
+    l = d[i] * diff * diff / S;
+    dy[i] = (float)(2.0 * d[i] * c * diff / S);
+  }
+  l = lp_block_sum(l, sh);
+  if (threadIdx.x == 0) atomicAdd(loss_acc, l);
+}
+
+__global__ void k_lp_adam(int64_t P, float* __restrict__ w, const float* __restrict__ g,
+                          float* __restrict__ m, float* __restrict__ v,
+                          __nv_bfloat16* __restrict__ wb, float lr, float b1, float b2,
+                          float eps, float c1, float c2, float gscale) {
+  const int64_t i = blockIdx.x * (int64_t)kLT + threadIdx.x;
+  if (i >= P) return;
+  const float gi = g[i] * gscale;
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  wb[i] = __float2bfloat16(wi);
+}
+
+__global__ void k_lp_to_bf16(int64_t P, const float* __restrict__ w,
+                             __nv_bfloat16* __restrict__ wb) {
+  const int64_t i = blockIdx.x * (int64_t)kLT + threadIdx.x;
+  if (i < P) wb[i] = __float2bfloat16(w[i]);
+}
+
+__global__ void k_lp_degree(int N, const int32_t* __restrict__ adj_off, float* __restrict__ deg_inv) {
+  const int a = blockIdx.x * kLT + threadIdx.x;
+  if (a < N) deg_inv[a] = 1.f / (float)max(1, adj_off[a + 1] - adj_off[a]);
+}
+
+// diagonal of K: d, 1/d (FP32 and FP64) and log(d / mean d) (mean taken on the host)
+template <typename TK>
+__global__ void k_lp_diag(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
+                          const TK* __restrict__ val, float* __restrict__ d,
+                          float* __restrict__ dinv, double* __restrict__ dinv64) {
+  const int row = blockIdx.x * kLT + threadIdx.x;
+  if (row >= n) return;
+  double dv = 0.0;
+  for (int s = 0; s < rownnz[row]; ++s) {
+    const int64_t o = (int64_t)s * n + row;
+    if (col[o] == row) { dv = (double)val[o]; break; }
+  }
+  if (!(dv > 0.0)) dv = 1.0;
+  d[row] = (float)dv;
+  dinv[row] = (float)(1.0 / dv);
+  dinv64[row] = 1.0 / dv;
+}
+
+__global__ void k_lp_dlog(int n, const float* __restrict__ d, double logmean, float* __restrict__ dlog) {
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  if (i < n) dlog[i] = (float)(log((double)d[i]) - logmean);
+}
+
+__global__ void k_lp_cast_f32(int n, const double* __restrict__ a, float* __restrict__ b) {
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+inline int lp_grid(int64_t work) {
+  int64_t b = (work + kLT - 1) / kLT;
+  return (int)std::min<int64_t>(std::max<int64_t>(b, 1), 148 * 16);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static void lp_free_buffers(LpState* s) {
+  auto f = [](auto*& p) { if (p) { cudaFree(p); p = nullptr; } };
+  f(s->deg_inv); f(s->dinv); f(s->dinv64); f(s->dlog); f(s->dvec); f(s->feat);
+  for (int l = 0; l <= kLayers; ++l) { f(s->pre[l]); f(s->h[l]); }
+  for (int l = 0; l < kLayers; ++l) f(s->agg[l]);
+  f(s->y); f(s->dy); f(s->rho); f(s->dh); f(s->dpre); f(s->tmp);
+  f(s->pr); f(s->pe);
+  s->npairs = 0;
+  s->ready = false;
+}
+
+void gf_lp_free(gf_ctx* ctx) {
+  LpState* s = ctx->lp;
+  if (!s) return;
+  lp_free_buffers(s);
+  auto f = [](auto*& p) { if (p) { cudaFree(p); p = nullptr; } };
+  f(s->w); f(s->wb); f(s->g); f(s->m); f(s->v); f(s->sc);
+  delete s;
+  ctx->lp = nullptr;
+}
+
+// Allocates the per-mesh buffers and the diagonal / graph data for the current matrix.
+gf_status gf_lp_prepare(gf_ctx* ctx) {
+  LpState* s = ctx->lp;
+  if (!s) return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner not initialised");
+  if (!ctx->has_mesh || !ctx->d_adj_off || !(ctx->has64 || ctx->has32))
+    return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner needs an assembled mesh");
+  if (s->dim != ctx->dim)
+    return gf_fail(ctx, GF_ERR_STATE, "weights are for dim %d, mesh has dim %d", s->dim, ctx->dim);
+  const int N = ctx->nnodes, n = ctx->n, dim = ctx->dim;
+  if (s->ready && s->N == N && s->n == n) {
+    // refresh the diagonal (the matrix may have changed)
+  } else {
+    lp_free_buffers(s);
+    s->N = N;
+    s->n = n;
+    gf_status st;
+#define LPA(p, cnt) if ((st = lp_alloc(ctx, &(p), (size_t)(cnt))) != GF_OK) return st
+    LPA(s->deg_inv, N); LPA(s->dinv, n); LPA(s->dinv64, n); LPA(s->dlog, n); LPA(s->dvec, n);
+    LPA(s->feat, (size_t)N * 2 * dim);
+    for (int l = 0; l <= kLayers; ++l) { LPA(s->pre[l], (size_t)N * H); LPA(s->h[l], (size_t)N * H); }
+    for (int l = 0; l < kLayers; ++l) LPA(s->agg[l], (size_t)N * H);
+    LPA(s->y, n); LPA(s->dy, n); LPA(s->rho, n); LPA(s->dh, (size_t)N * H); LPA(s->dpre, (size_t)N * H);
+    LPA(s->tmp, (size_t)N * H);
+#undef LPA
+  }
+  cudaStream_t st_ = ctx->stream;
+  k_lp_degree<<<gf_blocks(N, kLT), kLT, 0, st_>>>(N, ctx->d_adj_off, s->deg_inv);
+  ctx->launches++;
+  if (ctx->has64)
+    k_lp_diag<double><<<gf_blocks(n, kLT), kLT, 0, st_>>>(n, ctx->d_rownnz, ctx->d_colidx,
+                                                          ctx->d_K64, s->dvec, s->dinv, s->dinv64);
+  else
+    k_lp_diag<float><<<gf_blocks(n, kLT), kLT, 0, st_>>>(n, ctx->d_rownnz, ctx->d_colidx,
+                                                         ctx->d_K32, s->dvec, s->dinv, s->dinv64);
+  ctx->launches++;
+  std::vector<float> d(n);
+  GF_CUDA(ctx, cudaMemcpyAsync(d.data(), s->dvec, sizeof(float) * n, cudaMemcpyDeviceToHost, st_));
+  GF_CUDA(ctx, cudaStreamSynchronize(st_));
+  double lm = 0.0;
+  for (float x : d) lm += std::log((double)x);
+  lm /= n;
+  k_lp_dlog<<<gf_blocks(n, kLT), kLT, 0, st_>>>(n, s->dvec, lm, s->dlog);
+  ctx->launches++;
+  GF_CUDA(ctx, cudaGetLastError());
+  s->ready = true;
+  return GF_OK;
+}
+
+// Network forward on FP32 residual r (device, n); fills rho, y and the activations.
+static void lp_forward(gf_ctx* ctx, const float* r) {
+  LpState* s = ctx->lp;
+  cudaStream_t st = ctx->stream;
+  const int N = s->N, n = s->n, dim = s->dim;
+  const LpOffsets& o = s->off;
+  cudaMemsetAsync(&s->sc->sumsq, 0, sizeof(double), st);
+  k_lp_prep<<<gf_blocks(n, kLT), kLT, 0, st>>>(n, r, s->dinv, s->rho, s->sc);
+  k_lp_features<<<gf_blocks(N, kLT), kLT, 0, st>>>(N, dim, s->rho, s->dlog, s->feat, s->sc);
+  const int gH = lp_grid((int64_t)N * H);
+  if (dim == 2)
+    k_lp_dense<4, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
+                                                s->wb + o.b0, s->pre[0], s->h[0], 1);
+  else
+    k_lp_dense<6, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
+                                                s->wb + o.b0, s->pre[0], s->h[0], 1);
+  for (int l = 0; l < kLayers; ++l) {
+    k_lp_aggregate<<<gH, kLT, 0, st>>>(N, ctx->d_adj_off, ctx->d_adj, s->deg_inv, s->h[l],
+                                       s->agg[l], 0);
+    k_lp_dense<H, H, true><<<gH, kLT, 0, st>>>(N, s->h[l], s->agg[l], s->wb + o.Ws[l],
+                                               s->wb + o.Wn[l], s->wb + o.bl[l], s->pre[l + 1],
+                                               s->h[l + 1], 1);
+  }
+  const int gy = lp_grid((int64_t)N * dim);
+  if (dim == 2)
+    k_lp_dense<H, 2, false><<<gy, kLT, 0, st>>>(N, s->h[kLayers], nullptr, s->wb + o.Wout,
+                                                nullptr, s->wb + o.bout, nullptr, s->y, 0);
+  else
+    k_lp_dense<H, 3, false><<<gy, kLT, 0, st>>>(N, s->h[kLayers], nullptr, s->wb + o.Wout,
+                                                nullptr, s->wb + o.bout, nullptr, s->y, 0);
+  ctx->launches += 5 + 2 * kLayers;
+}
+
+// Backward from dy ([N][dim] == n floats) into s->g (accumulated).
+static void lp_backward(gf_ctx* ctx, const float* dy) {
+  LpState* s = ctx->lp;
+  cudaStream_t st = ctx->stream;
+  const int N = s->N, dim = s->dim;
+  const LpOffsets& o = s->off;
+  const int gH = lp_grid((int64_t)N * H);
+  const int gw = std::min(148 * 4, (N + 31) / 32);
+  // output layer
+  if (dim == 2) {
+    k_lp_wgrad<H, 2><<<gw, kLT, 0, st>>>(N, dy, s->h[kLayers], s->g + o.Wout, s->g + o.bout);
+    k_lp_dense_t<H, 2><<<gH, kLT, 0, st>>>(N, dy, s->wb + o.Wout, s->dh, 0);
+  } else {
+    k_lp_wgrad<H, 3><<<gw, kLT, 0, st>>>(N, dy, s->h[kLayers], s->g + o.Wout, s->g + o.bout);
+    k_lp_dense_t<H, 3><<<gH, kLT, 0, st>>>(N, dy, s->wb + o.Wout, s->dh, 0);
+  }
+  for (int l = kLayers - 1; l >= 0; --l) {
+    k_lp_relu_grad<<<gH, kLT, 0, st>>>((int64_t)N * H, s->dh, s->pre[l + 1], s->dpre);
+    k_lp_wgrad<H, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->h[l], s->g + o.Ws[l], s->g + o.bl[l]);
+    // the bias gradient was added by the call above; the Wn call adds into a scratch bias
+    k_lp_wgrad<H, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->agg[l], s->g + o.Wn[l],
+                                         s->g + o.total);  // scratch slot past the params
+    // dh_l = Ws^T dpre + aggregate^T(Wn^T dpre)
+    k_lp_dense_t<H, H><<<gH, kLT, 0, st>>>(N, s->dpre, s->wb + o.Wn[l], s->tmp, 0);
+    k_lp_aggregate<<<gH, kLT, 0, st>>>(N, ctx->d_adj_off, ctx->d_adj, s->deg_inv, s->tmp,
+                                       s->dh, 1);
+    k_lp_dense_t<H, H><<<gH, kLT, 0, st>>>(N, s->dpre, s->wb + o.Ws[l], s->dh, 1);
+  }
+  k_lp_relu_grad<<<gH, kLT, 0, st>>>((int64_t)N * H, s->dh, s->pre[0], s->dpre);
+  if (dim == 2)
+    k_lp_wgrad<4, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
+  else
+    k_lp_wgrad<6, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
+  ctx->launches += 3 + 6 * kLayers + 2;
+}
+
+// Preconditioner application for the solver: z = M(r) in FP64 from an FP64 residual.
+gf_status gf_lp_apply64(gf_ctx* ctx, const double* r64, float* r32_scratch, double* z) {
+  LpState* s = ctx->lp;
+  const int n = s->n;
+  k_lp_cast_f32<<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(n, r64, r32_scratch);
+  lp_forward(ctx, r32_scratch);
+  k_lp_output<double><<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(n, s->rho, s->y, s->sc, z);
+  ctx->launches += 2;
+  return GF_OK;
+}
+
+bool gf_lp_ready(const gf_ctx* ctx) { return ctx->lp && ctx->lp->ready; }
+
+// A new mesh or matrix invalidates the collected pairs and the diagonal; the
+// weights stay (they are mesh-independent).
+void gf_lp_mesh_changed(gf_ctx* ctx) {
+  if (!ctx->lp) return;
+  ctx->lp->ready = false;
+  if (ctx->lp->pr) { cudaFree(ctx->lp->pr); ctx->lp->pr = nullptr; }
+  if (ctx->lp->pe) { cudaFree(ctx->lp->pe); ctx->lp->pe = nullptr; }
+  ctx->lp->npairs = 0;
+}
+
+gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info);
+
+gf_status gf_lp_collect_impl(gf_ctx* ctx, int npairs, int every, double tol, int maxit) {
+  LpState* s = ctx->lp;
+  if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "pair collection needs the FP64 matrix");
+  const int n = s->n;
+  // reference solution u* (tighter than the recorded run)
+  gf_solve_opts o{};
+  o.solver = GF_SOLVER_PCG;
+  o.matrix = GF_F64;
+  o.tol = tol * 1e-3;
+  o.max_iter = maxit * 4;
+  gf_solve_info info{};
+  gf_status st = gf_solve_run(ctx, &o, &info);
+  if (st != GF_OK && st != GF_ERR_NOT_CONVERGED) return st;
+  double* ustar = nullptr;
+  if ((st = gf_alloc(ctx, &ustar, (size_t)n)) != GF_OK) return st;
+  cudaMemcpyAsync(ustar, ctx->d_u, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream);
+  if (s->pr) cudaFree(s->pr);
+  if (s->pe) cudaFree(s->pe);
+  s->pr = s->pe = nullptr;
+  s->npairs = 0;
+  if ((st = gf_alloc(ctx, &s->pr, (size_t)npairs * n)) != GF_OK) { cudaFree(ustar); return st; }
+  if ((st = gf_alloc(ctx, &s->pe, (size_t)npairs * n)) != GF_OK) { cudaFree(ustar); return st; }
+  int got = 0;
+  st = gf_pcg_record(ctx, ustar, npairs, every, tol, maxit, s->pr, s->pe, &got);
+  cudaFree(ustar);
+  if (st != GF_OK && st != GF_ERR_NOT_CONVERGED) return st;
+  s->npairs = got;
+  if (got == 0) return gf_fail(ctx, GF_ERR_STATE, "no pairs recorded");
+  return GF_OK;
+}
+
+// Pairs collection: Jacobi-PCG on the FP64 matrix and force, recording (r, x) at
+// chunk boundaries; e = u* - x with u* from a tighter solve.
+gf_status gf_lp_collect_impl(gf_ctx* ctx, int npairs, int every, double tol, int maxit);
+
+extern "C" {
+
+GF_API int64_t gf_lp_num_params(int32_t dim) {
+  if (dim != 2 && dim != 3) return 0;
+  return lp_offsets(dim).total;
+}
+
+GF_API gf_status gf_lp_init(gf_ctx* ctx, int32_t dim, uint64_t seed) {
+  if (!ctx) return GF_ERR_INVALID_ARG;
+  if (dim != 2 && dim != 3) return gf_fail(ctx, GF_ERR_INVALID_ARG, "dim must be 2 or 3");
+  cudaSetDevice(ctx->device);
+  gf_lp_free(ctx);
+  LpState* s = new LpState();
+  ctx->lp = s;
+  s->dim = dim;
+  s->off = lp_offsets(dim);
+  const int64_t P = s->off.total;
+  gf_status st;
+  if ((st = lp_alloc(ctx, &s->w, (size_t)P)) != GF_OK) return st;
+  if ((st = lp_alloc(ctx, &s->wb, (size_t)P)) != GF_OK) return st;
+  if ((st = lp_alloc(ctx, &s->g, (size_t)P + H)) != GF_OK) return st;
+  if ((st = lp_alloc(ctx, &s->m, (size_t)P)) != GF_OK) return st;
+  if ((st = lp_alloc(ctx, &s->v, (size_t)P)) != GF_OK) return st;
+  if ((st = lp_alloc(ctx, &s->sc, 1)) != GF_OK) return st;
+  // He-style init for hidden layers; output layer zero (untrained = Jacobi)
+  std::vector<float> w(P, 0.f);
+  std::mt19937_64 rng(seed);
+  std::normal_distribution<float> nd(0.f, 1.f);
+  const LpOffsets& o = s->off;
+  const int F = 2 * dim;
+  for (int64_t k = 0; k < (int64_t)H * F; ++k) w[o.W0 + k] = nd(rng) * std::sqrt(2.f / F);
+  for (int l = 0; l < kLayers; ++l)
+    for (int64_t k = 0; k < (int64_t)H * H; ++k) {
+      w[o.Ws[l] + k] = nd(rng) * std::sqrt(1.f / H);
+      w[o.Wn[l] + k] = nd(rng) * std::sqrt(1.f / H);
+    }
+  GF_CUDA(ctx, cudaMemcpy(s->w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice));
+  GF_CUDA(ctx, cudaMemset(s->m, 0, sizeof(float) * P));
+  GF_CUDA(ctx, cudaMemset(s->v, 0, sizeof(float) * P));
+  k_lp_to_bf16<<<gf_blocks(P, kLT), kLT, 0, ctx->stream>>>(P, s->w, s->wb);
+  GF_LAUNCH_CHECK(ctx, "k_lp_to_bf16");
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  s->adam_t = 0;
+  return GF_OK;
+}
+
+GF_API gf_status gf_lp_get_weights(gf_ctx* ctx, float* w) {
+  if (!ctx || !w) return GF_ERR_INVALID_ARG;
+  if (!ctx->lp) return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner not initialised");
+  cudaSetDevice(ctx->device);
+  GF_CUDA(ctx, cudaMemcpy(w, ctx->lp->w, sizeof(float) * ctx->lp->off.total, cudaMemcpyDeviceToHost));
+  return GF_OK;
+}
+
+GF_API gf_status gf_lp_set_weights(gf_ctx* ctx, const float* w) {
+  if (!ctx || !w) return GF_ERR_INVALID_ARG;
+  if (!ctx->lp) return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner not initialised");
+  cudaSetDevice(ctx->device);
+  LpState* s = ctx->lp;
+  const int64_t P = s->off.total;
+  for (int64_t k = 0; k < P; ++k)
+    if (!std::isfinite(w[k])) return gf_fail(ctx, GF_ERR_INVALID_ARG, "non-finite weight %lld", (long long)k);
+  GF_CUDA(ctx, cudaMemcpy(s->w, w, sizeof(float) * P, cudaMemcpyHostToDevice));
+  k_lp_to_bf16<<<gf_blocks(P, kLT), kLT, 0, ctx->stream>>>(P, s->w, s->wb);
+  GF_LAUNCH_CHECK(ctx, "k_lp_to_bf16");
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GF_OK;
+}
+
+// z = M(r) for FP32 device vectors of length n (the context's dof count).
+GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z) {
+  if (!ctx || !r || !z) return GF_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gf_status st = gf_lp_prepare(ctx);
+  if (st != GF_OK) return st;
+  LpState* s = ctx->lp;
+  lp_forward(ctx, r);
+  k_lp_output<float><<<gf_blocks(s->n, kLT), kLT, 0, ctx->stream>>>(s->n, s->rho, s->y, s->sc, z);
+  GF_LAUNCH_CHECK(ctx, "k_lp_output");
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GF_OK;
+}
+
+// Loss and gradient for one (r, e) pair of FP32 device vectors; the gradient of
+// the parameters (same layout as the weights) is copied to `grad` (host, may be
+// NULL) and the loss returned in *loss.  Does not update the weights.
+GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, float* loss,
+                                 float* grad) {
+  if (!ctx || !r || !e) return GF_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gf_status st = gf_lp_prepare(ctx);
+  if (st != GF_OK) return st;
+  LpState* s = ctx->lp;
+  const int64_t P = s->off.total;
+  cudaStream_t cs = ctx->stream;
+  GF_CUDA(ctx, cudaMemsetAsync(s->g, 0, sizeof(float) * (P + H), cs));
+  GF_CUDA(ctx, cudaMemsetAsync(&s->sc->loss, 0, 2 * sizeof(double), cs));  // loss, dsum
+  lp_forward(ctx, r);
+  k_lp_loss_sums<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->dvec, s->sc);
+  k_lp_loss_grad<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->rho, s->y, s->dvec, s->dy,
+                                                        s->sc, &s->sc->loss);
+  ctx->launches += 2;
+  lp_backward(ctx, s->dy);
+  GF_CUDA(ctx, cudaGetLastError());
+  double l = 0.0;
+  GF_CUDA(ctx, cudaMemcpyAsync(&l, &s->sc->loss, sizeof(double), cudaMemcpyDeviceToHost, cs));
+  GF_CUDA(ctx, cudaStreamSynchronize(cs));
+  if (loss) *loss = (float)l;
+  if (grad) GF_CUDA(ctx, cudaMemcpy(grad, s->g, sizeof(float) * P, cudaMemcpyDeviceToHost));
+  return GF_OK;
+}
+
+GF_API gf_status gf_lp_collect(gf_ctx* ctx, int32_t npairs, int32_t every, double tol,
+                               int32_t max_iter) {
+  if (!ctx || npairs <= 0 || every <= 0) return GF_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gf_status st = gf_lp_prepare(ctx);
+  if (st != GF_OK) return st;
+  return gf_lp_collect_impl(ctx, npairs, every, tol, max_iter > 0 ? max_iter : 100000);
+}
+
+GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed,
+                             float* final_loss) {
+  if (!ctx || steps < 0 || batch <= 0 || !(lr > 0.f)) return GF_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gf_status st = gf_lp_prepare(ctx);
+  if (st != GF_OK) return st;
+  LpState* s = ctx->lp;
+  if (s->npairs == 0) return gf_fail(ctx, GF_ERR_STATE, "no training pairs (gf_lp_collect)");
+  const int64_t P = s->off.total;
+  cudaStream_t cs = ctx->stream;
+  std::mt19937_64 rng(seed);
+  std::uniform_int_distribution<int> pick(0, s->npairs - 1);
+  double last = 0.0;
+  for (int it = 0; it < steps; ++it) {
+    GF_CUDA(ctx, cudaMemsetAsync(s->g, 0, sizeof(float) * (P + H), cs));
+    GF_CUDA(ctx, cudaMemsetAsync(&s->sc->loss, 0, sizeof(double), cs));
+    for (int b = 0; b < batch; ++b) {
+      const int k = pick(rng);
+      const float* r = s->pr + (int64_t)k * s->n;
+      const float* e = s->pe + (int64_t)k * s->n;
+      GF_CUDA(ctx, cudaMemsetAsync(&s->sc->dsum, 0, sizeof(double), cs));
+      lp_forward(ctx, r);
+      k_lp_loss_sums<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->dvec, s->sc);
+      k_lp_loss_grad<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->rho, s->y, s->dvec,
+                                                            s->dy, s->sc, &s->sc->loss);
+      ctx->launches += 2;
+      lp_backward(ctx, s->dy);
+    }
+    ++s->adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)s->adam_t), c2 = 1.f - std::pow(b2, (float)s->adam_t);
+    k_lp_adam<<<gf_blocks(P, kLT), kLT, 0, cs>>>(P, s->w, s->g, s->m, s->v, s->wb, lr, b1, b2,
+                                                 1e-8f, c1, c2, 1.f / batch);
+    GF_LAUNCH_CHECK(ctx, "k_lp_adam");
+    double l = 0.0;
+    GF_CUDA(ctx, cudaMemcpyAsync(&l, &s->sc->loss, sizeof(double), cudaMemcpyDeviceToHost, cs));
+    GF_CUDA(ctx, cudaStreamSynchronize(cs));
+    last = l / batch;
+    if (!std::isfinite(last)) return gf_fail(ctx, GF_ERR_STALLED, "training diverged at step %d", it);
+  }
+  if (final_loss) *final_loss = (float)last;
+  return GF_OK;
+}
+
+}  // extern "C"

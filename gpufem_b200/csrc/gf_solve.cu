@@ -54,46 +54,77 @@ __device__ inline double block_sum(T v, double* sh) {
   return s;  // valid in thread 0
 }
 
-// Row dot of the column-major ELL: sum_{slot < rownnz} val[slot*n+row] * x[col].
+// Where the solver's SpMVs find the matrix.  Two layouts share every kernel:
+//   ELL   (perm == nullptr): thread t owns row t; entry s at s*n + t.
+//   SELL  (perm != nullptr): thread t owns slot t of the sliced copy (gf_sell.cu):
+//         row perm[t] (-1 = padding slot), entry s at off[t/32] + 32 s + t%32.
+// Both walk a row's entries in slot order with the same four partial sums, so the
+// two layouts give bit-identical row dots.
+struct MatLayout {
+  int count;  // threads to launch: n (ELL) or the padded slot count (SELL)
+  int n;
+  const int32_t* __restrict__ rownnz;
+  const int32_t* __restrict__ col;
+  const int32_t* __restrict__ perm;
+  const int64_t* __restrict__ off;
+
+  __device__ inline bool at(int t, int& row, int& nz, int64_t& o, int64_t& stride) const {
+    if (t >= count) return false;
+    if (perm) {
+      row = __ldg(perm + t);
+      if (row < 0) return false;
+      o = __ldg(off + (t >> 5)) + (t & 31);
+      stride = 32;
+    } else {
+      row = t;
+      o = t;
+      stride = n;
+    }
+    nz = __ldg(rownnz + row);
+    return true;
+  }
+};
+
+// Row dot sum_{s < nz} val[o + s*stride] * x[col[o + s*stride]].
 template <typename TK, typename TX>
-__device__ inline double ell_row(int row, int n, int nz, const int32_t* __restrict__ col,
+__device__ inline double row_dot(int64_t o, int64_t stride, int nz, const int32_t* __restrict__ col,
                                  const TK* __restrict__ val, const TX* __restrict__ x) {
   using Acc = typename std::conditional<sizeof(TK) == 8 || sizeof(TX) == 8, double, float>::type;
   Acc a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-  int64_t o = row;
   int s = 0;
-  for (; s + 4 <= nz; s += 4, o += 4 * (int64_t)n) {
-    const int c0 = __ldg(col + o), c1 = __ldg(col + o + n), c2 = __ldg(col + o + 2 * (int64_t)n),
-              c3 = __ldg(col + o + 3 * (int64_t)n);
-    const TK v0 = __ldg(val + o), v1 = __ldg(val + o + n), v2 = __ldg(val + o + 2 * (int64_t)n),
-             v3 = __ldg(val + o + 3 * (int64_t)n);
+  for (; s + 4 <= nz; s += 4, o += 4 * stride) {
+    const int c0 = __ldg(col + o), c1 = __ldg(col + o + stride), c2 = __ldg(col + o + 2 * stride),
+              c3 = __ldg(col + o + 3 * stride);
+    const TK v0 = __ldg(val + o), v1 = __ldg(val + o + stride), v2 = __ldg(val + o + 2 * stride),
+             v3 = __ldg(val + o + 3 * stride);
     a0 += (Acc)v0 * (Acc)__ldg(x + c0);
     a1 += (Acc)v1 * (Acc)__ldg(x + c1);
     a2 += (Acc)v2 * (Acc)__ldg(x + c2);
     a3 += (Acc)v3 * (Acc)__ldg(x + c3);
   }
-  for (; s < nz; ++s, o += n) a0 += (Acc)__ldg(val + o) * (Acc)__ldg(x + __ldg(col + o));
+  for (; s < nz; ++s, o += stride) a0 += (Acc)__ldg(val + o) * (Acc)__ldg(x + __ldg(col + o));
   return (double)((a0 + a1) + (a2 + a3));
 }
 
 template <typename TK, typename TX, typename TY>
 __global__ void __launch_bounds__(kT)
-k_spmv(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
-       const TK* __restrict__ val, const TX* __restrict__ x, TY* __restrict__ y) {
-  const int row = blockIdx.x * kT + threadIdx.x;
-  if (row < n) y[row] = (TY)ell_row(row, n, rownnz[row], col, val, x);
+k_spmv(MatLayout L, const TK* __restrict__ val, const TX* __restrict__ x, TY* __restrict__ y) {
+  int row, nz;
+  int64_t o, st;
+  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st))
+    y[row] = (TY)row_dot(o, st, nz, L.col, val, x);
 }
 
 // r = f - K u (FP64), and r.r
 __global__ void __launch_bounds__(kT)
-k_residual64(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
-             const double* __restrict__ val, const double* __restrict__ u,
+k_residual64(MatLayout L, const double* __restrict__ val, const double* __restrict__ u,
              const double* __restrict__ f, double* __restrict__ r, double* __restrict__ acc) {
   __shared__ double sh[32];
-  const int row = blockIdx.x * kT + threadIdx.x;
+  int row, nz;
+  int64_t o, st;
   double rr = 0.0;
-  if (row < n) {
-    double v = f[row] - ell_row(row, n, rownnz[row], col, val, u);
+  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st)) {
+    double v = f[row] - row_dot(o, st, nz, L.col, val, u);
     r[row] = v;
     rr = v * v;
   }
@@ -136,9 +167,8 @@ __global__ void k_cg_init_fin(SolveScalars* sc, double eps, int maxit) {
 
 template <typename TK, typename V>
 __global__ void __launch_bounds__(kT)
-k_cg_spmv_dot(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
-              const TK* __restrict__ val, const V* __restrict__ p, V* __restrict__ q,
-              SolveScalars* sc) {
+k_cg_spmv_dot(MatLayout L, const TK* __restrict__ val, const V* __restrict__ p,
+              V* __restrict__ q, SolveScalars* sc) {
   __shared__ double sh[32];
   if (sc->done) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -146,10 +176,11 @@ k_cg_spmv_dot(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
     sc->rzn = 0.0;
     sc->rr = 0.0;
   }
-  const int row = blockIdx.x * kT + threadIdx.x;
+  int row, nz;
+  int64_t o, st;
   double pq = 0.0;
-  if (row < n) {
-    double v = ell_row(row, n, rownnz[row], col, val, p);
+  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st)) {
+    double v = row_dot(o, st, nz, L.col, val, p);
     q[row] = (V)v;
     pq = (double)p[row] * (double)(V)v;
   }
@@ -305,17 +336,31 @@ __global__ void k_zero_fixed(int n, const uint8_t* __restrict__ fixed, double* _
   if (i < n && fixed[i]) f[i] = 0.0;
 }
 
+// The sliced copy of the context's matrix in `dtype` (built or refreshed on demand).
+gf_status solver_matrix(gf_ctx* ctx, int dtype, MatLayout* L, const void** val) {
+  gf_status st = gf_sell_prepare(ctx, dtype);
+  if (st != GF_OK) return st;
+  *L = MatLayout{ctx->sell_nslots, ctx->n, ctx->d_rownnz, ctx->d_sell_col, ctx->d_sell_perm,
+                 ctx->d_sell_off};
+  *val = dtype == GF_F64 ? (const void*)ctx->d_sell_v64 : (const void*)ctx->d_sell_v32;
+  return GF_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y) {
+  MatLayout L;
+  const void* val = nullptr;
+  gf_status st = solver_matrix(ctx, dtype, &L, &val);
+  if (st != GF_OK) return st;
   cudaEventRecord(ctx->ev0, ctx->stream);
   if (dtype == GF_F64)
-    k_spmv<double, double, double><<<gf_blocks(ctx->n, kT), kT, 0, ctx->stream>>>(
-        ctx->n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, (const double*)x, (double*)y);
+    k_spmv<double, double, double><<<gf_blocks(L.count, kT), kT, 0, ctx->stream>>>(
+        L, (const double*)val, (const double*)x, (double*)y);
   else
-    k_spmv<float, float, float><<<gf_blocks(ctx->n, kT), kT, 0, ctx->stream>>>(
-        ctx->n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32, (const float*)x, (float*)y);
+    k_spmv<float, float, float><<<gf_blocks(L.count, kT), kT, 0, ctx->stream>>>(
+        L, (const float*)val, (const float*)x, (float*)y);
   GF_LAUNCH_CHECK(ctx, "k_spmv");
   cudaEventRecord(ctx->ev1, ctx->stream);
   GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
@@ -371,6 +416,8 @@ gf_status gf_constraints_apply(gf_ctx* ctx, int mode) {
   }
   GF_CUDA(ctx, cudaGetLastError());
   ctx->bc_mode_applied = mode;
+  ctx->kver64++;
+  ctx->kver32++;
   return GF_OK;
 }
 
@@ -380,6 +427,7 @@ void gf_solver_free(gf_ctx* ctx) {
   ctx->work_bytes = 0;
   gf_free(ctx->d_scal);
   gf_free(ctx->d_red);
+  if (ctx->d_fcg) { cudaFree(ctx->d_fcg); ctx->d_fcg = nullptr; }
   if (ctx->h_pinned) { cudaFreeHost(ctx->h_pinned); ctx->h_pinned = nullptr; }
 }
 
@@ -393,7 +441,8 @@ struct CgVecs {
 // device flag says done.  b must already be in vecs.r's type (copied into x's
 // buffer by the caller as `b`).  Returns iterations and final done code.
 template <typename TK, typename V>
-gf_status run_cg(gf_ctx* ctx, const TK* val, const V* b, CgVecs vv, bool precond, double eps,
+gf_status run_cg(gf_ctx* ctx, MatLayout L, const TK* val, const V* b, CgVecs vv, bool precond,
+                 double eps,
                  int maxit, int check_every, double max_seconds,
                  std::chrono::steady_clock::time_point t0, int* iters, int* done_code,
                  double* rr_final, double* rr0_out) {
@@ -415,7 +464,7 @@ gf_status run_cg(gf_ctx* ctx, const TK* val, const V* b, CgVecs vv, bool precond
   cudaGraphExec_t exec = nullptr;
   GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < check_every; ++k) {
-    k_cg_spmv_dot<TK, V><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, val, p, q, sc);
+    k_cg_spmv_dot<TK, V><<<gf_blocks(L.count, kT), kT, 0, s>>>(L, val, p, q, sc);
     k_cg_update<V><<<nb, kT, 0, s>>>(n, x, r, zz, p, q, dinv, sc);
     k_cg_direction<V><<<nb, kT, 0, s>>>(n, zz, p, sc);
   }
@@ -480,9 +529,12 @@ gf_status ensure_work(gf_ctx* ctx) {
 gf_status residual64(gf_ctx* ctx, double* r64, double* rr) {
   cudaStream_t s = ctx->stream;
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_red, 0, sizeof(double), s));
-  k_residual64<<<gf_blocks(ctx->n, kT), kT, 0, s>>>(ctx->n, ctx->d_rownnz, ctx->d_colidx,
-                                                    ctx->d_K64, ctx->d_u, ctx->d_f, r64,
-                                                    ctx->d_red);
+  MatLayout L;
+  const void* val = nullptr;
+  gf_status st = solver_matrix(ctx, GF_F64, &L, &val);
+  if (st != GF_OK) return st;
+  k_residual64<<<gf_blocks(L.count, kT), kT, 0, s>>>(L, (const double*)val, ctx->d_u, ctx->d_f,
+                                                     r64, ctx->d_red);
   GF_LAUNCH_CHECK(ctx, "k_residual64");
   double* h = (double*)ctx->h_pinned + 16;
   GF_CUDA(ctx, cudaMemcpyAsync(h, ctx->d_red, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -539,6 +591,11 @@ __global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv,
   if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
 }
 
+__global__ void k_add64(int n, const double* __restrict__ d, double* __restrict__ u) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) u[i] += d[i];
+}
+
 __global__ void k_mixed_scalars(SolveScalars* sc, double tol2) {
   sc->tol2 = tol2;
   sc->pq = 0.0;
@@ -559,13 +616,19 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   const double tol = o->tol;
   const double delta2 = 0.01;  // update when ||r|| fell 10x since the last update
   gf_status st;
+  MatLayout L32, L64;
+  const void *v32 = nullptr, *v64 = nullptr;
+  if ((st = solver_matrix(ctx, GF_F32, &L32, &v32)) != GF_OK) return st;
+  if ((st = solver_matrix(ctx, GF_F64, &L64, &v64)) != GF_OK) return st;
+  const float* val32 = (const float*)v32;
   k_diag_inv<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32, dinv);
   GF_LAUNCH_CHECK(ctx, "k_diag_inv");
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u, 0, sizeof(double) * n, s));
   double ff = 0.0;
   if ((st = residual64(ctx, r64, &ff)) != GF_OK) return st;  // u = 0: r64 = f
   double rr64 = ff;
-  int updates = 0, done_code = 1;
+  int updates = 0, done_code = 1, fp32_iters = 0, fp64_iters = 0;
+  bool fp64_fallback = false;
   if (ff > 0.0) {
     double sigma = std::sqrt(ff);
     k_scale_to_f32<<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
@@ -579,8 +642,7 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     cudaGraphExec_t exec = nullptr;
     GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < check; ++k) {
-      k_cg_spmv_dot<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32,
-                                                     p, q, sc);
+      k_cg_spmv_dot<float, float><<<gf_blocks(L32.count, kT), kT, 0, s>>>(L32, val32, p, q, sc);
       k_cg_update<float><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
       k_cg_direction<float><<<nb, kT, 0, s>>>(n, z, p, sc);
     }
@@ -591,8 +653,8 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       cudaGraphDestroy(graph);
       return gf_cuda_fail(ctx, ce, "graph instantiate");
     }
-    double rr_max = 1.0;
-    int breakdowns = 0;
+    double rr_max = 1.0, prev_rr64 = ff;
+    int breakdowns = 0, stagnant = 0;
     done_code = 3;
     for (;;) {
       ce = cudaGraphLaunch(exec, s);
@@ -619,6 +681,11 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       ++updates;
       if (std::sqrt(rr64 / ff) <= tol) { done_code = 1; break; }
       if (hs->done == 3 || timeout) { done_code = 3; break; }
+      // the true residual must at least halve between updates; three misses in a
+      // row mean FP32 cannot resolve this system (condition ~ 1/eps32): finish in FP64
+      stagnant = rr64 > 0.25 * prev_rr64 ? stagnant + 1 : 0;
+      prev_rr64 = rr64;
+      if (stagnant >= 3) { fp64_fallback = true; break; }
       const bool restart = hs->done == 2 || diverging;
       if (restart && ++breakdowns > 50) { done_code = 2; break; }
       const double sigma_new = std::sqrt(rr64);
@@ -636,13 +703,38 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     if (st != GF_OK) return st;
+    fp32_iters = hs->iter;
+    if (fp64_fallback) {
+      // FP64 Jacobi-PCG on the correction K64 d = r64, then u += d
+      double* w64 = (double*)ctx->d_work;
+      double* b = w64 + 7 * (size_t)n;
+      GF_CUDA(ctx, cudaMemcpyAsync(b, r64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      CgVecs vv{w64, w64 + n, w64 + 2 * (size_t)n, w64 + 3 * (size_t)n, w64 + 4 * (size_t)n,
+                w64 + 5 * (size_t)n};
+      k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
+                                                   (double*)vv.dinv);
+      GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+      int it2 = 0, done2 = 0;
+      double rr2 = 0.0, rr02 = 0.0;
+      st = run_cg<double, double>(ctx, L64, (const double*)v64, b, vv, true,
+                                  tol * std::sqrt(ff / rr64),
+                                  std::max(1, maxit - fp32_iters), check, o->max_seconds, t0,
+                                  &it2, &done2, &rr2, &rr02);
+      if (st != GF_OK) return st;
+      k_add64<<<nb, kT, 0, s>>>(n, (const double*)vv.x, ctx->d_u);
+      GF_LAUNCH_CHECK(ctx, "k_add64");
+      if ((st = residual64(ctx, r64, &rr64)) != GF_OK) return st;
+      fp64_iters = it2;
+      done_code = std::sqrt(rr64 / ff) <= tol * 1.01 ? 1 : done2;
+    }
   }
   cudaEventRecord(ctx->ev1, s);
   GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   info->seconds = ctx->last_seconds = ms * 1e-3;
-  info->iterations = ff > 0.0 ? hs->iter : 0;
+  info->iterations = fp32_iters + fp64_iters;
+  info->fallback = fp64_fallback ? 1 : 0;
   info->outer = updates;
   info->rel_residual = ff > 0.0 ? std::sqrt(rr64 / ff) : 0.0;
   info->status = status_of(done_code);
@@ -654,18 +746,318 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Flexible CG (Notay's FCG(1): Polak-Ribiere beta, alpha = p.r / p.K p) in FP64
+// with a variable preconditioner: the learned network (gf_learned.cu), or Jacobi
+// after a fallback.  Jacobi-PCG takes over — restarting the search direction from
+// the current iterate — when the learned preconditioner breaks down (z.r <= 0 or
+// p.Kp <= 0) or stalls (no net residual reduction over 512 iterations).
+// Convergence is decided on the FP64 residual.
+namespace {
+
+struct FcgScalars {
+  double zr, zrp, zr_prev, pq, pr, rr, rr0, tol2;
+  int iter, done, maxit, first;
+};
+
+__global__ void k_fcg_init(int n, const double* __restrict__ f, double* __restrict__ x,
+                           double* __restrict__ r, double* __restrict__ rold, FcgScalars* sc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kT + threadIdx.x;
+  double rr = 0.0;
+  if (i < n) {
+    x[i] = 0.0;
+    r[i] = f[i];
+    rold[i] = 0.0;
+    rr = f[i] * f[i];
+  }
+  double s1 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s1);
+}
+
+__global__ void k_fcg_init_fin(FcgScalars* sc, double tol, int maxit) {
+  sc->rr0 = sc->rr;
+  sc->tol2 = tol * tol * sc->rr;
+  sc->iter = 0;
+  sc->maxit = maxit;
+  sc->first = 1;
+  sc->zr_prev = 1.0;
+  sc->zr = sc->zrp = sc->pq = sc->pr = 0.0;
+  sc->done = (sc->rr <= 0.0) ? 1 : (maxit <= 0 ? 3 : 0);
+}
+
+__global__ void k_fcg_jacobi(int n, const double* __restrict__ r, const double* __restrict__ dinv,
+                             double* __restrict__ z, const FcgScalars* sc) {
+  if (sc->done) return;
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) z[i] = r[i] * dinv[i];
+}
+
+__global__ void k_fcg_dots(int n, const double* __restrict__ z, const double* __restrict__ r,
+                           const double* __restrict__ rold, FcgScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const int i = blockIdx.x * kT + threadIdx.x;
+  double a = 0.0, b = 0.0;
+  if (i < n) {
+    a = z[i] * r[i];
+    b = z[i] * rold[i];
+  }
+  double s1 = block_sum(a, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->zr, s1);
+  double s2 = block_sum(b, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->zrp, s2);
+}
+
+__global__ void k_fcg_dir(int n, const double* __restrict__ z, double* __restrict__ p,
+                          FcgScalars* sc) {
+  if (sc->done) return;
+  if (!(sc->zr > 0.0) || !isfinite(sc->zr)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 2;
+    return;
+  }
+  const double beta = sc->first ? 0.0 : (sc->zr - sc->zrp) / sc->zr_prev;
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) p[i] = z[i] + beta * p[i];
+}
+
+__global__ void __launch_bounds__(kT)
+k_fcg_spmv(MatLayout L, const double* __restrict__ val, const double* __restrict__ p,
+           const double* __restrict__ r, double* __restrict__ q, FcgScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->rr = 0.0;
+  int row, nz;
+  int64_t o, st;
+  double pq = 0.0, pr = 0.0;
+  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st)) {
+    const double v = row_dot(o, st, nz, L.col, val, p);
+    q[row] = v;
+    pq = p[row] * v;
+    pr = p[row] * r[row];
+  }
+  double s1 = block_sum(pq, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->pq, s1);
+  double s2 = block_sum(pr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->pr, s2);
+}
+
+__global__ void k_fcg_update(int n, double* __restrict__ x, double* __restrict__ r,
+                             double* __restrict__ rold, const double* __restrict__ p,
+                             const double* __restrict__ q, FcgScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  if (!(sc->pq > 0.0) || !isfinite(sc->pq)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 2;
+    return;
+  }
+  const double alpha = sc->pr / sc->pq;
+  const int i = blockIdx.x * kT + threadIdx.x;
+  double rr = 0.0;
+  if (i < n) {
+    x[i] += alpha * p[i];
+    const double ri = r[i];
+    rold[i] = ri;
+    const double rn = ri - alpha * q[i];
+    r[i] = rn;
+    rr = rn * rn;
+  }
+  double s = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s);
+}
+
+__global__ void k_fcg_finish(FcgScalars* sc) {
+  if (sc->done) return;
+  sc->zr_prev = sc->zr;
+  sc->zr = sc->zrp = sc->pq = sc->pr = 0.0;
+  sc->first = 0;
+  sc->iter += 1;
+  if (sc->rr <= sc->tol2) sc->done = 1;
+  else if (sc->iter >= sc->maxit) sc->done = 3;
+}
+
+__global__ void k_fcg_restart(FcgScalars* sc) {
+  sc->first = 1;
+  sc->zr = sc->zrp = sc->pq = sc->pr = 0.0;
+  sc->done = sc->iter >= sc->maxit ? 3 : 0;
+}
+
+__global__ void k_record_pair(int n, const double* __restrict__ r, const double* __restrict__ x,
+                              const double* __restrict__ ustar, float* __restrict__ rout,
+                              float* __restrict__ eout) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) {
+    rout[i] = (float)r[i];
+    eout[i] = (float)(ustar[i] - x[i]);
+  }
+}
+
+gf_status run_fcg(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
+                  std::chrono::steady_clock::time_point t0, gf_solve_info* info) {
+  const int n = ctx->n;
+  const int nb = gf_blocks(n, kT);
+  cudaStream_t s = ctx->stream;
+  gf_status st;
+  if (!ctx->lp) return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner not initialised (gf_lp_init)");
+  const bool learned = true;
+  if ((st = gf_lp_prepare(ctx)) != GF_OK) return st;
+  if (!ctx->d_fcg) {
+    if (cudaMalloc(&ctx->d_fcg, sizeof(FcgScalars)) != cudaSuccess) {
+      cudaGetLastError();
+      return gf_fail(ctx, GF_ERR_OOM, "FCG scalars");
+    }
+  }
+  FcgScalars* sc = static_cast<FcgScalars*>(ctx->d_fcg);
+  FcgScalars hs{};
+  double* w = (double*)ctx->d_work;
+  double *x = w, *r = w + n, *rold = w + 2 * (size_t)n, *z = w + 3 * (size_t)n;
+  double *p = w + 4 * (size_t)n, *q = w + 5 * (size_t)n, *dinv = w + 6 * (size_t)n;
+  float* r32 = reinterpret_cast<float*>(w + 7 * (size_t)n);
+  MatLayout L;
+  const void* vv = nullptr;
+  if ((st = solver_matrix(ctx, GF_F64, &L, &vv)) != GF_OK) return st;
+  const double* val = (const double*)vv;
+  k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
+  GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+  GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(FcgScalars), s));
+  k_fcg_init<<<nb, kT, 0, s>>>(n, ctx->d_f, x, r, rold, sc);
+  k_fcg_init_fin<<<1, 1, 0, s>>>(sc, o->tol, maxit);
+  GF_LAUNCH_CHECK(ctx, "k_fcg_init");
+  // two chunk graphs: learned preconditioner and Jacobi
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  for (int kind = learned ? 0 : 1; kind < 2; ++kind) {
+    GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < check; ++k) {
+      if (kind == 0) gf_lp_apply64(ctx, r, r32, z);
+      else k_fcg_jacobi<<<nb, kT, 0, s>>>(n, r, dinv, z, sc);
+      k_fcg_dots<<<nb, kT, 0, s>>>(n, z, r, rold, sc);
+      k_fcg_dir<<<nb, kT, 0, s>>>(n, z, p, sc);
+      k_fcg_spmv<<<gf_blocks(L.count, kT), kT, 0, s>>>(L, val, p, r, q, sc);
+      k_fcg_update<<<nb, kT, 0, s>>>(n, x, r, rold, p, q, sc);
+      k_fcg_finish<<<1, 1, 0, s>>>(sc);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph[kind]);
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec[kind], graph[kind], 0);
+    if (ce != cudaSuccess) {
+      for (int k2 = 0; k2 < 2; ++k2) {
+        if (exec[k2]) cudaGraphExecDestroy(exec[k2]);
+        if (graph[k2]) cudaGraphDestroy(graph[k2]);
+      }
+      return gf_cuda_fail(ctx, ce, "FCG graph");
+    }
+  }
+  int mode = learned ? 0 : 1;
+  int fallback = learned ? 0 : 1;
+  std::vector<std::pair<int, double>> hist;  // (iteration, rr) at chunk ends
+  st = GF_OK;
+  for (;;) {
+    cudaError_t ce = cudaGraphLaunch(exec[mode], s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&hs, sc, sizeof(FcgScalars), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "FCG chunk"); break; }
+    ctx->launches += (int64_t)check * (mode == 0 ? 20 : 6);
+    if (hs.done == 1 || hs.done == 3) break;
+    const bool timeout = o->max_seconds > 0.0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds;
+    if (timeout) { hs.done = 3; break; }
+    bool stall = false;
+    if (mode == 0) {
+      hist.emplace_back(hs.iter, hs.rr);
+      for (const auto& h : hist)
+        if (hs.iter - h.first >= 512 && hs.iter - h.first < 512 + check && hs.rr >= h.second)
+          stall = true;  // no net reduction of ||r|| over 512 iterations
+    }
+    if (hs.done == 2 || stall) {
+      if (mode == 1) break;  // Jacobi-PCG itself broke down
+      mode = 1;
+      fallback = 1;
+      k_fcg_restart<<<1, 1, 0, s>>>(sc);
+      ce = cudaGetLastError();
+      if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "FCG restart"); break; }
+    }
+  }
+  for (int k2 = 0; k2 < 2; ++k2) {
+    if (exec[k2]) cudaGraphExecDestroy(exec[k2]);
+    if (graph[k2]) cudaGraphDestroy(graph[k2]);
+  }
+  if (st != GF_OK) return st;
+  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_u, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  double rrt = 0.0;
+  double* rtrue = q;  // q is free now
+  if ((st = residual64(ctx, rtrue, &rrt)) != GF_OK) return st;
+  cudaEventRecord(ctx->ev1, s);
+  GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  info->seconds = ctx->last_seconds = ms * 1e-3;
+  info->iterations = hs.iter;
+  info->outer = 1;
+  info->fallback = fallback && learned ? 1 : 0;
+  info->rel_residual = hs.rr0 > 0.0 ? std::sqrt(rrt / hs.rr0) : 0.0;
+  info->status = status_of(hs.done);
+  if (hs.done != 1)
+    gf_fail(ctx, (gf_status)info->status, "FCG stopped with code %d after %d iterations", hs.done,
+            hs.iter);
+  return (gf_status)info->status;
+}
+
+}  // namespace
+
+gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every, double tol,
+                        int maxit, float* r_out, float* e_out, int* recorded) {
+  *recorded = 0;
+  if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "recording needs the FP64 matrix");
+  gf_status st;
+  if ((st = ensure_work(ctx)) != GF_OK) return st;
+  const int n = ctx->n;
+  const int nb = gf_blocks(n, kT);
+  cudaStream_t s = ctx->stream;
+  SolveScalars* sc = ctx->d_scal;
+  SolveScalars* hs = (SolveScalars*)ctx->h_pinned;
+  double* v = (double*)ctx->d_work;
+  double *x = v, *r = v + n, *z = v + 2 * (size_t)n, *p = v + 3 * (size_t)n, *q = v + 4 * (size_t)n;
+  double* dinv = v + 5 * (size_t)n;
+  MatLayout L;
+  const void* vk = nullptr;
+  if ((st = solver_matrix(ctx, GF_F64, &L, &vk)) != GF_OK) return st;
+  k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
+  GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
+  k_cg_init<double><<<nb, kT, 0, s>>>(n, ctx->d_f, dinv, x, r, z, p, sc);
+  k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
+  GF_LAUNCH_CHECK(ctx, "k_cg_init");
+  k_record_pair<<<nb, kT, 0, s>>>(n, r, x, ustar, r_out, e_out);  // iteration 0: e = u*
+  GF_LAUNCH_CHECK(ctx, "k_record_pair");
+  int got = 1;
+  while (got < npairs) {
+    for (int k = 0; k < every; ++k) {
+      k_cg_spmv_dot<double, double><<<gf_blocks(L.count, kT), kT, 0, s>>>(
+          L, (const double*)vk, p, q, sc);
+      k_cg_update<double><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+      k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
+    }
+    ctx->launches += 3 * every;
+    GF_CUDA(ctx, cudaMemcpyAsync(hs, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+    GF_CUDA(ctx, cudaStreamSynchronize(s));
+    if (hs->done) break;
+    k_record_pair<<<nb, kT, 0, s>>>(n, r, x, ustar, r_out + (size_t)got * n,
+                                    e_out + (size_t)got * n);
+    GF_LAUNCH_CHECK(ctx, "k_record_pair");
+    ++got;
+  }
+  GF_CUDA(ctx, cudaStreamSynchronize(s));
+  *recorded = got;
+  return GF_OK;
+}
+
 gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info) {
   *info = gf_solve_info{};
   const int solver = o->solver;
   if (solver < GF_SOLVER_CG || solver > GF_SOLVER_LEARNED_FCG)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown solver %d", solver);
-  if (solver == GF_SOLVER_LEARNED_FCG)
-    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "learned preconditioner not available in this build");
   if (!(o->tol > 0.0)) return gf_fail(ctx, GF_ERR_INVALID_ARG, "tol must be > 0");
   const int maxit = o->max_iter > 0 ? o->max_iter : 10000;
   const int check = o->check_every > 0 ? std::min(o->check_every, 256) : 16;
-  const int max_outer = o->max_outer > 0 ? o->max_outer : 50;
-  const double inner_tol = o->inner_tol > 0.0 ? o->inner_tol : 1e-4;
   const int n = ctx->n;
   gf_status st;
   if ((st = ensure_work(ctx)) != GF_OK) return st;
@@ -674,6 +1066,10 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
   char* w = (char*)ctx->d_work;
   auto t0 = std::chrono::steady_clock::now();
   cudaEventRecord(ctx->ev0, s);
+  if (solver == GF_SOLVER_LEARNED_FCG) {
+    if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "learned FCG needs the FP64 matrix");
+    return run_fcg(ctx, o, maxit, check, t0, info);
+  }
 
   if (solver == GF_SOLVER_CG || solver == GF_SOLVER_PCG) {
     const bool pre = solver == GF_SOLVER_PCG;
@@ -691,7 +1087,10 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
                                                      (double*)vv.dinv);
         GF_LAUNCH_CHECK(ctx, "k_diag_inv");
       }
-      st = run_cg<double, double>(ctx, ctx->d_K64, ctx->d_f, vv, pre, o->tol, maxit, check,
+      MatLayout L;
+      const void* vk = nullptr;
+      if ((st = solver_matrix(ctx, GF_F64, &L, &vk)) != GF_OK) return st;
+      st = run_cg<double, double>(ctx, L, (const double*)vk, ctx->d_f, vv, pre, o->tol, maxit, check,
                                   o->max_seconds, t0, &iters, &done, &rr, &rr0);
       if (st != GF_OK) return st;
       GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_u, vv.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
@@ -706,7 +1105,10 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
                                                    (float*)vv.dinv);
         GF_LAUNCH_CHECK(ctx, "k_diag_inv");
       }
-      st = run_cg<float, float>(ctx, ctx->d_K32, b32, vv, pre, o->tol, maxit, check,
+      MatLayout L;
+      const void* vk = nullptr;
+      if ((st = solver_matrix(ctx, GF_F32, &L, &vk)) != GF_OK) return st;
+      st = run_cg<float, float>(ctx, L, (const float*)vk, b32, vv, pre, o->tol, maxit, check,
                                 o->max_seconds, t0, &iters, &done, &rr, &rr0);
       if (st != GF_OK) return st;
       k_copy_to_f64<float><<<nb, kT, 0, s>>>(n, (const float*)vv.x, ctx->d_u);
@@ -817,6 +1219,7 @@ extern "C" GF_API gf_status gf_pcg_noalloc(int32_t n, int32_t width, const int32
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int nb = gf_blocks(n, kT);
   const int chunk = 16;
+  const MatLayout L{n, n, rownnz, colidx, nullptr, nullptr};  // the caller's ELL as given
   auto fail = [](cudaError_t e) {
     cudaGetLastError();
     return e == cudaSuccess ? GF_OK : GF_ERR_CUDA;
@@ -830,7 +1233,7 @@ extern "C" GF_API gf_status gf_pcg_noalloc(int32_t n, int32_t width, const int32
   SolveScalars hs{};  // pageable host copy: no pinned allocation
   for (;;) {
     for (int k = 0; k < chunk; ++k) {
-      k_cg_spmv_dot<double, double><<<nb, kT, 0, s>>>(n, rownnz, colidx, values, p, q, sc);
+      k_cg_spmv_dot<double, double><<<nb, kT, 0, s>>>(L, values, p, q, sc);
       k_cg_update<double><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
       k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
     }
@@ -844,7 +1247,7 @@ extern "C" GF_API gf_status gf_pcg_noalloc(int32_t n, int32_t width, const int32
   double rr = 0.0;
   e = cudaMemsetAsync(acc, 0, sizeof(double), s);
   if (e != cudaSuccess) return fail(e);
-  k_residual64<<<nb, kT, 0, s>>>(n, rownnz, colidx, values, x, b, r, acc);
+  k_residual64<<<nb, kT, 0, s>>>(L, values, x, b, r, acc);
   if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
   e = cudaMemcpyAsync(&rr, acc, sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);

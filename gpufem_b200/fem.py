@@ -173,6 +173,53 @@ class Context:
         self._c(lib.gf_get_solution(self.h, _ptr(u)))
         return u
 
+    # ---- learned preconditioner ------------------------------------------
+    def lp_init(self, dim: int, seed: int = 0) -> None:
+        self._c(lib.gf_lp_init(self.h, dim, seed))
+        self.lp_dim = dim
+
+    def lp_num_params(self, dim: int) -> int:
+        return int(lib.gf_lp_num_params(dim))
+
+    def lp_get_weights(self) -> np.ndarray:
+        w = np.empty(self.lp_num_params(self.lp_dim), np.float32)
+        self._c(lib.gf_lp_get_weights(self.h, _ptr(w)))
+        return w
+
+    def lp_set_weights(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, np.float32)
+        self._c(lib.gf_lp_set_weights(self.h, _ptr(w)))
+
+    def lp_collect(self, npairs: int, every: int, tol: float = 1e-6, max_iter: int = 100000) -> None:
+        self._c(lib.gf_lp_collect(self.h, npairs, every, tol, max_iter))
+
+    def lp_train(self, steps: int, batch: int = 4, lr: float = 1e-3, seed: int = 0) -> float:
+        loss = C.c_float()
+        self._c(lib.gf_lp_train(self.h, steps, batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def _dev(self, a: np.ndarray):
+        import torch
+        return torch.tensor(np.ascontiguousarray(a, np.float32), device="cuda")
+
+    def lp_apply(self, r: np.ndarray) -> np.ndarray:
+        import torch
+        rd = self._dev(r)
+        zd = torch.empty_like(rd)
+        torch.cuda.synchronize()
+        self._c(lib.gf_lp_apply(self.h, C.c_void_p(rd.data_ptr()), C.c_void_p(zd.data_ptr())))
+        return zd.cpu().numpy()
+
+    def lp_loss_grad(self, r: np.ndarray, e: np.ndarray):
+        import torch
+        rd, ed = self._dev(r), self._dev(e)
+        g = np.empty(self.lp_num_params(self.lp_dim), np.float32)
+        loss = C.c_float()
+        torch.cuda.synchronize()
+        self._c(lib.gf_lp_loss_grad(self.h, C.c_void_p(rd.data_ptr()), C.c_void_p(ed.data_ptr()),
+                                    C.byref(loss), _ptr(g)))
+        return loss.value, g
+
     def launches(self) -> int:
         return int(lib.gf_kernel_launches(self.h))
 

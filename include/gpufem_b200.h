@@ -201,6 +201,35 @@ GF_API gf_status gf_get_solution(gf_ctx* ctx, double* u);
 /* Device pointer of the FP64 solution. */
 GF_API gf_status gf_solution_view(gf_ctx* ctx, const double** u);
 
+/* ---- learned preconditioner (no counterpart in the reference) ---------------------------
+ * M(r) = D^-1 r + c * y, c = rms(D^-1 r), y from a 3-layer message-passing network over
+ * the node graph of K (nodes sharing an element): input layer (2*dim -> 64), three layers
+ * h' = relu(Ws h + Wn mean_neighbours(h) + b) (hidden width 64), output layer (64 -> dim)
+ * initialised to zero (an untrained network is Jacobi).  Weights are BF16 in use with an
+ * FP32 master copy; activations and accumulation are FP32.  Used by GF_SOLVER_LEARNED_FCG.
+ * Parameter layout: W0[64][2 dim], b0[64], then per layer Ws[64][64], Wn[64][64], b[64],
+ * then Wout[dim][64], bout[dim]. */
+GF_API int64_t gf_lp_num_params(int32_t dim);
+GF_API gf_status gf_lp_init(gf_ctx* ctx, int32_t dim, uint64_t seed);
+GF_API gf_status gf_lp_get_weights(gf_ctx* ctx, float* w);
+GF_API gf_status gf_lp_set_weights(gf_ctx* ctx, const float* w);
+/* Training pairs (r_k, e_k = u* - x_k) from Jacobi-PCG on the current FP64 matrix and
+ * force: one pair every `every` iterations of a run to `tol`, up to npairs (u* from a run
+ * to tol * 1e-3).  Replaces previously collected pairs. */
+GF_API gf_status gf_lp_collect(gf_ctx* ctx, int32_t npairs, int32_t every, double tol,
+                               int32_t max_iter);
+/* Adam steps (lr, batch pairs per step) on the collected pairs; loss per pair
+ * sum d (c y - (e - D^-1 r))^2 / sum d e^2 (d = diag K).  *final_loss = mean loss of the
+ * last step. */
+GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed,
+                             float* final_loss);
+/* z = M(r) on FP32 device vectors of n entries. */
+GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z);
+/* Loss of one (r, e) pair (FP32 device vectors) and its gradient w.r.t. every parameter
+ * (host buffer of gf_lp_num_params floats, or NULL); weights unchanged. */
+GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, float* loss,
+                                 float* grad);
+
 /* ---- allocation-free solve -------------------------------------------------------------
  * No counterpart in the reference.  FP64 Jacobi-PCG (x0 = 0, stop when the recursive
  * residual satisfies r.r <= tol^2 b.b, or after max_iter iterations) for callers that

@@ -1,0 +1,103 @@
+"""Learned preconditioner on the GPU: forward and gradients against the numpy
+oracle, training on residual/error pairs, flexible CG with the Jacobi fallback."""
+import numpy as np
+import pytest
+
+from gpufem_b200 import _lib
+from gpufem_b200 import meshgen as mg
+from oracle import gnn_oracle as G
+
+pytestmark = pytest.mark.gpu
+
+
+def brick8_problem(n=(4, 3, 3), seed=5, sigma=1.0):
+    from gpufem_b200.fem import Context
+    m = mg.clamp_and_load(mg.structured(mg.BRICK8, n, jitter=0.1, seed=seed))
+    m.E = mg.lognormal_correlated(m, sigma, 0.2, seed)
+    ctx = Context(0)
+    ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+    ctx.set_supports(m.supports)
+    ctx.set_force(m.f)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+    ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
+    return m, ctx
+
+
+def diag_of(ctx):
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    return np.array([v[np.nonzero(ci[: rn[r], r] == r)[0][0], r] for r in range(rn.size)])
+
+
+def random_weights(dim, seed=2, scale=0.25):
+    return np.random.default_rng(seed).normal(scale=scale, size=G.offsets(dim)["total"][0])
+
+
+def test_untrained_network_is_jacobi():
+    m, ctx = brick8_problem()
+    ctx.lp_init(3, seed=1)
+    r = np.random.default_rng(0).normal(size=m.ndof)
+    z = ctx.lp_apply(r)
+    d = diag_of(ctx)
+    assert np.allclose(z, r / d, rtol=1e-6, atol=0)
+
+
+def test_forward_and_gradient_match_oracle():
+    m, ctx = brick8_problem()
+    ctx.lp_init(3, seed=1)
+    w = random_weights(3).astype(np.float32)
+    ctx.lp_set_weights(w)
+    assert np.array_equal(ctx.lp_get_weights(), w)
+    rng = np.random.default_rng(1)
+    r = rng.normal(size=m.ndof).astype(np.float32)
+    e = rng.normal(size=m.ndof).astype(np.float32)
+    d = diag_of(ctx)
+    adj = G.node_adjacency(m.conn, m.nnodes)
+    z_gpu = ctx.lp_apply(r)
+    L_ref, g_ref, z_ref = G.loss_and_grad(w.astype(np.float64), 3, adj, d, r.astype(np.float64),
+                                          e.astype(np.float64))
+    assert np.linalg.norm(z_gpu - z_ref) <= 1e-4 * np.linalg.norm(z_ref)
+    L_gpu, g_gpu = ctx.lp_loss_grad(r, e)
+    assert abs(L_gpu - L_ref) <= 1e-4 * abs(L_ref)
+    for name, (p, size) in G.offsets(3).items():
+        if size == 0:
+            continue
+        a, b = g_gpu[p:p + size], g_ref[p:p + size]
+        assert np.linalg.norm(a - b) <= 1e-3 * max(np.linalg.norm(b), 1e-12), name
+
+
+def test_training_reduces_loss():
+    m, ctx = brick8_problem(n=(6, 6, 6))
+    ctx.lp_init(3, seed=3)
+    ctx.lp_collect(npairs=24, every=4, tol=1e-8)
+    l0 = ctx.lp_train(steps=1, batch=8, lr=1e-3, seed=1)
+    l1 = ctx.lp_train(steps=150, batch=8, lr=1e-3, seed=2)
+    assert np.isfinite(l1) and l1 < 0.9 * l0, (l0, l1)
+
+
+def test_learned_fcg_converges_and_matches_pcg():
+    m, ctx = brick8_problem(n=(6, 6, 6))
+    info = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-10, max_iter=100000)
+    u_pcg = ctx.solution()
+    ctx.lp_init(3, seed=3)
+    ctx.lp_collect(npairs=24, every=4, tol=1e-8)
+    ctx.lp_train(steps=100, batch=8, lr=1e-3, seed=2)
+    info2 = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
+    u = ctx.solution()
+    assert info2.status == _lib.GF_OK and info2.rel_residual <= 1e-9
+    assert np.linalg.norm(u - u_pcg) <= 1e-7 * np.linalg.norm(u_pcg)
+
+
+def test_fallback_to_jacobi_when_learned_preconditioner_is_bad():
+    m, ctx = brick8_problem(n=(6, 6, 6))
+    ctx.lp_init(3, seed=3)
+    ctx.lp_set_weights(random_weights(3, seed=9, scale=3.0).astype(np.float32))
+    info = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
+    assert info.status == _lib.GF_OK and info.rel_residual <= 1e-9
+    assert info.fallback == 1
+
+
+def test_learned_fcg_requires_init():
+    m, ctx = brick8_problem()
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-8)
+    assert ei.value.status == _lib.GF_ERR_STATE
