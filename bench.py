@@ -194,7 +194,8 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 6):
     """Brick8 cubes with correlated log-normal E (sigma U(0.5, 2), correlation length
     U(0.05, 0.3)) and nu U(0.2, 0.4), z = 0 clamped, pressure on z = 1.  The network is
     trained on small seeded cubes (edge 12..20) and evaluated on held-out cubes (edge
-    24, 32, 40): time and iterations to reach FP64-oracle relative error 1e-6, for FP64
+    24, 32, 40): time and iterations to reach relative residual 1e-8 (error against an FP64
+    PCG solution to 1e-12 reported), for FP64
     Jacobi-PCG, mixed-precision PCG and learned FCG (with its Jacobi fallback)."""
     from gpufem_b200 import _lib
     from gpufem_b200 import meshgen as mg
@@ -241,7 +242,7 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 6):
             info = ctx.solve(solver, _lib.GF_F64, tol=1e-8, max_iter=400000, raise_on_error=False)
             err = float(np.linalg.norm(ctx.solution() - ustar) / nrm)
             row[name] = {"seconds": info.seconds, "iterations": info.iterations,
-                         "rel_err_vs_oracle": err, "status": info.status,
+                         "rel_err_vs_reference": err, "status": info.status,
                          **({"fallback": info.fallback} if name == "learned_fcg" else {})}
         results.append(row)
     ctx.close()
@@ -385,25 +386,31 @@ def run_gpu_arm(args):
         ctx.assemble(_lib.GF_F64, scatter)
         ctx.convert_f64_to_f32()     # symmetric FP32 copy for the mixed solver
         ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
-        ref = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-13, max_iter=400000,
+        # FP64 PCG stops on its recursive residual; on this system (log-normal E) the
+        # true residual it can reach is ~5e-10, so the comparison runs at 1e-8
+        ref = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-12, max_iter=400000,
                         raise_on_error=False)
         ustar = ctx.solution()
-        p64 = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-10, max_iter=400000,
+        p64 = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-8, max_iter=400000,
                         raise_on_error=False)
         u64 = ctx.solution()
-        mix = ctx.solve(_lib.GF_SOLVER_MIXED_PCG, tol=1e-10, max_iter=400000, inner_tol=1e-4,
-                        raise_on_error=False)
-        umix = ctx.solution()
         nrm = np.linalg.norm(ustar)
-        solve = {"oracle": {"solver": "FP64 Jacobi-PCG", "rel_residual": ref.rel_residual,
-                            "iterations": ref.iterations, "seconds": ref.seconds},
+        solve = {"reference_solution": {"solver": "FP64 Jacobi-PCG to 1e-12",
+                                        "rel_residual": ref.rel_residual,
+                                        "iterations": ref.iterations, "seconds": ref.seconds},
                  "pcg_fp64": {"seconds": p64.seconds, "iterations": p64.iterations,
                               "rel_residual": p64.rel_residual,
-                              "rel_err_vs_oracle": float(np.linalg.norm(u64 - ustar) / nrm)},
-                 "mixed_pcg": {"seconds": mix.seconds, "iterations": mix.iterations,
-                               "outer": mix.outer, "rel_residual": mix.rel_residual,
-                               "rel_err_vs_oracle": float(np.linalg.norm(umix - ustar) / nrm)},
-                 "tol": 1e-10}
+                              "rel_err_vs_reference": float(np.linalg.norm(u64 - ustar) / nrm)},
+                 "tol": 1e-8}
+        for name, solver in (("mixed_pcg", _lib.GF_SOLVER_MIXED_PCG),
+                             ("mixed_pcg32", _lib.GF_SOLVER_MIXED_PCG32)):
+            mix = ctx.solve(solver, tol=1e-8, max_iter=400000, inner_tol=1e-4,
+                            raise_on_error=False)
+            umix = ctx.solution()
+            solve[name] = {"seconds": mix.seconds, "iterations": mix.iterations,
+                           "outer": mix.outer, "fp64_fallback": mix.fallback,
+                           "status": mix.status, "rel_residual": mix.rel_residual,
+                           "rel_err_vs_reference": float(np.linalg.norm(umix - ustar) / nrm)}
 
     learned = None
     if not args.no_solve and rank == 0:

@@ -23,7 +23,7 @@ GF_F64, GF_F32 = 0, 1
 GF_SCATTER_COLOR, GF_SCATTER_ATOMIC, GF_SCATTER_OWNER = 0, 1, 2
 GF_ENGINE_CUDA_CORE, GF_ENGINE_TF32_MMA = 0, 1
 GF_BC_PENALTY, GF_BC_ELIMINATION = 0, 1
-GF_SOLVER_CG, GF_SOLVER_PCG, GF_SOLVER_MIXED_PCG, GF_SOLVER_LEARNED_FCG = 0, 1, 2, 3
+GF_SOLVER_CG, GF_SOLVER_PCG, GF_SOLVER_MIXED_PCG, GF_SOLVER_LEARNED_FCG, GF_SOLVER_MIXED_PCG32 = 0, 1, 2, 3, 4
 
 
 class SolveOpts(C.Structure):

@@ -190,12 +190,11 @@ struct gf_ctx {
 
   // sliced-ELL copy for the solver's SpMVs (gf_sell.cu)
   bool sell_ready = false;
-  int sell_nslice = 0, sell_nslots = 0;
+  int sell_nslice = 0, sell_nslots = 0;  // slices of 32 rows; nslots = 32 * nslice
   int64_t sell_total = 0;
   int64_t sell_ver64 = -1, sell_ver32 = -1;
-  int32_t* d_sell_perm = nullptr;  // [nslots] row of each slot, -1 = padding
-  int64_t* d_sell_off = nullptr;   // [nslice + 1]
-  int32_t* d_sell_w = nullptr;     // [nslice]
+  int64_t* d_sell_off = nullptr;   // [nslice + 1] first entry of each slice
+  int32_t* d_sell_w = nullptr;     // [nslice] width of each slice
   int32_t* d_sell_col = nullptr;   // [total]
   double* d_sell_v64 = nullptr;
   float* d_sell_v32 = nullptr;

@@ -1,16 +1,16 @@
-// Sliced ELL (SELL-32-sigma) copy of K for the solver's SpMVs.
+// Sliced ELL (SELL-32) copy of K for the solver's SpMVs.
 //
-// The column-major ELL of the reference layout (ELLmatrix.h:35-44) pads every row
-// to the global width W, and neighbouring rows of different length share 32-byte
-// sectors, so a warp streams about W*n entries instead of nnz (Q8: corner-node rows
-// have 42 entries, mid-side rows 26, interleaved).  The solver therefore keeps a
-// second copy: rows sorted by length (descending, stable) inside windows of
-// kSigma rows, cut into slices of 32 rows, each slice padded only to its own
-// longest row and stored slot-major (entry s of lane l at off[k] + 32 s + l).
-// A warp then reads 128 contiguous bytes per slot with no idle lanes.  Padding
-// entries hold column = the row itself and value 0.  The ELL stays the layout of
-// the API (views, downloads, assembly, constraints); values are re-sliced only
-// when the matrix changed since the last conversion.
+// The column-major ELL of the reference layout (ELLmatrix.h:35-44) puts entry s of
+// row r at s*n + r: a warp's loads for one slot are coalesced, but the W slots of a
+// row sit n entries apart, so every step of the row loop opens new DRAM pages, and
+// lanes whose rows are shorter idle inside partially used sectors.  The solver
+// therefore keeps a second copy cut into slices of 32 consecutive rows, each slice
+// padded only to its own longest row and stored slot-major and contiguous (entry s
+// of lane l at off[k] + 32 s + l).  Rows keep their order, so vectors are indexed as
+// in the ELL.  Padding entries hold column = the row itself and value 0, which lets
+// every lane of a slice run the same trip count.  The ELL stays the layout of the
+// API (views, downloads, assembly, constraints); values are re-sliced only when the
+// matrix changed since the last conversion.
 #include <cub/cub.cuh>
 #include <algorithm>
 
@@ -18,62 +18,33 @@
 
 namespace {
 
-constexpr int kSigma = 1024;
-constexpr int kMaxBucket = 256;  // lengths sorted when W < 256, else window kept in order
-
-__global__ void k_sell_sort(int n, int nslots, int W, const int32_t* __restrict__ rownnz,
-                            int32_t* __restrict__ perm) {
-  const int win = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r0 = win * kSigma;
-  if (r0 >= nslots) return;
-  const int r1 = min(r0 + kSigma, nslots);
-  if (W >= kMaxBucket) {
-    for (int r = r0; r < r1; ++r) perm[r] = r < n ? r : -1;
-    return;
-  }
-  int cnt[kMaxBucket + 1];
-  for (int b = 0; b <= W; ++b) cnt[b] = 0;
-  for (int r = r0; r < min(r1, n); ++r) cnt[W - rownnz[r]]++;
-  int acc = 0;
-  for (int b = 0; b <= W; ++b) {
-    const int c = cnt[b];
-    cnt[b] = acc;
-    acc += c;
-  }
-  for (int r = r0; r < min(r1, n); ++r) perm[r0 + cnt[W - rownnz[r]]++] = r;
-  for (int r = r0 + acc; r < r1; ++r) perm[r] = -1;
-}
-
-__global__ void k_sell_width(int nslice, const int32_t* __restrict__ perm,
-                             const int32_t* __restrict__ rownnz, int64_t* __restrict__ wsz,
-                             int32_t* __restrict__ width) {
+__global__ void k_sell_width(int n, int nslice, const int32_t* __restrict__ rownnz,
+                             int64_t* __restrict__ wsz, int32_t* __restrict__ width) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nslice) return;
   int w = 0;
   for (int l = 0; l < 32; ++l) {
-    const int row = perm[k * 32 + l];
-    if (row >= 0) w = max(w, rownnz[row]);
+    const int row = k * 32 + l;
+    if (row < n) w = max(w, rownnz[row]);
   }
   width[k] = w;
   wsz[k] = (int64_t)w * 32;
 }
 
 template <typename TI, typename TO>
-__global__ void k_sell_fill(int n, int nslots, const int32_t* __restrict__ perm,
-                            const int64_t* __restrict__ off, const int32_t* __restrict__ width,
-                            const int32_t* __restrict__ rownnz, const TI* __restrict__ src,
-                            TO* __restrict__ dst, int is_col) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nslots) return;
-  const int k = t >> 5, lane = t & 31;
-  const int row = perm[t];
+__global__ void k_sell_fill(int n, int nslots, const int64_t* __restrict__ off,
+                            const int32_t* __restrict__ width, const int32_t* __restrict__ rownnz,
+                            const TI* __restrict__ src, TO* __restrict__ dst, int is_col) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;  // slot of the padded row range
+  if (row >= nslots) return;
+  const int k = row >> 5, lane = row & 31;
   const int w = width[k];
-  const int nz = row >= 0 ? rownnz[row] : 0;
+  const int nz = row < n ? rownnz[row] : 0;
   int64_t o = off[k] + lane;
   for (int s = 0; s < w; ++s, o += 32) {
     TO v;
     if (s < nz) v = (TO)src[(int64_t)s * n + row];
-    else v = is_col ? (TO)(row >= 0 ? row : 0) : (TO)0;
+    else v = is_col ? (TO)(row < n ? row : 0) : (TO)0;
     dst[o] = v;
   }
 }
@@ -81,7 +52,6 @@ __global__ void k_sell_fill(int n, int nslots, const int32_t* __restrict__ perm,
 }  // namespace
 
 void gf_sell_free(gf_ctx* ctx) {
-  gf_free(ctx->d_sell_perm);
   gf_free(ctx->d_sell_off);
   gf_free(ctx->d_sell_w);
   gf_free(ctx->d_sell_col);
@@ -104,16 +74,12 @@ gf_status gf_sell_prepare(gf_ctx* ctx, int dtype) {
     int64_t* wsz = nullptr;
     void* tmp = nullptr;
     size_t tb = 0;
-    if ((st = gf_alloc(ctx, &ctx->d_sell_perm, (size_t)nslots)) != GF_OK) return st;
     if ((st = gf_alloc(ctx, &ctx->d_sell_off, (size_t)nslice + 1)) != GF_OK) return st;
     if ((st = gf_alloc(ctx, &ctx->d_sell_w, (size_t)nslice)) != GF_OK) return st;
     if ((st = gf_alloc(ctx, &wsz, (size_t)nslice + 1)) != GF_OK) return st;
-    const int nwin = (nslots + kSigma - 1) / kSigma;
-    k_sell_sort<<<gf_blocks(nwin, 64), 64, 0, s>>>(n, nslots, ctx->W, ctx->d_rownnz,
-                                                   ctx->d_sell_perm);
-    k_sell_width<<<gf_blocks(nslice, 256), 256, 0, s>>>(nslice, ctx->d_sell_perm, ctx->d_rownnz,
-                                                        wsz, ctx->d_sell_w);
-    ctx->launches += 2;
+    k_sell_width<<<gf_blocks(nslice, 256), 256, 0, s>>>(n, nslice, ctx->d_rownnz, wsz,
+                                                        ctx->d_sell_w);
+    ctx->launches++;
     GF_CUDA(ctx, cudaMemsetAsync(wsz + nslice, 0, sizeof(int64_t), s));
     cub::DeviceScan::ExclusiveSum(nullptr, tb, wsz, ctx->d_sell_off, nslice + 1, s);
     if (cudaMalloc(&tmp, tb) != cudaSuccess) {
@@ -133,8 +99,8 @@ gf_status gf_sell_prepare(gf_ctx* ctx, int dtype) {
     ctx->sell_total = total;
     if ((st = gf_alloc(ctx, &ctx->d_sell_col, (size_t)std::max<int64_t>(total, 1))) != GF_OK) return st;
     k_sell_fill<int32_t, int32_t><<<gf_blocks(nslots, 256), 256, 0, s>>>(
-        n, nslots, ctx->d_sell_perm, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz,
-        ctx->d_colidx, ctx->d_sell_col, 1);
+        n, nslots, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz, ctx->d_colidx,
+        ctx->d_sell_col, 1);
     GF_LAUNCH_CHECK(ctx, "k_sell_fill(col)");
     ctx->sell_ready = true;
   }
@@ -142,16 +108,16 @@ gf_status gf_sell_prepare(gf_ctx* ctx, int dtype) {
   if (dtype == GF_F64 && ctx->sell_ver64 != ctx->kver64) {
     if (!ctx->d_sell_v64 && (st = gf_alloc(ctx, &ctx->d_sell_v64, total)) != GF_OK) return st;
     k_sell_fill<double, double><<<gf_blocks(ctx->sell_nslots, 256), 256, 0, s>>>(
-        n, ctx->sell_nslots, ctx->d_sell_perm, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz,
-        ctx->d_K64, ctx->d_sell_v64, 0);
+        n, ctx->sell_nslots, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz, ctx->d_K64,
+        ctx->d_sell_v64, 0);
     GF_LAUNCH_CHECK(ctx, "k_sell_fill(f64)");
     ctx->sell_ver64 = ctx->kver64;
   }
   if (dtype == GF_F32 && ctx->sell_ver32 != ctx->kver32) {
     if (!ctx->d_sell_v32 && (st = gf_alloc(ctx, &ctx->d_sell_v32, total)) != GF_OK) return st;
     k_sell_fill<float, float><<<gf_blocks(ctx->sell_nslots, 256), 256, 0, s>>>(
-        n, ctx->sell_nslots, ctx->d_sell_perm, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz,
-        ctx->d_K32, ctx->d_sell_v32, 0);
+        n, ctx->sell_nslots, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz, ctx->d_K32,
+        ctx->d_sell_v32, 0);
     GF_LAUNCH_CHECK(ctx, "k_sell_fill(f32)");
     ctx->sell_ver32 = ctx->kver32;
   }

@@ -54,65 +54,79 @@ __device__ inline double block_sum(T v, double* sh) {
   return s;  // valid in thread 0
 }
 
-// Where the solver's SpMVs find the matrix.  Two layouts share every kernel:
-//   ELL   (perm == nullptr): thread t owns row t; entry s at s*n + t.
-//   SELL  (perm != nullptr): thread t owns slot t of the sliced copy (gf_sell.cu):
-//         row perm[t] (-1 = padding slot), entry s at off[t/32] + 32 s + t%32.
-// Both walk a row's entries in slot order with the same four partial sums, so the
-// two layouts give bit-identical row dots.
+// Where the solver's SpMVs find the matrix.  Two layouts share every kernel, both
+// with thread t owning row t:
+//   ELL   (width == nullptr): entry s of row t at s*n + t, rownnz[t] entries.
+//   SELL  (width != nullptr): the sliced copy (gf_sell.cu); entry s of row t at
+//         off[t/32] + 32 s + t%32, and every row of a slice runs to the slice's
+//         width (padding entries hold column t and value 0).
 struct MatLayout {
-  int count;  // threads to launch: n (ELL) or the padded slot count (SELL)
+  int count;  // rows = threads to launch
   int n;
   const int32_t* __restrict__ rownnz;
   const int32_t* __restrict__ col;
-  const int32_t* __restrict__ perm;
+  const int32_t* __restrict__ width;
   const int64_t* __restrict__ off;
 
-  __device__ inline bool at(int t, int& row, int& nz, int64_t& o, int64_t& stride) const {
+  __device__ inline bool at(int t, int& nz, int64_t& o, int64_t& stride) const {
     if (t >= count) return false;
-    if (perm) {
-      row = __ldg(perm + t);
-      if (row < 0) return false;
+    if (width) {
+      nz = __ldg(width + (t >> 5));
       o = __ldg(off + (t >> 5)) + (t & 31);
       stride = 32;
     } else {
-      row = t;
+      nz = __ldg(rownnz + t);
       o = t;
       stride = n;
     }
-    nz = __ldg(rownnz + row);
     return true;
   }
 };
 
-// Row dot sum_{s < nz} val[o + s*stride] * x[col[o + s*stride]].
+// Row dot sum_{s < nz} val[o + s*stride] * x[col[o + s*stride]], software-pipelined:
+// the next four (column, value) pairs are loaded before the x gathers of the current
+// four, so a thread keeps eight matrix loads in flight across its gathers.
 template <typename TK, typename TX>
 __device__ inline double row_dot(int64_t o, int64_t stride, int nz, const int32_t* __restrict__ col,
                                  const TK* __restrict__ val, const TX* __restrict__ x) {
   using Acc = typename std::conditional<sizeof(TK) == 8 || sizeof(TX) == 8, double, float>::type;
   Acc a0 = 0, a1 = 0, a2 = 0, a3 = 0;
   int s = 0;
-  for (; s + 4 <= nz; s += 4, o += 4 * stride) {
-    const int c0 = __ldg(col + o), c1 = __ldg(col + o + stride), c2 = __ldg(col + o + 2 * stride),
-              c3 = __ldg(col + o + 3 * stride);
-    const TK v0 = __ldg(val + o), v1 = __ldg(val + o + stride), v2 = __ldg(val + o + 2 * stride),
-             v3 = __ldg(val + o + 3 * stride);
+  if (nz >= 4) {
+    int c0 = __ldcs(col + o), c1 = __ldcs(col + o + stride), c2 = __ldcs(col + o + 2 * stride),
+        c3 = __ldcs(col + o + 3 * stride);
+    TK v0 = __ldcs(val + o), v1 = __ldcs(val + o + stride), v2 = __ldcs(val + o + 2 * stride),
+       v3 = __ldcs(val + o + 3 * stride);
+    for (s = 4; s + 4 <= nz; s += 4) {
+      o += 4 * stride;
+      const int d0 = __ldcs(col + o), d1 = __ldcs(col + o + stride),
+                d2 = __ldcs(col + o + 2 * stride), d3 = __ldcs(col + o + 3 * stride);
+      const TK w0 = __ldcs(val + o), w1 = __ldcs(val + o + stride),
+               w2 = __ldcs(val + o + 2 * stride), w3 = __ldcs(val + o + 3 * stride);
+      a0 += (Acc)v0 * (Acc)__ldg(x + c0);
+      a1 += (Acc)v1 * (Acc)__ldg(x + c1);
+      a2 += (Acc)v2 * (Acc)__ldg(x + c2);
+      a3 += (Acc)v3 * (Acc)__ldg(x + c3);
+      c0 = d0; c1 = d1; c2 = d2; c3 = d3;
+      v0 = w0; v1 = w1; v2 = w2; v3 = w3;
+    }
     a0 += (Acc)v0 * (Acc)__ldg(x + c0);
     a1 += (Acc)v1 * (Acc)__ldg(x + c1);
     a2 += (Acc)v2 * (Acc)__ldg(x + c2);
     a3 += (Acc)v3 * (Acc)__ldg(x + c3);
+    o += 4 * stride;
   }
-  for (; s < nz; ++s, o += stride) a0 += (Acc)__ldg(val + o) * (Acc)__ldg(x + __ldg(col + o));
+  for (; s < nz; ++s, o += stride) a0 += (Acc)__ldcs(val + o) * (Acc)__ldg(x + __ldcs(col + o));
   return (double)((a0 + a1) + (a2 + a3));
 }
 
 template <typename TK, typename TX, typename TY>
 __global__ void __launch_bounds__(kT)
 k_spmv(MatLayout L, const TK* __restrict__ val, const TX* __restrict__ x, TY* __restrict__ y) {
-  int row, nz;
+  const int row = blockIdx.x * kT + threadIdx.x;
+  int nz;
   int64_t o, st;
-  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st))
-    y[row] = (TY)row_dot(o, st, nz, L.col, val, x);
+  if (L.at(row, nz, o, st)) y[row] = (TY)row_dot(o, st, nz, L.col, val, x);
 }
 
 // r = f - K u (FP64), and r.r
@@ -120,10 +134,11 @@ __global__ void __launch_bounds__(kT)
 k_residual64(MatLayout L, const double* __restrict__ val, const double* __restrict__ u,
              const double* __restrict__ f, double* __restrict__ r, double* __restrict__ acc) {
   __shared__ double sh[32];
-  int row, nz;
+  const int row = blockIdx.x * kT + threadIdx.x;
+  int nz;
   int64_t o, st;
   double rr = 0.0;
-  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st)) {
+  if (L.at(row, nz, o, st)) {
     double v = f[row] - row_dot(o, st, nz, L.col, val, u);
     r[row] = v;
     rr = v * v;
@@ -176,10 +191,11 @@ k_cg_spmv_dot(MatLayout L, const TK* __restrict__ val, const V* __restrict__ p,
     sc->rzn = 0.0;
     sc->rr = 0.0;
   }
-  int row, nz;
+  const int row = blockIdx.x * kT + threadIdx.x;
+  int nz;
   int64_t o, st;
   double pq = 0.0;
-  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st)) {
+  if (L.at(row, nz, o, st)) {
     double v = row_dot(o, st, nz, L.col, val, p);
     q[row] = (V)v;
     pq = (double)p[row] * (double)(V)v;
@@ -250,18 +266,6 @@ __global__ void k_diag_inv(int n, const int32_t* __restrict__ rownnz,
     if (col[o] == row) { d = (double)val[o]; break; }
   }
   dinv[row] = (d != 0.0) ? (V)(1.0 / d) : V(1);
-}
-
-__global__ void k_scale_to_f32(int n, const double* __restrict__ a, double s,
-                               float* __restrict__ b) {
-  const int i = blockIdx.x * kT + threadIdx.x;
-  if (i < n) b[i] = (float)(a[i] * s);
-}
-
-__global__ void k_axpy_f32_into_f64(int n, double alpha, const float* __restrict__ d,
-                                    double* __restrict__ u) {
-  const int i = blockIdx.x * kT + threadIdx.x;
-  if (i < n) u[i] += alpha * (double)d[i];
 }
 
 template <typename V>
@@ -340,8 +344,7 @@ __global__ void k_zero_fixed(int n, const uint8_t* __restrict__ fixed, double* _
 gf_status solver_matrix(gf_ctx* ctx, int dtype, MatLayout* L, const void** val) {
   gf_status st = gf_sell_prepare(ctx, dtype);
   if (st != GF_OK) return st;
-  *L = MatLayout{ctx->sell_nslots, ctx->n, ctx->d_rownnz, ctx->d_sell_col, ctx->d_sell_perm,
-                 ctx->d_sell_off};
+  *L = MatLayout{ctx->n, ctx->n, ctx->d_rownnz, ctx->d_sell_col, ctx->d_sell_w, ctx->d_sell_off};
   *val = dtype == GF_F64 ? (const void*)ctx->d_sell_v64 : (const void*)ctx->d_sell_v32;
   return GF_OK;
 }
@@ -550,35 +553,40 @@ gf_status status_of(int done) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Mixed precision: FP32 Jacobi-PCG whose residual is recomputed in FP64
-// ("reliable updates").  Vectors x, r, z, p, q are FP32 and scaled by the norm
-// sigma of the FP64 residual at the last update; the solution accumulates in
-// FP64 (u += sigma x).  When the FP32 residual has dropped by 10x since the last
-// update (or the recursion reports convergence / breakdown / the iteration cap),
-// the host triggers an update: u += sigma x, r64 = f - K64 u in FP64, and the
-// FP32 residual restarts from r64 / ||r64|| with the search direction rescaled and
-// kept, so the Krylov process continues instead of restarting.  Convergence is
-// decided on the true FP64 residual only.
+// Mixed precision: Jacobi-PCG on the FP32 matrix K32 whose residual is recomputed
+// on the FP64 matrix ("reliable updates").  The vectors x, r, z, p, q are FP64
+// (GF_SOLVER_MIXED_PCG) or FP32 (GF_SOLVER_MIXED_PCG32); they are scaled by the
+// norm sigma of the FP64 residual at the last update, and the solution
+// accumulates in FP64 (u += sigma x).  When the recursive residual has dropped by
+// 10x since the last update (or the recursion reports convergence / breakdown /
+// the iteration cap, or a segment ran longer than its cap), the host triggers an
+// update: u += sigma x, r64 = f - K64 u in FP64, and the recursion continues from
+// r64 / ||r64|| with the search direction rescaled and kept, so the Krylov process
+// is not restarted.  Convergence is decided on the true FP64 residual only.  When
+// the true residual stops halving between updates (the rounding of K to FP32
+// matters at this condition number), the correction is finished by FP64 PCG.
 namespace {
 
-__global__ void k_mixed_accumulate(int n, double sigma, float* __restrict__ x,
+template <typename V>
+__global__ void k_mixed_accumulate(int n, double sigma, V* __restrict__ x,
                                    double* __restrict__ u) {
   const int i = blockIdx.x * kT + threadIdx.x;
   if (i < n) {
     u[i] += sigma * (double)x[i];
-    x[i] = 0.f;
+    x[i] = V(0);
   }
 }
 
-__global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv, float pscale,
-                              int restart, const float* __restrict__ dinv, float* __restrict__ r,
-                              float* __restrict__ z, float* __restrict__ p, SolveScalars* sc) {
+template <typename V>
+__global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv, V pscale,
+                              int restart, const V* __restrict__ dinv, V* __restrict__ r,
+                              V* __restrict__ z, V* __restrict__ p, SolveScalars* sc) {
   __shared__ double sh[32];
   const int i = blockIdx.x * kT + threadIdx.x;
   double rz = 0.0, rr = 0.0;
   if (i < n) {
-    const float ri = (float)(r64[i] * inv);
-    const float zi = ri * dinv[i];
+    const V ri = (V)(r64[i] * inv);
+    const V zi = ri * dinv[i];
     r[i] = ri;
     z[i] = zi;
     p[i] = restart ? zi : p[i] * pscale;
@@ -589,6 +597,12 @@ __global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv,
   if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
   double s2 = block_sum(rr, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
+template <typename V>
+__global__ void k_scale_to(int n, const double* __restrict__ a, double s, V* __restrict__ b) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) b[i] = (V)(a[i] * s);
 }
 
 __global__ void k_add64(int n, const double* __restrict__ d, double* __restrict__ u) {
@@ -602,6 +616,7 @@ __global__ void k_mixed_scalars(SolveScalars* sc, double tol2) {
   sc->done = sc->iter >= sc->maxit ? 3 : 0;
 }
 
+template <typename V>
 gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
                     std::chrono::steady_clock::time_point t0, gf_solve_info* info) {
   const int n = ctx->n;
@@ -610,9 +625,9 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   SolveScalars* sc = ctx->d_scal;
   SolveScalars* hs = (SolveScalars*)ctx->h_pinned;
   double* r64 = (double*)ctx->d_work;
-  float* v = (float*)(r64 + n);
-  float *x = v, *r = v + n, *z = v + 2 * (size_t)n, *p = v + 3 * (size_t)n, *q = v + 4 * (size_t)n;
-  float* dinv = v + 5 * (size_t)n;
+  V* v = reinterpret_cast<V*>(r64 + n);
+  V *x = v, *r = v + n, *z = v + 2 * (size_t)n, *p = v + 3 * (size_t)n, *q = v + 4 * (size_t)n;
+  V* dinv = v + 5 * (size_t)n;
   const double tol = o->tol;
   const double delta2 = 0.01;  // update when ||r|| fell 10x since the last update
   gf_status st;
@@ -621,7 +636,7 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   if ((st = solver_matrix(ctx, GF_F32, &L32, &v32)) != GF_OK) return st;
   if ((st = solver_matrix(ctx, GF_F64, &L64, &v64)) != GF_OK) return st;
   const float* val32 = (const float*)v32;
-  k_diag_inv<float, float><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32, dinv);
+  k_diag_inv<double, V><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_LAUNCH_CHECK(ctx, "k_diag_inv");
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u, 0, sizeof(double) * n, s));
   double ff = 0.0;
@@ -631,10 +646,10 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   bool fp64_fallback = false;
   if (ff > 0.0) {
     double sigma = std::sqrt(ff);
-    k_scale_to_f32<<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
-    GF_LAUNCH_CHECK(ctx, "k_scale_to_f32");
+    k_scale_to<V><<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
+    GF_LAUNCH_CHECK(ctx, "k_scale_to");
     GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
-    k_cg_init<float><<<nb, kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
+    k_cg_init<V><<<nb, kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
     GF_LAUNCH_CHECK(ctx, "k_cg_init");
     k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
     GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
@@ -642,9 +657,9 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     cudaGraphExec_t exec = nullptr;
     GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < check; ++k) {
-      k_cg_spmv_dot<float, float><<<gf_blocks(L32.count, kT), kT, 0, s>>>(L32, val32, p, q, sc);
-      k_cg_update<float><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
-      k_cg_direction<float><<<nb, kT, 0, s>>>(n, z, p, sc);
+      k_cg_spmv_dot<float, V><<<gf_blocks(L32.count, kT), kT, 0, s>>>(L32, val32, p, q, sc);
+      k_cg_update<V><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+      k_cg_direction<V><<<nb, kT, 0, s>>>(n, z, p, sc);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (ce != cudaSuccess) return gf_cuda_fail(ctx, ce, "graph capture");
@@ -654,7 +669,10 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       return gf_cuda_fail(ctx, ce, "graph instantiate");
     }
     double rr_max = 1.0, prev_rr64 = ff;
-    int breakdowns = 0, stagnant = 0;
+    int breakdowns = 0, stagnant = 0, seg_start = 0;
+    // a segment between updates longer than this is cut short, so that a recursion
+    // that no longer reduces its residual still reaches the stagnation test
+    const int seg_cap = std::max(1000, 2 * (int)std::sqrt((double)n));
     done_code = 3;
     for (;;) {
       ce = cudaGraphLaunch(exec, s);
@@ -668,12 +686,13 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       // the FP32 recursion is diverging (K32 nearly indefinite for very ill-conditioned
       // systems): update and restart the direction
       const bool diverging = hs->done == 0 && hs->rr > 1e4;
-      if (hs->done == 0 && hs->rr > delta2 * rr_max && !timeout && !diverging) {
+      const bool long_segment = hs->iter - seg_start >= seg_cap;
+      if (hs->done == 0 && hs->rr > delta2 * rr_max && !timeout && !diverging && !long_segment) {
         rr_max = std::max(rr_max, hs->rr);
         continue;
       }
       // reliable update
-      k_mixed_accumulate<<<nb, kT, 0, s>>>(n, sigma, x, ctx->d_u);
+      k_mixed_accumulate<V><<<nb, kT, 0, s>>>(n, sigma, x, ctx->d_u);
       ce = cudaGetLastError();
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "k_mixed_accumulate"); break; }
       ctx->launches++;
@@ -682,7 +701,8 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       if (std::sqrt(rr64 / ff) <= tol) { done_code = 1; break; }
       if (hs->done == 3 || timeout) { done_code = 3; break; }
       // the true residual must at least halve between updates; three misses in a
-      // row mean FP32 cannot resolve this system (condition ~ 1/eps32): finish in FP64
+      // row mean the FP32 matrix (or FP32 recursion) cannot resolve this system: finish
+      // in FP64
       stagnant = rr64 > 0.25 * prev_rr64 ? stagnant + 1 : 0;
       prev_rr64 = rr64;
       if (stagnant >= 3) { fp64_fallback = true; break; }
@@ -691,14 +711,15 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       const double sigma_new = std::sqrt(rr64);
       ce = cudaMemsetAsync(&sc->rzn, 0, 2 * sizeof(double), s);  // rzn, rr
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "reset"); break; }
-      k_mixed_reset<<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma_new, (float)(sigma / sigma_new),
-                                      restart ? 1 : 0, dinv, r, z, p, sc);
+      k_mixed_reset<V><<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma_new, (V)(sigma / sigma_new),
+                                         restart ? 1 : 0, dinv, r, z, p, sc);
       k_mixed_scalars<<<1, 1, 0, s>>>(sc, tol * tol * ff / rr64);
       ce = cudaGetLastError();
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "k_mixed_reset"); break; }
       ctx->launches += 2;
       sigma = sigma_new;
       rr_max = 1.0;
+      seg_start = hs->iter;
     }
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
@@ -827,10 +848,11 @@ k_fcg_spmv(MatLayout L, const double* __restrict__ val, const double* __restrict
   __shared__ double sh[32];
   if (sc->done) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) sc->rr = 0.0;
-  int row, nz;
+  const int row = blockIdx.x * kT + threadIdx.x;
+  int nz;
   int64_t o, st;
   double pq = 0.0, pr = 0.0;
-  if (L.at(blockIdx.x * kT + threadIdx.x, row, nz, o, st)) {
+  if (L.at(row, nz, o, st)) {
     const double v = row_dot(o, st, nz, L.col, val, p);
     q[row] = v;
     pq = p[row] * v;
@@ -1053,7 +1075,7 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
 gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info) {
   *info = gf_solve_info{};
   const int solver = o->solver;
-  if (solver < GF_SOLVER_CG || solver > GF_SOLVER_LEARNED_FCG)
+  if (solver < GF_SOLVER_CG || solver > GF_SOLVER_MIXED_PCG32)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown solver %d", solver);
   if (!(o->tol > 0.0)) return gf_fail(ctx, GF_ERR_INVALID_ARG, "tol must be > 0");
   const int maxit = o->max_iter > 0 ? o->max_iter : 10000;
@@ -1139,10 +1161,11 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
     return (gf_status)info->status;
   }
 
-  // MIXED_PCG: FP32 Jacobi-PCG on K32 with FP64 reliable updates on K64
+  // MIXED_PCG / MIXED_PCG32: Jacobi-PCG on K32 with FP64 reliable updates on K64
   if (!ctx->has64 || !ctx->has32)
     return gf_fail(ctx, GF_ERR_STATE, "mixed solve needs both FP64 and FP32 matrices");
-  return run_mixed(ctx, o, maxit, check, t0, info);
+  if (solver == GF_SOLVER_MIXED_PCG32) return run_mixed<float>(ctx, o, maxit, check, t0, info);
+  return run_mixed<double>(ctx, o, maxit, check, t0, info);
 }
 
 // ---------------------------------------------------------------------------

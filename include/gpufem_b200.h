@@ -86,11 +86,15 @@ typedef enum gf_solver {
   GF_SOLVER_CG = 0,          /* reference CPU_CG semantics: plain CG, x0 = 0, stop on
                                 r.r <= eps^2 * r0.r0; runs in the dtype of `matrix`      */
   GF_SOLVER_PCG = 1,         /* Jacobi-preconditioned CG in the dtype of `matrix`        */
-  GF_SOLVER_MIXED_PCG = 2,   /* FP64 iterative refinement (r = f - K64 u in FP64) around
-                                an FP32 Jacobi-PCG inner solve on K32                     */
-  GF_SOLVER_LEARNED_FCG = 3  /* as MIXED_PCG, inner solve = FP32 flexible CG with the
-                                learned (message-passing) preconditioner, falling back to
-                                Jacobi-PCG when it stalls                                */
+  GF_SOLVER_MIXED_PCG = 2,   /* Jacobi-PCG whose SpMVs read the FP32 matrix K32, with
+                                FP64 vectors and FP64 residual replacement on K64
+                                (r = f - K64 u) every 10x drop; finishes in FP64 PCG when
+                                the true residual stops falling. Needs K64 and K32.       */
+  GF_SOLVER_LEARNED_FCG = 3, /* FP64 flexible CG on K64 with the learned (message-passing)
+                                preconditioner, falling back to Jacobi-PCG when it breaks
+                                down or stalls. Needs K64 and gf_lp_init.                 */
+  GF_SOLVER_MIXED_PCG32 = 4  /* as MIXED_PCG with FP32 vectors as well (half the vector
+                                traffic; for moderately conditioned systems)              */
 } gf_solver;
 
 typedef struct gf_solve_opts {

@@ -139,10 +139,11 @@ def test_pcg_and_mixed_match_oracle(Context, oracle, name):
     # a little above it in finite precision
     assert info.rel_residual <= 1e-11
     assert np.linalg.norm(u - ustar) <= 1e-8 * np.linalg.norm(ustar)
-    info = ctx.solve(_lib.GF_SOLVER_MIXED_PCG, tol=1e-12, max_iter=200000, inner_tol=1e-4)
-    u2 = ctx.solution()
-    assert info.rel_residual <= 1e-12 and info.outer >= 2
-    assert np.linalg.norm(u2 - ustar) <= 1e-8 * np.linalg.norm(ustar)
+    for solver in (_lib.GF_SOLVER_MIXED_PCG, _lib.GF_SOLVER_MIXED_PCG32):
+        info = ctx.solve(solver, tol=1e-12, max_iter=200000, inner_tol=1e-4)
+        u2 = ctx.solution()
+        assert info.rel_residual <= 1e-12 and info.outer >= 2, (solver, info)
+        assert np.linalg.norm(u2 - ustar) <= 1e-8 * np.linalg.norm(ustar), solver
 
 
 def test_fp32_pcg_and_spmv_vs_oracle(Context, oracle):
