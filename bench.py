@@ -324,7 +324,7 @@ def run_gpu_arm(args):
     achieved = alg_bytes / per_step / 1e9
     traffic = None
     tfile = ROOT / "profiles" / "ncu_traffic.json"
-    if tfile.exists():
+    if tfile.exists() and args.scatter == "owner":
         tr = json.loads(tfile.read_text()).get(f"{cfg}/assemble")
         traffic = None if tr is None else tr.get("bytes_per_assembly")
 
@@ -432,7 +432,8 @@ def run_gpu_arm(args):
                        "between timed steps", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "kernel": {"owner": "k_assemble_owner (one launch)",
+                         "kernel": {"owner": "k_elem_geometry + k_assemble_owner (one "
+                                             "launch each, timed together)",
                                     "colour": "k_assemble colour passes + K zero-fill",
                                     "atomic": "k_assemble atomic + K zero-fill"}[args.scatter],
                          "algorithmic_bytes": alg_bytes, "peak_source": peak_kind},
