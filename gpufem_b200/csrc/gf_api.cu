@@ -8,19 +8,6 @@
 
 #include "gf_internal.cuh"
 
-const signed char gf_node_nat_host[4][GF_MAX_NEN][3] = {
-    // Q4
-    {{-1, -1, 0}, {1, -1, 0}, {1, 1, 0}, {-1, 1, 0}},
-    // Q8
-    {{-1, -1, 0}, {0, -1, 0}, {1, -1, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {-1, 1, 0}, {-1, 0, 0}},
-    // Brick8
-    {{1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {1, -1, 1}, {-1, -1, -1}, {-1, 1, -1}, {-1, 1, 1}, {-1, -1, 1}},
-    // Brick20
-    {{1, -1, -1}, {1, 0, -1}, {1, 1, -1}, {1, 1, 0}, {1, 1, 1}, {1, 0, 1}, {1, -1, 1}, {1, -1, 0},
-     {0, -1, -1}, {0, 1, -1}, {0, 1, 1}, {0, -1, 1},
-     {-1, -1, -1}, {-1, 0, -1}, {-1, 1, -1}, {-1, 1, 0}, {-1, 1, 1}, {-1, 0, 1}, {-1, -1, 1}, {-1, -1, 0}},
-};
-
 gf_status gf_fail(gf_ctx* ctx, gf_status st, const char* fmt, ...) {
   if (ctx) {
     char buf[512];

@@ -16,7 +16,9 @@
 //                    H_j = sum_gp (w detJ E) g_i g_j^T, g = J^-1 dN, for the block
 //                    row i_a of Ke(e) and adds each block into the tile at the
 //                    neighbour slot of node j (shared-memory atomics: two elements
-//                    around a can hit the same slot).  The tile is then written to
+//                    around a can hit the same slot).  A task is split into work
+//                    items of JG element nodes j each, so that 3-D blocks, which own
+//                    few nodes, still give every thread work.  The tile is then written to
 //                    K: for each slot the CTA's rows are contiguous in the
 //                    column-major ELL, so the stores coalesce, and padding slots
 //                    get their zeros.
@@ -29,6 +31,7 @@
 // scatter of StiffAlgo::AssembleK (src/FEM/StiffAlgo.cc:304-401), by rows.
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "gf_elem.cuh"
 
@@ -120,8 +123,10 @@ k_elem_geometry(int nelem, int ngp, int EB, const int32_t* __restrict__ conn,
 }
 
 // ---------------------------------------------------------------------------
-// JG element nodes per pass (register budget: JG * dim^2 accumulators).
-template <int ET, typename TC, int JG>
+// One work item per (task, group of JG element nodes j): a task's NEN/JG items run
+// on neighbouring lanes and read the same element data.  The owning node of every
+// task is found once per CTA (binary search in the CTA's incidence offsets).
+template <int ET, typename TC, int JG, int NG1>
 __global__ void __launch_bounds__(kOT)
 k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
                  const int32_t* __restrict__ inc_off, const int32_t* __restrict__ inc,
@@ -130,6 +135,7 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
                  const AsmTables* __restrict__ tab, TC lam1, TC mu1, TC* __restrict__ K) {
   constexpr ElemInfo info = gf_elem_info(ET);
   constexpr int NEN = info.nen, DIM = info.dim, GS = DIM * DIM + 1;
+  constexpr int NJ = NEN / JG;
   static_assert(NEN % JG == 0, "node groups must tile the element");
   const bool f64 = sizeof(TC) == 8;
   const int RB = NB * DIM;
@@ -137,6 +143,7 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
   TC* tile = reinterpret_cast<TC*>(smem_raw);       // [W][RB]
   TC* sdN = tile + (size_t)W * RB;                  // [ngp][DIM][NEN]
   int* soff = reinterpret_cast<int*>(sdN + ngp * DIM * NEN);  // [NB + 1]
+  uint8_t* sal = reinterpret_cast<uint8_t*>(soff + NB + 1);    // [tasks] owning node
 
   const int a0 = blockIdx.x * NB;
   const int a1 = min(a0 + NB, nnodes);
@@ -147,29 +154,75 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
   __syncthreads();
   const int q0 = soff[0];
   const int T = soff[a1 - a0] - q0;
-
   for (int t = threadIdx.x; t < T; t += kOT) {
-    int lo = 0, hi = a1 - a0;  // owned node of this incidence entry
+    int lo = 0, hi = a1 - a0;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
       if (soff[mid] - q0 <= t) lo = mid; else hi = mid;
     }
-    const int al = lo;
+    sal[t] = (uint8_t)lo;
+  }
+  __syncthreads();
+
+  for (int w = threadIdx.x; w < T * NJ; w += kOT) {
+    const int t = w / NJ;
+    const int j0 = (w - t * NJ) * JG;
+    const int al = sal[t];
     const int q = q0 + t;
     const int e = inc[q];
     const int i = inc_loc[q];
     const TC Ee = Eel[e];
     const TC* ge = geo + (int64_t)e * ngp * GS;
     const uint16_t* slots = inc_slot + (int64_t)q * NEN;
-#pragma unroll 1
-    for (int j0 = 0; j0 < NEN; j0 += JG) {
-      TC H[JG][DIM][DIM];
+    TC H[JG][DIM][DIM];
 #pragma unroll
-      for (int jj = 0; jj < JG; ++jj)
+    for (int jj = 0; jj < JG; ++jj)
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) H[jj][a][b] = TC(0);
+    if constexpr (NG1 > 0 && JG == NEN) {
+      // Gauss rule known at compile time and the whole element in one item: every
+      // dN_j value is an instruction constant (only the owned node's row is read
+      // from shared memory)
+      constexpr GpTable<ET, NG1> Tab = gf_gp_table<ET, NG1>();
+#pragma unroll
+      for (int g = 0; g < GpTable<ET, NG1>::NGP; ++g) {
+        TC Ji[DIM][DIM];
 #pragma unroll
         for (int a = 0; a < DIM; ++a)
 #pragma unroll
-          for (int b = 0; b < DIM; ++b) H[jj][a][b] = TC(0);
+          for (int b = 0; b < DIM; ++b) Ji[a][b] = __ldg(ge + g * GS + a * DIM + b);
+        const TC wd = __ldg(ge + g * GS + DIM * DIM) * Ee;
+        const TC* dN = sdN + g * DIM * NEN;
+        TC gi[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          TC s = TC(0);
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i];
+          gi[c] = s * wd;
+        }
+#pragma unroll
+        for (int j = 0; j < NEN; ++j) {
+          TC gj[DIM];
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) {
+            TC s = TC(0);
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) {
+              const int q = (g * DIM + a) * NEN + j;
+              s += Ji[c][a] * (sizeof(TC) == 8 ? TC(Tab.d64[q]) : TC(Tab.d32[q]));
+            }
+            gj[c] = s;
+          }
+#pragma unroll
+          for (int a = 0; a < DIM; ++a)
+#pragma unroll
+            for (int b = 0; b < DIM; ++b) H[j][a][b] += gi[a] * gj[b];
+        }
+      }
+    } else {
 #pragma unroll 1
       for (int g = 0; g < ngp; ++g) {
         TC Ji[DIM][DIM];
@@ -204,42 +257,44 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
             for (int b = 0; b < DIM; ++b) H[jj][a][b] += gi[a] * gj[b];
         }
       }
+    }
 #pragma unroll
-      for (int jj = 0; jj < JG; ++jj) {
-        const int p = slots[j0 + jj];
-        TC tr = TC(0);
+    for (int jj = 0; jj < JG; ++jj) {
+      const int p = slots[j0 + jj];
+      TC tr = TC(0);
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) tr += H[jj][a][a];
+      for (int a = 0; a < DIM; ++a) tr += H[jj][a][a];
 #pragma unroll
-        for (int a = 0; a < DIM; ++a)
+      for (int a = 0; a < DIM; ++a)
 #pragma unroll
-          for (int b = 0; b < DIM; ++b) {
-            TC v = lam1 * H[jj][a][b] + mu1 * H[jj][b][a];
-            if (a == b) v += mu1 * tr;
-            atomicAdd(&tile[(size_t)(p * DIM + b) * RB + al * DIM + a], v);
-          }
-      }
+        for (int b = 0; b < DIM; ++b) {
+          TC v = lam1 * H[jj][a][b] + mu1 * H[jj][b][a];
+          if (a == b) v += mu1 * tr;
+          atomicAdd(&tile[(size_t)(p * DIM + b) * RB + al * DIM + a], v);
+        }
     }
   }
   __syncthreads();
+  // flush: warp w stores slots w, w + 8, ...; lanes stride the block's rows
   const int rows = (a1 - a0) * DIM;
   const int64_t row0 = (int64_t)a0 * DIM;
-  for (int idx = threadIdx.x; idx < W * RB; idx += kOT) {
-    const int s = idx / RB, r = idx % RB;
-    if (r < rows) K[(int64_t)s * n + row0 + r] = tile[idx];
-  }
+  for (int s = threadIdx.x >> 5; s < W; s += kOT >> 5)
+    for (int r = threadIdx.x & 31; r < rows; r += 32)
+      K[(int64_t)s * n + row0 + r] = tile[(size_t)s * RB + r];
 }
 
 template <int ET, typename TC>
-size_t owner_smem_bytes(int NB, int W, int ngp) {
+size_t owner_smem_bytes(int NB, int W, int ngp, int maxval) {
   constexpr ElemInfo info = gf_elem_info(ET);
   return sizeof(TC) * ((size_t)W * NB * info.dim + (size_t)ngp * info.dim * info.nen) +
-         sizeof(int) * (NB + 1) + 16;
+         sizeof(int) * (NB + 1) + (size_t)NB * maxval + 16;
 }
 
-template <int ET>
+// element nodes per work item: the whole element for Q4, Q8 and Brick8; for Brick20
+// (a CTA owns few nodes) 5 in FP32 and 2 in FP64 (measured on Brick20 64^3)
+template <int ET, typename TC>
 constexpr int owner_jgroup() {
-  return gf_elem_info(ET).nen <= 8 ? gf_elem_info(ET).nen : 5;
+  return gf_elem_info(ET).nen <= 8 ? gf_elem_info(ET).nen : sizeof(TC) == 4 ? 5 : 2;
 }
 
 template <int ET, typename TC>
@@ -262,13 +317,19 @@ gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   k_elem_geometry<ET, TC><<<(ctx->nelem + EB - 1) / EB, kOT, 0, ctx->stream>>>(
       ctx->nelem, ngp, EB, ctx->d_conn, ctx->d_coords64, d_tab, geo);
   GF_LAUNCH_CHECK(ctx, "k_elem_geometry");
-  int NB = 256;  // largest node block whose tile keeps several CTAs per SM
-  while (NB > 1 && owner_smem_bytes<ET, TC>(NB, W, ngp) > kOwnerSmemLimit) NB >>= 1;
-  const size_t sm = owner_smem_bytes<ET, TC>(NB, W, ngp);
+  // largest node block (at most 128: the owning node index is a byte) whose tile keeps
+  // three CTAs per SM
+  int NB = 128;
+  while (NB > 1 && owner_smem_bytes<ET, TC>(NB, W, ngp, ctx->maxval) > kOwnerSmemLimit) --NB;
+  const size_t sm = owner_smem_bytes<ET, TC>(NB, W, ngp, ctx->maxval);
   if (sm > kOwnerSmemLimit)
     return gf_fail(ctx, GF_ERR_UNSUPPORTED, "owner scatter: a row block does not fit");
-  constexpr int JG = owner_jgroup<ET>();
-  auto kern = k_assemble_owner<ET, TC, JG>;
+  constexpr int JG = owner_jgroup<ET, TC>();
+  // compile-time Gauss rule for 2-D elements (one work item per task; in 3-D the
+  // unrolled Gauss loop costs more registers than it saves)
+  auto kern = JG != info.nen || info.dim == 3 ? k_assemble_owner<ET, TC, JG, 0>
+              : ctx->ngauss == 2 ? k_assemble_owner<ET, TC, JG, 2>
+                                 : k_assemble_owner<ET, TC, JG, 3>;
   GF_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
   kern<<<(ctx->nnodes + NB - 1) / NB, kOT, sm, ctx->stream>>>(
@@ -302,3 +363,5 @@ gf_status gf_assemble_owner_check(gf_ctx* ctx) {
   (void)ctx;
   return GF_OK;
 }
+
+

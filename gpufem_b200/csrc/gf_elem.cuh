@@ -108,6 +108,43 @@ __device__ inline TC gf_gradients(const TC* dN, const TC* X, bool use64, TC* G, 
   }
 }
 
+// Shape derivatives of element type ET at the NG1-point tensor Gauss rule, evaluated
+// at compile time with the same formulas and point order as the runtime tables
+// (gf_dshape, gf_gauss_rule); kernels that index it with unrolled loop counters get
+// the values as instruction constants.
+template <int ET, int NG1>
+struct GpTable {
+  static constexpr int DIM = gf_elem_info(ET).dim;
+  static constexpr int NEN = gf_elem_info(ET).nen;
+  static constexpr int NGP = DIM == 2 ? NG1 * NG1 : NG1 * NG1 * NG1;
+  double d64[NGP * DIM * NEN] = {};
+  float d32[NGP * DIM * NEN] = {};
+};
+
+template <int ET, int NG1>
+constexpr GpTable<ET, NG1> gf_gp_table() {
+  using T = GpTable<ET, NG1>;
+  T t{};
+  // 1/sqrt(3) and sqrt(3/5)
+  const double xg = NG1 == 2 ? 0.57735026918962576451 : 0.77459666924148337704;
+  const double x[3] = {-xg, NG1 == 2 ? xg : 0.0, xg};
+  const int nk = T::DIM == 2 ? 1 : NG1;
+  int g = 0;
+  for (int i = 0; i < NG1; ++i)
+    for (int j = 0; j < NG1; ++j)
+      for (int k = 0; k < nk; ++k) {
+        const double p[3] = {x[i], x[j], T::DIM == 2 ? 0.0 : x[k]};
+        double dN[3 * GF_MAX_NEN] = {};
+        gf_dshape<double>(ET, gf_node_nat_host[ET], p, dN);
+        for (int q = 0; q < T::DIM * T::NEN; ++q) {
+          t.d64[g * T::DIM * T::NEN + q] = dN[q];
+          t.d32[g * T::DIM * T::NEN + q] = (float)dN[q];
+        }
+        ++g;
+      }
+  return t;
+}
+
 // Shape-derivative tables for the context's element type and Gauss rule (device
 // buffer owned by the context, built once per mesh).
 gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out);

@@ -35,8 +35,20 @@ __host__ __device__ constexpr ElemInfo gf_elem_info(int et) {
                          : ElemInfo{20, 3, 1};
 }
 
-// natural coordinates (xi, eta, zeta) of element nodes, [et][node][3]
-extern const signed char gf_node_nat_host[4][GF_MAX_NEN][3];
+// natural coordinates (xi, eta, zeta) of element nodes, [et][node][3], in the
+// reference's node order (StiffAlgo::GetdShapeFunctNatCoord, src/FEM/StiffAlgo.cc:47-202)
+constexpr signed char gf_node_nat_host[4][GF_MAX_NEN][3] = {
+    // Q4
+    {{-1, -1, 0}, {1, -1, 0}, {1, 1, 0}, {-1, 1, 0}},
+    // Q8
+    {{-1, -1, 0}, {0, -1, 0}, {1, -1, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {-1, 1, 0}, {-1, 0, 0}},
+    // Brick8
+    {{1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {1, -1, 1}, {-1, -1, -1}, {-1, 1, -1}, {-1, 1, 1}, {-1, -1, 1}},
+    // Brick20
+    {{1, -1, -1}, {1, 0, -1}, {1, 1, -1}, {1, 1, 0}, {1, 1, 1}, {1, 0, 1}, {1, -1, 1}, {1, -1, 0},
+     {0, -1, -1}, {0, 1, -1}, {0, 1, 1}, {0, -1, 1},
+     {-1, -1, -1}, {-1, 0, -1}, {-1, 1, -1}, {-1, 1, 0}, {-1, 1, 1}, {-1, 0, 1}, {-1, -1, 1}, {-1, -1, 0}},
+};
 
 // Derivatives dN_i/dxi_a at natural point p (host and device), written from:
 //   Lagrange:     N = prod_a (1 + xi_a p_a) / 2^dim
@@ -44,13 +56,13 @@ extern const signed char gf_node_nat_host[4][GF_MAX_NEN][3];
 //   Serendipity mid-side (one xi_c = 0):
 //                 N = (1 - p_c^2) * prod_{a != c} (1 + xi_a p_a) / 2^(dim-1)
 template <typename R>
-__host__ __device__ inline void gf_dshape(int et, const signed char (*nat)[3], const R* p,
-                                          R* dN /* [dim][nen] */) {
+__host__ __device__ constexpr void gf_dshape(int et, const signed char (*nat)[3], const R* p,
+                                             R* dN /* [dim][nen] */) {
   const ElemInfo info = gf_elem_info(et);
   const int dim = info.dim, nen = info.nen;
   for (int i = 0; i < nen; ++i) {
     R xi[3] = {R(nat[i][0]), R(nat[i][1]), R(nat[i][2])};
-    R f[3];    // linear factors (1 + xi_a p_a)
+    R f[3] = {R(0), R(0), R(0)};  // linear factors (1 + xi_a p_a)
     for (int a = 0; a < dim; ++a) f[a] = R(1) + xi[a] * p[a];
     if (!info.serendipity) {
       const R scale = dim == 2 ? R(0.25) : R(0.125);
@@ -81,7 +93,7 @@ __host__ __device__ inline void gf_dshape(int et, const signed char (*nat)[3], c
         const R scale = dim == 2 ? R(0.5) : R(0.25);
         R q = R(1) - p[c] * p[c];
         for (int a = 0; a < dim; ++a) {
-          R d;
+          R d = R(0);
           if (a == c) {
             d = scale * (R(-2) * p[c]);
             for (int b = 0; b < dim; ++b)
