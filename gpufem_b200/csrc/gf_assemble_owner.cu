@@ -428,9 +428,9 @@ gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   constexpr int JG = owner_jgroup<ET, TC>();
   // compile-time Gauss rule for 2-D elements (one work item per task; in 3-D the
   // unrolled Gauss loop costs more registers than it saves)
-  auto kern = JG != info.nen || info.dim == 3 ? k_assemble_owner<ET, TC, JG, 0>
-              : ctx->ngauss == 2 ? k_assemble_owner<ET, TC, JG, 2>
-                                 : k_assemble_owner<ET, TC, JG, 3>;
+  auto kern = k_assemble_owner<ET, TC, JG, 0>;
+  if constexpr (JG == info.nen && info.dim == 2)
+    kern = ctx->ngauss == 2 ? k_assemble_owner<ET, TC, JG, 2> : k_assemble_owner<ET, TC, JG, 3>;
   GF_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
   kern<<<(ctx->nnodes + NB - 1) / NB, kOT, sm, ctx->stream>>>(
