@@ -250,6 +250,16 @@ class FemData:
         self.stiffness: Optional[ELLmatrixCUDA] = None
         self.displacements: Optional[np.ndarray] = None
 
+    def InitFromFile(self, nf_path: str, n_gpts: int, E: float, Nu: float,
+                     E_elem=None) -> None:
+        """FemData::Init with a FileIO that has read a neutral file (FileIO::ReadNF,
+        src/Utils/fileIO.cc:73-404); see gpufem_b200.nf."""
+        from .nf import read_nf
+        m = read_nf(nf_path)
+        loads = m.loads if m.loads.shape[0] else None
+        self.Init(m.elem_type, m.coords, m.conn, n_gpts, E, Nu, supports=m.supports,
+                  nodal_loads=loads, E_elem=E_elem)
+
     def GetStiffnessMatrix(self) -> "ELLmatrixCUDA":
         return self.stiffness
 
