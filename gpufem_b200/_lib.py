@@ -54,6 +54,7 @@ SIGNATURES = {
     "gf_mesh_create": (I32, [P, I32, I32, P, I32, P, I32, D, P, D, I32]),
     "gf_mesh_set_modulus": (I32, [P, D, P]),
     "gf_mesh_color": (I32, [P, P, C.POINTER(I32)]),
+    "gf_mesh_color_device": (I32, [P, C.c_uint64, C.POINTER(I32)]),
     "gf_mesh_get_colors": (I32, [P, P]),
     "gf_ell_build_pattern": (I32, [P, C.POINTER(I32), C.POINTER(I32), C.POINTER(I64)]),
     "gf_assemble": (I32, [P, I32, I32, I32]),

@@ -86,6 +86,12 @@ class Context:
         self._c(lib.gf_mesh_color(self.h, _ptr(colors), C.byref(nc)))
         return nc.value
 
+    def color_device(self, seed: int = 0) -> int:
+        """Jones–Plassmann colouring on the device; returns the number of colours."""
+        nc = C.c_int32(0)
+        self._c(lib.gf_mesh_color_device(self.h, seed, C.byref(nc)))
+        return nc.value
+
     def colors(self, nelem: int) -> np.ndarray:
         out = np.empty(nelem, np.int32)
         self._c(lib.gf_mesh_get_colors(self.h, _ptr(out)))

@@ -152,6 +152,12 @@ GF_API gf_status gf_mesh_set_modulus(gf_ctx* ctx, double E, const double* E_elem
  * the number of colours.  A caller colouring is validated (no two elements of a colour
  * share a node) and rejected with GF_ERR_INVALID_ARG otherwise. */
 GF_API gf_status gf_mesh_color(gf_ctx* ctx, const int32_t* elem_color, int32_t* ncolors);
+/* Colour on the device instead (Jones–Plassmann rounds with pseudo-random priorities
+ * from `seed`, first-fit colours; at most 256 colours).  Same validity as gf_mesh_color,
+ * usually a few more colours than the greedy host order, no host pass over the dual
+ * graph.  Builds the ELL pattern first if needed (it walks the node incidence lists).
+ * No reference counterpart beyond femColor's role (femColor.cc:79-191). */
+GF_API gf_status gf_mesh_color_device(gf_ctx* ctx, uint64_t seed, int32_t* ncolors);
 /* Copy the colour of each element (0-based) to host. */
 GF_API gf_status gf_mesh_get_colors(gf_ctx* ctx, int32_t* elem_color);
 
