@@ -49,6 +49,7 @@ SIGNATURES = {
     "gf_last_error": (C.c_char_p, [P]),
     "gf_version": (C.c_char_p, []),
     "gf_last_device_seconds": (D, [P]),
+    "gf_last_assembly_split": (I32, [P, C.POINTER(D), C.POINTER(D)]),
     "gf_kernel_launches": (I64, [P]),
     "gf_sync": (I32, [P]),
     "gf_mesh_create": (I32, [P, I32, I32, P, I32, P, I32, D, P, D, I32]),

@@ -43,7 +43,8 @@ GF_API gf_status gf_create(gf_ctx** out, int32_t device) {
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+      cudaEventCreate(&ctx->evm) != cudaSuccess) {
     cudaGetLastError();
     delete ctx;
     return GF_ERR_CUDA;
@@ -65,6 +66,7 @@ GF_API gf_status gf_destroy(gf_ctx* ctx) {
   gf_free(ctx->d_fixed);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->evm) cudaEventDestroy(ctx->evm);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return GF_OK;
@@ -73,6 +75,14 @@ GF_API gf_status gf_destroy(gf_ctx* ctx) {
 GF_API const char* gf_last_error(const gf_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 GF_API double gf_last_device_seconds(const gf_ctx* ctx) { return ctx ? ctx->last_seconds : 0.0; }
 GF_API int64_t gf_kernel_launches(const gf_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+GF_API gf_status gf_last_assembly_split(const gf_ctx* ctx, double* geometry_seconds,
+                                        double* scatter_seconds) {
+  if (!ctx) return GF_ERR_INVALID_ARG;
+  if (geometry_seconds) *geometry_seconds = ctx->last_split[0];
+  if (scatter_seconds) *scatter_seconds = ctx->last_split[1];
+  return GF_OK;
+}
 
 GF_API gf_status gf_sync(gf_ctx* ctx) {
   if (!ctx) return GF_ERR_INVALID_ARG;

@@ -273,6 +273,16 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   ctx->last_seconds = ms * 1e-3;
+  if (scatter == GF_SCATTER_OWNER) {
+    float m0 = 0.f, m1 = 0.f;
+    cudaEventElapsedTime(&m0, ctx->ev0, ctx->evm);
+    cudaEventElapsedTime(&m1, ctx->evm, ctx->ev1);
+    ctx->last_split[0] = m0 * 1e-3;
+    ctx->last_split[1] = m1 * 1e-3;
+  } else {
+    ctx->last_split[0] = 0.0;
+    ctx->last_split[1] = ms * 1e-3;
+  }
   if (dtype == GF_F64) { ctx->has64 = true; ctx->kver64++; } else { ctx->has32 = true; ctx->kver32++; }
   ctx->bc_mode_applied = -1;
   return GF_OK;

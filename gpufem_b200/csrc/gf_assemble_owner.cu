@@ -123,8 +123,10 @@ k_elem_geometry(int nelem, int ngp, int EB, const int32_t* __restrict__ conn,
 }
 
 // Thread per element (element types with at most 24 coordinates): the element's
-// local coordinates stay in registers and the Gauss rule is a compile-time table;
-// same arithmetic and output as k_elem_geometry.
+// local coordinates stay in registers (FP64, plus their FP32 rounding) and the Gauss
+// rule is a compile-time table; same arithmetic and output as k_elem_geometry.  Each
+// warp stages its 32 elements' output in shared memory and stores it as one
+// contiguous, coalesced block.
 template <int ET, typename TC, int NG1>
 __global__ void __launch_bounds__(kOT)
 k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
@@ -132,89 +134,105 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
   constexpr ElemInfo info = gf_elem_info(ET);
   constexpr int NEN = info.nen, DIM = info.dim, GS = DIM * DIM + 1;
   constexpr int NGP = GpTable<ET, NG1>::NGP;
+  constexpr int PER = NGP * GS;  // output values per element
   constexpr GpTable<ET, NG1> Tab = gf_gp_table<ET, NG1>();
   // 1-D weights (1, 1) or (5/9, 8/9, 5/9), multiplied in the reference's tensor order
   constexpr double w1[3] = {NG1 == 2 ? 1.0 : 5.0 / 9.0, NG1 == 2 ? 1.0 : 8.0 / 9.0, 5.0 / 9.0};
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TC* stage = reinterpret_cast<TC*>(smem_raw) + (size_t)(threadIdx.x >> 5) * 32 * PER;
   const bool f64 = sizeof(TC) == 8;
-  const int e = blockIdx.x * kOT + threadIdx.x;
-  if (e >= nelem) return;
-  double X[NEN][DIM];
-  {
-    const int node0 = conn[(int64_t)e * NEN];
-    double x0[DIM];
+  const int lane = threadIdx.x & 31;
+  const int e0 = (blockIdx.x * kOT + threadIdx.x) & ~31;  // first element of the warp
+  const int e = e0 + lane;
+  if (e0 >= nelem) return;
+  if (e < nelem) {
+    double X[NEN][DIM];
+    float Xf[NEN][DIM];
+    {
+      const int node0 = conn[(int64_t)e * NEN];
+      double x0[DIM];
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) x0[c] = coords[(int64_t)node0 * DIM + c];
+      for (int c = 0; c < DIM; ++c) x0[c] = coords[(int64_t)node0 * DIM + c];
 #pragma unroll
-    for (int i = 0; i < NEN; ++i) {
-      const int node = conn[(int64_t)e * NEN + i];
+      for (int i = 0; i < NEN; ++i) {
+        const int node = conn[(int64_t)e * NEN + i];
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) X[i][c] = coords[(int64_t)node * DIM + c] - x0[c];
+        for (int c = 0; c < DIM; ++c) {
+          X[i][c] = coords[(int64_t)node * DIM + c] - x0[c];
+          Xf[i][c] = (float)X[i][c];
+        }
+      }
     }
-  }
-  bool use64 = f64;
-  if (!f64) {
-    float dmin = 3.4e38f, dmax = 0.f;
+    bool use64 = f64;
+    if (!f64) {
+      float dmin = 3.4e38f, dmax = 0.f;
+#pragma unroll
+      for (int g = 0; g < NGP; ++g) {
+        float J[3][3], Ji[3][3];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) {
+            float s = 0.f;
+#pragma unroll
+            for (int i = 0; i < NEN; ++i) s += Tab.d32[(g * DIM + a) * NEN + i] * Xf[i][c];
+            J[a][c] = s;
+          }
+        const float d = fabsf(gf_det_inv<DIM, float>(J, Ji));
+        dmin = fminf(dmin, d);
+        dmax = fmaxf(dmax, d);
+      }
+      use64 = dmax > 10.f * dmin;
+    }
+    TC* out = stage + lane * PER;
 #pragma unroll
     for (int g = 0; g < NGP; ++g) {
-      float J[3][3], Ji[3][3];
+      const int gi = DIM == 2 ? g / NG1 : g / (NG1 * NG1);
+      const int gj = DIM == 2 ? g % NG1 : (g / NG1) % NG1;
+      const int gk = DIM == 2 ? 0 : g % NG1;
+      const double wg = w1[gi] * w1[gj] * (DIM == 2 ? 1.0 : w1[gk]);
+      if (use64) {
+        double J[3][3], Ji[3][3];
 #pragma unroll
-      for (int a = 0; a < DIM; ++a)
+        for (int a = 0; a < DIM; ++a)
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          float s = 0.f;
+          for (int c = 0; c < DIM; ++c) {
+            double s = 0.0;
 #pragma unroll
-          for (int i = 0; i < NEN; ++i) s += Tab.d32[(g * DIM + a) * NEN + i] * (float)X[i][c];
-          J[a][c] = s;
-        }
-      const float d = fabsf(gf_det_inv<DIM, float>(J, Ji));
-      dmin = fminf(dmin, d);
-      dmax = fmaxf(dmax, d);
-    }
-    use64 = dmax > 10.f * dmin;
-  }
-  TC* out = geo + (int64_t)e * NGP * GS;
+            for (int i = 0; i < NEN; ++i) s += Tab.d64[(g * DIM + a) * NEN + i] * X[i][c];
+            J[a][c] = s;
+          }
+        const double d = gf_det_inv<DIM, double>(J, Ji);
 #pragma unroll
-  for (int g = 0; g < NGP; ++g) {
-    const int gi = DIM == 2 ? g / NG1 : g / (NG1 * NG1);
-    const int gj = DIM == 2 ? g % NG1 : (g / NG1) % NG1;
-    const int gk = DIM == 2 ? 0 : g % NG1;
-    const double wg = w1[gi] * w1[gj] * (DIM == 2 ? 1.0 : w1[gk]);
-    if (use64) {
-      double J[3][3], Ji[3][3];
+        for (int a = 0; a < DIM; ++a)
 #pragma unroll
-      for (int a = 0; a < DIM; ++a)
+          for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
+        out[g * GS + DIM * DIM] = TC(wg * d);
+      } else {
+        float J[3][3], Ji[3][3];
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          double s = 0.0;
+        for (int a = 0; a < DIM; ++a)
 #pragma unroll
-          for (int i = 0; i < NEN; ++i) s += Tab.d64[(g * DIM + a) * NEN + i] * X[i][c];
-          J[a][c] = s;
-        }
-      const double d = gf_det_inv<DIM, double>(J, Ji);
+          for (int c = 0; c < DIM; ++c) {
+            float s = 0.f;
 #pragma unroll
-      for (int a = 0; a < DIM; ++a)
+            for (int i = 0; i < NEN; ++i) s += Tab.d32[(g * DIM + a) * NEN + i] * Xf[i][c];
+            J[a][c] = s;
+          }
+        const float d = gf_det_inv<DIM, float>(J, Ji);
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
-      out[g * GS + DIM * DIM] = TC(wg * d);
-    } else {
-      float J[3][3], Ji[3][3];
+        for (int a = 0; a < DIM; ++a)
 #pragma unroll
-      for (int a = 0; a < DIM; ++a)
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          float s = 0.f;
-#pragma unroll
-          for (int i = 0; i < NEN; ++i) s += Tab.d32[(g * DIM + a) * NEN + i] * (float)X[i][c];
-          J[a][c] = s;
-        }
-      const float d = gf_det_inv<DIM, float>(J, Ji);
-#pragma unroll
-      for (int a = 0; a < DIM; ++a)
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
-      out[g * GS + DIM * DIM] = TC((float)wg * d);
+          for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
+        out[g * GS + DIM * DIM] = TC((float)wg * d);
+      }
     }
   }
+  __syncwarp();
+  // the warp's elements are consecutive: their outputs form one contiguous block
+  const int nw = min(32, nelem - e0);
+  TC* dst = geo + (int64_t)e0 * PER;
+  for (int k = lane; k < nw * PER; k += 32) dst[k] = stage[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -408,16 +426,25 @@ gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
     ctx->geo_bytes = need;
   }
   TC* geo = static_cast<TC*>(ctx->d_geo);
+  // per-element kernel where its output staging fits (Q4, Q8; Brick8 with 2x2x2 Gauss)
+  const size_t gsm = sizeof(TC) * (size_t)kOT * ngp * (info.dim * info.dim + 1);
+  bool per_element = false;
   if constexpr (info.nen * info.dim <= 24) {
-    auto gk = ctx->ngauss == 2 ? k_elem_geometry_pe<ET, TC, 2> : k_elem_geometry_pe<ET, TC, 3>;
-    gk<<<gf_blocks(ctx->nelem, kOT), kOT, 0, ctx->stream>>>(ctx->nelem, ctx->d_conn,
-                                                           ctx->d_coords64, geo);
-  } else {
+    if (gsm <= 100 * 1024) {
+      auto gk = ctx->ngauss == 2 ? k_elem_geometry_pe<ET, TC, 2> : k_elem_geometry_pe<ET, TC, 3>;
+      GF_CUDA(ctx, cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+      gk<<<gf_blocks(ctx->nelem, kOT), kOT, gsm, ctx->stream>>>(ctx->nelem, ctx->d_conn,
+                                                               ctx->d_coords64, geo);
+      per_element = true;
+    }
+  }
+  if (!per_element) {
     const int EB = kOT / ngp;
     k_elem_geometry<ET, TC><<<(ctx->nelem + EB - 1) / EB, kOT, 0, ctx->stream>>>(
         ctx->nelem, ngp, EB, ctx->d_conn, ctx->d_coords64, d_tab, geo);
   }
   GF_LAUNCH_CHECK(ctx, "k_elem_geometry");
+  cudaEventRecord(ctx->evm, ctx->stream);
   // largest node block (at most 128: the owning node index is a byte) whose tile keeps
   // three CTAs per SM
   int NB = 128;

@@ -150,6 +150,8 @@ struct gf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evm = nullptr;            // between the two kernels of an owner assembly
+  double last_split[2] = {0.0, 0.0};    // last assembly: geometry, scatter kernel seconds
   std::string err;
   double last_seconds = 0.0;
   int64_t launches = 0;

@@ -128,6 +128,10 @@ GF_API const char* gf_last_error(const gf_ctx* ctx);
 GF_API const char* gf_version(void);
 /* Device time (seconds) of the last timed phase: assemble, spmv or solve. */
 GF_API double gf_last_device_seconds(const gf_ctx* ctx);
+/* The last gf_assemble split by kernel (device seconds): for GF_SCATTER_OWNER the
+ * geometry kernel and the owner kernel; for the other schedules 0 and the whole. */
+GF_API gf_status gf_last_assembly_split(const gf_ctx* ctx, double* geometry_seconds,
+                                        double* scatter_seconds);
 /* Kernel launches issued by this context since creation (for accounting). */
 GF_API int64_t gf_kernel_launches(const gf_ctx* ctx);
 /* Synchronise the context's stream. */
