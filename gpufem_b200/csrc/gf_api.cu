@@ -62,8 +62,10 @@ GF_API gf_status gf_destroy(gf_ctx* ctx) {
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
-  gf_free(ctx->d_f);
-  gf_free(ctx->d_fixed);
+  gf_pfree(ctx, ctx->d_f);
+  gf_pfree(ctx, ctx->d_fixed);
+  if (ctx->d_geo) cudaFree(ctx->d_geo);
+  gf_pool_clear(ctx);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->evm) cudaEventDestroy(ctx->evm);
@@ -93,14 +95,14 @@ GF_API gf_status gf_sync(gf_ctx* ctx) {
 }  // extern "C"
 
 void gf_mesh_free(gf_ctx* ctx) {
-  gf_free(ctx->d_coords64);
-  gf_free(ctx->d_coords32);
-  gf_free(ctx->d_conn);
-  gf_free(ctx->d_Eel);
-  gf_free(ctx->d_Eel32);
+  gf_pfree(ctx, ctx->d_coords64);
+  gf_pfree(ctx, ctx->d_coords32);
+  gf_pfree(ctx, ctx->d_conn);
+  gf_pfree(ctx, ctx->d_Eel);
+  gf_pfree(ctx, ctx->d_Eel32);
   gf_free(ctx->d_asmtab);
   gf_free(ctx->d_perm);
-  gf_free(ctx->d_allperm);
+  gf_pfree(ctx, ctx->d_allperm);
   ctx->h_conn.clear();
   ctx->h_color.clear();
   ctx->color_off.clear();
@@ -109,22 +111,19 @@ void gf_mesh_free(gf_ctx* ctx) {
 }
 
 void gf_pattern_free(gf_ctx* ctx) {
-  gf_free(ctx->d_rownnz);
-  gf_free(ctx->d_colidx);
-  gf_free(ctx->d_slotmap);
-  gf_free(ctx->d_adj_off);
-  gf_free(ctx->d_adj);
-  gf_free(ctx->d_diagpos);
-  gf_free(ctx->d_inc_off);
-  gf_free(ctx->d_inc);
-  gf_free(ctx->d_inc_loc);
-  gf_free(ctx->d_inc_slot);
-  if (ctx->d_geo) cudaFree(ctx->d_geo);
-  ctx->d_geo = nullptr;
-  ctx->geo_bytes = 0;
-  ctx->maxval = 0;
-  gf_free(ctx->d_K64);
-  gf_free(ctx->d_K32);
+  gf_pfree(ctx, ctx->d_rownnz);
+  gf_pfree(ctx, ctx->d_colidx);
+  gf_pfree(ctx, ctx->d_slotmap);
+  gf_pfree(ctx, ctx->d_adj_off);
+  gf_pfree(ctx, ctx->d_adj);
+  gf_pfree(ctx, ctx->d_diagpos);
+  gf_pfree(ctx, ctx->d_inc_off);
+  gf_pfree(ctx, ctx->d_inc);
+  gf_pfree(ctx, ctx->d_inc_loc);
+  gf_pfree(ctx, ctx->d_inc_slot);
+  ctx->maxval = 0;  // the geometry buffer keeps its capacity (freed by gf_destroy)
+  gf_pfree(ctx, ctx->d_K64);
+  gf_pfree(ctx, ctx->d_K32);
   gf_sell_free(ctx);
   // n (the dof count) belongs to the mesh and survives; width and nnz do not
   ctx->has_pattern = ctx->has64 = ctx->has32 = false;
@@ -143,22 +142,122 @@ static __global__ void k_iota(int n, int32_t* p) {
   if (i < n) p[i] = i;
 }
 
-static gf_status upload_modulus(gf_ctx* ctx, double E, const double* E_elem) {
-  std::vector<double> e64(ctx->nelem);
-  std::vector<float> e32(ctx->nelem);
-  for (int i = 0; i < ctx->nelem; ++i) {
-    double v = E_elem ? E_elem[i] : E;
-    if (!(v > 0.0) || !std::isfinite(v))
-      return gf_fail(ctx, GF_ERR_INVALID_ARG, "modulus of element %d is %g (must be > 0)", i, v);
-    e64[i] = v;
-    e32[i] = (float)v;
+// ---- device buffer pool --------------------------------------------------------
+void* gf_pool_get(gf_ctx* ctx, size_t bytes) {
+  for (size_t k = 0; k < ctx->pool_free.size(); ++k)
+    if (ctx->pool_free[k].bytes == bytes) {
+      void* p = ctx->pool_free[k].p;
+      ctx->pool_free.erase(ctx->pool_free.begin() + (ptrdiff_t)k);
+      ctx->pool_live.emplace_back(p, bytes);
+      return p;
+    }
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    for (auto& b : ctx->pool_free) cudaFree(b.p);  // give unused blocks back, retry once
+    ctx->pool_free.clear();
+    p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
   }
-  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_Eel, e64.data(), sizeof(double) * ctx->nelem,
-                               cudaMemcpyHostToDevice, ctx->stream));
-  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_Eel32, e32.data(), sizeof(float) * ctx->nelem,
-                               cudaMemcpyHostToDevice, ctx->stream));
-  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->E = E;
+  ctx->pool_live.emplace_back(p, bytes);
+  return p;
+}
+
+void gf_pool_put(gf_ctx* ctx, void* p) {
+  for (size_t k = 0; k < ctx->pool_live.size(); ++k)
+    if (ctx->pool_live[k].first == p) {
+      ctx->pool_free.push_back({p, ctx->pool_live[k].second, ctx->pool_gen});
+      ctx->pool_live.erase(ctx->pool_live.begin() + (ptrdiff_t)k);
+      return;
+    }
+  cudaFree(p);  // not from the pool
+}
+
+void gf_pool_new_generation(gf_ctx* ctx) {
+  ++ctx->pool_gen;
+  std::vector<gf_ctx::PoolBlock> keep;
+  for (auto& b : ctx->pool_free) {
+    if (b.gen >= ctx->pool_gen - 1) keep.push_back(b);
+    else cudaFree(b.p);
+  }
+  ctx->pool_free.swap(keep);
+}
+
+void gf_pool_clear(gf_ctx* ctx) {
+  for (auto& b : ctx->pool_free) cudaFree(b.p);
+  for (auto& b : ctx->pool_live) cudaFree(b.first);
+  ctx->pool_free.clear();
+  ctx->pool_live.clear();
+}
+
+// ---- mesh validation on the device ------------------------------------------------
+// chk[0]: smallest index of a non-finite coordinate; chk[1]: smallest connectivity
+// entry outside 1..nnodes; chk[2]: smallest element repeating a node; chk[3]: smallest
+// element whose modulus is not finite and > 0.  All start at ~0 (none).
+static __global__ void k_mesh_check(int64_t ncoord, const double* __restrict__ coords,
+                                    int nelem, int nen, int nnodes, int32_t* __restrict__ conn,
+                                    unsigned long long* __restrict__ chk) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncoord; i += stride)
+    if (!isfinite(coords[i])) atomicMin(&chk[0], (unsigned long long)i);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nelem; e += stride) {
+    int32_t v[GF_MAX_NEN];
+    bool ok = true;
+    for (int a = 0; a < nen; ++a) {
+      v[a] = conn[e * nen + a];
+      if (v[a] < 1 || v[a] > nnodes) {
+        atomicMin(&chk[1], (unsigned long long)(e * nen + a));
+        ok = false;
+      }
+    }
+    for (int a = 0; a < nen && ok; ++a)
+      for (int b = a + 1; b < nen; ++b)
+        if (v[a] == v[b]) {
+          atomicMin(&chk[2], (unsigned long long)e);
+          ok = false;
+          break;
+        }
+    for (int a = 0; a < nen; ++a) conn[e * nen + a] = v[a] - 1;  // 0-based
+  }
+}
+
+// Eel <- E_elem (already copied to Eel) or the scalar E, FP32 copy, validity in chk[3].
+static __global__ void k_modulus(int nelem, int per_elem, double E, double* __restrict__ Eel,
+                                 float* __restrict__ Eel32, unsigned long long* __restrict__ chk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nelem) return;
+  const double v = per_elem ? Eel[i] : E;
+  if (!(v > 0.0) || !isfinite(v)) atomicMin(&chk[3], (unsigned long long)i);
+  Eel[i] = v;
+  Eel32[i] = (float)v;
+}
+
+// The first failed check, in the order coordinates, connectivity range, repeated
+// nodes, moduli, as a status and message (values read from the caller's arrays).
+static gf_status check_failure(gf_ctx* ctx, const unsigned long long* chk, int nen,
+                               int nnodes, const int32_t* connect, double E,
+                               const double* E_elem) {
+  const unsigned long long none = ~0ull;
+  if (chk[0] != none)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "non-finite coordinate at %llu", chk[0]);
+  if (chk[1] != none)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG,
+                   "connectivity entry %llu = %d outside 1..%d (1-based node ids)", chk[1],
+                   connect[chk[1]], nnodes);
+  if (chk[2] != none) {
+    const size_t e = (size_t)chk[2];
+    int rep = 0;
+    for (int a = 0; a < nen && !rep; ++a)
+      for (int b = a + 1; b < nen; ++b)
+        if (connect[e * nen + a] == connect[e * nen + b]) { rep = connect[e * nen + a]; break; }
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "element %zu repeats node %d", e, rep);
+  }
+  if (chk[3] != none)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "modulus of element %llu is %g (must be > 0)",
+                   chk[3], E_elem ? E_elem[chk[3]] : E);
   return GF_OK;
 }
 
@@ -183,31 +282,78 @@ GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
   const ElemInfo info = gf_elem_info(elem_type);
   if ((int64_t)nnodes * info.dim >= (int64_t)INT32_MAX)
     return gf_fail(ctx, GF_ERR_UNSUPPORTED, "too many dofs for int32 indexing");
-  for (int64_t i = 0; i < (int64_t)nnodes * info.dim; ++i)
-    if (!std::isfinite(coords[i]))
-      return gf_fail(ctx, GF_ERR_INVALID_ARG, "non-finite coordinate at %lld", (long long)i);
-  std::vector<int32_t> conn0((size_t)nelem * info.nen);
-  for (size_t i = 0; i < conn0.size(); ++i) {
-    int32_t v = connect[i];
-    if (v < 1 || v > nnodes)
-      return gf_fail(ctx, GF_ERR_INVALID_ARG,
-                     "connectivity entry %zu = %d outside 1..%d (1-based node ids)", i, v, nnodes);
-    conn0[i] = v - 1;
-  }
-  for (int e = 0; e < nelem; ++e)
-    for (int a = 0; a < info.nen; ++a)
-      for (int b = a + 1; b < info.nen; ++b)
-        if (conn0[(size_t)e * info.nen + a] == conn0[(size_t)e * info.nen + b])
-          return gf_fail(ctx, GF_ERR_INVALID_ARG, "element %d repeats node %d", e,
-                         conn0[(size_t)e * info.nen + a] + 1);
+  if ((int64_t)nelem * info.nen >= (int64_t)INT32_MAX)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "too many element-node entries for int32 indexing");
 
-  cudaStreamSynchronize(ctx->stream);
+  // The new mesh goes into fresh buffers and is validated on the device (one round
+  // trip); the current mesh is released only once the new one is accepted.
+  cudaStream_t s = ctx->stream;
+  cudaStreamSynchronize(s);
+  gf_pool_new_generation(ctx);
+  const size_t ncoord = (size_t)nnodes * info.dim;
+  const size_t nconn = (size_t)nelem * info.nen;
+  const int n = nnodes * info.dim;
+  double* coords64 = nullptr;
+  float* coords32 = nullptr;
+  int32_t *conn = nullptr, *allperm = nullptr;
+  double* Eel = nullptr;
+  float* Eel32 = nullptr;
+  double* f = nullptr;
+  uint8_t* fixed = nullptr;
+  unsigned long long* d_chk = nullptr;
+  auto release = [&]() {
+    gf_pfree(ctx, coords64); gf_pfree(ctx, coords32); gf_pfree(ctx, conn);
+    gf_pfree(ctx, allperm); gf_pfree(ctx, Eel); gf_pfree(ctx, Eel32); gf_pfree(ctx, f);
+    gf_pfree(ctx, fixed); gf_pfree(ctx, d_chk);
+  };
+  gf_status st;
+  if ((st = gf_palloc(ctx, &coords64, ncoord)) != GF_OK ||
+      (st = gf_palloc(ctx, &coords32, ncoord)) != GF_OK ||
+      (st = gf_palloc(ctx, &conn, nconn)) != GF_OK ||
+      (st = gf_palloc(ctx, &allperm, (size_t)nelem)) != GF_OK ||
+      (st = gf_palloc(ctx, &Eel, (size_t)nelem)) != GF_OK ||
+      (st = gf_palloc(ctx, &Eel32, (size_t)nelem)) != GF_OK ||
+      (st = gf_palloc(ctx, &f, (size_t)n)) != GF_OK ||
+      (st = gf_palloc(ctx, &fixed, (size_t)n)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_chk, 4)) != GF_OK) {
+    release();
+    return st;
+  }
+  unsigned long long h_chk[4];
+  cudaMemcpyAsync(coords64, coords, sizeof(double) * ncoord, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(conn, connect, sizeof(int32_t) * nconn, cudaMemcpyHostToDevice, s);
+  if (E_elem) cudaMemcpyAsync(Eel, E_elem, sizeof(double) * nelem, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(d_chk, 0xff, 4 * sizeof(unsigned long long), s);
+  const int cblocks = (int)std::min<int64_t>(gf_blocks(std::max<int64_t>(ncoord, nelem), 256),
+                                             (int64_t)ctx->sm_count * 8);
+  k_mesh_check<<<cblocks, 256, 0, s>>>((int64_t)ncoord, coords64, nelem, info.nen, nnodes, conn,
+                                       d_chk);
+  k_modulus<<<gf_blocks(nelem, 256), 256, 0, s>>>(nelem, E_elem ? 1 : 0, E, Eel, Eel32, d_chk);
+  k_f64_to_f32<<<gf_blocks(ncoord, 256), 256, 0, s>>>((int64_t)ncoord, coords64, coords32);
+  k_iota<<<gf_blocks(nelem, 256), 256, 0, s>>>(nelem, allperm);
+  cudaMemsetAsync(f, 0, sizeof(double) * n, s);
+  cudaMemsetAsync(fixed, 0, n, s);
+  ctx->launches += 4;
+  cudaMemcpyAsync(h_chk, d_chk, sizeof(h_chk), cudaMemcpyDeviceToHost, s);
+  cudaError_t ce = cudaStreamSynchronize(s);
+  if (ce == cudaSuccess) ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    release();
+    return gf_cuda_fail(ctx, ce, "mesh upload");
+  }
+  if ((st = check_failure(ctx, h_chk, info.nen, nnodes, connect, E, E_elem)) != GF_OK) {
+    release();
+    return st;
+  }
+
+  // accepted: drop the current mesh and everything built on it
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
   gf_lp_mesh_changed(ctx);
-  gf_free(ctx->d_f);
-  gf_free(ctx->d_fixed);
+  gf_pfree(ctx, ctx->d_f);
+  gf_pfree(ctx, ctx->d_fixed);
+  gf_pfree(ctx, d_chk);
   ctx->h_supports.clear();
   ctx->nsup = 0;
   ctx->bc_mode_applied = -1;
@@ -221,6 +367,7 @@ GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
   ctx->nelem = nelem;
   ctx->analysis = analysis;
   ctx->nu = nu;
+  ctx->E = E;
   // Per unit modulus: Ke = sum_gp w detJ E [lam1 g_i g_j^T + mu1 g_j g_i^T + mu1 (g_i.g_j) I]
   // which equals B^T D B for the reference's D (FemData.cc:322-365):
   //   plane stress: D = E/(1-nu^2) [[1, nu, 0], [nu, 1, 0], [0, 0, (1-nu)/2]]
@@ -233,32 +380,16 @@ GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
     ctx->lam1 = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
     ctx->mu1 = 1.0 / (2.0 * (1.0 + nu));
   }
-  ctx->n = nnodes * info.dim;
-  ctx->h_conn = conn0;
-
-  gf_status st;
-  const size_t ncoord = (size_t)nnodes * info.dim;
-  if ((st = gf_alloc(ctx, &ctx->d_coords64, ncoord)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_coords32, ncoord)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_conn, conn0.size())) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_Eel, (size_t)nelem)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_Eel32, (size_t)nelem)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_allperm, (size_t)nelem)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_f, (size_t)ctx->n)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_fixed, (size_t)ctx->n)) != GF_OK) return st;
-  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_coords64, coords, sizeof(double) * ncoord,
-                               cudaMemcpyHostToDevice, ctx->stream));
-  k_f64_to_f32<<<gf_blocks(ncoord, 256), 256, 0, ctx->stream>>>((int64_t)ncoord, ctx->d_coords64,
-                                                                 ctx->d_coords32);
-  GF_LAUNCH_CHECK(ctx, "k_f64_to_f32");
-  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_conn, conn0.data(), sizeof(int32_t) * conn0.size(),
-                               cudaMemcpyHostToDevice, ctx->stream));
-  k_iota<<<gf_blocks(nelem, 256), 256, 0, ctx->stream>>>(nelem, ctx->d_allperm);
-  GF_LAUNCH_CHECK(ctx, "k_iota");
-  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_f, 0, sizeof(double) * ctx->n, ctx->stream));
-  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_fixed, 0, ctx->n, ctx->stream));
-  ctx->h_f.assign(ctx->n, 0.0);
-  if ((st = upload_modulus(ctx, E, E_elem)) != GF_OK) return st;
+  ctx->n = n;
+  ctx->d_coords64 = coords64;
+  ctx->d_coords32 = coords32;
+  ctx->d_conn = conn;
+  ctx->d_allperm = allperm;
+  ctx->d_Eel = Eel;
+  ctx->d_Eel32 = Eel32;
+  ctx->d_f = f;
+  ctx->d_fixed = fixed;
+  ctx->h_f.assign(n, 0.0);
   ctx->has_mesh = true;
   return GF_OK;
 }
@@ -267,7 +398,43 @@ GF_API gf_status gf_mesh_set_modulus(gf_ctx* ctx, double E, const double* E_elem
   if (!ctx) return GF_ERR_INVALID_ARG;
   if (!ctx->has_mesh) return gf_fail(ctx, GF_ERR_STATE, "no mesh");
   cudaSetDevice(ctx->device);
-  return upload_modulus(ctx, E, E_elem);
+  // into fresh buffers first, so that an invalid modulus leaves the current one
+  const int nelem = ctx->nelem;
+  cudaStream_t s = ctx->stream;
+  double* Eel = nullptr;
+  float* Eel32 = nullptr;
+  unsigned long long* d_chk = nullptr;
+  unsigned long long h_chk[4];
+  gf_status st;
+  auto release = [&]() { gf_pfree(ctx, Eel); gf_pfree(ctx, Eel32); gf_pfree(ctx, d_chk); };
+  if ((st = gf_palloc(ctx, &Eel, (size_t)nelem)) != GF_OK ||
+      (st = gf_palloc(ctx, &Eel32, (size_t)nelem)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_chk, 4)) != GF_OK) {
+    release();
+    return st;
+  }
+  cudaMemsetAsync(d_chk, 0xff, 4 * sizeof(unsigned long long), s);
+  if (E_elem) cudaMemcpyAsync(Eel, E_elem, sizeof(double) * nelem, cudaMemcpyHostToDevice, s);
+  k_modulus<<<gf_blocks(nelem, 256), 256, 0, s>>>(nelem, E_elem ? 1 : 0, E, Eel, Eel32, d_chk);
+  ctx->launches++;
+  cudaMemcpyAsync(h_chk, d_chk, sizeof(h_chk), cudaMemcpyDeviceToHost, s);
+  cudaError_t ce = cudaStreamSynchronize(s);
+  if (ce == cudaSuccess) ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    release();
+    return gf_cuda_fail(ctx, ce, "modulus upload");
+  }
+  if ((st = check_failure(ctx, h_chk, ctx->nen, ctx->nnodes, nullptr, E, E_elem)) != GF_OK) {
+    release();
+    return st;
+  }
+  gf_pfree(ctx, d_chk);
+  gf_pfree(ctx, ctx->d_Eel);
+  gf_pfree(ctx, ctx->d_Eel32);
+  ctx->d_Eel = Eel;
+  ctx->d_Eel32 = Eel32;
+  ctx->E = E;
+  return GF_OK;
 }
 
 GF_API gf_status gf_mesh_color(gf_ctx* ctx, const int32_t* elem_color, int32_t* ncolors) {
@@ -325,7 +492,7 @@ GF_API gf_status gf_ell_convert_f64_to_f32(gf_ctx* ctx) {
   cudaSetDevice(ctx->device);
   gf_status st;
   const int64_t total = (int64_t)ctx->n * ctx->W;
-  if (!ctx->d_K32 && (st = gf_alloc(ctx, &ctx->d_K32, (size_t)total)) != GF_OK) return st;
+  if (!ctx->d_K32 && (st = gf_palloc(ctx, &ctx->d_K32, (size_t)total)) != GF_OK) return st;
   k_f64_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(total, ctx->d_K64, ctx->d_K32);
   GF_LAUNCH_CHECK(ctx, "k_f64_to_f32");
   ctx->has32 = true;
@@ -423,8 +590,8 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
   gf_lp_mesh_changed(ctx);
-  gf_free(ctx->d_f);
-  gf_free(ctx->d_fixed);
+  gf_pfree(ctx, ctx->d_f);
+  gf_pfree(ctx, ctx->d_fixed);
   ctx->h_supports.clear();
   ctx->nsup = 0;
   ctx->bc_mode_applied = -1;
@@ -432,12 +599,12 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
   ctx->n = n;
   ctx->W = width;
   ctx->nnz = nnz;
-  if ((st = gf_alloc(ctx, &ctx->d_rownnz, (size_t)n)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_colidx, total)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_K64, total)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_K32, total)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_f, (size_t)n)) != GF_OK) return st;
-  if ((st = gf_alloc(ctx, &ctx->d_fixed, (size_t)n)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &ctx->d_rownnz, (size_t)n)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &ctx->d_colidx, total)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &ctx->d_K64, total)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &ctx->d_K32, total)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &ctx->d_f, (size_t)n)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &ctx->d_fixed, (size_t)n)) != GF_OK) return st;
   ctx->h_f.assign(n, 0.0);
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_f, 0, sizeof(double) * n, ctx->stream));
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_fixed, 0, n, ctx->stream));

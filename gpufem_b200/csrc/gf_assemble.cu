@@ -250,9 +250,9 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   if ((st = gf_asm_tables(ctx, &d_tab)) != GF_OK) return st;
   const int64_t total = (int64_t)ctx->n * ctx->W;
   if (dtype == GF_F64) {
-    if (!ctx->d_K64 && (st = gf_alloc(ctx, &ctx->d_K64, (size_t)total)) != GF_OK) return st;
+    if (!ctx->d_K64 && (st = gf_palloc(ctx, &ctx->d_K64, (size_t)total)) != GF_OK) return st;
   } else {
-    if (!ctx->d_K32 && (st = gf_alloc(ctx, &ctx->d_K32, (size_t)total)) != GF_OK) return st;
+    if (!ctx->d_K32 && (st = gf_palloc(ctx, &ctx->d_K32, (size_t)total)) != GF_OK) return st;
   }
   cudaEventRecord(ctx->ev0, ctx->stream);
   if (scatter == GF_SCATTER_OWNER) {

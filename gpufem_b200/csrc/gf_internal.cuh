@@ -163,7 +163,16 @@ struct gf_ctx {
   int nnodes = 0, nelem = 0, analysis = 0;
   double E = 0.0, nu = 0.0;
   double lam1 = 0.0, mu1 = 0.0;  // Lame-type factors per unit modulus
-  std::vector<int32_t> h_conn;   // 0-based, host copy (colouring)
+  std::vector<int32_t> h_conn;   // 0-based, host copy (host colouring; filled on demand)
+  // device buffer pool (gf_palloc / gf_pfree)
+  struct PoolBlock {
+    void* p;
+    size_t bytes;
+    int64_t gen;
+  };
+  std::vector<std::pair<void*, size_t>> pool_live;
+  std::vector<PoolBlock> pool_free;
+  int64_t pool_gen = 0;
   double* d_coords64 = nullptr;
   float* d_coords32 = nullptr;
   int32_t* d_conn = nullptr;     // 0-based node ids
@@ -271,6 +280,32 @@ gf_status gf_alloc(gf_ctx* ctx, T** p, size_t count) {
 template <typename T>
 void gf_free(T*& p) {
   if (p) { cudaFree(p); p = nullptr; }
+}
+
+// Pooled device buffers for the per-mesh arrays (mesh, pattern, K): a released block
+// is kept by the context and handed out again for a request of exactly its size, so
+// re-creating a mesh of the same shape (a time loop, a parameter sweep) allocates
+// nothing.  Blocks released before the previous mesh generation are returned to the
+// driver when a new mesh is created; all of them at gf_destroy, and all of them
+// before an allocation that failed is retried.
+void* gf_pool_get(gf_ctx* ctx, size_t bytes);
+void gf_pool_put(gf_ctx* ctx, void* p);
+void gf_pool_new_generation(gf_ctx* ctx);
+void gf_pool_clear(gf_ctx* ctx);
+
+template <typename T>
+gf_status gf_palloc(gf_ctx* ctx, T** p, size_t count) {
+  if (*p) { gf_pool_put(ctx, *p); *p = nullptr; }
+  if (count == 0) count = 1;
+  *p = static_cast<T*>(gf_pool_get(ctx, count * sizeof(T)));
+  if (!*p)
+    return gf_fail(ctx, GF_ERR_OOM, "device allocation of %zu bytes failed", count * sizeof(T));
+  return GF_OK;
+}
+
+template <typename T>
+void gf_pfree(gf_ctx* ctx, T*& p) {
+  if (p) { gf_pool_put(ctx, p); p = nullptr; }
 }
 
 inline int gf_blocks(int64_t work, int threads) {

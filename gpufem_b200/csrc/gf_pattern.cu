@@ -216,12 +216,11 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
 
   int32_t *d_cnt = nullptr, *d_inc_off = nullptr, *d_fill = nullptr, *d_inc = nullptr;
   int32_t *d_nadj = nullptr, *d_err = nullptr, *d_max = nullptr;
-  void* d_tmp = nullptr;
+  char* d_tmp = nullptr;
   size_t tmp_bytes = 0, b1 = 0, b2 = 0, b3 = 0;
   auto cleanup = [&]() {
-    gf_free(d_cnt); gf_free(d_inc_off); gf_free(d_fill); gf_free(d_inc);
-    gf_free(d_nadj); gf_free(d_err); gf_free(d_max);
-    if (d_tmp) cudaFree(d_tmp);
+    gf_pfree(ctx, d_cnt); gf_pfree(ctx, d_inc_off); gf_pfree(ctx, d_fill); gf_pfree(ctx, d_inc);
+    gf_pfree(ctx, d_nadj); gf_pfree(ctx, d_err); gf_pfree(ctx, d_max); gf_pfree(ctx, d_tmp);
   };
 #define GF_TRY(x)             \
   do {                        \
@@ -233,14 +232,14 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
     if (e__ != cudaSuccess) { cleanup(); return gf_cuda_fail(ctx, e__, #call); } \
   } while (0)
 
-  GF_TRY(gf_alloc(ctx, &d_cnt, (size_t)nnodes + 1));
-  GF_TRY(gf_alloc(ctx, &d_inc_off, (size_t)nnodes + 1));
-  GF_TRY(gf_alloc(ctx, &d_fill, (size_t)nnodes + 1));
-  GF_TRY(gf_alloc(ctx, &d_inc, (size_t)total));
-  GF_TRY(gf_alloc(ctx, &d_nadj, (size_t)nnodes + 1));
-  GF_TRY(gf_alloc(ctx, &d_err, 1));
-  GF_TRY(gf_alloc(ctx, &d_max, 1));
-  GF_TRY(gf_alloc(ctx, &ctx->d_adj_off, (size_t)nnodes + 1));
+  GF_TRY(gf_palloc(ctx, &d_cnt, (size_t)nnodes + 1));
+  GF_TRY(gf_palloc(ctx, &d_inc_off, (size_t)nnodes + 1));
+  GF_TRY(gf_palloc(ctx, &d_fill, (size_t)nnodes + 1));
+  GF_TRY(gf_palloc(ctx, &d_inc, (size_t)total));
+  GF_TRY(gf_palloc(ctx, &d_nadj, (size_t)nnodes + 1));
+  GF_TRY(gf_palloc(ctx, &d_err, 1));
+  GF_TRY(gf_palloc(ctx, &d_max, 1));
+  GF_TRY(gf_palloc(ctx, &ctx->d_adj_off, (size_t)nnodes + 1));
   GF_TRYC(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (nnodes + 1), s));
   GF_TRYC(cudaMemsetAsync(d_nadj, 0, sizeof(int32_t) * (nnodes + 1), s));
   GF_TRYC(cudaMemsetAsync(d_err, 0, sizeof(int32_t), s));
@@ -249,7 +248,7 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   cub::DeviceReduce::Max(nullptr, b2, d_nadj, d_max, nnodes, s);
   b3 = b1;
   tmp_bytes = std::max(b1, std::max(b2, b3));
-  GF_TRYC(cudaMalloc(&d_tmp, tmp_bytes));
+  GF_TRY(gf_palloc(ctx, &d_tmp, tmp_bytes));
 
   k_count_incidence<<<gf_blocks(total, 256), 256, 0, s>>>(total, ctx->d_conn, d_cnt);
   ctx->launches++;
@@ -285,11 +284,11 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   ctx->nnz = (int64_t)h_tot * dim * dim;
   const int n = ctx->n;
   const int64_t slots = (int64_t)n * ctx->W;
-  GF_TRY(gf_alloc(ctx, &ctx->d_adj, (size_t)h_tot));
-  GF_TRY(gf_alloc(ctx, &ctx->d_rownnz, (size_t)n));
-  GF_TRY(gf_alloc(ctx, &ctx->d_colidx, (size_t)slots));
-  GF_TRY(gf_alloc(ctx, &ctx->d_slotmap, (size_t)nelem * nen * nen));
-  GF_TRY(gf_alloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
+  GF_TRY(gf_palloc(ctx, &ctx->d_adj, (size_t)h_tot));
+  GF_TRY(gf_palloc(ctx, &ctx->d_rownnz, (size_t)n));
+  GF_TRY(gf_palloc(ctx, &ctx->d_colidx, (size_t)slots));
+  GF_TRY(gf_palloc(ctx, &ctx->d_slotmap, (size_t)nelem * nen * nen));
+  GF_TRY(gf_palloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
   k_node_adjacency<1><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
       nnodes, nen, ctx->d_conn, d_inc_off, d_inc, nullptr, ctx->d_adj_off, ctx->d_adj, d_err);
   ctx->launches++;
@@ -305,8 +304,8 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
                                                    ctx->d_diagpos);
   ctx->launches++;
   // incidence kept for the owner-computes scatter
-  GF_TRY(gf_alloc(ctx, &ctx->d_inc_loc, (size_t)total));
-  GF_TRY(gf_alloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
+  GF_TRY(gf_palloc(ctx, &ctx->d_inc_loc, (size_t)total));
+  GF_TRY(gf_palloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
   k_incidence_finish<<<gf_blocks(nnodes, 128), 128, 0, s>>>(
       nnodes, nen, ctx->d_conn, d_inc_off, d_inc, ctx->d_adj_off, ctx->d_adj, ctx->d_inc_loc,
       ctx->d_inc_slot, d_err);
@@ -338,6 +337,13 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
 // ---------------------------------------------------------------------------
 gf_status gf_color_build(gf_ctx* ctx, const int32_t* user_colors) {
   const int nelem = ctx->nelem, nen = ctx->nen, nnodes = ctx->nnodes;
+  if (ctx->h_conn.size() != (size_t)nelem * nen) {  // host copy on first use
+    ctx->h_conn.resize((size_t)nelem * nen);
+    GF_CUDA(ctx, cudaMemcpyAsync(ctx->h_conn.data(), ctx->d_conn,
+                                 sizeof(int32_t) * ctx->h_conn.size(), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   const std::vector<int32_t>& conn = ctx->h_conn;
   // node -> element incidence
   std::vector<int32_t> off(nnodes + 1, 0), inc((size_t)nelem * nen);

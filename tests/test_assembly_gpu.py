@@ -210,3 +210,42 @@ def test_full_size_rigid_translation(fem, name):
     y32 = ctx.spmv(x, _lib.GF_F32)
     y64 = ctx.spmv(x, _lib.GF_F64)
     assert np.linalg.norm(y32 - y64) <= 1e-5 * np.linalg.norm(y64)
+
+
+def test_rejected_mesh_keeps_current_and_reuse_is_exact(fem, oracle):
+    """A mesh that fails validation leaves the current one usable; re-creating meshes
+    (same shape, then another shape, then the first again) reuses pooled buffers and
+    gives the same matrix every time."""
+    m = mg.structured(mg.Q8, (6, 5), jitter=0.2, seed=4, ngauss=3)
+    other = mg.structured(mg.BRICK8, (3, 3, 2), jitter=0.1, seed=5, ngauss=2)
+    ctx = fem(0)
+    ctx.mesh_create(m.elem_type, m.coords, m.conn, 3, 210e3, None, 0.3)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+    first = ctx.ell_download(_lib.GF_F64)
+    bad = m.conn.copy()
+    bad[2, 3] = bad[2, 0]
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.mesh_create(m.elem_type, m.coords, bad, 3, 210e3, None, 0.3)
+    assert ei.value.status == _lib.GF_ERR_INVALID_ARG
+    assert "repeats node" in str(ei.value)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)      # the current mesh still works
+    again = ctx.ell_download(_lib.GF_F64)
+    for a, b in zip(first, again):
+        assert np.array_equal(a, b)
+    ctx.mesh_create(other.elem_type, other.coords, other.conn, 2, 210e3, None, 0.3)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    rno, cio, vo = oracle.assemble(other.elem_type, 2, other.coords, other.conn, 210e3, 0.3)
+    assert np.array_equal(rn, rno)
+    for _ in range(2):
+        ctx.mesh_create(m.elem_type, m.coords, m.conn, 3, 210e3, None, 0.3)
+        ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+        third = ctx.ell_download(_lib.GF_F64)
+        for a, b in zip(first, third):
+            assert np.array_equal(a, b)
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.set_modulus(-5.0)
+    assert ei.value.status == _lib.GF_ERR_INVALID_ARG
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)      # modulus unchanged
+    for a, b in zip(first, ctx.ell_download(_lib.GF_F64)):
+        assert np.array_equal(a, b)
