@@ -31,6 +31,7 @@
 // scatter of StiffAlgo::AssembleK (src/FEM/StiffAlgo.cc:304-401), by rows.
 #include <algorithm>
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "gf_elem.cuh"
@@ -235,6 +236,62 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
   for (int k = lane; k < nw * PER; k += 32) dst[k] = stage[k];
 }
 
+// Block rows H_j, j in [J0, J0 + JG), of one task with the Gauss rule known at compile
+// time: every dN_j value is an instruction constant, only J^-1 / w*detJ (global) and
+// the owned node's row of dN (shared memory) are read.
+template <int ET, typename TC, int JG, int NG1, int J0>
+__device__ __forceinline__ void owner_rows_ct(const TC* __restrict__ ge, TC Ee,
+                                              const TC* __restrict__ sdN, int i,
+                                              TC (&H)[JG][gf_elem_info(ET).dim][gf_elem_info(ET).dim]) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  constexpr int NEN = info.nen, DIM = info.dim, GS = DIM * DIM + 1;
+  constexpr GpTable<ET, NG1> Tab = gf_gp_table<ET, NG1>();
+#pragma unroll
+  for (int g = 0; g < GpTable<ET, NG1>::NGP; ++g) {
+    TC Ji[DIM][DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) Ji[a][b] = __ldg(ge + g * GS + a * DIM + b);
+    const TC wd = __ldg(ge + g * GS + DIM * DIM) * Ee;
+    const TC* dN = sdN + g * DIM * NEN;
+    TC gi[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      TC s = TC(0);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i];
+      gi[c] = s * wd;
+    }
+#pragma unroll
+    for (int jj = 0; jj < JG; ++jj) {
+      TC gj[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        TC s = TC(0);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          const int q = (g * DIM + a) * NEN + J0 + jj;
+          s += Ji[c][a] * (sizeof(TC) == 8 ? TC(Tab.d64[q]) : TC(Tab.d32[q]));
+        }
+        gj[c] = s;
+      }
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) H[jj][a][b] += gi[a] * gj[b];
+    }
+  }
+}
+
+// Runtime node-group index -> the compile-time instance for that group.
+template <int ET, typename TC, int JG, int NG1, int... G>
+__device__ __forceinline__ void owner_rows_ct_switch(
+    int jg, const TC* ge, TC Ee, const TC* sdN, int i,
+    TC (&H)[JG][gf_elem_info(ET).dim][gf_elem_info(ET).dim], std::integer_sequence<int, G...>) {
+  ((jg == G ? owner_rows_ct<ET, TC, JG, NG1, G * JG>(ge, Ee, sdN, i, H) : void()), ...);
+}
+
 // ---------------------------------------------------------------------------
 // One work item per (task, group of JG element nodes j): a task's NEN/JG items run
 // on neighbouring lanes and read the same element data.  The owning node of every
@@ -294,47 +351,9 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
       for (int a = 0; a < DIM; ++a)
 #pragma unroll
         for (int b = 0; b < DIM; ++b) H[jj][a][b] = TC(0);
-    if constexpr (NG1 > 0 && JG == NEN) {
-      // Gauss rule known at compile time and the whole element in one item: every
-      // dN_j value is an instruction constant (only the owned node's row is read
-      // from shared memory)
-      constexpr GpTable<ET, NG1> Tab = gf_gp_table<ET, NG1>();
-#pragma unroll
-      for (int g = 0; g < GpTable<ET, NG1>::NGP; ++g) {
-        TC Ji[DIM][DIM];
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int b = 0; b < DIM; ++b) Ji[a][b] = __ldg(ge + g * GS + a * DIM + b);
-        const TC wd = __ldg(ge + g * GS + DIM * DIM) * Ee;
-        const TC* dN = sdN + g * DIM * NEN;
-        TC gi[DIM];
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          TC s = TC(0);
-#pragma unroll
-          for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i];
-          gi[c] = s * wd;
-        }
-#pragma unroll
-        for (int j = 0; j < NEN; ++j) {
-          TC gj[DIM];
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            TC s = TC(0);
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) {
-              const int q = (g * DIM + a) * NEN + j;
-              s += Ji[c][a] * (sizeof(TC) == 8 ? TC(Tab.d64[q]) : TC(Tab.d32[q]));
-            }
-            gj[c] = s;
-          }
-#pragma unroll
-          for (int a = 0; a < DIM; ++a)
-#pragma unroll
-            for (int b = 0; b < DIM; ++b) H[j][a][b] += gi[a] * gj[b];
-        }
-      }
+    if constexpr (NG1 > 0) {
+      owner_rows_ct_switch<ET, TC, JG, NG1>(j0 / JG, ge, Ee, sdN, i, H,
+                                            std::make_integer_sequence<int, NJ>{});
     } else {
 #pragma unroll 1
       for (int g = 0; g < ngp; ++g) {
@@ -410,6 +429,13 @@ constexpr int owner_jgroup() {
   return gf_elem_info(ET).nen <= 8 ? gf_elem_info(ET).nen : sizeof(TC) == 4 ? 5 : 2;
 }
 
+// Element types whose owner kernel unrolls the Gauss loop against the compile-time
+// table (2-D; in 3-D the unrolled loop costs more registers than it saves).
+template <int ET, typename TC>
+constexpr bool owner_compile_time_gauss() {
+  return gf_elem_info(ET).dim == 2;
+}
+
 template <int ET, typename TC>
 gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   constexpr ElemInfo info = gf_elem_info(ET);
@@ -453,10 +479,8 @@ gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   if (sm > kOwnerSmemLimit)
     return gf_fail(ctx, GF_ERR_UNSUPPORTED, "owner scatter: a row block does not fit");
   constexpr int JG = owner_jgroup<ET, TC>();
-  // compile-time Gauss rule for 2-D elements (one work item per task; in 3-D the
-  // unrolled Gauss loop costs more registers than it saves)
   auto kern = k_assemble_owner<ET, TC, JG, 0>;
-  if constexpr (JG == info.nen && info.dim == 2)
+  if constexpr (owner_compile_time_gauss<ET, TC>())
     kern = ctx->ngauss == 2 ? k_assemble_owner<ET, TC, JG, 2> : k_assemble_owner<ET, TC, JG, 3>;
   GF_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
