@@ -35,7 +35,7 @@ UNIT = "elements/s"
 WORKLOADS = {
     # name: (description, dtype of the timed assembly)
     "q8_512": "Q8 512x512 plane stress, jitter 0.15h, 3x3 Gauss, log-normal E (sigma 0.5), "
-              "FP32 colour-scheduled assembly into ELL",
+              "FP32 owner-computes assembly into ELL",
     "q4_64": "Q4 64x64 plane stress, jitter 0.2h, 2x2 Gauss, FP64 assembly",
     "brick8_128": "Brick8 128^3, jitter 0.1h, 2x2x2 Gauss, FP32 assembly",
     "brick20_64": "Brick20 64^3, jitter 0.05h, 3x3x3 Gauss, correlated log-normal E, FP32",
@@ -168,6 +168,26 @@ def reference_sample(config: str, steps: int, warmup: int):
     t = float(np.median(times))
     return {"value": m.nelem / t, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
             "cpu": cpu_model(), "seconds_per_step": t}
+
+
+def reference_cg_sample(m, iters: int = 20):
+    """The reference's own flow on the full workload mesh (FP32 build as shipped):
+    ReadNF -> StiffAlgoCPU (naive, all cores) -> ApplyConstraint(PEN) -> CPU_CG in
+    DEV_OMP for `iters` iterations.  Returns the full-size assembly rate and the CG time
+    per iteration; None without the reference build."""
+    from oracle.oracle import Reference
+    if not Reference.available("fp32"):
+        return None
+    cores = os.cpu_count() or 1
+    s = Reference("fp32").open_mesh(m)
+    try:
+        t_asm = s.assemble(coloring=False, nthreads=cores)
+        s.penalty()
+        _, t_cg = s.cg(iters, 1e-30, nthreads=cores)   # eps far below reach: exactly iters
+    finally:
+        s.close()
+    return {"assembly_elements_per_s": m.nelem / t_asm, "cg_us_per_iteration": t_cg / iters * 1e6,
+            "cg_iterations_timed": iters, "threads": cores, "cpu": cpu_model()}
 
 
 def run_reference_arm(args):
@@ -430,6 +450,15 @@ def run_gpu_arm(args):
                            "outer": mix.outer, "fp64_fallback": mix.fallback,
                            "status": mix.status, "rel_residual": mix.rel_residual,
                            "rel_err_vs_reference": float(np.linalg.norm(umix - ustar) / nrm)}
+        if rank == 0 and world == 1 and not args.no_cpu and cfg in ("q4_64", "q8_512"):
+            # (the reference's assembly of the full 3-D meshes alone takes minutes)
+            rc = reference_cg_sample(m)
+            if rc is not None:
+                rc["extrapolated_seconds"] = rc["cg_us_per_iteration"] * 1e-6 * p64.iterations
+                rc["label"] = ("extrapolated: reference CPU_CG (unpreconditioned CG, FP32, OpenMP) "
+                               "time per iteration on the full system x the FP64 Jacobi-PCG "
+                               "iteration count above; assembly timed once on the full mesh")
+                solve["cpu_reference"] = rc
 
     learned = None
     if not args.no_solve and rank == 0:
