@@ -304,7 +304,7 @@ def run_gpu_arm(args):
         torch.cuda.synchronize()
 
     scatter = {"owner": _lib.GF_SCATTER_OWNER, "colour": _lib.GF_SCATTER_COLOR,
-               "atomic": _lib.GF_SCATTER_ATOMIC}[args.scatter]
+               "atomic": _lib.GF_SCATTER_ATOMIC, "auto": _lib.GF_SCATTER_AUTO}[args.scatter]
     for _ in range(args.warmup):
         ctx.assemble(dtype, scatter)
     barrier()
@@ -519,7 +519,7 @@ def main():
     ap.add_argument("--config", default="q8_512", choices=sorted(WORKLOADS))
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--scatter", default="owner", choices=["owner", "colour", "atomic"])
+    ap.add_argument("--scatter", default="owner", choices=["owner", "colour", "atomic", "auto"])
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "GF_OK", 1: "GF_ERR_INVALID_ARG", 2: "GF_ERR_OOM", 3: "GF_ERR
 GF_Q4, GF_Q8, GF_BRICK8, GF_BRICK20 = 0, 1, 2, 3
 GF_PLANE_STRESS, GF_PLANE_STRAIN = 0, 1
 GF_F64, GF_F32 = 0, 1
-GF_SCATTER_COLOR, GF_SCATTER_ATOMIC, GF_SCATTER_OWNER = 0, 1, 2
+GF_SCATTER_COLOR, GF_SCATTER_ATOMIC, GF_SCATTER_OWNER, GF_SCATTER_AUTO = 0, 1, 2, 3
 GF_ENGINE_CUDA_CORE, GF_ENGINE_TF32_MMA = 0, 1
 GF_BC_PENALTY, GF_BC_ELIMINATION = 0, 1
 GF_SOLVER_CG, GF_SOLVER_PCG, GF_SOLVER_MIXED_PCG, GF_SOLVER_LEARNED_FCG, GF_SOLVER_MIXED_PCG32 = 0, 1, 2, 3, 4

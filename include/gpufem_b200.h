@@ -64,9 +64,11 @@ typedef enum gf_dtype { GF_F64 = 0, GF_F32 = 1 } gf_dtype;
 typedef enum gf_scatter {
   GF_SCATTER_COLOR = 0,  /* colour classes in turn, plain read-modify-write (no atomics) */
   GF_SCATTER_ATOMIC = 1, /* all elements at once, red.global.add into K               */
-  GF_SCATTER_OWNER = 2   /* owner computes: each CTA owns a node range, sums the blocks
+  GF_SCATTER_OWNER = 2,  /* owner computes: each CTA owns a node range, sums the blocks
                             of its rows in shared memory and writes every K entry once
                             (no colouring, no global atomics, no zero-fill)            */
+  GF_SCATTER_AUTO = 3    /* the fastest of the above for the element type, as measured
+                            on B200: OWNER for Q4, Q8 and Brick8, ATOMIC for Brick20  */
 } gf_scatter;
 
 /* Element-integration engine of gf_assemble (FP32 only; FP64 always uses CUDA cores). */

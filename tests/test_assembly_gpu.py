@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
 TOL32 = 1e-6
-SCATTERS = [_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC, _lib.GF_SCATTER_OWNER]
+SCATTERS = [_lib.GF_SCATTER_COLOR, _lib.GF_SCATTER_ATOMIC, _lib.GF_SCATTER_OWNER,
+            _lib.GF_SCATTER_AUTO]
 
 
 @pytest.fixture(scope="module")
