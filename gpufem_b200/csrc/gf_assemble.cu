@@ -212,7 +212,6 @@ gf_status launch_dispatch(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* 
 }  // namespace
 
 gf_status gf_assemble_owner(gf_ctx* ctx, int dtype, const AsmTables* d_tab);
-gf_status gf_assemble_owner_check(gf_ctx* ctx);
 
 gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out) {
   if (ctx->d_asmtab) {
@@ -269,7 +268,6 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (st != GF_OK) return st;
   if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "assembly");
-  if (scatter == GF_SCATTER_OWNER && (st = gf_assemble_owner_check(ctx)) != GF_OK) return st;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   ctx->last_seconds = ms * 1e-3;

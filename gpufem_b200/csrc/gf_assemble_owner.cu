@@ -511,9 +511,5 @@ gf_status gf_assemble_owner(gf_ctx* ctx, int dtype, const AsmTables* d_tab) {
   return owner_dispatch<float>(ctx, ctx->d_K32, d_tab);
 }
 
-gf_status gf_assemble_owner_check(gf_ctx* ctx) {
-  (void)ctx;
-  return GF_OK;
-}
 
 
