@@ -36,12 +36,35 @@ namespace {
 
 constexpr int kThreads = 256;
 
-template <typename T>
-__device__ inline void k_add(T* p, T v, bool atomic) {
-  if (atomic) {
-    atomicAdd(p, v);
+// Adds DIM values to DIM consecutive rows of one ELL slot column (the rows of one
+// node).  Atomic FP32 uses vector reductions where the address allows: one
+// red.global.add.v2.f32 for a 2-D node (its two rows start 8-byte aligned because n
+// is even), a v2 plus a scalar reduction for a 3-D node; FP64 and the colour schedule
+// (plain read-modify-write) go per value.
+__device__ inline void red_v2_f32(float* p, float a, float b) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
+
+template <int DIM, typename T, bool ATOMIC>
+__device__ inline void add_rows(T* p, const T (&v)[DIM]) {
+  if constexpr (ATOMIC && sizeof(T) == 4 && DIM >= 2) {
+    float* q = reinterpret_cast<float*>(p);
+    if ((reinterpret_cast<uintptr_t>(q) & 7) == 0) {
+      red_v2_f32(q, (float)v[0], (float)v[1]);
+      if (DIM == 3) atomicAdd(q + 2, (float)v[DIM - 1]);
+    } else if (DIM == 3) {
+      atomicAdd(q, (float)v[0]);
+      red_v2_f32(q + 1, (float)v[1], (float)v[DIM - 1]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) atomicAdd(q + c, (float)v[c]);
+    }
+  } else if constexpr (ATOMIC) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) atomicAdd(p + c, v[c]);
   } else {
-    *p += v;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) p[c] += v[c];
   }
 }
 
@@ -142,15 +165,28 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
     const int ni = sconn[e * NEN + i], nj = sconn[e * NEN + j];
     const int sij = slotmap[(int64_t)(i * NEN + j) * nelem + el] * DIM;
     const int sji = slotmap[(int64_t)(j * NEN + i) * nelem + el] * DIM;
+    TC V[DIM][DIM];
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
 #pragma unroll
       for (int b = 0; b < DIM; ++b) {
-        TC v = lam1 * H[a][b] + mu1 * H[b][a];
-        if (a == b) v += mu1 * tr;
-        k_add(&K[(int64_t)(sij + b) * n + (ni * DIM + a)], v, ATOMIC);
-        if (i != j) k_add(&K[(int64_t)(sji + a) * n + (nj * DIM + b)], v, ATOMIC);
+        V[a][b] = lam1 * H[a][b] + mu1 * H[b][a];
+        if (a == b) V[a][b] += mu1 * tr;
       }
+    // block (i, j): column b of the block goes to rows ni*DIM .. ni*DIM + DIM - 1 of slot
+    // column sij + b; block (j, i) is the transpose
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) {
+      TC col[DIM];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) col[a] = V[a][b];
+      add_rows<DIM, TC, ATOMIC>(&K[(int64_t)(sij + b) * n + ni * DIM], col);
+    }
+    if (i != j) {
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+        add_rows<DIM, TC, ATOMIC>(&K[(int64_t)(sji + a) * n + nj * DIM], V[a]);
+    }
   }
 }
 
