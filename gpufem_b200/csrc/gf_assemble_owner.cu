@@ -407,12 +407,14 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
     }
   }
   __syncthreads();
-  // flush: warp w stores slots w, w + 8, ...; lanes stride the block's rows
+  // flush: warp w stores slots w, w + 8, ...; lanes stride the block's rows.  Streaming
+  // (evict-first) stores keep K, written once, from displacing the geometry buffer
+  // the other CTAs still read from L2.
   const int rows = (a1 - a0) * DIM;
   const int64_t row0 = (int64_t)a0 * DIM;
   for (int s = threadIdx.x >> 5; s < W; s += kOT >> 5)
     for (int r = threadIdx.x & 31; r < rows; r += 32)
-      K[(int64_t)s * n + row0 + r] = tile[(size_t)s * RB + r];
+      __stcs(&K[(int64_t)s * n + row0 + r], tile[(size_t)s * RB + r]);
 }
 
 template <int ET, typename TC>
