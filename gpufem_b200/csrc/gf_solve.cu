@@ -134,14 +134,14 @@ __global__ void __launch_bounds__(kT)
 k_residual64(MatLayout L, const double* __restrict__ val, const double* __restrict__ u,
              const double* __restrict__ f, double* __restrict__ r, double* __restrict__ acc) {
   __shared__ double sh[32];
-  const int row = blockIdx.x * kT + threadIdx.x;
   int nz;
   int64_t o, st;
   double rr = 0.0;
-  if (L.at(row, nz, o, st)) {
+  for (int row = blockIdx.x * kT + threadIdx.x; row < L.count; row += gridDim.x * kT) {
+    if (!L.at(row, nz, o, st)) continue;
     double v = f[row] - row_dot(o, st, nz, L.col, val, u);
     r[row] = v;
-    rr = v * v;
+    rr += v * v;
   }
   double s = block_sum(rr, sh);
   if (threadIdx.x == 0) atomicAdd(acc, s);
@@ -153,17 +153,16 @@ __global__ void __launch_bounds__(kT)
 k_cg_init(int n, const V* __restrict__ b, const V* __restrict__ dinv, V* __restrict__ x,
           V* __restrict__ r, V* __restrict__ z, V* __restrict__ p, SolveScalars* sc) {
   __shared__ double sh[32];
-  const int i = blockIdx.x * kT + threadIdx.x;
   double rz = 0.0, rr = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
     V bi = b[i];
     x[i] = V(0);
     r[i] = bi;
     V zi = dinv ? bi * dinv[i] : bi;
     z[i] = zi;
     p[i] = zi;
-    rz = (double)bi * (double)zi;
-    rr = (double)bi * (double)bi;
+    rz += (double)bi * (double)zi;
+    rr += (double)bi * (double)bi;
   }
   double s1 = block_sum(rz, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
@@ -191,14 +190,14 @@ k_cg_spmv_dot(MatLayout L, const TK* __restrict__ val, const V* __restrict__ p,
     sc->rzn = 0.0;
     sc->rr = 0.0;
   }
-  const int row = blockIdx.x * kT + threadIdx.x;
   int nz;
   int64_t o, st;
   double pq = 0.0;
-  if (L.at(row, nz, o, st)) {
+  for (int row = blockIdx.x * kT + threadIdx.x; row < L.count; row += gridDim.x * kT) {
+    if (!L.at(row, nz, o, st)) continue;
     double v = row_dot(o, st, nz, L.col, val, p);
     q[row] = (V)v;
-    pq = (double)p[row] * (double)(V)v;
+    pq += (double)p[row] * (double)(V)v;
   }
   double s = block_sum(pq, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->pq, s);
@@ -217,9 +216,8 @@ k_cg_update(int n, V* __restrict__ x, V* __restrict__ r, V* __restrict__ z,
     return;
   }
   const V alpha = (V)(sc->rz / pq);
-  const int i = blockIdx.x * kT + threadIdx.x;
   double rz = 0.0, rr = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
     x[i] += alpha * p[i];
     V ri = r[i] - alpha * q[i];
     r[i] = ri;
@@ -228,8 +226,8 @@ k_cg_update(int n, V* __restrict__ x, V* __restrict__ r, V* __restrict__ z,
       zi = ri * dinv[i];
       z[i] = zi;
     }
-    rz = (double)ri * (double)zi;
-    rr = (double)ri * (double)ri;
+    rz += (double)ri * (double)zi;
+    rr += (double)ri * (double)ri;
   }
   double s1 = block_sum(rz, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
@@ -338,6 +336,12 @@ __global__ void k_eliminate(int n, int W, const int32_t* __restrict__ rownnz,
 __global__ void k_zero_fixed(int n, const uint8_t* __restrict__ fixed, double* __restrict__ f) {
   const int i = blockIdx.x * kT + threadIdx.x;
   if (i < n && fixed[i]) f[i] = 0.0;
+}
+
+// Grid of the reducing kernels: at most 8 CTAs per SM, rows strided over the grid, so
+// that each reduction issues a few thousand global atomics at most (one per CTA).
+inline int red_grid(const gf_ctx* ctx, int64_t work) {
+  return std::min(gf_blocks(work, kT), ctx->sm_count * 8);
 }
 
 // The sliced copy of the context's matrix in `dtype` (built or refreshed on demand).
@@ -457,7 +461,7 @@ gf_status run_cg(gf_ctx* ctx, MatLayout L, const TK* val, const V* b, CgVecs vv,
   const V* dinv = precond ? (const V*)vv.dinv : nullptr;
   V* zz = precond ? z : r;  // without a preconditioner z aliases r
   GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
-  k_cg_init<V><<<nb, kT, 0, s>>>(n, b, dinv, x, r, zz, p, sc);
+  k_cg_init<V><<<red_grid(ctx, n), kT, 0, s>>>(n, b, dinv, x, r, zz, p, sc);
   GF_LAUNCH_CHECK(ctx, "k_cg_init");
   k_cg_init_fin<<<1, 1, 0, s>>>(sc, eps, maxit);
   GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
@@ -467,8 +471,8 @@ gf_status run_cg(gf_ctx* ctx, MatLayout L, const TK* val, const V* b, CgVecs vv,
   cudaGraphExec_t exec = nullptr;
   GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < check_every; ++k) {
-    k_cg_spmv_dot<TK, V><<<gf_blocks(L.count, kT), kT, 0, s>>>(L, val, p, q, sc);
-    k_cg_update<V><<<nb, kT, 0, s>>>(n, x, r, zz, p, q, dinv, sc);
+    k_cg_spmv_dot<TK, V><<<red_grid(ctx, L.count), kT, 0, s>>>(L, val, p, q, sc);
+    k_cg_update<V><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, zz, p, q, dinv, sc);
     k_cg_direction<V><<<nb, kT, 0, s>>>(n, zz, p, sc);
   }
   cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -536,7 +540,7 @@ gf_status residual64(gf_ctx* ctx, double* r64, double* rr) {
   const void* val = nullptr;
   gf_status st = solver_matrix(ctx, GF_F64, &L, &val);
   if (st != GF_OK) return st;
-  k_residual64<<<gf_blocks(L.count, kT), kT, 0, s>>>(L, (const double*)val, ctx->d_u, ctx->d_f,
+  k_residual64<<<red_grid(ctx, L.count), kT, 0, s>>>(L, (const double*)val, ctx->d_u, ctx->d_f,
                                                      r64, ctx->d_red);
   GF_LAUNCH_CHECK(ctx, "k_residual64");
   double* h = (double*)ctx->h_pinned + 16;
@@ -582,16 +586,15 @@ __global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv,
                               int restart, const V* __restrict__ dinv, V* __restrict__ r,
                               V* __restrict__ z, V* __restrict__ p, SolveScalars* sc) {
   __shared__ double sh[32];
-  const int i = blockIdx.x * kT + threadIdx.x;
   double rz = 0.0, rr = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
     const V ri = (V)(r64[i] * inv);
     const V zi = ri * dinv[i];
     r[i] = ri;
     z[i] = zi;
     p[i] = restart ? zi : p[i] * pscale;
-    rz = (double)ri * (double)zi;
-    rr = (double)ri * (double)ri;
+    rz += (double)ri * (double)zi;
+    rr += (double)ri * (double)ri;
   }
   double s1 = block_sum(rz, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
@@ -649,7 +652,7 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     k_scale_to<V><<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
     GF_LAUNCH_CHECK(ctx, "k_scale_to");
     GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
-    k_cg_init<V><<<nb, kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
+    k_cg_init<V><<<red_grid(ctx, n), kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
     GF_LAUNCH_CHECK(ctx, "k_cg_init");
     k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
     GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
@@ -657,8 +660,8 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     cudaGraphExec_t exec = nullptr;
     GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < check; ++k) {
-      k_cg_spmv_dot<float, V><<<gf_blocks(L32.count, kT), kT, 0, s>>>(L32, val32, p, q, sc);
-      k_cg_update<V><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+      k_cg_spmv_dot<float, V><<<red_grid(ctx, L32.count), kT, 0, s>>>(L32, val32, p, q, sc);
+      k_cg_update<V><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
       k_cg_direction<V><<<nb, kT, 0, s>>>(n, z, p, sc);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -711,7 +714,7 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       const double sigma_new = std::sqrt(rr64);
       ce = cudaMemsetAsync(&sc->rzn, 0, 2 * sizeof(double), s);  // rzn, rr
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "reset"); break; }
-      k_mixed_reset<V><<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma_new, (V)(sigma / sigma_new),
+      k_mixed_reset<V><<<red_grid(ctx, n), kT, 0, s>>>(n, r64, 1.0 / sigma_new, (V)(sigma / sigma_new),
                                          restart ? 1 : 0, dinv, r, z, p, sc);
       k_mixed_scalars<<<1, 1, 0, s>>>(sc, tol * tol * ff / rr64);
       ce = cudaGetLastError();
@@ -784,13 +787,12 @@ struct FcgScalars {
 __global__ void k_fcg_init(int n, const double* __restrict__ f, double* __restrict__ x,
                            double* __restrict__ r, double* __restrict__ rold, FcgScalars* sc) {
   __shared__ double sh[32];
-  const int i = blockIdx.x * kT + threadIdx.x;
   double rr = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
     x[i] = 0.0;
     r[i] = f[i];
     rold[i] = 0.0;
-    rr = f[i] * f[i];
+    rr += f[i] * f[i];
   }
   double s1 = block_sum(rr, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->rr, s1);
@@ -818,11 +820,10 @@ __global__ void k_fcg_dots(int n, const double* __restrict__ z, const double* __
                            const double* __restrict__ rold, FcgScalars* sc) {
   __shared__ double sh[32];
   if (sc->done) return;
-  const int i = blockIdx.x * kT + threadIdx.x;
   double a = 0.0, b = 0.0;
-  if (i < n) {
-    a = z[i] * r[i];
-    b = z[i] * rold[i];
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
+    a += z[i] * r[i];
+    b += z[i] * rold[i];
   }
   double s1 = block_sum(a, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->zr, s1);
@@ -848,15 +849,15 @@ k_fcg_spmv(MatLayout L, const double* __restrict__ val, const double* __restrict
   __shared__ double sh[32];
   if (sc->done) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) sc->rr = 0.0;
-  const int row = blockIdx.x * kT + threadIdx.x;
   int nz;
   int64_t o, st;
   double pq = 0.0, pr = 0.0;
-  if (L.at(row, nz, o, st)) {
+  for (int row = blockIdx.x * kT + threadIdx.x; row < L.count; row += gridDim.x * kT) {
+    if (!L.at(row, nz, o, st)) continue;
     const double v = row_dot(o, st, nz, L.col, val, p);
     q[row] = v;
-    pq = p[row] * v;
-    pr = p[row] * r[row];
+    pq += p[row] * v;
+    pr += p[row] * r[row];
   }
   double s1 = block_sum(pq, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->pq, s1);
@@ -874,15 +875,14 @@ __global__ void k_fcg_update(int n, double* __restrict__ x, double* __restrict__
     return;
   }
   const double alpha = sc->pr / sc->pq;
-  const int i = blockIdx.x * kT + threadIdx.x;
   double rr = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
     x[i] += alpha * p[i];
     const double ri = r[i];
     rold[i] = ri;
     const double rn = ri - alpha * q[i];
     r[i] = rn;
-    rr = rn * rn;
+    rr += rn * rn;
   }
   double s = block_sum(rr, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->rr, s);
@@ -942,7 +942,7 @@ gf_status run_fcg(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_LAUNCH_CHECK(ctx, "k_diag_inv");
   GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(FcgScalars), s));
-  k_fcg_init<<<nb, kT, 0, s>>>(n, ctx->d_f, x, r, rold, sc);
+  k_fcg_init<<<red_grid(ctx, n), kT, 0, s>>>(n, ctx->d_f, x, r, rold, sc);
   k_fcg_init_fin<<<1, 1, 0, s>>>(sc, o->tol, maxit);
   GF_LAUNCH_CHECK(ctx, "k_fcg_init");
   // two chunk graphs: learned preconditioner and Jacobi
@@ -953,10 +953,10 @@ gf_status run_fcg(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     for (int k = 0; k < check; ++k) {
       if (kind == 0) gf_lp_apply64(ctx, r, r32, z);
       else k_fcg_jacobi<<<nb, kT, 0, s>>>(n, r, dinv, z, sc);
-      k_fcg_dots<<<nb, kT, 0, s>>>(n, z, r, rold, sc);
+      k_fcg_dots<<<red_grid(ctx, n), kT, 0, s>>>(n, z, r, rold, sc);
       k_fcg_dir<<<nb, kT, 0, s>>>(n, z, p, sc);
-      k_fcg_spmv<<<gf_blocks(L.count, kT), kT, 0, s>>>(L, val, p, r, q, sc);
-      k_fcg_update<<<nb, kT, 0, s>>>(n, x, r, rold, p, q, sc);
+      k_fcg_spmv<<<red_grid(ctx, L.count), kT, 0, s>>>(L, val, p, r, q, sc);
+      k_fcg_update<<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, rold, p, q, sc);
       k_fcg_finish<<<1, 1, 0, s>>>(sc);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph[kind]);
@@ -1045,7 +1045,7 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
   if ((st = solver_matrix(ctx, GF_F64, &L, &vk)) != GF_OK) return st;
   k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
-  k_cg_init<double><<<nb, kT, 0, s>>>(n, ctx->d_f, dinv, x, r, z, p, sc);
+  k_cg_init<double><<<red_grid(ctx, n), kT, 0, s>>>(n, ctx->d_f, dinv, x, r, z, p, sc);
   k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
   GF_LAUNCH_CHECK(ctx, "k_cg_init");
   k_record_pair<<<nb, kT, 0, s>>>(n, r, x, ustar, r_out, e_out);  // iteration 0: e = u*
@@ -1053,9 +1053,9 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
   int got = 1;
   while (got < npairs) {
     for (int k = 0; k < every; ++k) {
-      k_cg_spmv_dot<double, double><<<gf_blocks(L.count, kT), kT, 0, s>>>(
+      k_cg_spmv_dot<double, double><<<red_grid(ctx, L.count), kT, 0, s>>>(
           L, (const double*)vk, p, q, sc);
-      k_cg_update<double><<<nb, kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+      k_cg_update<double><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
       k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
     }
     ctx->launches += 3 * every;
