@@ -211,6 +211,40 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # learned preconditioner vs plain Jacobi-PCG (multi-mesh Brick8 workload)
 # ---------------------------------------------------------------------------
+def _preconditioner_diagnostic(ctx, ustar):
+    """How the learned preconditioner M acts on residuals r_k of Jacobi-PCG after k
+    iterations, against Jacobi (D^-1 r): the cosine between the two corrections, and the
+    energy norm of the error left after the best multiple of each correction,
+    ||e - a z||_K / ||e||_K (1.0 = no reduction)."""
+    import scipy.sparse as sp
+    from gpufem_b200 import _lib
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    W, n = ci.shape
+    mask = np.arange(W)[:, None] < rn[None, :]
+    rows = np.broadcast_to(np.arange(n)[None, :], (W, n))
+    K = sp.csr_matrix((v[mask], (rows[mask], ci[mask])), shape=(n, n))
+    f = ctx.get_force()
+    d = K.diagonal()
+    out = []
+    for it in (1, 20, 100):
+        ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-14, max_iter=it, raise_on_error=False)
+        u = ctx.solution()
+        r = f - K @ u
+        e = ustar - u
+        eKe = float(e @ (K @ e))
+        row = {"pcg_iterations": it}
+        zs = {"jacobi": r / d, "learned": ctx.lp_apply(r)}
+        for k, z in zs.items():
+            Kz = K @ z
+            a = float(z @ (K @ e)) / float(z @ Kz)
+            w = e - a * z
+            row[f"energy_error_after_{k}"] = float(np.sqrt(max(w @ (K @ w), 0.0) / eKe))
+        zj, zl = zs["jacobi"], zs["learned"]
+        row["cosine_learned_jacobi"] = float(zj @ zl / (np.linalg.norm(zj) * np.linalg.norm(zl)))
+        out.append(row)
+    return out
+
+
 def learned_comparison(seed_base: int = 20260105, n_train: int = 6):
     """Brick8 cubes with correlated log-normal E (sigma U(0.5, 2), correlation length
     U(0.05, 0.3)) and nu U(0.2, 0.4), z = 0 clamped, pressure on z = 1.  The network is
@@ -265,6 +299,8 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 6):
             row[name] = {"seconds": info.seconds, "iterations": info.iterations,
                          "rel_err_vs_reference": err, "status": info.status,
                          **({"fallback": info.fallback} if name == "learned_fcg" else {})}
+        if nn == 24:
+            row["diagnostic"] = _preconditioner_diagnostic(ctx, ustar)
         results.append(row)
     ctx.close()
     return {"train_meshes": 2 * n_train, "train_seconds": train_s,
