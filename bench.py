@@ -486,6 +486,21 @@ def run_gpu_arm(args):
                            "outer": mix.outer, "fp64_fallback": mix.fallback,
                            "status": mix.status, "rel_residual": mix.rel_residual,
                            "rel_err_vs_reference": float(np.linalg.norm(umix - ustar) / nrm)}
+        # two-level PCG: coarse-space build (aggregation, P^T K P, inverse; host wall
+        # time, synchronised) timed apart from the solve that uses it
+        t0 = time.perf_counter()
+        nc = ctx.twolevel_setup(0)
+        tl_setup = time.perf_counter() - t0
+        tl = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, tol=1e-8, max_iter=400000,
+                       raise_on_error=False)
+        utl = ctx.solution()
+        solve["twolevel_pcg"] = {
+            "setup_seconds": tl_setup, "seconds": tl.seconds,
+            "seconds_with_setup": tl_setup + tl.seconds,
+            "iterations": tl.iterations, "status": tl.status, "rel_residual": tl.rel_residual,
+            "rel_err_vs_reference": float(np.linalg.norm(utl - ustar) / nrm),
+            "coarse_unknowns": nc,
+            "label": "FP64 PCG, M = Jacobi + rigid-body modes of box aggregates"}
         if rank == 0 and world == 1 and not args.no_cpu and cfg in ("q4_64", "q8_512"):
             # (the reference's assembly of the full 3-D meshes alone takes minutes)
             rc = reference_cg_sample(m)

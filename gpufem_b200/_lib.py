@@ -24,6 +24,7 @@ GF_SCATTER_COLOR, GF_SCATTER_ATOMIC, GF_SCATTER_OWNER, GF_SCATTER_AUTO = 0, 1, 2
 GF_ENGINE_CUDA_CORE, GF_ENGINE_TF32_MMA = 0, 1
 GF_BC_PENALTY, GF_BC_ELIMINATION = 0, 1
 GF_SOLVER_CG, GF_SOLVER_PCG, GF_SOLVER_MIXED_PCG, GF_SOLVER_LEARNED_FCG, GF_SOLVER_MIXED_PCG32 = 0, 1, 2, 3, 4
+GF_SOLVER_TWOLEVEL_PCG = 5
 
 
 class SolveOpts(C.Structure):
@@ -82,6 +83,9 @@ SIGNATURES = {
     "gf_lp_train": (I32, [P, I32, I32, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "gf_lp_apply": (I32, [P, P, P]),
     "gf_lp_loss_grad": (I32, [P, P, P, C.POINTER(C.c_float), P]),
+    "gf_twolevel_setup": (I32, [P, I32, C.POINTER(I32)]),
+    "gf_twolevel_apply": (I32, [P, P, P]),
+    "gf_twolevel_aggregates": (I32, [P, P, C.POINTER(D)]),
     "gf_pcg_noalloc": (I32, [I32, I32, P, P, P, P, P, D, I32, P, C.POINTER(I32),
                              C.POINTER(D)]),
 }

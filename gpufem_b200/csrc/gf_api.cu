@@ -59,6 +59,7 @@ GF_API gf_status gf_destroy(gf_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   gf_lp_free(ctx);
+  gf_coarse_free(ctx);
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
@@ -351,6 +352,7 @@ GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
   gf_lp_mesh_changed(ctx);
+  gf_coarse_free(ctx);
   gf_pfree(ctx, ctx->d_f);
   gf_pfree(ctx, ctx->d_fixed);
   gf_pfree(ctx, d_chk);
@@ -592,6 +594,7 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
   gf_lp_mesh_changed(ctx);
+  gf_coarse_free(ctx);
   gf_pfree(ctx, ctx->d_f);
   gf_pfree(ctx, ctx->d_fixed);
   ctx->h_supports.clear();
@@ -643,6 +646,7 @@ GF_API gf_status gf_set_supports(gf_ctx* ctx, int32_t nsup, const int32_t* suppo
   }
   ctx->h_supports.assign(supports, supports + (size_t)nsup * w);
   ctx->nsup = nsup;
+  gf_coarse_free(ctx);  // P depends on the constrained dofs
   GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_fixed, fixed.data(), ctx->n, cudaMemcpyHostToDevice,
                                ctx->stream));
   GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -241,6 +241,8 @@ struct gf_ctx {
 
   // learned preconditioner
   LpState* lp = nullptr;
+  void* coarse = nullptr;  // two-level preconditioner (gf_twolevel.cu)
+  int coarse_target = 0;   // requested coarse unknowns (0: default)
 };
 
 // ---------------------------------------------------------------------------
@@ -332,6 +334,14 @@ void gf_sell_free(gf_ctx* ctx);
 
 // learned preconditioner (gf_learned.cu)
 void gf_lp_free(gf_ctx* ctx);
+
+// two-level preconditioner (gf_twolevel.cu)
+void gf_coarse_free(gf_ctx* ctx);
+gf_status gf_coarse_prepare(gf_ctx* ctx, int target_coarse);
+// z = D^-1 r + P Ac^-1 P^T r (FP64 vectors), rz_acc += r.z; launches only (capturable).
+// The kernels return at once while *done != 0 (done may be null).
+void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z,
+                     double* rz_acc, const int* done);
 void gf_lp_mesh_changed(gf_ctx* ctx);
 gf_status gf_lp_prepare(gf_ctx* ctx);
 bool gf_lp_ready(const gf_ctx* ctx);

@@ -250,6 +250,45 @@ k_cg_direction(int n, const V* __restrict__ z, V* __restrict__ p, SolveScalars* 
   }
 }
 
+// Two-level PCG: the preconditioner (gf_twolevel.cu) writes z and accumulates r.z, so
+// the update carries x, r and r.r only.
+__global__ void __launch_bounds__(kT)
+k_cg_init_xr(int n, const double* __restrict__ b, double* __restrict__ x, double* __restrict__ r,
+             SolveScalars* sc) {
+  __shared__ double sh[32];
+  double rr = 0.0;
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
+    const double bi = b[i];
+    x[i] = 0.0;
+    r[i] = bi;
+    rr += bi * bi;
+  }
+  const double s2 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
+__global__ void __launch_bounds__(kT)
+k_cg_update_xr(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+               const double* __restrict__ q, SolveScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const double pq = sc->pq;
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 2;
+    return;
+  }
+  const double alpha = sc->rz / pq;
+  double rr = 0.0;
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
+    x[i] += alpha * p[i];
+    const double ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    rr += ri * ri;
+  }
+  const double s2 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
 // Jacobi: 1 / K_rr (0 for an empty or zero diagonal -> identity row)
 template <typename TK, typename V>
 __global__ void k_diag_inv(int n, const int32_t* __restrict__ rownnz,
@@ -1072,10 +1111,89 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
   return GF_OK;
 }
 
+namespace {
+
+// FP64 PCG on K64 with M = D^-1 + P Ac^-1 P^T (gf_twolevel.cu): per iteration the SpMV
+// with p.q, the x/r update with r.r, the three preconditioner kernels (z, r.z) and
+// the direction update; chunks are captured as CUDA graphs like run_cg.
+gf_status run_twolevel(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
+                       gf_solve_info* info) {
+  const int n = ctx->n;
+  const int nb = gf_blocks(n, kT);
+  cudaStream_t s = ctx->stream;
+  gf_status st;
+  if ((st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
+  double* v = (double*)ctx->d_work;
+  double *x = v, *r = v + n, *z = v + 2 * (size_t)n, *p = v + 3 * (size_t)n,
+         *q = v + 4 * (size_t)n, *dinv = v + 5 * (size_t)n;
+  SolveScalars* sc = ctx->d_scal;
+  k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
+  GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+  MatLayout L;
+  const void* vk = nullptr;
+  if ((st = solver_matrix(ctx, GF_F64, &L, &vk)) != GF_OK) return st;
+  const double* val = (const double*)vk;
+  GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
+  k_cg_init_xr<<<red_grid(ctx, n), kT, 0, s>>>(n, ctx->d_f, x, r, sc);
+  GF_LAUNCH_CHECK(ctx, "k_cg_init_xr");
+  gf_coarse_apply(ctx, r, dinv, z, &sc->rzn, nullptr);
+  GF_LAUNCH_CHECK(ctx, "gf_coarse_apply");
+  GF_CUDA(ctx, cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  k_cg_init_fin<<<1, 1, 0, s>>>(sc, o->tol, maxit);
+  GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const int64_t l0 = ctx->launches;
+  GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < check; ++k) {
+    k_cg_spmv_dot<double, double><<<red_grid(ctx, L.count), kT, 0, s>>>(L, val, p, q, sc);
+    k_cg_update_xr<<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, p, q, sc);
+    gf_coarse_apply(ctx, r, dinv, z, &sc->rzn, &sc->done);
+    k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
+  }
+  cudaError_t ce = cudaStreamEndCapture(s, &graph);
+  if (ce != cudaSuccess) return gf_cuda_fail(ctx, ce, "graph capture");
+  const int64_t per_chunk = ctx->launches - l0 + 3 * (int64_t)check;
+  ctx->launches = l0;
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  if (ce != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return gf_cuda_fail(ctx, ce, "graph instantiate");
+  }
+  SolveScalars* hs = (SolveScalars*)ctx->h_pinned;
+  auto t0 = std::chrono::steady_clock::now();
+  st = GF_OK;
+  for (;;) {
+    ce = cudaGraphLaunch(exec, s);
+    if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "graph launch"); break; }
+    ctx->launches += per_chunk;
+    ce = cudaMemcpyAsync(hs, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "two-level chunk"); break; }
+    if (hs->done) break;
+    if (o->max_seconds > 0.0) {
+      double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (el > o->max_seconds) break;
+    }
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  if (st != GF_OK) return st;
+  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_u, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  info->iterations = hs->iter;
+  info->outer = 1;
+  info->status = status_of(hs->done);
+  info->rel_residual = hs->rr0 > 0.0 ? std::sqrt(hs->rr / hs->rr0) : 0.0;
+  return GF_OK;
+}
+
+}  // namespace
+
 gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info) {
   *info = gf_solve_info{};
   const int solver = o->solver;
-  if (solver < GF_SOLVER_CG || solver > GF_SOLVER_MIXED_PCG32)
+  if (solver < GF_SOLVER_CG || solver > GF_SOLVER_TWOLEVEL_PCG)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown solver %d", solver);
   if (!(o->tol > 0.0)) return gf_fail(ctx, GF_ERR_INVALID_ARG, "tol must be > 0");
   const int maxit = o->max_iter > 0 ? o->max_iter : 10000;
@@ -1091,6 +1209,27 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
   if (solver == GF_SOLVER_LEARNED_FCG) {
     if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "learned FCG needs the FP64 matrix");
     return run_fcg(ctx, o, maxit, check, t0, info);
+  }
+
+  if (solver == GF_SOLVER_TWOLEVEL_PCG) {
+    if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "two-level PCG needs the FP64 matrix");
+    if ((st = run_twolevel(ctx, o, maxit, check, info)) != GF_OK) return st;
+    cudaEventRecord(ctx->ev1, s);
+    GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    info->seconds = ctx->last_seconds = ms * 1e-3;
+    double* r64 = (double*)w + 7 * (size_t)n;
+    double rrt = 0.0, ff = 0.0;
+    if ((st = residual64(ctx, r64, &rrt)) != GF_OK) return st;
+    std::vector<double> f(n);
+    GF_CUDA(ctx, cudaMemcpy(f.data(), ctx->d_f, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    for (double v : f) ff += v * v;
+    info->rel_residual = ff > 0.0 ? std::sqrt(rrt / ff) : 0.0;
+    if (info->status != GF_OK)
+      gf_fail(ctx, (gf_status)info->status, "two-level PCG stopped after %d iterations",
+              info->iterations);
+    return (gf_status)info->status;
   }
 
   if (solver == GF_SOLVER_CG || solver == GF_SOLVER_PCG) {

@@ -1,0 +1,828 @@
+// Two-level preconditioner: Jacobi plus a coarse correction on rigid-body modes of
+// geometric node aggregates (GF_SOLVER_TWOLEVEL_PCG).  No counterpart in the reference (its CG
+// is unpreconditioned, src/SPRmatrix/SPRmatrix.cc:405-480).
+//
+//   M r = D^-1 r + P (P^T K P)^-1 P^T r
+//
+// Nodes are grouped into aggregates by boxes of a regular grid over the mesh's
+// bounding box, sized so that the coarse space has about `target` unknowns.  The
+// columns of P for aggregate A are its rigid-body modes restricted to its nodes: the
+// dim translations and the dim(dim-1)/2 rotations about the aggregate centroid c_A
+// (offsets d = (x - c_A) / s, s = the box side); rows of constrained dofs are zero.
+// M is symmetric positive definite, so plain PCG applies.  The coarse matrix
+// Ac = P^T K P is assembled on the device from the ELL node blocks, regularised by
+// 1e-10 * max diag (modes that the constraints pin down), and inverted in place by a
+// blocked Gauss-Jordan sweep (SPD: no pivoting); the inverse is symmetrised and kept in
+// FP64 for the per-iteration product.
+//
+// One application: restriction (block per aggregate over its node list), dense coarse
+// product (warp per coarse row), prolongation fused with the Jacobi term and the r.z
+// dot.  Everything is launched on the context stream without synchronisation.
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "gf_internal.cuh"
+
+namespace {
+
+constexpr int kCT = 256;
+constexpr int kMaxCoarse = 4096;
+constexpr int kDefaultCoarse = 3072;
+
+struct Coarse {
+  int64_t ver = -1;  // K64 version it was built for
+  int dim = 0, nm = 0, na = 0, nc = 0;
+  double s = 1.0;           // box side (rotation-mode scale)
+  double lo[3] = {0, 0, 0};
+  int nb[3] = {1, 1, 1};
+  int32_t* node_agg = nullptr;   // [nnodes]
+  int32_t* agg_off = nullptr;    // [na + 1]
+  int32_t* agg_nodes = nullptr;  // [nnodes], nodes grouped by aggregate
+  double* cen = nullptr;         // [na * dim]
+  double* ainv = nullptr;        // [nc * nc], row-major, symmetrised
+  double* rc = nullptr;          // [nc]
+  double* zc = nullptr;          // [nc]
+};
+
+// P row of dof (node, comp c): modes m (translations first, then rotations) with the
+// node's scaled offset d from its aggregate centroid.
+//   2-D: t_x, t_y, rot_z = (-d_y, d_x)
+//   3-D: t_x, t_y, t_z, rot_x = (0, -d_z, d_y), rot_y = (d_z, 0, -d_x), rot_z = (-d_y, d_x, 0)
+template <int DIM>
+__device__ inline void p_row(int c, const double* d, double (&row)[DIM == 2 ? 3 : 6]) {
+  constexpr int NM = DIM == 2 ? 3 : 6;
+#pragma unroll
+  for (int m = 0; m < NM; ++m) row[m] = (m == c) ? 1.0 : 0.0;  // translations
+  if (DIM == 2) {
+    row[2] = c == 0 ? -d[1] : d[0];
+  } else {
+    if (c == 0) { row[4] = d[2]; row[5] = -d[1]; }
+    if (c == 1) { row[3] = -d[2]; row[5] = d[0]; }
+    if (c == 2) { row[3] = d[1]; row[4] = -d[0]; }
+  }
+}
+
+// per-block min / max of each coordinate
+__global__ void k_bbox(int nnodes, int dim, const double* __restrict__ x, double* __restrict__ out) {
+  __shared__ double smin[3][kCT], smax[3][kCT];
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (int a = blockIdx.x * kCT + threadIdx.x; a < nnodes; a += gridDim.x * kCT)
+    for (int c = 0; c < dim; ++c) {
+      const double v = x[(int64_t)a * dim + c];
+      mn[c] = fmin(mn[c], v);
+      mx[c] = fmax(mx[c], v);
+    }
+  for (int c = 0; c < 3; ++c) { smin[c][threadIdx.x] = mn[c]; smax[c][threadIdx.x] = mx[c]; }
+  __syncthreads();
+  for (int o = kCT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int c = 0; c < 3; ++c) {
+        smin[c][threadIdx.x] = fmin(smin[c][threadIdx.x], smin[c][threadIdx.x + o]);
+        smax[c][threadIdx.x] = fmax(smax[c][threadIdx.x], smax[c][threadIdx.x + o]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) {
+      out[blockIdx.x * 6 + c] = smin[c][0];
+      out[blockIdx.x * 6 + 3 + c] = smax[c][0];
+    }
+}
+
+__device__ inline int box_of(const double* x, int dim, const double* lo, const double* ext,
+                             const int* nb) {
+  int key = 0, mul = 1;
+  for (int c = 0; c < dim; ++c) {
+    int b = ext[c] > 0.0 ? (int)floor((x[c] - lo[c]) / ext[c] * nb[c]) : 0;
+    b = min(max(b, 0), nb[c] - 1);
+    key += b * mul;
+    mul *= nb[c];
+  }
+  return key;
+}
+
+struct BoxGrid {
+  double lo[3], ext[3];
+  int nb[3];
+};
+
+__global__ void k_box_flags(int nnodes, int dim, const double* __restrict__ x, BoxGrid g,
+                            int32_t* __restrict__ key, int32_t* __restrict__ used) {
+  const int a = blockIdx.x * kCT + threadIdx.x;
+  if (a >= nnodes) return;
+  const int k = box_of(x + (int64_t)a * dim, dim, g.lo, g.ext, g.nb);
+  key[a] = k;
+  used[k] = 1;
+}
+
+__global__ void k_node_agg(int nnodes, const int32_t* __restrict__ key,
+                           const int32_t* __restrict__ box_id, int32_t* __restrict__ agg,
+                           int32_t* __restrict__ cnt) {
+  const int a = blockIdx.x * kCT + threadIdx.x;
+  if (a >= nnodes) return;
+  const int A = box_id[key[a]];
+  agg[a] = A;
+  atomicAdd(&cnt[A], 1);
+}
+
+__global__ void k_agg_fill(int nnodes, int dim, const int32_t* __restrict__ agg,
+                           const double* __restrict__ x, int32_t* __restrict__ cursor,
+                           int32_t* __restrict__ nodes, double* __restrict__ csum) {
+  const int a = blockIdx.x * kCT + threadIdx.x;
+  if (a >= nnodes) return;
+  const int A = agg[a];
+  nodes[atomicAdd(&cursor[A], 1)] = a;
+  for (int c = 0; c < dim; ++c) atomicAdd(&csum[(int64_t)A * dim + c], x[(int64_t)a * dim + c]);
+}
+
+__global__ void k_centroid(int na, int dim, const int32_t* __restrict__ off,
+                           double* __restrict__ cen) {
+  const int A = blockIdx.x * kCT + threadIdx.x;
+  if (A >= na) return;
+  const int c = off[A + 1] - off[A];
+  for (int k = 0; k < dim; ++k) cen[(int64_t)A * dim + k] /= (double)max(c, 1);
+}
+
+// Row block A of Ac = P^T K P: block per aggregate A over its nodes a and their ELL node
+// blocks (a, b).  C = P_a^T K_ab P_b goes to registers when b lies in A (most pairs), else
+// to a shared-memory table keyed by B = agg[b] (open addressing, atomicCAS insertion; a
+// full table falls back to global atomics).  The block owns rows A*NM .. A*NM+NM-1 of Ac,
+// which it adds once at the end.
+constexpr int kCMT = 128;  // threads per block
+constexpr int kTab = 64;   // neighbour-aggregate table slots (power of two)
+
+__device__ inline int tab_slot(volatile int* ids, int B) {
+  const int h = (B * 0x9E3779B1u) >> 26;  // 6 bits
+  for (int k = 0; k < kTab; ++k) {
+    const int s = (h + k) & (kTab - 1);
+    const int cur = ids[s];
+    if (cur == B) return s;
+    if (cur == -1) {
+      const int old = atomicCAS((int*)&ids[s], -1, B);
+      if (old == -1 || old == B) return s;
+    }
+  }
+  return -1;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kCMT)
+k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ colidx,
+              const double* __restrict__ K, const uint8_t* __restrict__ fixed,
+              const int32_t* __restrict__ agg, const int32_t* __restrict__ off,
+              const int32_t* __restrict__ nodes, const double* __restrict__ x,
+              const double* __restrict__ cen, double sinv, int nc, double* __restrict__ Ac) {
+  constexpr int NM = DIM == 2 ? 3 : 6;
+  constexpr int NMM = NM * NM;
+  __shared__ int ids[kTab];
+  __shared__ double tab[kTab][NMM];
+  __shared__ double wsum[kCMT / 32][NMM];
+  const int A = blockIdx.x;
+  for (int i = threadIdx.x; i < kTab; i += kCMT) ids[i] = -1;
+  for (int i = threadIdx.x; i < kTab * NMM; i += kCMT) (&tab[0][0])[i] = 0.0;
+  __syncthreads();
+  double acc[NM][NM];
+#pragma unroll
+  for (int m = 0; m < NM; ++m)
+#pragma unroll
+    for (int m2 = 0; m2 < NM; ++m2) acc[m][m2] = 0.0;
+  double cA[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) cA[c] = cen[(int64_t)A * DIM + c];
+  for (int q = off[A] + threadIdx.x; q < off[A + 1]; q += kCMT) {
+    const int a = nodes[q];
+    const int ra = a * DIM;
+    double da[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) da[c] = (x[(int64_t)ra + c] - cA[c]) * sinv;
+    const int nzb = rownnz[ra] / DIM;
+    for (int p = 0; p < nzb; ++p) {
+      const int b = colidx[(int64_t)(p * DIM) * n + ra] / DIM;
+      const int B = agg[b];
+      double db[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+        db[c] = (x[(int64_t)b * DIM + c] - cen[(int64_t)B * DIM + c]) * sinv;
+      // KPb[c][m] = sum_c2 K_ab[c][c2] P_b[c2][m]
+      double KPb[DIM][NM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) KPb[c][m] = 0.0;
+#pragma unroll
+      for (int c2 = 0; c2 < DIM; ++c2) {
+        if (fixed[b * DIM + c2]) continue;
+        double pr[NM];
+        p_row<DIM>(c2, db, pr);
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          const double k = K[(int64_t)(p * DIM + c2) * n + ra + c];
+#pragma unroll
+          for (int m = 0; m < NM; ++m) KPb[c][m] += k * pr[m];
+        }
+      }
+      double pa[DIM][NM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        p_row<DIM>(c, da, pa[c]);
+        if (fixed[ra + c]) {
+#pragma unroll
+          for (int m = 0; m < NM; ++m) pa[c][m] = 0.0;
+        }
+      }
+      if (B == A) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+          for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int m2 = 0; m2 < NM; ++m2) acc[m][m2] += pa[c][m] * KPb[c][m2];
+      } else {
+        const int sl = tab_slot(ids, B);
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+#pragma unroll
+          for (int m2 = 0; m2 < NM; ++m2) {
+            double v = 0.0;
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) v += pa[c][m] * KPb[c][m2];
+            if (v == 0.0) continue;
+            if (sl >= 0) atomicAdd(&tab[sl][m * NM + m2], v);
+            else atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
+          }
+        }
+      }
+    }
+  }
+  // the (A, A) block: warp sums, then one pass over the warps' partials
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int m = 0; m < NM; ++m)
+#pragma unroll
+    for (int m2 = 0; m2 < NM; ++m2) {
+      double v = acc[m][m2];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (l == 0) wsum[w][m * NM + m2] = v;
+    }
+  __syncthreads();
+  for (int e = threadIdx.x; e < NMM; e += kCMT) {
+    double v = 0.0;
+    for (int k = 0; k < kCMT / 32; ++k) v += wsum[k][e];
+    Ac[(int64_t)(A * NM + e / NM) * nc + A * NM + e % NM] += v;
+  }
+  for (int e = threadIdx.x; e < kTab * NMM; e += kCMT) {
+    const int sl = e / NMM, B = ids[sl];
+    if (B < 0) continue;
+    const int m = (e % NMM) / NM, m2 = e % NM;
+    Ac[(int64_t)(A * NM + m) * nc + B * NM + m2] += tab[sl][e % NMM];
+  }
+}
+
+__global__ void k_diag_max(int nc, const double* __restrict__ Ac, double* __restrict__ out) {
+  __shared__ double sh[kCT];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < nc; i += kCT) m = fmax(m, Ac[(int64_t)i * nc + i]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = kCT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+// regularise: Ac_ii += eps * max diag; an empty mode (zero diagonal) becomes 1
+__global__ void k_regularise(int nc, const double* __restrict__ dmax, double eps,
+                             double* __restrict__ Ac) {
+  const int i = blockIdx.x * kCT + threadIdx.x;
+  if (i >= nc) return;
+  double& d = Ac[(int64_t)i * nc + i];
+  d = d > 0.0 ? d + eps * (*dmax) : 1.0;
+}
+
+// Blocked Gauss-Jordan sweep (in place, SPD: no pivoting).  For the pivot block P of
+// kGJ rows/columns at kb and the rest R:
+//   A_PP <- A_PP^-1,  A_PR <- A_PP^-1 A_PR,  A_RP <- -A_RP A_PP^-1,
+//   A_RR <- A_RR - A_RP A_PP^-1 A_PR
+// After a sweep over every block A holds its inverse.  Three kernels per block:
+// the pivot block's inverse (one CTA), the two panels, and the rank-kGJ update.
+constexpr int kGJ = 32;
+
+// Pi = A_PP^-1 by scalar sweeps in shared memory (bs <= 32; one thread per entry)
+__global__ void __launch_bounds__(kGJ * kGJ)
+k_gj_pivot(int nc, int kb, int bs, const double* __restrict__ A, double* __restrict__ Pi) {
+  __shared__ double M[kGJ][kGJ + 1];
+  __shared__ double row[kGJ], col[kGJ];
+  const int i = threadIdx.y, j = threadIdx.x;
+  if (i < bs && j < bs) M[i][j] = A[(int64_t)(kb + i) * nc + kb + j];
+  __syncthreads();
+  for (int k = 0; k < bs; ++k) {
+    if (i == 0 && j < bs) row[j] = M[k][j];
+    if (j == 0 && i < bs) col[i] = M[i][k];
+    __syncthreads();
+    if (i < bs && j < bs) {
+      const double p = 1.0 / row[k];
+      double v;
+      if (i == k && j == k) v = p;
+      else if (i == k) v = row[j] * p;
+      else if (j == k) v = -col[i] * p;
+      else v = M[i][j] - col[i] * row[j] * p;
+      M[i][j] = v;
+    }
+    __syncthreads();
+  }
+  if (i < bs && j < bs) Pi[i * kGJ + j] = M[i][j];
+}
+
+// Rw[t][j] = sum_u Pi[t][u] A[kb+u][j]   (row panel, every column j)
+// Cold[i][t] = A[i][kb+t]; Cn[i][t] = -sum_u A[i][kb+u] Pi[u][t]   (column panel)
+__global__ void __launch_bounds__(128)
+k_gj_panels(int nc, int kb, int bs, const double* __restrict__ A, const double* __restrict__ Pi,
+            double* __restrict__ Rw, double* __restrict__ Cold, double* __restrict__ Cn) {
+  __shared__ double sP[kGJ][kGJ];
+  for (int e = threadIdx.x; e < kGJ * kGJ; e += 128) sP[e / kGJ][e % kGJ] = Pi[e];
+  __syncthreads();
+  const int t = blockIdx.x * 128 + threadIdx.x;
+  if (t >= nc) return;
+  if (blockIdx.y == 0) {
+    const int j = t;
+    double a[kGJ];
+#pragma unroll
+    for (int u = 0; u < kGJ; ++u) a[u] = u < bs ? A[(int64_t)(kb + u) * nc + j] : 0.0;
+#pragma unroll
+    for (int r = 0; r < kGJ; ++r) {
+      if (r >= bs) break;
+      double v = 0.0;
+#pragma unroll
+      for (int u = 0; u < kGJ; ++u) v += sP[r][u] * a[u];
+      Rw[(int64_t)r * nc + j] = v;
+    }
+  } else {
+    const int i = t;
+    double a[kGJ];
+#pragma unroll
+    for (int u = 0; u < kGJ; ++u) a[u] = u < bs ? A[(int64_t)i * nc + kb + u] : 0.0;
+#pragma unroll
+    for (int r = 0; r < kGJ; ++r) {
+      if (r >= bs) break;
+      double v = 0.0;
+#pragma unroll
+      for (int u = 0; u < kGJ; ++u) v += a[u] * sP[u][r];
+      Cold[(int64_t)i * kGJ + r] = a[r];
+      Cn[(int64_t)i * kGJ + r] = -v;
+    }
+  }
+}
+
+// Every entry (i, j): 64 x 64 tile per CTA, 4 x 4 per thread.
+constexpr int kGT = 64;
+__global__ void __launch_bounds__(256)
+k_gj_update(int nc, int kb, int bs, double* __restrict__ A, const double* __restrict__ Pi,
+            const double* __restrict__ Rw, const double* __restrict__ Cold,
+            const double* __restrict__ Cn) {
+  __shared__ double sC[kGT][kGJ + 1];  // Cold rows of this tile
+  __shared__ double sR[kGJ][kGT];      // Rw columns of this tile
+  const int i0 = blockIdx.y * kGT, j0 = blockIdx.x * kGT;
+  for (int e = threadIdx.x; e < kGT * kGJ; e += 256) {
+    const int r = e / kGJ, u = e % kGJ;
+    sC[r][u] = (i0 + r < nc && u < bs) ? Cold[(int64_t)(i0 + r) * kGJ + u] : 0.0;
+    const int u2 = e / kGT, c2 = e % kGT;
+    sR[u2][c2] = (j0 + c2 < nc && u2 < bs) ? Rw[(int64_t)u2 * nc + j0 + c2] : 0.0;
+  }
+  __syncthreads();
+  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+#pragma unroll 8
+  for (int u = 0; u < kGJ; ++u) {
+    double cv[4], rv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) cv[a] = sC[ty + 16 * a][u];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) rv[b] = sR[u][tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += cv[a] * rv[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + ty + 16 * a;
+    if (i >= nc) continue;
+    const bool ip = i >= kb && i < kb + bs;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = j0 + tx + 16 * b;
+      if (j >= nc) continue;
+      const bool jp = j >= kb && j < kb + bs;
+      double* dst = A + (int64_t)i * nc + j;
+      if (ip && jp) *dst = Pi[(i - kb) * kGJ + (j - kb)];
+      else if (ip) *dst = Rw[(int64_t)(i - kb) * nc + j];
+      else if (jp) *dst = Cn[(int64_t)i * kGJ + (j - kb)];
+      else *dst -= acc[a][b];
+    }
+  }
+}
+
+__global__ void k_symmetrise(int nc, const double* __restrict__ A, double* __restrict__ out) {
+  const int64_t t = blockIdx.x * (int64_t)kCT + threadIdx.x;
+  if (t >= (int64_t)nc * nc) return;
+  const int i = (int)(t / nc), j = (int)(t % nc);
+  out[t] = 0.5 * (A[t] + A[(int64_t)j * nc + i]);
+}
+
+// rc = P^T r: block per aggregate over its node list
+constexpr int kRT = 256;
+template <int DIM>
+__global__ void __launch_bounds__(kRT)
+k_restrict(const int32_t* __restrict__ off, const int32_t* __restrict__ nodes,
+           const double* __restrict__ x, const double* __restrict__ cen, double sinv,
+           const uint8_t* __restrict__ fixed, const double* __restrict__ r,
+           double* __restrict__ rc, const int* __restrict__ done) {
+  constexpr int NM = DIM == 2 ? 3 : 6;
+  __shared__ double ws[kRT / 32][NM];
+  if (done && *done) return;
+  const int A = blockIdx.x;
+  double acc[NM];
+#pragma unroll
+  for (int m = 0; m < NM; ++m) acc[m] = 0.0;
+  double cA[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) cA[c] = cen[(int64_t)A * DIM + c];
+  for (int q = off[A] + threadIdx.x; q < off[A + 1]; q += kRT) {
+    const int a = nodes[q];
+    double d[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) d[c] = (x[(int64_t)a * DIM + c] - cA[c]) * sinv;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      if (fixed[a * DIM + c]) continue;
+      const double rv = r[a * DIM + c];
+      double pr[NM];
+      p_row<DIM>(c, d, pr);
+#pragma unroll
+      for (int m = 0; m < NM; ++m) acc[m] += pr[m] * rv;
+    }
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int m = 0; m < NM; ++m) {
+    double v = acc[m];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (l == 0) ws[w][m] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NM) {
+    double v = 0.0;
+    for (int k = 0; k < kRT / 32; ++k) v += ws[k][threadIdx.x];
+    rc[A * NM + threadIdx.x] = v;
+  }
+}
+
+// zc = Ainv rc: warp per row
+__global__ void k_coarse_gemv(int nc, const double* __restrict__ Ainv, const double* __restrict__ rc,
+                              double* __restrict__ zc, const int* __restrict__ done) {
+  if (done && *done) return;
+  const int i = blockIdx.x * (kCT / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= nc) return;
+  const double* row = Ainv + (int64_t)i * nc;
+  double acc = 0.0;
+  for (int j = lane; j < nc; j += 32) acc += __ldg(row + j) * rc[j];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) zc[i] = acc;
+}
+
+__device__ inline double cg_block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  return s;
+}
+
+// z = dinv r + P zc, and rz_acc += r.z (grid-stride over dofs)
+template <int DIM>
+__global__ void __launch_bounds__(kCT)
+k_prolong(int n, const int32_t* __restrict__ agg, const double* __restrict__ x,
+          const double* __restrict__ cen, double sinv, const uint8_t* __restrict__ fixed,
+          const double* __restrict__ dinv, const double* __restrict__ r,
+          const double* __restrict__ zc, double* __restrict__ z, double* __restrict__ rz_acc,
+          const int* __restrict__ done) {
+  constexpr int NM = DIM == 2 ? 3 : 6;
+  __shared__ double sh[32];
+  if (done && *done) return;
+  double rz = 0.0;
+  for (int i = blockIdx.x * kCT + threadIdx.x; i < n; i += gridDim.x * kCT) {
+    const int a = i / DIM, c = i - a * DIM;
+    double zi = dinv[i] * r[i];
+    if (!fixed[i]) {
+      const int A = agg[a];
+      double d[DIM];
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) d[k] = (x[(int64_t)a * DIM + k] - cen[(int64_t)A * DIM + k]) * sinv;
+      double pr[NM];
+      p_row<DIM>(c, d, pr);
+#pragma unroll
+      for (int m = 0; m < NM; ++m) zi += pr[m] * zc[A * NM + m];
+    }
+    z[i] = zi;
+    rz += r[i] * zi;
+  }
+  const double s = cg_block_sum(rz, sh);
+  if (threadIdx.x == 0) atomicAdd(rz_acc, s);
+}
+
+void coarse_release(Coarse* c) {
+  gf_free(c->node_agg);
+  gf_free(c->agg_off);
+  gf_free(c->agg_nodes);
+  gf_free(c->cen);
+  gf_free(c->ainv);
+  gf_free(c->rc);
+  gf_free(c->zc);
+}
+
+gf_status build(gf_ctx* ctx, Coarse* C, int target) {
+  const int dim = ctx->dim, nnodes = ctx->nnodes, n = ctx->n;
+  cudaStream_t s = ctx->stream;
+  const int nm = dim == 2 ? 3 : 6;
+  gf_status st;
+  // bounding box
+  const int bb = std::min(gf_blocks(nnodes, kCT), 256);
+  double* d_bb = nullptr;
+  if ((st = gf_alloc(ctx, &d_bb, (size_t)bb * 6)) != GF_OK) return st;
+  k_bbox<<<bb, kCT, 0, s>>>(nnodes, dim, ctx->d_coords64, d_bb);
+  std::vector<double> hb((size_t)bb * 6);
+  GF_CUDA(ctx, cudaMemcpyAsync(hb.data(), d_bb, sizeof(double) * bb * 6, cudaMemcpyDeviceToHost, s));
+  GF_CUDA(ctx, cudaStreamSynchronize(s));
+  gf_free(d_bb);
+  BoxGrid g{};
+  double vol = 1.0;
+  int dpos = 0;  // axes of positive extent
+  for (int c = 0; c < dim; ++c) {
+    double lo = 1e300, hi = -1e300;
+    for (int k = 0; k < bb; ++k) {
+      lo = std::min(lo, hb[k * 6 + c]);
+      hi = std::max(hi, hb[k * 6 + 3 + c]);
+    }
+    g.lo[c] = lo;
+    g.ext[c] = hi - lo;
+    if (hi > lo) { vol *= hi - lo; ++dpos; }
+  }
+  // box side for about cap / nm aggregates over the axes of positive extent; grow it
+  // until the grid fits the cap (at the latest when every axis has one box)
+  const int cap = std::min(std::max(target, nm), kMaxCoarse);
+  double side = dpos ? std::pow(vol / std::max(1.0, (double)cap / nm), 1.0 / dpos) : 1.0;
+  int64_t nbox = 1;
+  for (int it = 0; it < 100000; ++it) {
+    nbox = 1;
+    for (int c = 0; c < dim; ++c) {
+      const double q = g.ext[c] / side;
+      g.nb[c] = q >= (double)cap ? cap : std::max(1, (int)std::lround(q));
+      nbox *= g.nb[c];
+    }
+    if (nbox * nm <= cap) break;
+    side *= 1.05;
+  }
+  for (int c = dim; c < 3; ++c) { g.nb[c] = 1; g.lo[c] = 0; g.ext[c] = 0; }
+  // aggregates = occupied boxes, numbered in box order
+  int32_t *d_key = nullptr, *d_used = nullptr, *d_id = nullptr, *d_cnt = nullptr;
+  void* d_tmp = nullptr;
+  auto cleanup = [&]() {
+    gf_free(d_key); gf_free(d_used); gf_free(d_id); gf_free(d_cnt);
+    if (d_tmp) cudaFree(d_tmp);
+  };
+  if ((st = gf_alloc(ctx, &d_key, (size_t)nnodes)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_used, (size_t)nbox + 1)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_id, (size_t)nbox + 1)) != GF_OK) {
+    cleanup();
+    return st;
+  }
+  cudaMemsetAsync(d_used, 0, sizeof(int32_t) * (nbox + 1), s);
+  k_box_flags<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, dim, ctx->d_coords64, g, d_key, d_used);
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, d_used, d_id, (int)nbox + 1, s);
+  if (cudaMalloc(&d_tmp, tb) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return gf_fail(ctx, GF_ERR_OOM, "coarse scan scratch");
+  }
+  cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_used, d_id, (int)nbox + 1, s);
+  int32_t na = 0;
+  GF_CUDA(ctx, cudaMemcpyAsync(&na, d_id + nbox, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GF_CUDA(ctx, cudaStreamSynchronize(s));
+  const int nc = na * nm;
+  C->dim = dim; C->nm = nm; C->na = na; C->nc = nc; C->s = side;
+  for (int c = 0; c < 3; ++c) { C->lo[c] = g.lo[c]; C->nb[c] = g.nb[c]; }
+  double* d_Ac = nullptr;
+  double *d_pi = nullptr, *d_rw = nullptr, *d_cold = nullptr, *d_cn = nullptr,
+         *d_dmax = nullptr;
+  auto cleanup2 = [&]() {
+    cleanup();
+    gf_free(d_Ac); gf_free(d_pi); gf_free(d_rw); gf_free(d_cold); gf_free(d_cn);
+    gf_free(d_dmax);
+  };
+  if ((st = gf_alloc(ctx, &C->node_agg, (size_t)nnodes)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_cnt, (size_t)na + 1)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->agg_off, (size_t)na + 1)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->agg_nodes, (size_t)nnodes)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->cen, (size_t)na * dim)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->ainv, (size_t)nc * nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->rc, (size_t)nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->zc, (size_t)nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_Ac, (size_t)nc * nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_pi, (size_t)kGJ * kGJ)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_rw, (size_t)kGJ * nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_cold, (size_t)kGJ * nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_cn, (size_t)kGJ * nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_dmax, 1)) != GF_OK) {
+    cleanup2();
+    return st;
+  }
+  cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (na + 1), s);
+  cudaMemsetAsync(C->cen, 0, sizeof(double) * na * dim, s);
+  k_node_agg<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, d_key, d_id, C->node_agg, d_cnt);
+  size_t tb2 = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb2, d_cnt, C->agg_off, na + 1, s);
+  if (tb2 > tb) {
+    cudaFree(d_tmp);
+    d_tmp = nullptr;
+    if (cudaMalloc(&d_tmp, tb2) != cudaSuccess) {
+      cudaGetLastError();
+      cleanup2();
+      return gf_fail(ctx, GF_ERR_OOM, "coarse scan scratch");
+    }
+    tb = tb2;
+  }
+  cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_cnt, C->agg_off, na + 1, s);
+  cudaMemcpyAsync(d_cnt, C->agg_off, sizeof(int32_t) * (na + 1), cudaMemcpyDeviceToDevice, s);
+  k_agg_fill<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, dim, C->node_agg, ctx->d_coords64,
+                                                   d_cnt, C->agg_nodes, C->cen);
+  k_centroid<<<gf_blocks(na, kCT), kCT, 0, s>>>(na, dim, C->agg_off, C->cen);
+  // coarse matrix
+  cudaMemsetAsync(d_Ac, 0, sizeof(double) * nc * nc, s);
+  const double sinv = 1.0 / side;
+  if (dim == 2)
+    k_coarse_rows<2><<<na, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
+                                         ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
+                                         ctx->d_coords64, C->cen, sinv, nc, d_Ac);
+  else
+    k_coarse_rows<3><<<na, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
+                                         ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
+                                         ctx->d_coords64, C->cen, sinv, nc, d_Ac);
+  k_diag_max<<<1, kCT, 0, s>>>(nc, d_Ac, d_dmax);
+  k_regularise<<<gf_blocks(nc, kCT), kCT, 0, s>>>(nc, d_dmax, 1e-10, d_Ac);
+  ctx->launches += 8;
+  // blocked Gauss-Jordan inverse
+  const dim3 gp((nc + 127) / 128, 2), gu((nc + kGT - 1) / kGT, (nc + kGT - 1) / kGT);
+  for (int kb = 0; kb < nc; kb += kGJ) {
+    const int bs = std::min(kGJ, nc - kb);
+    k_gj_pivot<<<1, dim3(kGJ, kGJ), 0, s>>>(nc, kb, bs, d_Ac, d_pi);
+    k_gj_panels<<<gp, 128, 0, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
+    k_gj_update<<<gu, 256, 0, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
+    ctx->launches += 3;
+  }
+  k_symmetrise<<<gf_blocks((int64_t)nc * nc, kCT), kCT, 0, s>>>(nc, d_Ac, C->ainv);
+  ctx->launches++;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cleanup2();
+  if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "coarse set-up");
+  return GF_OK;
+}
+
+}  // namespace
+
+void gf_coarse_free(gf_ctx* ctx) {
+  if (!ctx->coarse) return;
+  Coarse* c = static_cast<Coarse*>(ctx->coarse);
+  coarse_release(c);
+  delete c;
+  ctx->coarse = nullptr;
+}
+
+// Builds the coarse space for the current FP64 matrix and constraints (once per matrix
+// version and target size).
+gf_status gf_coarse_prepare(gf_ctx* ctx, int target) {
+  if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "the two-level preconditioner needs K64");
+  if (!ctx->has_mesh || !ctx->d_diagpos)
+    return gf_fail(ctx, GF_ERR_STATE, "the two-level preconditioner needs a mesh-built pattern");
+  if (target <= 0) target = ctx->coarse_target > 0 ? ctx->coarse_target : kDefaultCoarse;
+  Coarse* c = static_cast<Coarse*>(ctx->coarse);
+  if (c && c->ver == ctx->kver64) return GF_OK;
+  gf_coarse_free(ctx);
+  c = new Coarse();
+  ctx->coarse = c;
+  gf_status st = build(ctx, c, target);
+  if (st != GF_OK) {
+    gf_coarse_free(ctx);
+    return st;
+  }
+  c->ver = ctx->kver64;
+  return GF_OK;
+}
+
+void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z, double* rz_acc,
+                     const int* done) {
+  Coarse* c = static_cast<Coarse*>(ctx->coarse);
+  cudaStream_t s = ctx->stream;
+  const double sinv = 1.0 / c->s;
+  const int gbk = (c->nc + kCT / 32 - 1) / (kCT / 32);
+  const int pb = std::min(gf_blocks(ctx->n, kCT), ctx->sm_count * 8);
+  if (c->dim == 2) {
+    k_restrict<2><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
+                                        ctx->d_fixed, r, c->rc, done);
+    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ainv, c->rc, c->zc, done);
+    k_prolong<2><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
+                                    ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
+  } else {
+    k_restrict<3><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
+                                        ctx->d_fixed, r, c->rc, done);
+    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ainv, c->rc, c->zc, done);
+    k_prolong<3><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
+                                    ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
+  }
+  ctx->launches += 3;
+}
+
+extern "C" GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse,
+                                              int32_t* ncoarse) {
+  if (!ctx) return GF_ERR_INVALID_ARG;
+  if (target_coarse < 0) return gf_fail(ctx, GF_ERR_INVALID_ARG, "negative coarse size");
+  cudaSetDevice(ctx->device);
+  ctx->coarse_target = target_coarse;
+  gf_coarse_free(ctx);  // a new target always rebuilds
+  gf_status st = gf_coarse_prepare(ctx, target_coarse);
+  if (st != GF_OK) return st;
+  if (ncoarse) *ncoarse = static_cast<Coarse*>(ctx->coarse)->nc;
+  return GF_OK;
+}
+
+extern "C" GF_API gf_status gf_twolevel_apply(gf_ctx* ctx, const double* r, double* z) {
+  if (!ctx || !r || !z) return GF_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gf_status st = gf_coarse_prepare(ctx, 0);
+  if (st != GF_OK) return st;
+  const int n = ctx->n;
+  double *d_r = nullptr, *d_z = nullptr, *d_dinv = nullptr, *d_acc = nullptr;
+  auto cleanup = [&]() { gf_free(d_r); gf_free(d_z); gf_free(d_dinv); gf_free(d_acc); };
+  if ((st = gf_alloc(ctx, &d_r, (size_t)n)) != GF_OK || (st = gf_alloc(ctx, &d_z, (size_t)n)) != GF_OK ||
+      (st = gf_alloc(ctx, &d_dinv, (size_t)n)) != GF_OK || (st = gf_alloc(ctx, &d_acc, 1)) != GF_OK) {
+    cleanup();
+    return st;
+  }
+  cudaStream_t s = ctx->stream;
+  // Jacobi part from the ELL diagonal (1 / K_rr; 1 where the diagonal is zero)
+  std::vector<int32_t> rn(n);
+  std::vector<int32_t> col((size_t)n * ctx->W);
+  std::vector<double> val((size_t)n * ctx->W);
+  cudaMemcpyAsync(rn.data(), ctx->d_rownnz, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(col.data(), ctx->d_colidx, sizeof(int32_t) * col.size(), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(val.data(), ctx->d_K64, sizeof(double) * val.size(), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cleanup();
+    return gf_cuda_fail(ctx, e, "coarse apply");
+  }
+  std::vector<double> dinv(n, 1.0);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < rn[i]; ++k)
+      if (col[(size_t)k * n + i] == i && val[(size_t)k * n + i] != 0.0)
+        dinv[i] = 1.0 / val[(size_t)k * n + i];
+  cudaMemcpyAsync(d_r, r, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d_dinv, dinv.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(d_acc, 0, sizeof(double), s);
+  gf_coarse_apply(ctx, d_r, d_dinv, d_z, d_acc, nullptr);
+  cudaMemcpyAsync(z, d_z, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cleanup();
+  if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "coarse apply");
+  return GF_OK;
+}
+
+extern "C" GF_API gf_status gf_twolevel_aggregates(gf_ctx* ctx, int32_t* node_agg,
+                                                   double* box_side) {
+  if (!ctx || !node_agg) return GF_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gf_status st = gf_coarse_prepare(ctx, 0);
+  if (st != GF_OK) return st;
+  Coarse* c = static_cast<Coarse*>(ctx->coarse);
+  GF_CUDA(ctx, cudaMemcpyAsync(node_agg, c->node_agg, sizeof(int32_t) * ctx->nnodes,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (box_side) *box_side = c->s;
+  return GF_OK;
+}

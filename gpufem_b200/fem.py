@@ -226,6 +226,24 @@ class Context:
                                     C.byref(loss), _ptr(g)))
         return loss.value, g
 
+    # ---- two-level preconditioner -----------------------------------------
+    def twolevel_setup(self, target_coarse: int = 0) -> int:
+        nc = C.c_int32()
+        self._c(lib.gf_twolevel_setup(self.h, target_coarse, C.byref(nc)))
+        return nc.value
+
+    def twolevel_apply(self, r: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.empty_like(r)
+        self._c(lib.gf_twolevel_apply(self.h, _ptr(r), _ptr(z)))
+        return z
+
+    def twolevel_aggregates(self):
+        agg = np.empty(self.n // self.dim, np.int32)
+        s = C.c_double()
+        self._c(lib.gf_twolevel_aggregates(self.h, _ptr(agg), C.byref(s)))
+        return agg, s.value
+
     def launches(self) -> int:
         return int(lib.gf_kernel_launches(self.h))
 

@@ -95,8 +95,10 @@ typedef enum gf_solver {
   GF_SOLVER_LEARNED_FCG = 3, /* FP64 flexible CG on K64 with the learned (message-passing)
                                 preconditioner, falling back to Jacobi-PCG when it breaks
                                 down or stalls. Needs K64 and gf_lp_init.                 */
-  GF_SOLVER_MIXED_PCG32 = 4  /* as MIXED_PCG with FP32 vectors as well (half the vector
+  GF_SOLVER_MIXED_PCG32 = 4, /* as MIXED_PCG with FP32 vectors as well (half the vector
                                 traffic; for moderately conditioned systems)              */
+  GF_SOLVER_TWOLEVEL_PCG = 5 /* FP64 PCG on K64 with the two-level preconditioner
+                                (gf_twolevel_setup); needs a mesh-built pattern          */
 } gf_solver;
 
 typedef struct gf_solve_opts {
@@ -245,6 +247,21 @@ GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z);
  * (host buffer of gf_lp_num_params floats, or NULL); weights unchanged. */
 GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, float* loss,
                                  float* grad);
+
+/* ---- two-level preconditioner (no counterpart in the reference) ------------------------
+ * M r = D^-1 r + P (P^T K P)^-1 P^T r.  Nodes are grouped into aggregates by the boxes of a
+ * regular grid over the mesh's bounding box (box side s chosen so that the coarse space has
+ * at most target_coarse unknowns); P holds, per aggregate, its dim translations and
+ * dim(dim-1)/2 rotations about the aggregate's centroid c (offsets (x - c) / s), with the
+ * rows of constrained dofs zero.  P^T K P is assembled and inverted on the device (FP64,
+ * regularised by 1e-10 * its largest diagonal entry; a zero diagonal entry becomes 1).  Built
+ * for the current FP64 matrix and supports; rebuilt by the next TWOLEVEL_PCG solve after
+ * either changes.  target_coarse 0 = 3072; at most 4096.  *ncoarse may be NULL. */
+GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse, int32_t* ncoarse);
+/* z = M r on HOST vectors of n doubles (builds the coarse space if needed). */
+GF_API gf_status gf_twolevel_apply(gf_ctx* ctx, const double* r, double* z);
+/* Aggregate (0-based, in box order) of every node, and the box side s. */
+GF_API gf_status gf_twolevel_aggregates(gf_ctx* ctx, int32_t* node_agg, double* box_side);
 
 /* ---- allocation-free solve -------------------------------------------------------------
  * No counterpart in the reference.  FP64 Jacobi-PCG (x0 = 0, stop when the recursive
