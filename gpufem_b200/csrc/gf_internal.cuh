@@ -143,7 +143,19 @@ inline void gf_gauss_rule(int dim, int ng1, std::vector<R>& pts, std::vector<R>&
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------
-struct SolveScalars;  // device-side solver scalars (gf_solve.cu)
+// device-side CG scalars (gf_solve.cu, gf_twolevel.cu)
+struct SolveScalars {
+  double pq;    // p . A p (accumulated by the SpMV)
+  double rz;    // r . z of the current iteration
+  double rzn;   // r . z of the next iteration (accumulated by the update)
+  double rr;    // r . r after the update
+  double rr0;   // initial r . r
+  double tol2;  // stop when rr <= tol2
+  int iter;
+  int done;     // 0 running, 1 converged, 2 breakdown, 3 iteration cap
+  int maxit;
+  int pad;
+};
 struct LpState;       // learned preconditioner (gf_learned.cu)
 
 struct gf_ctx {
@@ -338,10 +350,16 @@ void gf_lp_free(gf_ctx* ctx);
 // two-level preconditioner (gf_twolevel.cu)
 void gf_coarse_free(gf_ctx* ctx);
 gf_status gf_coarse_prepare(gf_ctx* ctx, int target_coarse);
-// z = D^-1 r + P Ac^-1 P^T r (FP64 vectors), rz_acc += r.z; launches only (capturable).
-// The kernels return at once while *done != 0 (done may be null).
+// z = D^-1 r + P Ac^-1 P^T r (FP64 vectors), rz_acc += r.z; launches only.
 void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z,
                      double* rz_acc, const int* done);
+// Two-level PCG steps (launches only, capturable).  Begin: x = 0, r = b, p = M r,
+// sc->rr = b.b, sc->rzn = r.M r.  Iterate (after the SpMV q = K p, p.q): x, r update,
+// then p = M r + beta p; the kernels return at once while sc->done != 0.
+void gf_tl_begin(gf_ctx* ctx, const double* b, double* x, double* r, double* p,
+                 const double* dinv, SolveScalars* sc);
+void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q,
+                   const double* dinv, SolveScalars* sc);
 void gf_lp_mesh_changed(gf_ctx* ctx);
 gf_status gf_lp_prepare(gf_ctx* ctx);
 bool gf_lp_ready(const gf_ctx* ctx);

@@ -21,19 +21,6 @@
 
 #include "gf_internal.cuh"
 
-struct SolveScalars {
-  double pq;    // p . A p (accumulated by K1)
-  double rz;    // r . z of the current iteration
-  double rzn;   // r . z of the next iteration (accumulated by K2)
-  double rr;    // r . r after the update (accumulated by K2)
-  double rr0;   // initial r . r
-  double tol2;  // stop when rr <= tol2
-  int iter;
-  int done;     // 0 running, 1 converged, 2 breakdown, 3 iteration cap
-  int maxit;
-  int pad;
-};
-
 namespace {
 
 constexpr int kT = 256;
@@ -248,45 +235,6 @@ k_cg_direction(int n, const V* __restrict__ z, V* __restrict__ p, SolveScalars* 
     if (sc->rr <= sc->tol2) sc->done = 1;
     else if (sc->iter >= sc->maxit) sc->done = 3;
   }
-}
-
-// Two-level PCG: the preconditioner (gf_twolevel.cu) writes z and accumulates r.z, so
-// the update carries x, r and r.r only.
-__global__ void __launch_bounds__(kT)
-k_cg_init_xr(int n, const double* __restrict__ b, double* __restrict__ x, double* __restrict__ r,
-             SolveScalars* sc) {
-  __shared__ double sh[32];
-  double rr = 0.0;
-  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
-    const double bi = b[i];
-    x[i] = 0.0;
-    r[i] = bi;
-    rr += bi * bi;
-  }
-  const double s2 = block_sum(rr, sh);
-  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
-}
-
-__global__ void __launch_bounds__(kT)
-k_cg_update_xr(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
-               const double* __restrict__ q, SolveScalars* sc) {
-  __shared__ double sh[32];
-  if (sc->done) return;
-  const double pq = sc->pq;
-  if (!(pq > 0.0) || !isfinite(pq)) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 2;
-    return;
-  }
-  const double alpha = sc->rz / pq;
-  double rr = 0.0;
-  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
-    x[i] += alpha * p[i];
-    const double ri = r[i] - alpha * q[i];
-    r[i] = ri;
-    rr += ri * ri;
-  }
-  const double s2 = block_sum(rr, sh);
-  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
 }
 
 // Jacobi: 1 / K_rr (0 for an empty or zero diagonal -> identity row)
@@ -1114,8 +1062,8 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
 namespace {
 
 // FP64 PCG on K64 with M = D^-1 + P Ac^-1 P^T (gf_twolevel.cu): per iteration the SpMV
-// with p.q, the x/r update with r.r, the three preconditioner kernels (z, r.z) and
-// the direction update; chunks are captured as CUDA graphs like run_cg.
+// with p.q, then the update with the restriction, the coarse product and the direction
+// with the prolongation (gf_tl_iterate); chunks are captured as CUDA graphs like run_cg.
 gf_status run_twolevel(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
                        gf_solve_info* info) {
   const int n = ctx->n;
@@ -1124,8 +1072,8 @@ gf_status run_twolevel(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check
   gf_status st;
   if ((st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
   double* v = (double*)ctx->d_work;
-  double *x = v, *r = v + n, *z = v + 2 * (size_t)n, *p = v + 3 * (size_t)n,
-         *q = v + 4 * (size_t)n, *dinv = v + 5 * (size_t)n;
+  double *x = v, *r = v + n, *p = v + 3 * (size_t)n, *q = v + 4 * (size_t)n,
+         *dinv = v + 5 * (size_t)n;
   SolveScalars* sc = ctx->d_scal;
   k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_LAUNCH_CHECK(ctx, "k_diag_inv");
@@ -1134,11 +1082,8 @@ gf_status run_twolevel(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check
   if ((st = solver_matrix(ctx, GF_F64, &L, &vk)) != GF_OK) return st;
   const double* val = (const double*)vk;
   GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
-  k_cg_init_xr<<<red_grid(ctx, n), kT, 0, s>>>(n, ctx->d_f, x, r, sc);
-  GF_LAUNCH_CHECK(ctx, "k_cg_init_xr");
-  gf_coarse_apply(ctx, r, dinv, z, &sc->rzn, nullptr);
-  GF_LAUNCH_CHECK(ctx, "gf_coarse_apply");
-  GF_CUDA(ctx, cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  gf_tl_begin(ctx, ctx->d_f, x, r, p, dinv, sc);
+  GF_LAUNCH_CHECK(ctx, "gf_tl_begin");
   k_cg_init_fin<<<1, 1, 0, s>>>(sc, o->tol, maxit);
   GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
 
@@ -1148,13 +1093,11 @@ gf_status run_twolevel(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check
   GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < check; ++k) {
     k_cg_spmv_dot<double, double><<<red_grid(ctx, L.count), kT, 0, s>>>(L, val, p, q, sc);
-    k_cg_update_xr<<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, p, q, sc);
-    gf_coarse_apply(ctx, r, dinv, z, &sc->rzn, &sc->done);
-    k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
+    gf_tl_iterate(ctx, x, r, p, q, dinv, sc);
   }
   cudaError_t ce = cudaStreamEndCapture(s, &graph);
   if (ce != cudaSuccess) return gf_cuda_fail(ctx, ce, "graph capture");
-  const int64_t per_chunk = ctx->launches - l0 + 3 * (int64_t)check;
+  const int64_t per_chunk = ctx->launches - l0 + (int64_t)check;
   ctx->launches = l0;
   ce = cudaGraphInstantiate(&exec, graph, 0);
   if (ce != cudaSuccess) {

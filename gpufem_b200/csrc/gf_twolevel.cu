@@ -41,7 +41,8 @@ struct Coarse {
   int32_t* agg_off = nullptr;    // [na + 1]
   int32_t* agg_nodes = nullptr;  // [nnodes], nodes grouped by aggregate
   double* cen = nullptr;         // [na * dim]
-  double* ainv = nullptr;        // [nc * nc], row-major, symmetrised
+  int ld = 0;                     // row stride of ainv: nc rounded up to 8
+  double* ainv = nullptr;        // [nc][ld], symmetrised, zero beyond column nc
   double* rc = nullptr;          // [nc]
   double* zc = nullptr;          // [nc]
 };
@@ -127,13 +128,13 @@ __global__ void k_node_agg(int nnodes, const int32_t* __restrict__ key,
   atomicAdd(&cnt[A], 1);
 }
 
-__global__ void k_agg_fill(int nnodes, int dim, const int32_t* __restrict__ agg,
-                           const double* __restrict__ x, int32_t* __restrict__ cursor,
-                           int32_t* __restrict__ nodes, double* __restrict__ csum) {
+__global__ void k_agg_sums(int nnodes, int dim, const int32_t* __restrict__ agg,
+                           const double* __restrict__ x, int32_t* __restrict__ iota,
+                           double* __restrict__ csum) {
   const int a = blockIdx.x * kCT + threadIdx.x;
   if (a >= nnodes) return;
   const int A = agg[a];
-  nodes[atomicAdd(&cursor[A], 1)] = a;
+  iota[a] = a;
   for (int c = 0; c < dim; ++c) atomicAdd(&csum[(int64_t)A * dim + c], x[(int64_t)a * dim + c]);
 }
 
@@ -145,12 +146,12 @@ __global__ void k_centroid(int na, int dim, const int32_t* __restrict__ off,
   for (int k = 0; k < dim; ++k) cen[(int64_t)A * dim + k] /= (double)max(c, 1);
 }
 
-// Row block A of Ac = P^T K P: block per aggregate A over its nodes a and their ELL node
-// blocks (a, b).  C = P_a^T K_ab P_b goes to registers when b lies in A (most pairs), else
-// to a shared-memory table keyed by B = agg[b] (open addressing, atomicCAS insertion; a
-// full table falls back to global atomics).  The block owns rows A*NM .. A*NM+NM-1 of Ac,
-// which it adds once at the end.
-constexpr int kCMT = 128;  // threads per block
+// Row block A of Ac = P^T K P: blocks (A, y) over chunk y of kCMT * per nodes a of aggregate A
+// and their ELL node blocks (a, b).  C = P_a^T K_ab P_b goes to registers when b lies in
+// A (most pairs), else to a shared-memory table keyed by B = agg[b] (open addressing,
+// atomicCAS insertion; a full table falls back to global atomics); each block adds its
+// sums to rows A*NM .. A*NM+NM-1 of Ac once at the end.
+constexpr int kCMT = 128;  // threads per block = nodes per chunk
 constexpr int kTab = 64;   // neighbour-aggregate table slots (power of two)
 
 __device__ inline int tab_slot(volatile int* ids, int B) {
@@ -173,13 +174,16 @@ k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
               const double* __restrict__ K, const uint8_t* __restrict__ fixed,
               const int32_t* __restrict__ agg, const int32_t* __restrict__ off,
               const int32_t* __restrict__ nodes, const double* __restrict__ x,
-              const double* __restrict__ cen, double sinv, int nc, double* __restrict__ Ac) {
+              const double* __restrict__ cen, double sinv, int nc, int per,
+              double* __restrict__ Ac) {
   constexpr int NM = DIM == 2 ? 3 : 6;
   constexpr int NMM = NM * NM;
   __shared__ int ids[kTab];
   __shared__ double tab[kTab][NMM];
   __shared__ double wsum[kCMT / 32][NMM];
   const int A = blockIdx.x;
+  const int q0 = off[A] + blockIdx.y * kCMT * per;
+  if (q0 >= off[A + 1]) return;  // block-uniform: this aggregate has fewer chunks
   for (int i = threadIdx.x; i < kTab; i += kCMT) ids[i] = -1;
   for (int i = threadIdx.x; i < kTab * NMM; i += kCMT) (&tab[0][0])[i] = 0.0;
   __syncthreads();
@@ -191,7 +195,9 @@ k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
   double cA[DIM];
 #pragma unroll
   for (int c = 0; c < DIM; ++c) cA[c] = cen[(int64_t)A * DIM + c];
-  for (int q = off[A] + threadIdx.x; q < off[A + 1]; q += kCMT) {
+  for (int k = 0; k < per; ++k) {
+    const int q = q0 + k * kCMT + threadIdx.x;
+    if (q >= off[A + 1]) break;
     const int a = nodes[q];
     const int ra = a * DIM;
     double da[DIM];
@@ -270,13 +276,14 @@ k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
   for (int e = threadIdx.x; e < NMM; e += kCMT) {
     double v = 0.0;
     for (int k = 0; k < kCMT / 32; ++k) v += wsum[k][e];
-    Ac[(int64_t)(A * NM + e / NM) * nc + A * NM + e % NM] += v;
+    atomicAdd(&Ac[(int64_t)(A * NM + e / NM) * nc + A * NM + e % NM], v);
   }
   for (int e = threadIdx.x; e < kTab * NMM; e += kCMT) {
     const int sl = e / NMM, B = ids[sl];
     if (B < 0) continue;
     const int m = (e % NMM) / NM, m2 = e % NM;
-    Ac[(int64_t)(A * NM + m) * nc + B * NM + m2] += tab[sl][e % NMM];
+    const double v = tab[sl][e % NMM];
+    if (v != 0.0) atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
   }
 }
 
@@ -429,11 +436,12 @@ k_gj_update(int nc, int kb, int bs, double* __restrict__ A, const double* __rest
   }
 }
 
-__global__ void k_symmetrise(int nc, const double* __restrict__ A, double* __restrict__ out) {
+__global__ void k_symmetrise(int nc, int ld, const double* __restrict__ A,
+                             double* __restrict__ out) {
   const int64_t t = blockIdx.x * (int64_t)kCT + threadIdx.x;
-  if (t >= (int64_t)nc * nc) return;
-  const int i = (int)(t / nc), j = (int)(t % nc);
-  out[t] = 0.5 * (A[t] + A[(int64_t)j * nc + i]);
+  if (t >= (int64_t)nc * ld) return;
+  const int i = (int)(t / ld), j = (int)(t % ld);
+  out[t] = j < nc ? 0.5 * (A[(int64_t)i * nc + j] + A[(int64_t)j * nc + i]) : 0.0;
 }
 
 // rc = P^T r: block per aggregate over its node list
@@ -484,17 +492,43 @@ k_restrict(const int32_t* __restrict__ off, const int32_t* __restrict__ nodes,
   }
 }
 
+// Row i of Ainv . rc for warp-per-row products: rows start on 64-byte boundaries (ld is a
+// multiple of 8) and every entry beyond nc, of the row and of rc, is zero, so the warp
+// reads 16-byte pairs, four pairs in flight per lane.
+__device__ inline double coarse_row_dot(const double* __restrict__ row,
+                                        const double* __restrict__ rc, int ld, int lane) {
+  const double2* r2 = reinterpret_cast<const double2*>(row);
+  const double2* c2 = reinterpret_cast<const double2*>(rc);
+  const int h = ld >> 1;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int j = lane;
+  for (; j + 96 < h; j += 128) {
+    const double2 v0 = __ldg(r2 + j), v1 = __ldg(r2 + j + 32), v2 = __ldg(r2 + j + 64),
+                  v3 = __ldg(r2 + j + 96);
+    const double2 x0 = c2[j], x1 = c2[j + 32], x2 = c2[j + 64], x3 = c2[j + 96];
+    a0 += v0.x * x0.x + v0.y * x0.y;
+    a1 += v1.x * x1.x + v1.y * x1.y;
+    a2 += v2.x * x2.x + v2.y * x2.y;
+    a3 += v3.x * x3.x + v3.y * x3.y;
+  }
+  for (; j < h; j += 32) {
+    const double2 v0 = __ldg(r2 + j), x0 = c2[j];
+    a0 += v0.x * x0.x + v0.y * x0.y;
+  }
+  double acc = (a0 + a1) + (a2 + a3);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
 // zc = Ainv rc: warp per row
-__global__ void k_coarse_gemv(int nc, const double* __restrict__ Ainv, const double* __restrict__ rc,
-                              double* __restrict__ zc, const int* __restrict__ done) {
+__global__ void k_coarse_gemv(int nc, int ld, const double* __restrict__ Ainv,
+                              const double* __restrict__ rc, double* __restrict__ zc,
+                              const int* __restrict__ done) {
   if (done && *done) return;
   const int i = blockIdx.x * (kCT / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (i >= nc) return;
-  const double* row = Ainv + (int64_t)i * nc;
-  double acc = 0.0;
-  for (int j = lane; j < nc; j += 32) acc += __ldg(row + j) * rc[j];
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  const double acc = coarse_row_dot(Ainv + (int64_t)i * ld, rc, ld, lane);
   if (lane == 0) zc[i] = acc;
 }
 
@@ -542,6 +576,113 @@ k_prolong(int n, const int32_t* __restrict__ agg, const double* __restrict__ x,
   }
   const double s = cg_block_sum(rz, sh);
   if (threadIdx.x == 0) atomicAdd(rz_acc, s);
+}
+
+// ---- fused two-level PCG steps ---------------------------------------------------
+// The direction kernel forms z = D^-1 r + P zc on the fly, using
+//   r.z = r.D^-1 r + (P^T r).zc = r.D^-1 r + rc.zc,
+// so z is never stored: r.D^-1 r comes with the x/r update, rc.zc with the coarse
+// product.  (Folding the restriction into the update as well, with warp-aggregated
+// atomics per aggregate, measured slower than the block-per-aggregate kernel: the
+// shuffles cost more than the second read of r.)
+
+// INIT: x = 0, r = b (bq = b).  Else: alpha = rz / p.q, x += alpha p, r -= alpha q (bq = q).
+// Accumulates rr = r.r and rzn += r.D^-1 r.
+template <bool INIT>
+__global__ void __launch_bounds__(kCT)
+k_tl_update(int n, const double* __restrict__ bq, double* __restrict__ x, double* __restrict__ r,
+            const double* __restrict__ p, const double* __restrict__ dinv, SolveScalars* sc) {
+  __shared__ double sh[32];
+  double alpha = 0.0;
+  if (!INIT) {
+    if (sc->done) return;
+    const double pq = sc->pq;
+    if (!(pq > 0.0) || !isfinite(pq)) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 2;
+      return;
+    }
+    alpha = sc->rz / pq;
+  }
+  double rr = 0.0, rdr = 0.0;
+  for (int i = blockIdx.x * kCT + threadIdx.x; i < n; i += gridDim.x * kCT) {
+    double ri;
+    if (INIT) {
+      ri = bq[i];
+      x[i] = 0.0;
+    } else {
+      x[i] += alpha * p[i];
+      ri = r[i] - alpha * bq[i];
+    }
+    r[i] = ri;
+    rr += ri * ri;
+    rdr += ri * ri * dinv[i];
+  }
+  const double s1 = cg_block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s1);
+  const double s2 = cg_block_sum(rdr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rzn, s2);
+}
+
+// zc = Ainv rc (warp per row) and rzn += rc.zc
+__global__ void __launch_bounds__(kCT)
+k_tl_gemv(int nc, int ld, const double* __restrict__ Ainv, const double* __restrict__ rc,
+          double* __restrict__ zc, SolveScalars* sc) {
+  __shared__ double sh[kCT / 32];
+  if (sc->done) return;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (kCT / 32) + w;
+  double part = 0.0;
+  if (i < nc) {
+    const double acc = coarse_row_dot(Ainv + (int64_t)i * ld, rc, ld, lane);
+    if (lane == 0) {
+      zc[i] = acc;
+      part = acc * rc[i];
+    }
+  }
+  if (lane == 0) sh[w] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < kCT / 32; ++k) t += sh[k];
+    atomicAdd(&sc->rzn, t);
+  }
+}
+
+// z = D^-1 r + P zc on the fly; FIRST: p = z, else p = z + beta p with beta = rzn / rz,
+// then the iteration count and the convergence test.
+template <int DIM, bool FIRST>
+__global__ void __launch_bounds__(kCT)
+k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ dinv,
+               const uint8_t* __restrict__ fixed, const int32_t* __restrict__ agg,
+               const double* __restrict__ xc, const double* __restrict__ cen, double sinv,
+               const double* __restrict__ zc, double* __restrict__ p, SolveScalars* sc) {
+  constexpr int NM = DIM == 2 ? 3 : 6;
+  if (sc->done) return;
+  const double beta = FIRST ? 0.0 : sc->rzn / sc->rz;
+  const int64_t stride = (int64_t)gridDim.x * kCT;
+  for (int64_t t = (int64_t)blockIdx.x * kCT + threadIdx.x; t < n; t += stride) {
+    const int i = (int)t;
+    double zi = dinv[i] * r[i];
+    if (!fixed[i]) {
+      const int a = i / DIM, c = i - a * DIM;
+      const int A = agg[a];
+      double d[DIM];
+#pragma unroll
+      for (int k = 0; k < DIM; ++k)
+        d[k] = (xc[(int64_t)a * DIM + k] - cen[(int64_t)A * DIM + k]) * sinv;
+      double pr[NM];
+      p_row<DIM>(c, d, pr);
+#pragma unroll
+      for (int m = 0; m < NM; ++m) zi += pr[m] * zc[A * NM + m];
+    }
+    p[i] = FIRST ? zi : zi + beta * p[i];
+  }
+  if (!FIRST && blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->pq = 0.0;
+    sc->iter += 1;
+    if (sc->rr <= sc->tol2) sc->done = 1;
+    else if (sc->iter >= sc->maxit) sc->done = 3;
+  }
 }
 
 void coarse_release(Coarse* c) {
@@ -624,6 +765,8 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   GF_CUDA(ctx, cudaMemcpyAsync(&na, d_id + nbox, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_CUDA(ctx, cudaStreamSynchronize(s));
   const int nc = na * nm;
+  const int ld = (nc + 7) & ~7;
+  C->ld = ld;
   C->dim = dim; C->nm = nm; C->na = na; C->nc = nc; C->s = side;
   for (int c = 0; c < 3; ++c) { C->lo[c] = g.lo[c]; C->nb[c] = g.nb[c]; }
   double* d_Ac = nullptr;
@@ -639,9 +782,9 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
       (st = gf_alloc(ctx, &C->agg_off, (size_t)na + 1)) != GF_OK ||
       (st = gf_alloc(ctx, &C->agg_nodes, (size_t)nnodes)) != GF_OK ||
       (st = gf_alloc(ctx, &C->cen, (size_t)na * dim)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->ainv, (size_t)nc * nc)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->rc, (size_t)nc)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->zc, (size_t)nc)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->ainv, (size_t)nc * ld)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->rc, (size_t)ld)) != GF_OK ||
+      (st = gf_alloc(ctx, &C->zc, (size_t)ld)) != GF_OK ||
       (st = gf_alloc(ctx, &d_Ac, (size_t)nc * nc)) != GF_OK ||
       (st = gf_alloc(ctx, &d_pi, (size_t)kGJ * kGJ)) != GF_OK ||
       (st = gf_alloc(ctx, &d_rw, (size_t)kGJ * nc)) != GF_OK ||
@@ -667,21 +810,54 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
     tb = tb2;
   }
   cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_cnt, C->agg_off, na + 1, s);
-  cudaMemcpyAsync(d_cnt, C->agg_off, sizeof(int32_t) * (na + 1), cudaMemcpyDeviceToDevice, s);
-  k_agg_fill<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, dim, C->node_agg, ctx->d_coords64,
-                                                   d_cnt, C->agg_nodes, C->cen);
+  // node lists: a stable sort of the nodes by aggregate keeps each list ascending, so
+  // the per-aggregate kernels read runs of neighbouring nodes
+  int32_t* d_iota = nullptr;
+  if ((st = gf_alloc(ctx, &d_iota, (size_t)nnodes)) != GF_OK) {
+    cleanup2();
+    return st;
+  }
+  k_agg_sums<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, dim, C->node_agg, ctx->d_coords64,
+                                                   d_iota, C->cen);
+  int end_bit = 1;
+  while ((1 << end_bit) < na) ++end_bit;
+  size_t tb3 = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb3, C->node_agg, d_key, d_iota, C->agg_nodes, nnodes,
+                                  0, end_bit, s);
+  if (tb3 > tb) {
+    cudaFree(d_tmp);
+    d_tmp = nullptr;
+    if (cudaMalloc(&d_tmp, tb3) != cudaSuccess) {
+      cudaGetLastError();
+      gf_free(d_iota);
+      cleanup2();
+      return gf_fail(ctx, GF_ERR_OOM, "coarse sort scratch");
+    }
+    tb = tb3;
+  }
+  cub::DeviceRadixSort::SortPairs(d_tmp, tb, C->node_agg, d_key, d_iota, C->agg_nodes, nnodes, 0,
+                                  end_bit, s);
+  gf_free(d_iota);
   k_centroid<<<gf_blocks(na, kCT), kCT, 0, s>>>(na, dim, C->agg_off, C->cen);
   // coarse matrix
   cudaMemsetAsync(d_Ac, 0, sizeof(double) * nc * nc, s);
   const double sinv = 1.0 / side;
+  std::vector<int32_t> hoff(na + 1);
+  GF_CUDA(ctx, cudaMemcpyAsync(hoff.data(), C->agg_off, sizeof(int32_t) * (na + 1),
+                               cudaMemcpyDeviceToHost, s));
+  GF_CUDA(ctx, cudaStreamSynchronize(s));
+  int maxcnt = 1;
+  for (int A = 0; A < na; ++A) maxcnt = std::max(maxcnt, hoff[A + 1] - hoff[A]);
+  const int per = (int)((maxcnt + (int64_t)kCMT * 65535 - 1) / ((int64_t)kCMT * 65535));
+  const dim3 gcm(na, (maxcnt + kCMT * per - 1) / (kCMT * per));
   if (dim == 2)
-    k_coarse_rows<2><<<na, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
-                                         ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
-                                         ctx->d_coords64, C->cen, sinv, nc, d_Ac);
+    k_coarse_rows<2><<<gcm, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
+                                          ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
+                                          ctx->d_coords64, C->cen, sinv, nc, per, d_Ac);
   else
-    k_coarse_rows<3><<<na, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
-                                         ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
-                                         ctx->d_coords64, C->cen, sinv, nc, d_Ac);
+    k_coarse_rows<3><<<gcm, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
+                                          ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
+                                          ctx->d_coords64, C->cen, sinv, nc, per, d_Ac);
   k_diag_max<<<1, kCT, 0, s>>>(nc, d_Ac, d_dmax);
   k_regularise<<<gf_blocks(nc, kCT), kCT, 0, s>>>(nc, d_dmax, 1e-10, d_Ac);
   ctx->launches += 8;
@@ -694,7 +870,8 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
     k_gj_update<<<gu, 256, 0, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
     ctx->launches += 3;
   }
-  k_symmetrise<<<gf_blocks((int64_t)nc * nc, kCT), kCT, 0, s>>>(nc, d_Ac, C->ainv);
+  k_symmetrise<<<gf_blocks((int64_t)nc * ld, kCT), kCT, 0, s>>>(nc, ld, d_Ac, C->ainv);
+  cudaMemsetAsync(C->rc, 0, sizeof(double) * ld, s);  // the tail beyond nc stays zero
   ctx->launches++;
   cudaError_t e = cudaStreamSynchronize(s);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -744,17 +921,52 @@ void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z
   if (c->dim == 2) {
     k_restrict<2><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
                                         ctx->d_fixed, r, c->rc, done);
-    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ainv, c->rc, c->zc, done);
+    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ld, c->ainv, c->rc, c->zc, done);
     k_prolong<2><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
                                     ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
   } else {
     k_restrict<3><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
                                         ctx->d_fixed, r, c->rc, done);
-    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ainv, c->rc, c->zc, done);
+    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ld, c->ainv, c->rc, c->zc, done);
     k_prolong<3><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
                                     ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
   }
   ctx->launches += 3;
+}
+
+template <int DIM>
+static void tl_launch(gf_ctx* ctx, bool init, const double* bq, double* x, double* r, double* p,
+                      const double* dinv, SolveScalars* sc) {
+  Coarse* c = static_cast<Coarse*>(ctx->coarse);
+  cudaStream_t s = ctx->stream;
+  const int n = ctx->n;
+  const double sinv = 1.0 / c->s;
+  const int grid = std::min(gf_blocks(n, kCT), ctx->sm_count * 8);
+  const int gbk = (c->nc + kCT / 32 - 1) / (kCT / 32);
+  if (init) k_tl_update<true><<<grid, kCT, 0, s>>>(n, bq, x, r, nullptr, dinv, sc);
+  else k_tl_update<false><<<grid, kCT, 0, s>>>(n, bq, x, r, p, dinv, sc);
+  k_restrict<DIM><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
+                                        ctx->d_fixed, r, c->rc, &sc->done);
+  k_tl_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ld, c->ainv, c->rc, c->zc, sc);
+  if (init)
+    k_tl_direction<DIM, true><<<grid, kCT, 0, s>>>(n, r, dinv, ctx->d_fixed, c->node_agg,
+                                                   ctx->d_coords64, c->cen, sinv, c->zc, p, sc);
+  else
+    k_tl_direction<DIM, false><<<grid, kCT, 0, s>>>(n, r, dinv, ctx->d_fixed, c->node_agg,
+                                                    ctx->d_coords64, c->cen, sinv, c->zc, p, sc);
+  ctx->launches += 4;
+}
+
+void gf_tl_begin(gf_ctx* ctx, const double* b, double* x, double* r, double* p,
+                 const double* dinv, SolveScalars* sc) {
+  if (static_cast<Coarse*>(ctx->coarse)->dim == 2) tl_launch<2>(ctx, true, b, x, r, p, dinv, sc);
+  else tl_launch<3>(ctx, true, b, x, r, p, dinv, sc);
+}
+
+void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q,
+                   const double* dinv, SolveScalars* sc) {
+  if (static_cast<Coarse*>(ctx->coarse)->dim == 2) tl_launch<2>(ctx, false, q, x, r, p, dinv, sc);
+  else tl_launch<3>(ctx, false, q, x, r, p, dinv, sc);
 }
 
 extern "C" GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse,
