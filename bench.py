@@ -404,7 +404,8 @@ def run_gpu_arm(args):
             traffic_asm = tr.get("bytes_per_assembly")
             traffic = tr.get("kernels", {}).get("k_assemble_owner")
 
-    # SpMV roofline (FP32 values + int32 columns + x gather + y write)
+    # SpMV roofline: node-block slices, i.e. the values, one int32 column per dim x dim
+    # block, x read once and y written once
     ctx.assemble(dtype, scatter)
     xs = torch.randn(n, device="cuda", dtype=torch.float32 if esize == 4 else torch.float64)
     ys = torch.empty_like(xs)
@@ -415,7 +416,7 @@ def run_gpu_arm(args):
         _lib.check(_lib.lib.gf_spmv(ctx.h, dtype, xs.data_ptr(), ys.data_ptr()), ctx.h)
         sp.append(_lib.lib.gf_last_device_seconds(ctx.h))
     t_spmv = float(np.median(sp))
-    spmv_bytes = nnz * (esize + 4) + n * (4 + 2 * esize)
+    spmv_bytes = nnz * esize + (nnz // (m.dim * m.dim)) * 4 + n * 2 * esize
 
     # e2e through the public API from pinned host buffers, every step
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()

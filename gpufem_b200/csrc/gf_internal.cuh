@@ -225,7 +225,8 @@ struct gf_ctx {
 
   // sliced-ELL copy for the solver's SpMVs (gf_sell.cu)
   bool sell_ready = false;
-  int sell_nslice = 0, sell_nslots = 0;  // slices of 32 rows; nslots = 32 * nslice
+  int sell_nslice = 0, sell_nslots = 0;  // slices of 32 rows (nodes); nslots = 32 * nslice
+  int sell_bdim = 0;                     // 0: row slices; 2, 3: node-block slices
   int64_t sell_total = 0;
   int64_t sell_ver64 = -1, sell_ver32 = -1;
   int64_t* d_sell_off = nullptr;   // [nslice + 1] first entry of each slice

@@ -48,12 +48,15 @@ __device__ inline double block_sum(T v, double* sh) {
 //         off[t/32] + 32 s + t%32, and every row of a slice runs to the slice's
 //         width (padding entries hold column t and value 0).
 struct MatLayout {
-  int count;  // rows = threads to launch
+  int count;  // threads to launch
   int n;
   const int32_t* __restrict__ rownnz;
   const int32_t* __restrict__ col;
   const int32_t* __restrict__ width;
   const int64_t* __restrict__ off;
+  int bdim = 0;      // 0: rows (ELL / SELL); 2, 3: node-block slices (gf_sell.cu)
+  int nnodes = 0;
+  int threads = kT;  // block size; a multiple of 32 * bdim for node blocks
 
   __device__ inline bool at(int t, int& nz, int64_t& o, int64_t& stride) const {
     if (t >= count) return false;
@@ -70,9 +73,6 @@ struct MatLayout {
   }
 };
 
-// Row dot sum_{s < nz} val[o + s*stride] * x[col[o + s*stride]], software-pipelined:
-// the next four (column, value) pairs are loaded before the x gathers of the current
-// four, so a thread keeps eight matrix loads in flight across its gathers.
 template <typename TK, typename TX>
 __device__ inline double row_dot(int64_t o, int64_t stride, int nz, const int32_t* __restrict__ col,
                                  const TK* __restrict__ val, const TX* __restrict__ x) {
@@ -107,13 +107,100 @@ __device__ inline double row_dot(int64_t o, int64_t stride, int nz, const int32_
   return (double)((a0 + a1) + (a2 + a3));
 }
 
+// Node-block slices: thread t is component c = (t / 32) % DIM of node 32 k + t % 32,
+// k = t / (32 DIM).  Per neighbour block: one column word (shared by the DIM warps of the
+// slice, cached), DIM coalesced values, DIM consecutive entries of x.  Two blocks are
+// loaded ahead of the gathers that use them.
+template <int DIM, typename TK, typename TX>
+__device__ inline double bsell_dot(const int32_t* __restrict__ bc, const TK* __restrict__ vp, int w,
+                                   const TX* __restrict__ x) {
+  using Acc = typename std::conditional<sizeof(TK) == 8 || sizeof(TX) == 8, double, float>::type;
+  constexpr int SS = DIM * DIM * 32;  // value stride between neighbour slots
+  Acc a0 = 0, a1 = 0;
+  int p = 0;
+  if (w >= 2) {
+    int b0 = __ldg(bc), b1 = __ldg(bc + 32);
+    TK u0[DIM], u1[DIM];
+#pragma unroll
+    for (int c2 = 0; c2 < DIM; ++c2) {
+      u0[c2] = __ldcs(vp + c2 * 32);
+      u1[c2] = __ldcs(vp + SS + c2 * 32);
+    }
+    for (p = 2; p + 2 <= w; p += 2) {
+      bc += 64;
+      vp += 2 * SS;
+      const int e0 = __ldg(bc), e1 = __ldg(bc + 32);
+      TK t0[DIM], t1[DIM];
+#pragma unroll
+      for (int c2 = 0; c2 < DIM; ++c2) {
+        t0[c2] = __ldcs(vp + c2 * 32);
+        t1[c2] = __ldcs(vp + SS + c2 * 32);
+      }
+#pragma unroll
+      for (int c2 = 0; c2 < DIM; ++c2) {
+        a0 += (Acc)u0[c2] * (Acc)__ldg(x + b0 * DIM + c2);
+        a1 += (Acc)u1[c2] * (Acc)__ldg(x + b1 * DIM + c2);
+      }
+      b0 = e0;
+      b1 = e1;
+#pragma unroll
+      for (int c2 = 0; c2 < DIM; ++c2) {
+        u0[c2] = t0[c2];
+        u1[c2] = t1[c2];
+      }
+    }
+#pragma unroll
+    for (int c2 = 0; c2 < DIM; ++c2) {
+      a0 += (Acc)u0[c2] * (Acc)__ldg(x + b0 * DIM + c2);
+      a1 += (Acc)u1[c2] * (Acc)__ldg(x + b1 * DIM + c2);
+    }
+    bc += 64;
+    vp += 2 * SS;
+  }
+  if (p < w) {
+    const int b0 = __ldg(bc);
+#pragma unroll
+    for (int c2 = 0; c2 < DIM; ++c2) a0 += (Acc)__ldcs(vp + c2 * 32) * (Acc)__ldg(x + b0 * DIM + c2);
+  }
+  return (double)(a0 + a1);
+}
+
+template <int DIM, typename TK, typename TX>
+__device__ inline bool block_row(const MatLayout& L, int t, const TK* __restrict__ val,
+                                 const TX* __restrict__ x, int& row, double& v) {
+  const int k = t / (32 * DIM);
+  const int c = (t >> 5) - k * DIM;
+  const int l = t & 31;
+  const int node = k * 32 + l;
+  if (node >= L.nnodes) return false;
+  row = node * DIM + c;
+  const int64_t o = __ldg(L.off + k);
+  v = bsell_dot<DIM>(L.col + o + l, val + o * (DIM * DIM) + c * (DIM * 32) + l,
+                     __ldg(L.width + k), x);
+  return true;
+}
+
+// Row (or, for node blocks, the row of thread t) of K x; false for a thread with no row.
+template <typename TK, typename TX>
+__device__ inline bool mat_row(const MatLayout& L, int t, const TK* __restrict__ val,
+                               const TX* __restrict__ x, int& row, double& v) {
+  if (L.bdim == 2) return block_row<2>(L, t, val, x, row, v);
+  if (L.bdim == 3) return block_row<3>(L, t, val, x, row, v);
+  int nz;
+  int64_t o, st;
+  if (!L.at(t, nz, o, st)) return false;
+  row = t;
+  v = row_dot(o, st, nz, L.col, val, x);
+  return true;
+}
+
 template <typename TK, typename TX, typename TY>
 __global__ void __launch_bounds__(kT)
 k_spmv(MatLayout L, const TK* __restrict__ val, const TX* __restrict__ x, TY* __restrict__ y) {
-  const int row = blockIdx.x * kT + threadIdx.x;
-  int nz;
-  int64_t o, st;
-  if (L.at(row, nz, o, st)) y[row] = (TY)row_dot(o, st, nz, L.col, val, x);
+  int row;
+  double v;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L.count; t += gridDim.x * blockDim.x)
+    if (mat_row(L, t, val, x, row, v)) y[row] = (TY)v;
 }
 
 // r = f - K u (FP64), and r.r
@@ -121,12 +208,12 @@ __global__ void __launch_bounds__(kT)
 k_residual64(MatLayout L, const double* __restrict__ val, const double* __restrict__ u,
              const double* __restrict__ f, double* __restrict__ r, double* __restrict__ acc) {
   __shared__ double sh[32];
-  int nz;
-  int64_t o, st;
+  int row;
+  double kv;
   double rr = 0.0;
-  for (int row = blockIdx.x * kT + threadIdx.x; row < L.count; row += gridDim.x * kT) {
-    if (!L.at(row, nz, o, st)) continue;
-    double v = f[row] - row_dot(o, st, nz, L.col, val, u);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L.count; t += gridDim.x * blockDim.x) {
+    if (!mat_row(L, t, val, u, row, kv)) continue;
+    const double v = f[row] - kv;
     r[row] = v;
     rr += v * v;
   }
@@ -177,12 +264,11 @@ k_cg_spmv_dot(MatLayout L, const TK* __restrict__ val, const V* __restrict__ p,
     sc->rzn = 0.0;
     sc->rr = 0.0;
   }
-  int nz;
-  int64_t o, st;
+  int row;
+  double v;
   double pq = 0.0;
-  for (int row = blockIdx.x * kT + threadIdx.x; row < L.count; row += gridDim.x * kT) {
-    if (!L.at(row, nz, o, st)) continue;
-    double v = row_dot(o, st, nz, L.col, val, p);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L.count; t += gridDim.x * blockDim.x) {
+    if (!mat_row(L, t, val, p, row, v)) continue;
     q[row] = (V)v;
     pq += (double)p[row] * (double)(V)v;
   }
@@ -331,11 +417,22 @@ inline int red_grid(const gf_ctx* ctx, int64_t work) {
   return std::min(gf_blocks(work, kT), ctx->sm_count * 8);
 }
 
+// grid of the SpMV kernels for layout L (block size L.threads)
+inline int mat_grid(const gf_ctx* ctx, const MatLayout& L) {
+  return std::min(gf_blocks(L.count, L.threads), ctx->sm_count * 8);
+}
+
 // The sliced copy of the context's matrix in `dtype` (built or refreshed on demand).
 gf_status solver_matrix(gf_ctx* ctx, int dtype, MatLayout* L, const void** val) {
   gf_status st = gf_sell_prepare(ctx, dtype);
   if (st != GF_OK) return st;
   *L = MatLayout{ctx->n, ctx->n, ctx->d_rownnz, ctx->d_sell_col, ctx->d_sell_w, ctx->d_sell_off};
+  if (ctx->sell_bdim) {
+    L->bdim = ctx->sell_bdim;
+    L->nnodes = ctx->nnodes;
+    L->count = ctx->sell_nslice * 32 * ctx->sell_bdim;
+    L->threads = 32 * ctx->sell_bdim * (ctx->sell_bdim == 2 ? 4 : 2);  // 256 / 192
+  }
   *val = dtype == GF_F64 ? (const void*)ctx->d_sell_v64 : (const void*)ctx->d_sell_v32;
   return GF_OK;
 }
@@ -350,10 +447,10 @@ gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y) {
   if (st != GF_OK) return st;
   cudaEventRecord(ctx->ev0, ctx->stream);
   if (dtype == GF_F64)
-    k_spmv<double, double, double><<<gf_blocks(L.count, kT), kT, 0, ctx->stream>>>(
+    k_spmv<double, double, double><<<mat_grid(ctx, L), L.threads, 0, ctx->stream>>>(
         L, (const double*)val, (const double*)x, (double*)y);
   else
-    k_spmv<float, float, float><<<gf_blocks(L.count, kT), kT, 0, ctx->stream>>>(
+    k_spmv<float, float, float><<<mat_grid(ctx, L), L.threads, 0, ctx->stream>>>(
         L, (const float*)val, (const float*)x, (float*)y);
   GF_LAUNCH_CHECK(ctx, "k_spmv");
   cudaEventRecord(ctx->ev1, ctx->stream);
@@ -458,7 +555,7 @@ gf_status run_cg(gf_ctx* ctx, MatLayout L, const TK* val, const V* b, CgVecs vv,
   cudaGraphExec_t exec = nullptr;
   GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < check_every; ++k) {
-    k_cg_spmv_dot<TK, V><<<red_grid(ctx, L.count), kT, 0, s>>>(L, val, p, q, sc);
+    k_cg_spmv_dot<TK, V><<<mat_grid(ctx, L), L.threads, 0, s>>>(L, val, p, q, sc);
     k_cg_update<V><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, zz, p, q, dinv, sc);
     k_cg_direction<V><<<nb, kT, 0, s>>>(n, zz, p, sc);
   }
@@ -527,7 +624,7 @@ gf_status residual64(gf_ctx* ctx, double* r64, double* rr) {
   const void* val = nullptr;
   gf_status st = solver_matrix(ctx, GF_F64, &L, &val);
   if (st != GF_OK) return st;
-  k_residual64<<<red_grid(ctx, L.count), kT, 0, s>>>(L, (const double*)val, ctx->d_u, ctx->d_f,
+  k_residual64<<<mat_grid(ctx, L), L.threads, 0, s>>>(L, (const double*)val, ctx->d_u, ctx->d_f,
                                                      r64, ctx->d_red);
   GF_LAUNCH_CHECK(ctx, "k_residual64");
   double* h = (double*)ctx->h_pinned + 16;
@@ -647,7 +744,7 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     cudaGraphExec_t exec = nullptr;
     GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < check; ++k) {
-      k_cg_spmv_dot<float, V><<<red_grid(ctx, L32.count), kT, 0, s>>>(L32, val32, p, q, sc);
+      k_cg_spmv_dot<float, V><<<mat_grid(ctx, L32), L32.threads, 0, s>>>(L32, val32, p, q, sc);
       k_cg_update<V><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
       k_cg_direction<V><<<nb, kT, 0, s>>>(n, z, p, sc);
     }
@@ -836,12 +933,11 @@ k_fcg_spmv(MatLayout L, const double* __restrict__ val, const double* __restrict
   __shared__ double sh[32];
   if (sc->done) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) sc->rr = 0.0;
-  int nz;
-  int64_t o, st;
+  int row;
+  double v;
   double pq = 0.0, pr = 0.0;
-  for (int row = blockIdx.x * kT + threadIdx.x; row < L.count; row += gridDim.x * kT) {
-    if (!L.at(row, nz, o, st)) continue;
-    const double v = row_dot(o, st, nz, L.col, val, p);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L.count; t += gridDim.x * blockDim.x) {
+    if (!mat_row(L, t, val, p, row, v)) continue;
     q[row] = v;
     pq += p[row] * v;
     pr += p[row] * r[row];
@@ -942,7 +1038,7 @@ gf_status run_fcg(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       else k_fcg_jacobi<<<nb, kT, 0, s>>>(n, r, dinv, z, sc);
       k_fcg_dots<<<red_grid(ctx, n), kT, 0, s>>>(n, z, r, rold, sc);
       k_fcg_dir<<<nb, kT, 0, s>>>(n, z, p, sc);
-      k_fcg_spmv<<<red_grid(ctx, L.count), kT, 0, s>>>(L, val, p, r, q, sc);
+      k_fcg_spmv<<<mat_grid(ctx, L), L.threads, 0, s>>>(L, val, p, r, q, sc);
       k_fcg_update<<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, rold, p, q, sc);
       k_fcg_finish<<<1, 1, 0, s>>>(sc);
     }
@@ -1040,7 +1136,7 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
   int got = 1;
   while (got < npairs) {
     for (int k = 0; k < every; ++k) {
-      k_cg_spmv_dot<double, double><<<red_grid(ctx, L.count), kT, 0, s>>>(
+      k_cg_spmv_dot<double, double><<<mat_grid(ctx, L), L.threads, 0, s>>>(
           L, (const double*)vk, p, q, sc);
       k_cg_update<double><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
       k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
@@ -1092,7 +1188,7 @@ gf_status run_twolevel(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check
   const int64_t l0 = ctx->launches;
   GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < check; ++k) {
-    k_cg_spmv_dot<double, double><<<red_grid(ctx, L.count), kT, 0, s>>>(L, val, p, q, sc);
+    k_cg_spmv_dot<double, double><<<mat_grid(ctx, L), L.threads, 0, s>>>(L, val, p, q, sc);
     gf_tl_iterate(ctx, x, r, p, q, dinv, sc);
   }
   cudaError_t ce = cudaStreamEndCapture(s, &graph);
