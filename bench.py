@@ -502,6 +502,15 @@ def run_gpu_arm(args):
             "rel_err_vs_reference": float(np.linalg.norm(utl - ustar) / nrm),
             "coarse_unknowns": nc,
             "label": "FP64 PCG, M = Jacobi + rigid-body modes of box aggregates"}
+        tl32 = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, _lib.GF_F32, tol=1e-8, max_iter=400000,
+                         raise_on_error=False)
+        utl32 = ctx.solution()
+        solve["twolevel_pcg_k32"] = {
+            "seconds": tl32.seconds, "iterations": tl32.iterations, "outer": tl32.outer,
+            "fp64_fallback": tl32.fallback, "status": tl32.status,
+            "rel_residual": tl32.rel_residual,
+            "rel_err_vs_reference": float(np.linalg.norm(utl32 - ustar) / nrm),
+            "label": "two-level PCG with K32 SpMVs, FP64 vectors, reliable updates on K64"}
         if rank == 0 and world == 1 and not args.no_cpu and cfg in ("q4_64", "q8_512"):
             # (the reference's assembly of the full 3-D meshes alone takes minutes)
             rc = reference_cg_sample(m)

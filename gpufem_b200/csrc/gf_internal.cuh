@@ -361,6 +361,10 @@ void gf_tl_begin(gf_ctx* ctx, const double* b, double* x, double* r, double* p,
                  const double* dinv, SolveScalars* sc);
 void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q,
                    const double* dinv, SolveScalars* sc);
+// Reliable update: x = 0, r = scale * b, rr and rzn as in begin; then p = M r (restart)
+// or p = pscale * p (direction kept).  sc->rr and sc->rzn must be zero on entry.
+void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
+                 double* x, double* r, double* p, const double* dinv, SolveScalars* sc);
 void gf_lp_mesh_changed(gf_ctx* ctx);
 gf_status gf_lp_prepare(gf_ctx* ctx);
 bool gf_lp_ready(const gf_ctx* ctx);

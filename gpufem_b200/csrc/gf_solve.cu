@@ -703,9 +703,12 @@ __global__ void k_mixed_scalars(SolveScalars* sc, double tol2) {
   sc->done = sc->iter >= sc->maxit ? 3 : 0;
 }
 
+// twolevel (V = double only): the two-level preconditioner (gf_twolevel.cu) in place of
+// Jacobi, in the recursion and at every reliable update.
 template <typename V>
 gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
-                    std::chrono::steady_clock::time_point t0, gf_solve_info* info) {
+                    std::chrono::steady_clock::time_point t0, gf_solve_info* info,
+                    bool twolevel = false) {
   const int n = ctx->n;
   const int nb = gf_blocks(n, kT);
   cudaStream_t s = ctx->stream;
@@ -723,6 +726,9 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   if ((st = solver_matrix(ctx, GF_F32, &L32, &v32)) != GF_OK) return st;
   if ((st = solver_matrix(ctx, GF_F64, &L64, &v64)) != GF_OK) return st;
   const float* val32 = (const float*)v32;
+  if (twolevel && sizeof(V) != sizeof(double))
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "two-level mixed solve runs on FP64 vectors");
+  if (twolevel && (st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
   k_diag_inv<double, V><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_LAUNCH_CHECK(ctx, "k_diag_inv");
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u, 0, sizeof(double) * n, s));
@@ -733,21 +739,35 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   bool fp64_fallback = false;
   if (ff > 0.0) {
     double sigma = std::sqrt(ff);
-    k_scale_to<V><<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
-    GF_LAUNCH_CHECK(ctx, "k_scale_to");
     GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
-    k_cg_init<V><<<red_grid(ctx, n), kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
-    GF_LAUNCH_CHECK(ctx, "k_cg_init");
+    if (twolevel) {
+      gf_tl_reset(ctx, r64, 1.0 / sigma, true, 1.0, (double*)x, (double*)r, (double*)p,
+                  (const double*)dinv, sc);
+      GF_LAUNCH_CHECK(ctx, "gf_tl_reset");
+    } else {
+      k_scale_to<V><<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
+      GF_LAUNCH_CHECK(ctx, "k_scale_to");
+      k_cg_init<V><<<red_grid(ctx, n), kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
+      GF_LAUNCH_CHECK(ctx, "k_cg_init");
+    }
     k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
     GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int64_t l0 = ctx->launches;
     for (int k = 0; k < check; ++k) {
       k_cg_spmv_dot<float, V><<<mat_grid(ctx, L32), L32.threads, 0, s>>>(L32, val32, p, q, sc);
-      k_cg_update<V><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
-      k_cg_direction<V><<<nb, kT, 0, s>>>(n, z, p, sc);
+      if (twolevel) {
+        gf_tl_iterate(ctx, (double*)x, (double*)r, (double*)p, (const double*)q,
+                      (const double*)dinv, sc);
+      } else {
+        k_cg_update<V><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+        k_cg_direction<V><<<nb, kT, 0, s>>>(n, z, p, sc);
+      }
     }
+    const int64_t per_chunk = twolevel ? ctx->launches - l0 + check : 3 * (int64_t)check;
+    ctx->launches = l0;
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (ce != cudaSuccess) return gf_cuda_fail(ctx, ce, "graph capture");
     ce = cudaGraphInstantiate(&exec, graph, 0);
@@ -766,7 +786,7 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       if (ce == cudaSuccess) ce = cudaMemcpyAsync(hs, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s);
       if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "mixed chunk"); break; }
-      ctx->launches += 3 * check;
+      ctx->launches += per_chunk;
       const bool timeout = o->max_seconds > 0.0 &&
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds;
       // growth of the FP32 residual by 100x over its value at the last update means
@@ -793,17 +813,26 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       stagnant = rr64 > 0.25 * prev_rr64 ? stagnant + 1 : 0;
       prev_rr64 = rr64;
       if (stagnant >= 3) { fp64_fallback = true; break; }
-      const bool restart = hs->done == 2 || diverging;
+      // with the two-level preconditioner a chunk can take the recursion far past the
+      // 10x trigger, down to its own convergence: its direction is spent, so restart
+      const bool restart = hs->done == 2 || diverging ||
+                           (twolevel && (hs->done == 1 || hs->rr < 1e-12));
       if (restart && ++breakdowns > 50) { done_code = 2; break; }
       const double sigma_new = std::sqrt(rr64);
       ce = cudaMemsetAsync(&sc->rzn, 0, 2 * sizeof(double), s);  // rzn, rr
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "reset"); break; }
-      k_mixed_reset<V><<<red_grid(ctx, n), kT, 0, s>>>(n, r64, 1.0 / sigma_new, (V)(sigma / sigma_new),
-                                         restart ? 1 : 0, dinv, r, z, p, sc);
+      // done flag and pq first: the two-level kernels skip their work while done != 0
       k_mixed_scalars<<<1, 1, 0, s>>>(sc, tol * tol * ff / rr64);
+      if (twolevel)
+        gf_tl_reset(ctx, r64, 1.0 / sigma_new, restart, sigma / sigma_new, (double*)x,
+                    (double*)r, (double*)p, (const double*)dinv, sc);
+      else
+        k_mixed_reset<V><<<red_grid(ctx, n), kT, 0, s>>>(n, r64, 1.0 / sigma_new,
+                                                         (V)(sigma / sigma_new), restart ? 1 : 0,
+                                                         dinv, r, z, p, sc);
       ce = cudaGetLastError();
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "k_mixed_reset"); break; }
-      ctx->launches += 2;
+      ctx->launches += twolevel ? 1 : 2;  // gf_tl_reset counts its own
       sigma = sigma_new;
       rr_max = 1.0;
       seg_start = hs->iter;
@@ -1250,7 +1279,13 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
     return run_fcg(ctx, o, maxit, check, t0, info);
   }
 
+  if (solver == GF_SOLVER_TWOLEVEL_PCG && o->matrix == GF_F32) {
+    if (!ctx->has64 || !ctx->has32)
+      return gf_fail(ctx, GF_ERR_STATE, "two-level PCG on K32 needs both FP64 and FP32 matrices");
+    return run_mixed<double>(ctx, o, maxit, check, t0, info, true);
+  }
   if (solver == GF_SOLVER_TWOLEVEL_PCG) {
+    if (o->matrix != GF_F64) return gf_fail(ctx, GF_ERR_INVALID_ARG, "matrix dtype %d", o->matrix);
     if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "two-level PCG needs the FP64 matrix");
     if ((st = run_twolevel(ctx, o, maxit, check, info)) != GF_OK) return st;
     cudaEventRecord(ctx->ev1, s);

@@ -586,12 +586,13 @@ k_prolong(int n, const int32_t* __restrict__ agg, const double* __restrict__ x,
 // atomics per aggregate, measured slower than the block-per-aggregate kernel: the
 // shuffles cost more than the second read of r.)
 
-// INIT: x = 0, r = b (bq = b).  Else: alpha = rz / p.q, x += alpha p, r -= alpha q (bq = q).
-// Accumulates rr = r.r and rzn += r.D^-1 r.
+// INIT: x = 0, r = scale * b (bq = b).  Else: alpha = rz / p.q, x += alpha p,
+// r -= alpha q (bq = q).  Accumulates rr = r.r and rzn += r.D^-1 r.
 template <bool INIT>
 __global__ void __launch_bounds__(kCT)
-k_tl_update(int n, const double* __restrict__ bq, double* __restrict__ x, double* __restrict__ r,
-            const double* __restrict__ p, const double* __restrict__ dinv, SolveScalars* sc) {
+k_tl_update(int n, const double* __restrict__ bq, double scale, double* __restrict__ x,
+            double* __restrict__ r, const double* __restrict__ p, const double* __restrict__ dinv,
+            SolveScalars* sc) {
   __shared__ double sh[32];
   double alpha = 0.0;
   if (!INIT) {
@@ -607,7 +608,7 @@ k_tl_update(int n, const double* __restrict__ bq, double* __restrict__ x, double
   for (int i = blockIdx.x * kCT + threadIdx.x; i < n; i += gridDim.x * kCT) {
     double ri;
     if (INIT) {
-      ri = bq[i];
+      ri = bq[i] * scale;
       x[i] = 0.0;
     } else {
       x[i] += alpha * p[i];
@@ -648,17 +649,25 @@ k_tl_gemv(int nc, int ld, const double* __restrict__ Ainv, const double* __restr
   }
 }
 
-// z = D^-1 r + P zc on the fly; FIRST: p = z, else p = z + beta p with beta = rzn / rz,
-// then the iteration count and the convergence test.
-template <int DIM, bool FIRST>
+// z = D^-1 r + P zc on the fly.  MODE kTlFirst: p = z; kTlKeep: p = pscale p (a
+// reliable update that keeps the direction); kTlStep: p = z + beta p with
+// beta = rzn / rz, then the iteration count and the convergence test.
+constexpr int kTlFirst = 0, kTlKeep = 1, kTlStep = 2;
+template <int DIM, int MODE>
 __global__ void __launch_bounds__(kCT)
 k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ dinv,
                const uint8_t* __restrict__ fixed, const int32_t* __restrict__ agg,
                const double* __restrict__ xc, const double* __restrict__ cen, double sinv,
-               const double* __restrict__ zc, double* __restrict__ p, SolveScalars* sc) {
+               const double* __restrict__ zc, double* __restrict__ p, double pscale,
+               SolveScalars* sc) {
   constexpr int NM = DIM == 2 ? 3 : 6;
   if (sc->done) return;
-  const double beta = FIRST ? 0.0 : sc->rzn / sc->rz;
+  if (MODE == kTlKeep) {
+    for (int64_t t = (int64_t)blockIdx.x * kCT + threadIdx.x; t < n; t += (int64_t)gridDim.x * kCT)
+      p[t] *= pscale;
+    return;
+  }
+  const double beta = MODE == kTlFirst ? 0.0 : sc->rzn / sc->rz;
   const int64_t stride = (int64_t)gridDim.x * kCT;
   for (int64_t t = (int64_t)blockIdx.x * kCT + threadIdx.x; t < n; t += stride) {
     const int i = (int)t;
@@ -675,9 +684,9 @@ k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ d
 #pragma unroll
       for (int m = 0; m < NM; ++m) zi += pr[m] * zc[A * NM + m];
     }
-    p[i] = FIRST ? zi : zi + beta * p[i];
+    p[i] = MODE == kTlFirst ? zi : zi + beta * p[i];
   }
-  if (!FIRST && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (MODE == kTlStep && blockIdx.x == 0 && threadIdx.x == 0) {
     sc->pq = 0.0;
     sc->iter += 1;
     if (sc->rr <= sc->tol2) sc->done = 1;
@@ -935,38 +944,55 @@ void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z
 }
 
 template <int DIM>
-static void tl_launch(gf_ctx* ctx, bool init, const double* bq, double* x, double* r, double* p,
-                      const double* dinv, SolveScalars* sc) {
+static void tl_launch(gf_ctx* ctx, int mode, const double* bq, double scale, double pscale,
+                      double* x, double* r, double* p, const double* dinv, SolveScalars* sc) {
   Coarse* c = static_cast<Coarse*>(ctx->coarse);
   cudaStream_t s = ctx->stream;
   const int n = ctx->n;
   const double sinv = 1.0 / c->s;
   const int grid = std::min(gf_blocks(n, kCT), ctx->sm_count * 8);
   const int gbk = (c->nc + kCT / 32 - 1) / (kCT / 32);
-  if (init) k_tl_update<true><<<grid, kCT, 0, s>>>(n, bq, x, r, nullptr, dinv, sc);
-  else k_tl_update<false><<<grid, kCT, 0, s>>>(n, bq, x, r, p, dinv, sc);
+  if (mode == kTlStep) k_tl_update<false><<<grid, kCT, 0, s>>>(n, bq, 1.0, x, r, p, dinv, sc);
+  else k_tl_update<true><<<grid, kCT, 0, s>>>(n, bq, scale, x, r, nullptr, dinv, sc);
   k_restrict<DIM><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
                                         ctx->d_fixed, r, c->rc, &sc->done);
   k_tl_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ld, c->ainv, c->rc, c->zc, sc);
-  if (init)
-    k_tl_direction<DIM, true><<<grid, kCT, 0, s>>>(n, r, dinv, ctx->d_fixed, c->node_agg,
-                                                   ctx->d_coords64, c->cen, sinv, c->zc, p, sc);
+  const uint8_t* fx = ctx->d_fixed;
+  if (mode == kTlFirst)
+    k_tl_direction<DIM, kTlFirst><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
+                                                       ctx->d_coords64, c->cen, sinv, c->zc, p,
+                                                       1.0, sc);
+  else if (mode == kTlKeep)
+    k_tl_direction<DIM, kTlKeep><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
+                                                      ctx->d_coords64, c->cen, sinv, c->zc, p,
+                                                      pscale, sc);
   else
-    k_tl_direction<DIM, false><<<grid, kCT, 0, s>>>(n, r, dinv, ctx->d_fixed, c->node_agg,
-                                                    ctx->d_coords64, c->cen, sinv, c->zc, p, sc);
+    k_tl_direction<DIM, kTlStep><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
+                                                      ctx->d_coords64, c->cen, sinv, c->zc, p,
+                                                      1.0, sc);
   ctx->launches += 4;
 }
 
 void gf_tl_begin(gf_ctx* ctx, const double* b, double* x, double* r, double* p,
                  const double* dinv, SolveScalars* sc) {
-  if (static_cast<Coarse*>(ctx->coarse)->dim == 2) tl_launch<2>(ctx, true, b, x, r, p, dinv, sc);
-  else tl_launch<3>(ctx, true, b, x, r, p, dinv, sc);
+  gf_tl_reset(ctx, b, 1.0, true, 1.0, x, r, p, dinv, sc);
+}
+
+void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
+                 double* x, double* r, double* p, const double* dinv, SolveScalars* sc) {
+  const int mode = restart ? kTlFirst : kTlKeep;
+  if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
+    tl_launch<2>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc);
+  else
+    tl_launch<3>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc);
 }
 
 void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q,
                    const double* dinv, SolveScalars* sc) {
-  if (static_cast<Coarse*>(ctx->coarse)->dim == 2) tl_launch<2>(ctx, false, q, x, r, p, dinv, sc);
-  else tl_launch<3>(ctx, false, q, x, r, p, dinv, sc);
+  if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
+    tl_launch<2>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc);
+  else
+    tl_launch<3>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc);
 }
 
 extern "C" GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse,

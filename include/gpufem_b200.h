@@ -97,8 +97,10 @@ typedef enum gf_solver {
                                 down or stalls. Needs K64 and gf_lp_init.                 */
   GF_SOLVER_MIXED_PCG32 = 4, /* as MIXED_PCG with FP32 vectors as well (half the vector
                                 traffic; for moderately conditioned systems)              */
-  GF_SOLVER_TWOLEVEL_PCG = 5 /* FP64 PCG on K64 with the two-level preconditioner
-                                (gf_twolevel_setup); needs a mesh-built pattern          */
+  GF_SOLVER_TWOLEVEL_PCG = 5 /* PCG with the two-level preconditioner (gf_twolevel_setup);
+                                needs a mesh-built pattern.  matrix = GF_F64: FP64 PCG on
+                                K64; GF_F32: SpMVs on K32 with FP64 vectors and reliable
+                                updates on K64 as in MIXED_PCG (needs K64 and K32)       */
 } gf_solver;
 
 typedef struct gf_solve_opts {
