@@ -18,11 +18,10 @@
 // padded to its longest neighbour list, with
 //   bcol[off[k] + 32 p + l]                          neighbour p of node 32 k + l
 //   val[dim^2 off[k] + ((p dim + c) dim + c2) 32 + l] K(row (32k+l) dim + c, col bcol dim + c2)
-// A warp handles one component c of the 32 nodes of a slice: per neighbour it reads one
-// coalesced column word (shared by the dim warps of the slice) and dim coalesced value
-// words, and gathers dim consecutive entries of x.  Index bytes per entry fall from 4
-// to 4 / dim^2 (12 -> 9 B per FP64 entry in 2-D, 8.4 B in 3-D).  Padding: column = the
-// node itself, value 0.
+// A thread computes the dim rows of one node: per neighbour it reads one coalesced
+// column word, dim^2 coalesced value words and dim consecutive entries of x.  Index
+// bytes per entry fall from 4 to 4 / dim^2 (12 -> 9 B per FP64 entry in 2-D, 8.4 B in
+// 3-D).  Padding: column = the node itself, value 0.
 #include <cub/cub.cuh>
 #include <algorithm>
 
