@@ -694,14 +694,14 @@ k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ d
   }
 }
 
-void coarse_release(Coarse* c) {
-  gf_free(c->node_agg);
-  gf_free(c->agg_off);
-  gf_free(c->agg_nodes);
-  gf_free(c->cen);
-  gf_free(c->ainv);
-  gf_free(c->rc);
-  gf_free(c->zc);
+void coarse_release(gf_ctx* ctx, Coarse* c) {
+  gf_pfree(ctx, c->node_agg);
+  gf_pfree(ctx, c->agg_off);
+  gf_pfree(ctx, c->agg_nodes);
+  gf_pfree(ctx, c->cen);
+  gf_pfree(ctx, c->ainv);
+  gf_pfree(ctx, c->rc);
+  gf_pfree(ctx, c->zc);
 }
 
 gf_status build(gf_ctx* ctx, Coarse* C, int target) {
@@ -712,12 +712,12 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   // bounding box
   const int bb = std::min(gf_blocks(nnodes, kCT), 256);
   double* d_bb = nullptr;
-  if ((st = gf_alloc(ctx, &d_bb, (size_t)bb * 6)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &d_bb, (size_t)bb * 6)) != GF_OK) return st;
   k_bbox<<<bb, kCT, 0, s>>>(nnodes, dim, ctx->d_coords64, d_bb);
   std::vector<double> hb((size_t)bb * 6);
   GF_CUDA(ctx, cudaMemcpyAsync(hb.data(), d_bb, sizeof(double) * bb * 6, cudaMemcpyDeviceToHost, s));
   GF_CUDA(ctx, cudaStreamSynchronize(s));
-  gf_free(d_bb);
+  gf_pfree(ctx, d_bb);
   BoxGrid g{};
   double vol = 1.0;
   int dpos = 0;  // axes of positive extent
@@ -749,27 +749,32 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   for (int c = dim; c < 3; ++c) { g.nb[c] = 1; g.lo[c] = 0; g.ext[c] = 0; }
   // aggregates = occupied boxes, numbered in box order
   int32_t *d_key = nullptr, *d_used = nullptr, *d_id = nullptr, *d_cnt = nullptr;
-  void* d_tmp = nullptr;
+  char* d_tmp = nullptr;  // cub scratch, grown on demand
+  size_t tb = 0;
   auto cleanup = [&]() {
-    gf_free(d_key); gf_free(d_used); gf_free(d_id); gf_free(d_cnt);
-    if (d_tmp) cudaFree(d_tmp);
+    gf_pfree(ctx, d_key); gf_pfree(ctx, d_used); gf_pfree(ctx, d_id); gf_pfree(ctx, d_cnt);
+    gf_pfree(ctx, d_tmp);
   };
-  if ((st = gf_alloc(ctx, &d_key, (size_t)nnodes)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_used, (size_t)nbox + 1)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_id, (size_t)nbox + 1)) != GF_OK) {
+  auto ensure_tmp = [&](size_t need) -> gf_status {
+    if (need <= tb) return GF_OK;
+    tb = need;
+    return gf_palloc(ctx, &d_tmp, need);
+  };
+  if ((st = gf_palloc(ctx, &d_key, (size_t)nnodes)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_used, (size_t)nbox + 1)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_id, (size_t)nbox + 1)) != GF_OK) {
     cleanup();
     return st;
   }
   cudaMemsetAsync(d_used, 0, sizeof(int32_t) * (nbox + 1), s);
   k_box_flags<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, dim, ctx->d_coords64, g, d_key, d_used);
-  size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, d_used, d_id, (int)nbox + 1, s);
-  if (cudaMalloc(&d_tmp, tb) != cudaSuccess) {
-    cudaGetLastError();
+  size_t tb1 = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb1, d_used, d_id, (int)nbox + 1, s);
+  if ((st = ensure_tmp(tb1)) != GF_OK) {
     cleanup();
-    return gf_fail(ctx, GF_ERR_OOM, "coarse scan scratch");
+    return st;
   }
-  cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_used, d_id, (int)nbox + 1, s);
+  cub::DeviceScan::ExclusiveSum(d_tmp, tb1, d_used, d_id, (int)nbox + 1, s);
   int32_t na = 0;
   GF_CUDA(ctx, cudaMemcpyAsync(&na, d_id + nbox, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_CUDA(ctx, cudaStreamSynchronize(s));
@@ -783,23 +788,23 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
          *d_dmax = nullptr;
   auto cleanup2 = [&]() {
     cleanup();
-    gf_free(d_Ac); gf_free(d_pi); gf_free(d_rw); gf_free(d_cold); gf_free(d_cn);
-    gf_free(d_dmax);
+    gf_pfree(ctx, d_Ac); gf_pfree(ctx, d_pi); gf_pfree(ctx, d_rw); gf_pfree(ctx, d_cold); gf_pfree(ctx, d_cn);
+    gf_pfree(ctx, d_dmax);
   };
-  if ((st = gf_alloc(ctx, &C->node_agg, (size_t)nnodes)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_cnt, (size_t)na + 1)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->agg_off, (size_t)na + 1)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->agg_nodes, (size_t)nnodes)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->cen, (size_t)na * dim)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->ainv, (size_t)nc * ld)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->rc, (size_t)ld)) != GF_OK ||
-      (st = gf_alloc(ctx, &C->zc, (size_t)ld)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_Ac, (size_t)nc * nc)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_pi, (size_t)kGJ * kGJ)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_rw, (size_t)kGJ * nc)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_cold, (size_t)kGJ * nc)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_cn, (size_t)kGJ * nc)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_dmax, 1)) != GF_OK) {
+  if ((st = gf_palloc(ctx, &C->node_agg, (size_t)nnodes)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_cnt, (size_t)na + 1)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->agg_off, (size_t)na + 1)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->agg_nodes, (size_t)nnodes)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->cen, (size_t)na * dim)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->ainv, (size_t)nc * ld)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->rc, (size_t)ld)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->zc, (size_t)ld)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_Ac, (size_t)nc * nc)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_pi, (size_t)kGJ * kGJ)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_rw, (size_t)kGJ * nc)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_cold, (size_t)kGJ * nc)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_cn, (size_t)kGJ * nc)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_dmax, 1)) != GF_OK) {
     cleanup2();
     return st;
   }
@@ -808,21 +813,15 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   k_node_agg<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, d_key, d_id, C->node_agg, d_cnt);
   size_t tb2 = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb2, d_cnt, C->agg_off, na + 1, s);
-  if (tb2 > tb) {
-    cudaFree(d_tmp);
-    d_tmp = nullptr;
-    if (cudaMalloc(&d_tmp, tb2) != cudaSuccess) {
-      cudaGetLastError();
-      cleanup2();
-      return gf_fail(ctx, GF_ERR_OOM, "coarse scan scratch");
-    }
-    tb = tb2;
+  if ((st = ensure_tmp(tb2)) != GF_OK) {
+    cleanup2();
+    return st;
   }
-  cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_cnt, C->agg_off, na + 1, s);
+  cub::DeviceScan::ExclusiveSum(d_tmp, tb2, d_cnt, C->agg_off, na + 1, s);
   // node lists: a stable sort of the nodes by aggregate keeps each list ascending, so
   // the per-aggregate kernels read runs of neighbouring nodes
   int32_t* d_iota = nullptr;
-  if ((st = gf_alloc(ctx, &d_iota, (size_t)nnodes)) != GF_OK) {
+  if ((st = gf_palloc(ctx, &d_iota, (size_t)nnodes)) != GF_OK) {
     cleanup2();
     return st;
   }
@@ -833,20 +832,14 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   size_t tb3 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tb3, C->node_agg, d_key, d_iota, C->agg_nodes, nnodes,
                                   0, end_bit, s);
-  if (tb3 > tb) {
-    cudaFree(d_tmp);
-    d_tmp = nullptr;
-    if (cudaMalloc(&d_tmp, tb3) != cudaSuccess) {
-      cudaGetLastError();
-      gf_free(d_iota);
-      cleanup2();
-      return gf_fail(ctx, GF_ERR_OOM, "coarse sort scratch");
-    }
-    tb = tb3;
+  if ((st = ensure_tmp(tb3)) != GF_OK) {
+    gf_pfree(ctx, d_iota);
+    cleanup2();
+    return st;
   }
-  cub::DeviceRadixSort::SortPairs(d_tmp, tb, C->node_agg, d_key, d_iota, C->agg_nodes, nnodes, 0,
+  cub::DeviceRadixSort::SortPairs(d_tmp, tb3, C->node_agg, d_key, d_iota, C->agg_nodes, nnodes, 0,
                                   end_bit, s);
-  gf_free(d_iota);
+  gf_pfree(ctx, d_iota);
   k_centroid<<<gf_blocks(na, kCT), kCT, 0, s>>>(na, dim, C->agg_off, C->cen);
   // coarse matrix
   cudaMemsetAsync(d_Ac, 0, sizeof(double) * nc * nc, s);
@@ -894,7 +887,7 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
 void gf_coarse_free(gf_ctx* ctx) {
   if (!ctx->coarse) return;
   Coarse* c = static_cast<Coarse*>(ctx->coarse);
-  coarse_release(c);
+  coarse_release(ctx, c);
   delete c;
   ctx->coarse = nullptr;
 }
@@ -1015,9 +1008,9 @@ extern "C" GF_API gf_status gf_twolevel_apply(gf_ctx* ctx, const double* r, doub
   if (st != GF_OK) return st;
   const int n = ctx->n;
   double *d_r = nullptr, *d_z = nullptr, *d_dinv = nullptr, *d_acc = nullptr;
-  auto cleanup = [&]() { gf_free(d_r); gf_free(d_z); gf_free(d_dinv); gf_free(d_acc); };
-  if ((st = gf_alloc(ctx, &d_r, (size_t)n)) != GF_OK || (st = gf_alloc(ctx, &d_z, (size_t)n)) != GF_OK ||
-      (st = gf_alloc(ctx, &d_dinv, (size_t)n)) != GF_OK || (st = gf_alloc(ctx, &d_acc, 1)) != GF_OK) {
+  auto cleanup = [&]() { gf_pfree(ctx, d_r); gf_pfree(ctx, d_z); gf_pfree(ctx, d_dinv); gf_pfree(ctx, d_acc); };
+  if ((st = gf_palloc(ctx, &d_r, (size_t)n)) != GF_OK || (st = gf_palloc(ctx, &d_z, (size_t)n)) != GF_OK ||
+      (st = gf_palloc(ctx, &d_dinv, (size_t)n)) != GF_OK || (st = gf_palloc(ctx, &d_acc, 1)) != GF_OK) {
     cleanup();
     return st;
   }
