@@ -31,6 +31,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "elems/s assembled"
+SOLVERS = ["reference", "pcg_fp64", "mixed_pcg", "mixed_pcg32", "twolevel_pcg", "twolevel_pcg_k32",
+           "learned"]
 UNIT = "elements/s"
 WORKLOADS = {
     # name: (description, dtype of the timed assembly)
@@ -453,65 +455,69 @@ def run_gpu_arm(args):
     h2d = m.coords.nbytes + m.conn.nbytes + (m.E.nbytes if m.E is not None else 0)
     d2h = n * 4 + n * W * 4 + n * W * esize
 
-    # solve: FP64 Jacobi-PCG vs FP32/FP64 mixed refinement on the same problem
+    # solve: every solver on the same problem, to a true relative residual of 1e-8
     solve = None
-    if not args.no_solve:
+    solvers = [x for x in args.solvers.split(",") if x]
+    unknown = set(solvers) - set(SOLVERS)
+    if unknown:
+        raise SystemExit(f"unknown solver(s) {sorted(unknown)}; choose from {SOLVERS}")
+    if not args.no_solve and any(x != "learned" for x in solvers):
         ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
         ctx.set_supports(m.supports)
         ctx.set_force(m.f)
         ctx.assemble(_lib.GF_F64, scatter)
-        ctx.convert_f64_to_f32()     # symmetric FP32 copy for the mixed solver
+        ctx.convert_f64_to_f32()     # symmetric FP32 copy for the mixed solvers
         ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
-        # FP64 PCG stops on its recursive residual; on this system (log-normal E) the
-        # true residual it can reach is ~5e-10, so the comparison runs at 1e-8
-        ref = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-12, max_iter=400000,
-                        raise_on_error=False)
-        ustar = ctx.solution()
-        p64 = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-8, max_iter=400000,
-                        raise_on_error=False)
-        u64 = ctx.solution()
-        nrm = np.linalg.norm(ustar)
-        solve = {"reference_solution": {"solver": "FP64 Jacobi-PCG to 1e-12",
-                                        "rel_residual": ref.rel_residual,
-                                        "iterations": ref.iterations, "seconds": ref.seconds},
-                 "pcg_fp64": {"seconds": p64.seconds, "iterations": p64.iterations,
-                              "rel_residual": p64.rel_residual,
-                              "rel_err_vs_reference": float(np.linalg.norm(u64 - ustar) / nrm)},
-                 "tol": 1e-8}
+        solve = {"tol": 1e-8}
+        ustar = nrm = None
+        if "reference" in solvers:
+            # FP64 PCG stops on its recursive residual; on this system (log-normal E) the
+            # true residual it can reach is ~5e-10, so the comparison runs at 1e-8
+            ref = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-12, max_iter=400000,
+                            raise_on_error=False)
+            ustar = ctx.solution()
+            nrm = np.linalg.norm(ustar)
+            solve["reference_solution"] = {"solver": "FP64 Jacobi-PCG to 1e-12",
+                                           "rel_residual": ref.rel_residual,
+                                           "iterations": ref.iterations, "seconds": ref.seconds}
+
+        def record(name, info, **extra):
+            d = {"seconds": info.seconds, "iterations": info.iterations, "status": info.status,
+                 "rel_residual": info.rel_residual, **extra}
+            if ustar is not None:
+                d["rel_err_vs_reference"] = float(np.linalg.norm(ctx.solution() - ustar) / nrm)
+            solve[name] = d
+
+        p64 = None
+        if "pcg_fp64" in solvers:
+            p64 = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-8, max_iter=400000,
+                            raise_on_error=False)
+            record("pcg_fp64", p64)
         for name, solver in (("mixed_pcg", _lib.GF_SOLVER_MIXED_PCG),
                              ("mixed_pcg32", _lib.GF_SOLVER_MIXED_PCG32)):
-            mix = ctx.solve(solver, tol=1e-8, max_iter=400000, inner_tol=1e-4,
-                            raise_on_error=False)
-            umix = ctx.solution()
-            solve[name] = {"seconds": mix.seconds, "iterations": mix.iterations,
-                           "outer": mix.outer, "fp64_fallback": mix.fallback,
-                           "status": mix.status, "rel_residual": mix.rel_residual,
-                           "rel_err_vs_reference": float(np.linalg.norm(umix - ustar) / nrm)}
-        # two-level PCG: coarse-space build (aggregation, P^T K P, inverse; host wall
-        # time, synchronised) timed apart from the solve that uses it
-        t0 = time.perf_counter()
-        nc = ctx.twolevel_setup(0)
-        tl_setup = time.perf_counter() - t0
-        tl = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, tol=1e-8, max_iter=400000,
-                       raise_on_error=False)
-        utl = ctx.solution()
-        solve["twolevel_pcg"] = {
-            "setup_seconds": tl_setup, "seconds": tl.seconds,
-            "seconds_with_setup": tl_setup + tl.seconds,
-            "iterations": tl.iterations, "status": tl.status, "rel_residual": tl.rel_residual,
-            "rel_err_vs_reference": float(np.linalg.norm(utl - ustar) / nrm),
-            "coarse_unknowns": nc,
-            "label": "FP64 PCG, M = Jacobi + rigid-body modes of box aggregates"}
-        tl32 = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, _lib.GF_F32, tol=1e-8, max_iter=400000,
-                         raise_on_error=False)
-        utl32 = ctx.solution()
-        solve["twolevel_pcg_k32"] = {
-            "seconds": tl32.seconds, "iterations": tl32.iterations, "outer": tl32.outer,
-            "fp64_fallback": tl32.fallback, "status": tl32.status,
-            "rel_residual": tl32.rel_residual,
-            "rel_err_vs_reference": float(np.linalg.norm(utl32 - ustar) / nrm),
-            "label": "two-level PCG with K32 SpMVs, FP64 vectors, reliable updates on K64"}
-        if rank == 0 and world == 1 and not args.no_cpu and cfg in ("q4_64", "q8_512"):
+            if name in solvers:
+                mix = ctx.solve(solver, tol=1e-8, max_iter=400000, inner_tol=1e-4,
+                                raise_on_error=False)
+                record(name, mix, outer=mix.outer, fp64_fallback=mix.fallback)
+        if "twolevel_pcg" in solvers or "twolevel_pcg_k32" in solvers:
+            # two-level PCG: coarse-space build (aggregation, P^T K P, inverse; host wall
+            # time, synchronised) timed apart from the solves that use it
+            t0 = time.perf_counter()
+            nc = ctx.twolevel_setup(0)
+            tl_setup = time.perf_counter() - t0
+        if "twolevel_pcg" in solvers:
+            tl = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, tol=1e-8, max_iter=400000,
+                           raise_on_error=False)
+            record("twolevel_pcg", tl, setup_seconds=tl_setup,
+                   seconds_with_setup=tl_setup + tl.seconds, coarse_unknowns=nc,
+                   label="FP64 PCG, M = Jacobi + rigid-body modes of box aggregates")
+        if "twolevel_pcg_k32" in solvers:
+            tl32 = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, _lib.GF_F32, tol=1e-8, max_iter=400000,
+                             raise_on_error=False)
+            record("twolevel_pcg_k32", tl32, outer=tl32.outer, fp64_fallback=tl32.fallback,
+                   label="two-level PCG with K32 SpMVs, FP64 vectors, reliable updates on K64")
+        if (rank == 0 and world == 1 and not args.no_cpu and p64 is not None
+                and cfg in ("q4_64", "q8_512")):
             # (the reference's assembly of the full 3-D meshes alone takes minutes)
             rc = reference_cg_sample(m)
             if rc is not None:
@@ -522,7 +528,7 @@ def run_gpu_arm(args):
                 solve["cpu_reference"] = rc
 
     learned = None
-    if not args.no_solve and rank == 0:
+    if not args.no_solve and rank == 0 and "learned" in solvers:
         learned = learned_comparison()
 
     cpu_baseline = None
@@ -579,6 +585,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="q8_512", choices=sorted(WORKLOADS))
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--solvers", default=",".join(SOLVERS),
+                    help="comma list of the solve block's entries (default: all)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scatter", default="owner", choices=["owner", "colour", "atomic", "auto"])
     args = ap.parse_args()

@@ -65,6 +65,7 @@ SIGNATURES = {
                           C.POINTER(P)]),
     "gf_ell_download": (I32, [P, I32, P, P, P]),
     "gf_ell_upload": (I32, [P, I32, I32, P, P, P]),
+    "gf_ell_diagonal": (I32, [P, I32, P]),
     "gf_set_supports": (I32, [P, I32, P]),
     "gf_set_nodal_loads": (I32, [P, I32, P]),
     "gf_set_force": (I32, [P, P]),

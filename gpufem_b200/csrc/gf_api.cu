@@ -262,6 +262,20 @@ static gf_status check_failure(gf_ctx* ctx, const unsigned long long* chk, int n
   return GF_OK;
 }
 
+namespace {
+template <typename T>
+__global__ void k_ell_diag(int n, const int32_t* __restrict__ rownnz,
+                           const int32_t* __restrict__ col, const T* __restrict__ val,
+                           double* __restrict__ diag) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  double d = 0.0;
+  for (int s = 0; s < rownnz[row]; ++s)
+    if (col[(int64_t)s * n + row] == row) d = (double)val[(int64_t)s * n + row];
+  diag[row] = d;
+}
+}  // namespace
+
 extern "C" {
 
 GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
@@ -553,6 +567,32 @@ GF_API gf_status gf_ell_download(gf_ctx* ctx, int32_t dtype, int32_t* rownnz, in
     }
   }
   GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GF_OK;
+}
+
+
+GF_API gf_status gf_ell_diagonal(gf_ctx* ctx, int32_t dtype, double* diag) {
+  if (!ctx || !diag) return GF_ERR_INVALID_ARG;
+  if (!ctx->has_pattern) return gf_fail(ctx, GF_ERR_STATE, "no matrix");
+  if ((dtype == GF_F64 && !ctx->has64) || (dtype == GF_F32 && !ctx->has32) ||
+      (dtype != GF_F64 && dtype != GF_F32))
+    return gf_fail(ctx, GF_ERR_STATE, "matrix of dtype %d not assembled", dtype);
+  cudaSetDevice(ctx->device);
+  const int n = ctx->n;
+  double* d = nullptr;
+  gf_status st = gf_palloc(ctx, &d, (size_t)n);
+  if (st != GF_OK) return st;
+  if (dtype == GF_F64)
+    k_ell_diag<double><<<gf_blocks(n, 256), 256, 0, ctx->stream>>>(n, ctx->d_rownnz, ctx->d_colidx,
+                                                                   ctx->d_K64, d);
+  else
+    k_ell_diag<float><<<gf_blocks(n, 256), 256, 0, ctx->stream>>>(n, ctx->d_rownnz, ctx->d_colidx,
+                                                                  ctx->d_K32, d);
+  ctx->launches++;
+  cudaError_t e = cudaMemcpyAsync(diag, d, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  gf_pfree(ctx, d);
+  if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "ELL diagonal");
   return GF_OK;
 }
 

@@ -124,6 +124,11 @@ class Context:
         self._c(lib.gf_ell_download(self.h, dtype, _ptr(rownnz), _ptr(colidx), _ptr(vals)))
         return rownnz, colidx.reshape(w, n), vals.reshape(w, n)
 
+    def ell_diagonal(self, dtype: int = _lib.GF_F64) -> np.ndarray:
+        d = np.empty(self.n, np.float64)
+        self._c(lib.gf_ell_diagonal(self.h, dtype, _ptr(d)))
+        return d
+
     def ell_upload(self, rownnz: np.ndarray, colidx: np.ndarray, vals: np.ndarray) -> None:
         """colidx / vals: (width, n) column-major ELL as the reference stores it."""
         rownnz = np.ascontiguousarray(rownnz, np.int32)

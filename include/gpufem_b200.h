@@ -192,6 +192,10 @@ GF_API gf_status gf_ell_view(gf_ctx* ctx, int32_t dtype, int32_t* n, int32_t* wi
 /* Copy to host: rownnz[n], colidx[n*width], values[n*width] (dtype-sized). */
 GF_API gf_status gf_ell_download(gf_ctx* ctx, int32_t dtype, int32_t* rownnz,
                                  int32_t* colidx, void* values);
+/* Diagonal K(i, i) of the matrix of `dtype` into a host buffer of n doubles (0 where a row
+ * has no diagonal entry); the device-side form of the reference's GetElem(i, i) scan
+ * (SPRmatrix::GetElem, src/SPRmatrix/ELLmatrix.cc:142-159). */
+GF_API gf_status gf_ell_diagonal(gf_ctx* ctx, int32_t dtype, double* diag);
 /* Replace the matrix with a host-built ELL (n, width, rownnz, colidx, FP64 values);
  * fills both the FP64 and FP32 matrices.  Slots past rownnz are ignored. */
 GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width,
