@@ -15,9 +15,9 @@
 // blocked Gauss-Jordan sweep (SPD: no pivoting); the inverse is symmetrised and kept in
 // FP64 for the per-iteration product.
 //
-// One application: restriction (block per aggregate over its node list), dense coarse
-// product (warp per coarse row), prolongation fused with the Jacobi term and the r.z
-// dot.  Everything is launched on the context stream without synchronisation.
+// One application: restriction (block per aggregate over its node list), the coarse
+// product from the packed upper triangle of the symmetric inverse (64 x 64 tiles, read
+// once at half the size), prolongation fused with the Jacobi term and the r.z dot.  Everything is launched on the context stream without synchronisation.
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <cmath>
@@ -41,10 +41,13 @@ struct Coarse {
   int32_t* agg_off = nullptr;    // [na + 1]
   int32_t* agg_nodes = nullptr;  // [nnodes], nodes grouped by aggregate
   double* cen = nullptr;         // [na * dim]
-  int ld = 0;                     // row stride of ainv: nc rounded up to 8
-  double* ainv = nullptr;        // [nc][ld], symmetrised, zero beyond column nc
+  int nt = 0;                     // 64 x 64 tiles per side; rc, zc hold 64 nt entries
+  int ntiles = 0;                 // nt (nt + 1) / 2 tiles (I <= J) of the symmetric inverse
+  int2* tile_ij = nullptr;        // [ntiles] (I, J)
+  double* ainv = nullptr;         // [ntiles][64][64], zero beyond nc
+  unsigned* counter = nullptr;    // blocks done in the current coarse product
   double* rc = nullptr;          // [nc]
-  double* zc = nullptr;          // [nc]
+  double* zc = nullptr;          // [64 nt]
 };
 
 // P row of dof (node, comp c): modes m (translations first, then rotations) with the
@@ -436,22 +439,28 @@ k_gj_update(int nc, int kb, int bs, double* __restrict__ A, const double* __rest
   }
 }
 
-__global__ void k_symmetrise(int nc, int ld, const double* __restrict__ A,
-                             double* __restrict__ out) {
-  const int64_t t = blockIdx.x * (int64_t)kCT + threadIdx.x;
-  if (t >= (int64_t)nc * ld) return;
-  const int i = (int)(t / ld), j = (int)(t % ld);
-  out[t] = j < nc ? 0.5 * (A[(int64_t)i * nc + j] + A[(int64_t)j * nc + i]) : 0.0;
+// Upper-triangle tiles (I <= J) of the symmetrised inverse, zero beyond nc.
+constexpr int kTS = 64;
+__global__ void k_pack_tiles(int nc, const int2* __restrict__ ij, const double* __restrict__ A,
+                             double* __restrict__ T) {
+  const int2 t = ij[blockIdx.x];
+  double* dst = T + (int64_t)blockIdx.x * kTS * kTS;
+  for (int e = threadIdx.x; e < kTS * kTS; e += blockDim.x) {
+    const int gi = t.x * kTS + e / kTS, gj = t.y * kTS + e % kTS;
+    dst[e] = (gi < nc && gj < nc)
+                 ? 0.5 * (A[(int64_t)gi * nc + gj] + A[(int64_t)gj * nc + gi])
+                 : 0.0;
+  }
 }
 
-// rc = P^T r: block per aggregate over its node list
+// rc = P^T r (and zc = 0 for the coarse product): block per aggregate over its node list
 constexpr int kRT = 256;
 template <int DIM>
 __global__ void __launch_bounds__(kRT)
 k_restrict(const int32_t* __restrict__ off, const int32_t* __restrict__ nodes,
            const double* __restrict__ x, const double* __restrict__ cen, double sinv,
            const uint8_t* __restrict__ fixed, const double* __restrict__ r,
-           double* __restrict__ rc, const int* __restrict__ done) {
+           double* __restrict__ rc, double* __restrict__ zc, const int* __restrict__ done) {
   constexpr int NM = DIM == 2 ? 3 : 6;
   __shared__ double ws[kRT / 32][NM];
   if (done && *done) return;
@@ -489,47 +498,87 @@ k_restrict(const int32_t* __restrict__ off, const int32_t* __restrict__ nodes,
     double v = 0.0;
     for (int k = 0; k < kRT / 32; ++k) v += ws[k][threadIdx.x];
     rc[A * NM + threadIdx.x] = v;
+    zc[A * NM + threadIdx.x] = 0.0;  // the coarse product accumulates into zc
   }
 }
 
-// Row i of Ainv . rc for warp-per-row products: rows start on 64-byte boundaries (ld is a
-// multiple of 8) and every entry beyond nc, of the row and of rc, is zero, so the warp
-// reads 16-byte pairs, four pairs in flight per lane.
-__device__ inline double coarse_row_dot(const double* __restrict__ row,
-                                        const double* __restrict__ rc, int ld, int lane) {
-  const double2* r2 = reinterpret_cast<const double2*>(row);
-  const double2* c2 = reinterpret_cast<const double2*>(rc);
-  const int h = ld >> 1;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  int j = lane;
-  for (; j + 96 < h; j += 128) {
-    const double2 v0 = __ldg(r2 + j), v1 = __ldg(r2 + j + 32), v2 = __ldg(r2 + j + 64),
-                  v3 = __ldg(r2 + j + 96);
-    const double2 x0 = c2[j], x1 = c2[j + 32], x2 = c2[j + 64], x3 = c2[j + 96];
-    a0 += v0.x * x0.x + v0.y * x0.y;
-    a1 += v1.x * x1.x + v1.y * x1.y;
-    a2 += v2.x * x2.x + v2.y * x2.y;
-    a3 += v3.x * x3.x + v3.y * x3.y;
-  }
-  for (; j < h; j += 32) {
-    const double2 v0 = __ldg(r2 + j), x0 = c2[j];
-    a0 += v0.x * x0.x + v0.y * x0.y;
-  }
-  double acc = (a0 + a1) + (a2 + a3);
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  return acc;
-}
-
-// zc = Ainv rc: warp per row
-__global__ void k_coarse_gemv(int nc, int ld, const double* __restrict__ Ainv,
-                              const double* __restrict__ rc, double* __restrict__ zc,
-                              const int* __restrict__ done) {
+// zc += Ainv rc from the packed upper-triangle tiles: block per tile (I, J) adds A_IJ rc_J
+// to zc_I and, off the diagonal, A_IJ^T rc_I to zc_J (double atomics; zc is zeroed by the
+// restriction), so the symmetric inverse is read once at half its size.  Warp w reads
+// rows 8w .. 8w+7 of the tile as 16-byte pairs, one contiguous 512-byte row per load
+// (lane l: columns 2l, 2l+1).  Row sums: a butterfly that halves the 8 partial sums per
+// step (9 shuffles); column sums: per thread over its 8 rows, then over the warps in
+// shared memory.  With sc: the last block to finish (counter, after a fence) adds
+// rc.zc to sc->rzn and resets the counter.
+__global__ void __launch_bounds__(256)
+k_coarse_symv(int nc, const int2* __restrict__ ij, const double* __restrict__ T,
+              const double* __restrict__ rc, double* __restrict__ zc, unsigned* counter,
+              SolveScalars* sc, const int* __restrict__ done) {
+  __shared__ double xI[kTS], xJ[kTS], colp[8][kTS], red[8];
+  __shared__ bool last;
   if (done && *done) return;
-  const int i = blockIdx.x * (kCT / 32) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (i >= nc) return;
-  const double acc = coarse_row_dot(Ainv + (int64_t)i * ld, rc, ld, lane);
-  if (lane == 0) zc[i] = acc;
+  const int2 t = ij[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid < kTS) xI[tid] = rc[t.x * kTS + tid];
+  else if (tid < 2 * kTS) xJ[tid - kTS] = rc[t.y * kTS + tid - kTS];
+  __syncthreads();
+  const double2* base =
+      reinterpret_cast<const double2*>(T + (int64_t)blockIdx.x * kTS * kTS + w * 8 * kTS);
+  double2 a[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) a[c] = __ldcs(base + c * 32 + lane);
+  const double x0 = xJ[2 * lane], x1 = xJ[2 * lane + 1];
+  double rs[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) rs[c] = a[c].x * x0 + a[c].y * x1;
+  const bool u16 = lane & 16, u8 = lane & 8, u4 = lane & 4;
+  double v4[4], v2[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    v4[k] = (u16 ? rs[4 + k] : rs[k]) + __shfl_xor_sync(0xffffffffu, u16 ? rs[k] : rs[4 + k], 16);
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+    v2[k] = (u8 ? v4[2 + k] : v4[k]) + __shfl_xor_sync(0xffffffffu, u8 ? v4[k] : v4[2 + k], 8);
+  double v = (u4 ? v2[1] : v2[0]) + __shfl_xor_sync(0xffffffffu, u4 ? v2[0] : v2[1], 4);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  if ((lane & 3) == 0) atomicAdd(&zc[t.x * kTS + w * 8 + (lane >> 2)], v);
+  if (t.x != t.y) {
+    double cx = 0.0, cy = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double xi = xI[w * 8 + c];
+      cx += a[c].x * xi;
+      cy += a[c].y * xi;
+    }
+    colp[w][2 * lane] = cx;
+    colp[w][2 * lane + 1] = cy;
+    __syncthreads();
+    if (tid < kTS) {
+      double u = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) u += colp[q][tid];
+      atomicAdd(&zc[t.y * kTS + tid], u);
+    }
+  }
+  if (!sc) return;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double part = 0.0;
+  for (int j = tid; j < nc; j += blockDim.x) part += rc[j] * __ldcg(zc + j);
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+  if (lane == 0) red[w] = part;
+  __syncthreads();
+  if (tid == 0) {
+    double u = 0.0;
+    for (int q = 0; q < 8; ++q) u += red[q];
+    atomicAdd(&sc->rzn, u);
+    *counter = 0u;
+  }
 }
 
 __device__ inline double cg_block_sum(double v, double* sh) {
@@ -624,31 +673,6 @@ k_tl_update(int n, const double* __restrict__ bq, double scale, double* __restri
   if (threadIdx.x == 0) atomicAdd(&sc->rzn, s2);
 }
 
-// zc = Ainv rc (warp per row) and rzn += rc.zc
-__global__ void __launch_bounds__(kCT)
-k_tl_gemv(int nc, int ld, const double* __restrict__ Ainv, const double* __restrict__ rc,
-          double* __restrict__ zc, SolveScalars* sc) {
-  __shared__ double sh[kCT / 32];
-  if (sc->done) return;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * (kCT / 32) + w;
-  double part = 0.0;
-  if (i < nc) {
-    const double acc = coarse_row_dot(Ainv + (int64_t)i * ld, rc, ld, lane);
-    if (lane == 0) {
-      zc[i] = acc;
-      part = acc * rc[i];
-    }
-  }
-  if (lane == 0) sh[w] = part;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int k = 0; k < kCT / 32; ++k) t += sh[k];
-    atomicAdd(&sc->rzn, t);
-  }
-}
-
 // z = D^-1 r + P zc on the fly.  MODE kTlFirst: p = z; kTlKeep: p = pscale p (a
 // reliable update that keeps the direction); kTlStep: p = z + beta p with
 // beta = rzn / rz, then the iteration count and the convergence test.
@@ -700,6 +724,8 @@ void coarse_release(gf_ctx* ctx, Coarse* c) {
   gf_pfree(ctx, c->agg_nodes);
   gf_pfree(ctx, c->cen);
   gf_pfree(ctx, c->ainv);
+  gf_pfree(ctx, c->tile_ij);
+  gf_pfree(ctx, c->counter);
   gf_pfree(ctx, c->rc);
   gf_pfree(ctx, c->zc);
 }
@@ -779,8 +805,10 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   GF_CUDA(ctx, cudaMemcpyAsync(&na, d_id + nbox, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_CUDA(ctx, cudaStreamSynchronize(s));
   const int nc = na * nm;
-  const int ld = (nc + 7) & ~7;
-  C->ld = ld;
+  const int nt = (nc + kTS - 1) / kTS, ntiles = nt * (nt + 1) / 2;
+  const int ld = nt * kTS;  // length of rc, zc
+  C->nt = nt;
+  C->ntiles = ntiles;
   C->dim = dim; C->nm = nm; C->na = na; C->nc = nc; C->s = side;
   for (int c = 0; c < 3; ++c) { C->lo[c] = g.lo[c]; C->nb[c] = g.nb[c]; }
   double* d_Ac = nullptr;
@@ -796,7 +824,9 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
       (st = gf_palloc(ctx, &C->agg_off, (size_t)na + 1)) != GF_OK ||
       (st = gf_palloc(ctx, &C->agg_nodes, (size_t)nnodes)) != GF_OK ||
       (st = gf_palloc(ctx, &C->cen, (size_t)na * dim)) != GF_OK ||
-      (st = gf_palloc(ctx, &C->ainv, (size_t)nc * ld)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->ainv, (size_t)ntiles * kTS * kTS)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->tile_ij, (size_t)ntiles)) != GF_OK ||
+      (st = gf_palloc(ctx, &C->counter, 1)) != GF_OK ||
       (st = gf_palloc(ctx, &C->rc, (size_t)ld)) != GF_OK ||
       (st = gf_palloc(ctx, &C->zc, (size_t)ld)) != GF_OK ||
       (st = gf_palloc(ctx, &d_Ac, (size_t)nc * nc)) != GF_OK ||
@@ -872,8 +902,16 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
     k_gj_update<<<gu, 256, 0, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
     ctx->launches += 3;
   }
-  k_symmetrise<<<gf_blocks((int64_t)nc * ld, kCT), kCT, 0, s>>>(nc, ld, d_Ac, C->ainv);
-  cudaMemsetAsync(C->rc, 0, sizeof(double) * ld, s);  // the tail beyond nc stays zero
+  std::vector<int2> hij;
+  hij.reserve(ntiles);
+  for (int I = 0; I < nt; ++I)
+    for (int J = I; J < nt; ++J) hij.push_back(make_int2(I, J));
+  GF_CUDA(ctx, cudaMemcpyAsync(C->tile_ij, hij.data(), sizeof(int2) * ntiles,
+                               cudaMemcpyHostToDevice, s));
+  k_pack_tiles<<<ntiles, 256, 0, s>>>(nc, C->tile_ij, d_Ac, C->ainv);
+  cudaMemsetAsync(C->rc, 0, sizeof(double) * ld, s);  // the tails beyond nc stay zero
+  cudaMemsetAsync(C->zc, 0, sizeof(double) * ld, s);
+  cudaMemsetAsync(C->counter, 0, sizeof(unsigned), s);
   ctx->launches++;
   cudaError_t e = cudaStreamSynchronize(s);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -918,18 +956,19 @@ void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z
   Coarse* c = static_cast<Coarse*>(ctx->coarse);
   cudaStream_t s = ctx->stream;
   const double sinv = 1.0 / c->s;
-  const int gbk = (c->nc + kCT / 32 - 1) / (kCT / 32);
   const int pb = std::min(gf_blocks(ctx->n, kCT), ctx->sm_count * 8);
   if (c->dim == 2) {
     k_restrict<2><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
-                                        ctx->d_fixed, r, c->rc, done);
-    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ld, c->ainv, c->rc, c->zc, done);
+                                        ctx->d_fixed, r, c->rc, c->zc, done);
+    k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, nullptr,
+                                            nullptr, done);
     k_prolong<2><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
                                     ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
   } else {
     k_restrict<3><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
-                                        ctx->d_fixed, r, c->rc, done);
-    k_coarse_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ld, c->ainv, c->rc, c->zc, done);
+                                        ctx->d_fixed, r, c->rc, c->zc, done);
+    k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, nullptr,
+                                            nullptr, done);
     k_prolong<3><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
                                     ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
   }
@@ -944,12 +983,12 @@ static void tl_launch(gf_ctx* ctx, int mode, const double* bq, double scale, dou
   const int n = ctx->n;
   const double sinv = 1.0 / c->s;
   const int grid = std::min(gf_blocks(n, kCT), ctx->sm_count * 8);
-  const int gbk = (c->nc + kCT / 32 - 1) / (kCT / 32);
   if (mode == kTlStep) k_tl_update<false><<<grid, kCT, 0, s>>>(n, bq, 1.0, x, r, p, dinv, sc);
   else k_tl_update<true><<<grid, kCT, 0, s>>>(n, bq, scale, x, r, nullptr, dinv, sc);
   k_restrict<DIM><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
-                                        ctx->d_fixed, r, c->rc, &sc->done);
-  k_tl_gemv<<<gbk, kCT, 0, s>>>(c->nc, c->ld, c->ainv, c->rc, c->zc, sc);
+                                        ctx->d_fixed, r, c->rc, c->zc, &sc->done);
+  k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, c->counter,
+                                          sc, &sc->done);
   const uint8_t* fx = ctx->d_fixed;
   if (mode == kTlFirst)
     k_tl_direction<DIM, kTlFirst><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
