@@ -232,6 +232,7 @@ struct gf_ctx {
   int64_t* d_sell_off = nullptr;   // [nslice + 1] first entry of each slice
   int32_t* d_sell_w = nullptr;     // [nslice] width of each slice
   int32_t* d_sell_col = nullptr;   // [total]
+  int32_t* d_sell_perm = nullptr;  // node slices: node of each slot (degree-sorted windows)
   double* d_sell_v64 = nullptr;
   float* d_sell_v32 = nullptr;
 

@@ -56,6 +56,7 @@ struct MatLayout {
   const int64_t* __restrict__ off;
   int bdim = 0;      // 0: rows (ELL / SELL); 2, 3: node-block slices (gf_sell.cu)
   int nnodes = 0;
+  const int32_t* __restrict__ perm = nullptr;  // node-block slices: node of each slot
   int threads = kT;  // block size
 
   __device__ inline bool at(int t, int& nz, int64_t& o, int64_t& stride) const {
@@ -107,18 +108,19 @@ __device__ inline double row_dot(int64_t o, int64_t stride, int nz, const int32_
   return (double)((a0 + a1) + (a2 + a3));
 }
 
-// Node-block slices: thread t computes the DIM rows of node t (slice k = t / 32, lane
-// l = t % 32).  Per neighbour block it reads one coalesced column word, DIM x DIM
+// Node-block slices: thread t computes the DIM rows of node perm[t] (slice k = t / 32,
+// lane l = t % 32).  Per neighbour block it reads one coalesced column word, DIM x DIM
 // coalesced values and DIM consecutive entries of x (once for all DIM rows), and it
 // writes its DIM results contiguously.  Measured against a warp per (slice, component),
 // which gathers x DIM times: Q8 512 FP64 113 -> 96 us, FP32 78 -> 60 us, Brick8 128
 // FP32 459 -> 373 us (B200, L2 flushed).
 template <int DIM, typename TK, typename TX>
 __device__ inline bool node_rows(const MatLayout& L, int t, const TK* __restrict__ val,
-                                 const TX* __restrict__ x, double (&out)[DIM]) {
+                                 const TX* __restrict__ x, int& node, double (&out)[DIM]) {
   using Acc = typename std::conditional<sizeof(TK) == 8 || sizeof(TX) == 8, double, float>::type;
   constexpr int SS = DIM * DIM * 32;  // value stride between neighbour slots
   if (t >= L.nnodes) return false;
+  node = __ldg(L.perm + t);
   const int k = t >> 5, l = t & 31;
   const int64_t o = __ldg(L.off + k);
   const int w = __ldg(L.width + k);
@@ -149,18 +151,19 @@ __device__ inline bool node_rows(const MatLayout& L, int t, const TK* __restrict
 template <typename TK, typename TX, typename F>
 __device__ inline void mat_rows(const MatLayout& L, int t, const TK* __restrict__ val,
                                 const TX* __restrict__ x, F&& f) {
+  int a;
   if (L.bdim == 2) {
     double v[2];
-    if (node_rows<2>(L, t, val, x, v)) {
-      f(2 * t, v[0]);
-      f(2 * t + 1, v[1]);
+    if (node_rows<2>(L, t, val, x, a, v)) {
+      f(2 * a, v[0]);
+      f(2 * a + 1, v[1]);
     }
   } else if (L.bdim == 3) {
     double v[3];
-    if (node_rows<3>(L, t, val, x, v)) {
-      f(3 * t, v[0]);
-      f(3 * t + 1, v[1]);
-      f(3 * t + 2, v[2]);
+    if (node_rows<3>(L, t, val, x, a, v)) {
+      f(3 * a, v[0]);
+      f(3 * a + 1, v[1]);
+      f(3 * a + 2, v[2]);
     }
   } else {
     int nz;
@@ -401,7 +404,8 @@ gf_status solver_matrix(gf_ctx* ctx, int dtype, MatLayout* L, const void** val) 
   if (ctx->sell_bdim) {
     L->bdim = ctx->sell_bdim;
     L->nnodes = ctx->nnodes;
-    L->count = ctx->nnodes;  // a thread per node
+    L->perm = ctx->d_sell_perm;
+    L->count = ctx->nnodes;  // a thread per node slot
   }
   *val = dtype == GF_F64 ? (const void*)ctx->d_sell_v64 : (const void*)ctx->d_sell_v32;
   return GF_OK;
