@@ -190,6 +190,240 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   }
 }
 
+// ---- TF32 tensor-core engine (GF_ENGINE_TF32_MMA, FP32) ---------------------------
+// The node-pair blocks of one element are blocks of one Gram matrix: with rows
+// r = a*NEN + i (component a of node i) and k over the Gauss points,
+//   M[r][c] = sum_k w_k G[r][k] G[c][k],   H_ij[a][b] = M[a*NEN+i][b*NEN+j],
+// where G[r][k] = g_i[a] at point k and w_k = w detJ E.  A warp forms M for one element
+// with mma.sync.m16n8k8 TF32 tiles (rows and k padded with zeros to multiples of 16 and 8)
+// over the upper triangle (column tile >= row tile), in three TF32 products
+// (hi*hi + hi*lo + lo*hi, each operand split as x = hi + lo) so that M keeps close to
+// FP32 accuracy, writes it to its shared-memory buffer, and then its lanes form the
+// blocks of the pairs i <= j and scatter them as the CUDA-core kernel does.
+__device__ inline uint32_t f2tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ inline void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = f2tf32(x);
+  lo = f2tf32(x - __uint_as_float(hi));
+}
+
+__device__ inline void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+constexpr int kMmaMaxKS = (GF_MAX_GP + 7) / 8;  // k-steps of 8 Gauss points
+
+template <int ET>
+struct MmaShape {
+  static constexpr ElemInfo info = gf_elem_info(ET);
+  static constexpr int R = info.nen * info.dim;
+  static constexpr int RP = (R + 15) / 16 * 16;  // padded rows / columns of M
+  static constexpr int LDM = RP + 4;             // row stride of M in shared memory
+};
+
+template <int ET, bool ATOMIC>
+__global__ void __launch_bounds__(kThreads)
+k_assemble_mma(const int32_t* __restrict__ elems, int count, int TE, int ngp,
+               const int32_t* __restrict__ conn, const double* __restrict__ coords,
+               const float* __restrict__ Eel, const uint16_t* __restrict__ slotmap, int nelem,
+               int n, const AsmTables* __restrict__ tab, float lam1, float mu1,
+               float* __restrict__ K) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  constexpr int NEN = info.nen, DIM = info.dim;
+  constexpr int R = MmaShape<ET>::R, RP = MmaShape<ET>::RP, LDM = MmaShape<ET>::LDM;
+  constexpr int NPAIR = NEN * (NEN + 1) / 2;
+  constexpr int NW = kThreads / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* sM = reinterpret_cast<float*>(smem_raw);                // NW * RP * LDM
+  float* sdN = sM + NW * RP * LDM;                               // ngp*DIM*NEN
+  float* sw = sdN + ngp * DIM * NEN;                             // ngp
+  float* sX = sw + ngp;                                          // TE*NEN*DIM
+  float* sG = sX + TE * NEN * DIM;                               // ngp*NEN*DIM*TE
+  float* swd = sG + ngp * NEN * DIM * TE;                        // ngp*TE
+  int* sconn = reinterpret_cast<int*>(swd + ngp * TE);           // TE*NEN
+  int* sel = sconn + TE * NEN;                                   // TE
+  int* sflag = sel + TE;                                         // TE
+
+  const int tile0 = blockIdx.x * TE;
+  const int nt = min(TE, count - tile0);
+  for (int k = threadIdx.x; k < ngp * DIM * NEN; k += kThreads) sdN[k] = tab->dN32[k];
+  for (int k = threadIdx.x; k < ngp; k += kThreads) sw[k] = tab->w32[k];
+  for (int e = threadIdx.x; e < TE; e += kThreads) {
+    sel[e] = e < nt ? elems[tile0 + e] : -1;
+    sflag[e] = 0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nt * NEN; k += kThreads) {
+    const int e = k / NEN, i = k % NEN;
+    const int node = conn[(int64_t)sel[e] * NEN + i];
+    const int node0 = conn[(int64_t)sel[e] * NEN];
+    sconn[k] = node;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c)
+      sX[k * DIM + c] = float(coords[(int64_t)node * DIM + c] - coords[(int64_t)node0 * DIM + c]);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nt; e += kThreads)
+    sflag[e] = gf_distorted<NEN, DIM, float>(sdN, ngp, sX + e * NEN * DIM);
+  __syncthreads();
+  for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
+    const int e = t % TE, g = t / TE;
+    if (e >= nt) continue;
+    const float detJ = gf_gradients<NEN, DIM, float>(sdN + g * DIM * NEN, sX + e * NEN * DIM,
+                                                     sflag[e], sG + (g * NEN * DIM) * TE + e, TE);
+    swd[g * TE + e] = sw[g] * detJ * Eel[sel[e]];
+  }
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gid = lane >> 2, tig = lane & 3;
+  const int KS = (ngp + 7) >> 3;
+  float* M = sM + warp * RP * LDM;
+  // G[r][k] of element e (0 outside r < R, k < ngp)
+  auto Gv = [&](int r, int k, int e) -> float {
+    if (r >= R || k >= ngp) return 0.f;
+    const int a = r / NEN, i = r - a * NEN;
+    return sG[((k * NEN + i) * DIM + a) * TE + e];
+  };
+  for (int e = warp; e < nt; e += NW) {
+    for (int mt = 0; mt < RP / 16; ++mt) {
+      const int r0 = mt * 16 + gid, r1 = r0 + 8;
+      uint32_t ah[kMmaMaxKS][4], al[kMmaMaxKS][4];
+#pragma unroll
+      for (int ks = 0; ks < kMmaMaxKS; ++ks) {
+        if (ks >= KS) break;
+        const int k0 = ks * 8 + tig, k1 = k0 + 4;
+        const float w0 = k0 < ngp ? swd[k0 * TE + e] : 0.f;
+        const float w1 = k1 < ngp ? swd[k1 * TE + e] : 0.f;
+        split_tf32(Gv(r0, k0, e) * w0, ah[ks][0], al[ks][0]);
+        split_tf32(Gv(r1, k0, e) * w0, ah[ks][1], al[ks][1]);
+        split_tf32(Gv(r0, k1, e) * w1, ah[ks][2], al[ks][2]);
+        split_tf32(Gv(r1, k1, e) * w1, ah[ks][3], al[ks][3]);
+      }
+      for (int ntl = 2 * mt; ntl < RP / 8; ++ntl) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        const int c = ntl * 8 + gid;
+#pragma unroll
+        for (int ks = 0; ks < kMmaMaxKS; ++ks) {
+          if (ks >= KS) break;
+          uint32_t bh0, bl0, bh1, bl1;
+          split_tf32(Gv(c, ks * 8 + tig, e), bh0, bl0);
+          split_tf32(Gv(c, ks * 8 + tig + 4, e), bh1, bl1);
+          mma_tf32(acc, al[ks], bh0, bh1);
+          mma_tf32(acc, ah[ks], bl0, bl1);
+          mma_tf32(acc, ah[ks], bh0, bh1);
+        }
+        float* m0 = M + r0 * LDM + ntl * 8 + 2 * tig;
+        float* m1 = M + r1 * LDM + ntl * 8 + 2 * tig;
+        m0[0] = acc[0];
+        m0[1] = acc[1];
+        m1[0] = acc[2];
+        m1[1] = acc[3];
+      }
+    }
+    __syncwarp();
+    const int el = sel[e];
+    for (int p0 = lane; p0 < NPAIR; p0 += 32) {
+      int p = p0, i = 0;
+      while (p >= NEN - i) { p -= NEN - i; ++i; }
+      const int j = i + p;
+      float H[DIM][DIM];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) {
+          const int r = a * NEN + i, c = b * NEN + j;
+          H[a][b] = r <= c ? M[r * LDM + c] : M[c * LDM + r];
+        }
+      float tr = 0.f;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) tr += H[a][a];
+      const int ni = sconn[e * NEN + i], nj = sconn[e * NEN + j];
+      const int sij = slotmap[(int64_t)(i * NEN + j) * nelem + el] * DIM;
+      const int sji = slotmap[(int64_t)(j * NEN + i) * nelem + el] * DIM;
+      float V[DIM][DIM];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) {
+          V[a][b] = lam1 * H[a][b] + mu1 * H[b][a];
+          if (a == b) V[a][b] += mu1 * tr;
+        }
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        float col[DIM];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) col[a] = V[a][b];
+        add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sij + b) * n + ni * DIM], col);
+      }
+      if (i != j) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+          add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sji + a) * n + nj * DIM], V[a]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <int ET>
+size_t smem_bytes_mma(int TE, int ngp) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  const size_t nf = (size_t)(kThreads / 32) * MmaShape<ET>::RP * MmaShape<ET>::LDM +
+                    (size_t)ngp * info.dim * info.nen + ngp + (size_t)TE * info.nen * info.dim +
+                    (size_t)ngp * info.nen * info.dim * TE + (size_t)ngp * TE;
+  return nf * sizeof(float) + sizeof(int) * ((size_t)TE * info.nen + 2 * TE) + 16;
+}
+
+template <int ET>
+gf_status launch_mma(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K) {
+  // elements per CTA: a multiple of the 8 warps, as many as fit 200 KB (at most 64)
+  int TE = 64;
+  while (TE > 8 && smem_bytes_mma<ET>(TE, ctx->ngp) > 200 * 1024) TE -= 8;
+  const size_t sm = smem_bytes_mma<ET>(TE, ctx->ngp);
+  if (sm > 227 * 1024)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "TF32 engine: %zu bytes of shared memory", sm);
+  auto kc = k_assemble_mma<ET, false>;
+  auto ka = k_assemble_mma<ET, true>;
+  GF_CUDA(ctx, cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const float lam1 = (float)ctx->lam1, mu1 = (float)ctx->mu1;
+  if (scatter == GF_SCATTER_ATOMIC) {
+    const int count = ctx->nelem;
+    ka<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
+        ctx->d_allperm, count, TE, ctx->ngp, ctx->d_conn, ctx->d_coords64, ctx->d_Eel32,
+        ctx->d_slotmap, ctx->nelem, ctx->n, d_tab, lam1, mu1, K);
+    GF_LAUNCH_CHECK(ctx, "k_assemble_mma(atomic)");
+  } else {
+    for (int c = 0; c < ctx->ncolors; ++c) {
+      const int c0 = ctx->color_off[c], count = ctx->color_off[c + 1] - c0;
+      if (count == 0) continue;
+      kc<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
+          ctx->d_perm + c0, count, TE, ctx->ngp, ctx->d_conn, ctx->d_coords64, ctx->d_Eel32,
+          ctx->d_slotmap, ctx->nelem, ctx->n, d_tab, lam1, mu1, K);
+      GF_LAUNCH_CHECK(ctx, "k_assemble_mma(colour)");
+    }
+  }
+  return GF_OK;
+}
+
+gf_status launch_mma_dispatch(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K) {
+  switch (ctx->elem_type) {
+    case GF_Q4: return launch_mma<GF_Q4>(ctx, scatter, d_tab, K);
+    case GF_Q8: return launch_mma<GF_Q8>(ctx, scatter, d_tab, K);
+    case GF_BRICK8: return launch_mma<GF_BRICK8>(ctx, scatter, d_tab, K);
+    default: return launch_mma<GF_BRICK20>(ctx, scatter, d_tab, K);
+  }
+}
+
 template <int ET, typename TC>
 size_t smem_bytes(int TE, int ngp) {
   constexpr ElemInfo info = gf_elem_info(ET);
@@ -278,8 +512,10 @@ gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out) {
 }
 
 gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
-  if (engine != GF_ENGINE_CUDA_CORE)
-    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "tensor-core engine not available in this build");
+  const bool mma = engine == GF_ENGINE_TF32_MMA;
+  if (mma && scatter == GF_SCATTER_OWNER)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED,
+                   "the TF32 engine runs the element-wise schedules (colour, atomic)");
   gf_status st;
   const AsmTables* d_tab = nullptr;
   if ((st = gf_asm_tables(ctx, &d_tab)) != GF_OK) return st;
@@ -298,7 +534,8 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
     st = launch_dispatch<double>(ctx, scatter, d_tab, ctx->d_K64);
   } else {
     cudaMemsetAsync(ctx->d_K32, 0, sizeof(float) * total, ctx->stream);
-    st = launch_dispatch<float>(ctx, scatter, d_tab, ctx->d_K32);
+    st = mma ? launch_mma_dispatch(ctx, scatter, d_tab, ctx->d_K32)
+             : launch_dispatch<float>(ctx, scatter, d_tab, ctx->d_K32);
   }
   cudaEventRecord(ctx->ev1, ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);

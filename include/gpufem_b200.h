@@ -74,8 +74,11 @@ typedef enum gf_scatter {
 /* Element-integration engine of gf_assemble (FP32 only; FP64 always uses CUDA cores). */
 typedef enum gf_engine {
   GF_ENGINE_CUDA_CORE = 0, /* FP32/FP64 FMA                                             */
-  GF_ENGINE_TF32_MMA = 1   /* per-element Gram contraction G.G^T on tensor cores (TF32,
-                              FP32 accumulate); tolerance is TF32's, not FP32's        */
+  GF_ENGINE_TF32_MMA = 1   /* per-element Gram matrix M = G diag(w) G^T on tensor cores
+                              (mma.sync TF32, three products hi*hi + hi*lo + lo*hi,
+                              FP32 accumulate; within the FP32 tolerance).  Colour and
+                              atomic schedules only (AUTO picks atomic); OWNER returns
+                              GF_ERR_UNSUPPORTED.  Slower than CUDA cores on B200.    */
 } gf_engine;
 
 /* Constraint treatment (FEM::ConstraintMode, src/FEM/fem.h:51-54). */
