@@ -129,6 +129,29 @@ __device__ inline bool node_rows(const MatLayout& L, int t, const TK* __restrict
   Acc acc[DIM];
 #pragma unroll
   for (int c = 0; c < DIM; ++c) acc[c] = 0;
+  if constexpr (DIM == 2) {
+    // short 2-D rows: all column words first, so every x gather's address is known
+    // before the first one is issued
+    constexpr int kPre = 24;
+    if (w <= kPre) {
+      int bb[kPre];
+#pragma unroll
+      for (int p = 0; p < kPre; ++p) bb[p] = p < w ? __ldcs(bc + 32 * p) : 0;
+#pragma unroll
+      for (int p = 0; p < kPre; ++p) {
+        if (p < w) {
+          const TK* v = vp + p * SS;
+          const TK u0 = __ldcs(v), u1 = __ldcs(v + 32), u2 = __ldcs(v + 64), u3 = __ldcs(v + 96);
+          const Acc x0 = (Acc)__ldg(x + (int64_t)bb[p] * 2), x1 = (Acc)__ldg(x + (int64_t)bb[p] * 2 + 1);
+          acc[0] += (Acc)u0 * x0 + (Acc)u1 * x1;
+          acc[1] += (Acc)u2 * x0 + (Acc)u3 * x1;
+        }
+      }
+      out[0] = (double)acc[0];
+      out[1] = (double)acc[1];
+      return true;
+    }
+  }
   for (int p = 0; p < w; ++p, bc += 32, vp += SS) {
     const int b = __ldcs(bc);
     TK u[DIM * DIM];
