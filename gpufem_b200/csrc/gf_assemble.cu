@@ -224,9 +224,10 @@ constexpr int kMmaMaxKS = (GF_MAX_GP + 7) / 8;  // k-steps of 8 Gauss points
 template <int ET>
 struct MmaShape {
   static constexpr ElemInfo info = gf_elem_info(ET);
-  static constexpr int R = info.nen * info.dim;
-  static constexpr int RP = (R + 15) / 16 * 16;  // padded rows / columns of M
-  static constexpr int LDM = RP + 4;             // row stride of M in shared memory
+  static constexpr int DP = info.dim == 3 ? 4 : 2;   // rows per node (3-D padded to 4)
+  static constexpr int NPB = 16 / DP;                // nodes per 16-row strip
+  static constexpr int RP = (info.nen * DP + 15) / 16 * 16;  // padded rows / columns of M
+  static constexpr int LDS = RP + 4;                 // row stride of a strip in shared memory
 };
 
 template <int ET, bool ATOMIC>
@@ -238,16 +239,20 @@ k_assemble_mma(const int32_t* __restrict__ elems, int count, int TE, int ngp,
                float* __restrict__ K) {
   constexpr ElemInfo info = gf_elem_info(ET);
   constexpr int NEN = info.nen, DIM = info.dim;
-  constexpr int R = MmaShape<ET>::R, RP = MmaShape<ET>::RP, LDM = MmaShape<ET>::LDM;
+  constexpr int DP = MmaShape<ET>::DP, NPB = MmaShape<ET>::NPB;
+  constexpr int RP = MmaShape<ET>::RP, LDS = MmaShape<ET>::LDS;
   constexpr int NPAIR = NEN * (NEN + 1) / 2;
   constexpr int NW = kThreads / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float* sM = reinterpret_cast<float*>(smem_raw);                // NW * RP * LDM
-  float* sdN = sM + NW * RP * LDM;                               // ngp*DIM*NEN
+  float* sM = reinterpret_cast<float*>(smem_raw);                // NW * 16 * LDS
+  float* sdN = sM + NW * 16 * LDS;                               // ngp*DIM*NEN
   float* sw = sdN + ngp * DIM * NEN;                             // ngp
   float* sX = sw + ngp;                                          // TE*NEN*DIM
-  float* sG = sX + TE * NEN * DIM;                               // ngp*NEN*DIM*TE
-  float* swd = sG + ngp * NEN * DIM * TE;                        // ngp*TE
+  // G with an odd element stride SE = TE + 1: the fragment loads of one warp (one element,
+  // rows and Gauss points varying across lanes) then fall into different banks
+  const int SE = TE + 1;
+  float* sG = sX + TE * NEN * DIM;                               // ngp*NEN*DIM*SE
+  float* swd = sG + ngp * NEN * DIM * SE;                        // ngp*TE
   int* sconn = reinterpret_cast<int*>(swd + ngp * TE);           // TE*NEN
   int* sel = sconn + TE * NEN;                                   // TE
   int* sflag = sel + TE;                                         // TE
@@ -271,14 +276,30 @@ k_assemble_mma(const int32_t* __restrict__ elems, int count, int TE, int ngp,
       sX[k * DIM + c] = float(coords[(int64_t)node * DIM + c] - coords[(int64_t)node0 * DIM + c]);
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < nt; e += kThreads)
-    sflag[e] = gf_distorted<NEN, DIM, float>(sdN, ngp, sX + e * NEN * DIM);
+  // distortion flag (max/min |detJ| > 10): |detJ| at every (element, Gauss point) in
+  // parallel first (a CTA holds only a few elements here), then the ratio per element
+  for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
+    const int e = t % TE, g = t / TE;
+    if (e >= nt) continue;
+    float J[3][3], Ji[3][3];
+    gf_jacobian<NEN, DIM, float, float>(sdN + g * DIM * NEN, sX + e * NEN * DIM, J);
+    swd[g * TE + e] = fabsf(gf_det_inv<DIM, float>(J, Ji));
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nt; e += kThreads) {
+    float dmin = 3.4e38f, dmax = 0.f;
+    for (int g = 0; g < ngp; ++g) {
+      dmin = fminf(dmin, swd[g * TE + e]);
+      dmax = fmaxf(dmax, swd[g * TE + e]);
+    }
+    sflag[e] = dmax > 10.f * dmin ? 1 : 0;
+  }
   __syncthreads();
   for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
     const int e = t % TE, g = t / TE;
     if (e >= nt) continue;
     const float detJ = gf_gradients<NEN, DIM, float>(sdN + g * DIM * NEN, sX + e * NEN * DIM,
-                                                     sflag[e], sG + (g * NEN * DIM) * TE + e, TE);
+                                                     sflag[e], sG + (g * NEN * DIM) * SE + e, SE);
     swd[g * TE + e] = sw[g] * detJ * Eel[sel[e]];
   }
   __syncthreads();
@@ -286,14 +307,17 @@ k_assemble_mma(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gid = lane >> 2, tig = lane & 3;
   const int KS = (ngp + 7) >> 3;
-  float* M = sM + warp * RP * LDM;
-  // G[r][k] of element e (0 outside r < R, k < ngp)
+  float* S = sM + warp * 16 * LDS;  // this warp's strip of M: 16 rows x RP columns
+  // G[r][k] of element e, rows node-major (r = i*DP + a; 0 for a >= DIM, i >= NEN, k >= ngp)
   auto Gv = [&](int r, int k, int e) -> float {
-    if (r >= R || k >= ngp) return 0.f;
-    const int a = r / NEN, i = r - a * NEN;
-    return sG[((k * NEN + i) * DIM + a) * TE + e];
+    const int i = r / DP, a = r - i * DP;
+    if (a >= DIM || i >= NEN || k >= ngp) return 0.f;
+    return sG[((k * NEN + i) * DIM + a) * SE + e];
   };
   for (int e = warp; e < nt; e += NW) {
+    const int el = sel[e];
+    // strip mt: rows of nodes NPB*mt .. NPB*mt + NPB-1 against the columns of every node
+    // j >= NPB*mt; then the blocks of the pairs (i, j >= i) with i in the strip
     for (int mt = 0; mt < RP / 16; ++mt) {
       const int r0 = mt * 16 + gid, r1 = r0 + 8;
       uint32_t ah[kMmaMaxKS][4], al[kMmaMaxKS][4];
@@ -321,73 +345,73 @@ k_assemble_mma(const int32_t* __restrict__ elems, int count, int TE, int ngp,
           mma_tf32(acc, ah[ks], bl0, bl1);
           mma_tf32(acc, ah[ks], bh0, bh1);
         }
-        float* m0 = M + r0 * LDM + ntl * 8 + 2 * tig;
-        float* m1 = M + r1 * LDM + ntl * 8 + 2 * tig;
+        float* m0 = S + gid * LDS + ntl * 8 + 2 * tig;
+        float* m1 = m0 + 8 * LDS;
         m0[0] = acc[0];
         m0[1] = acc[1];
         m1[0] = acc[2];
         m1[1] = acc[3];
       }
-    }
-    __syncwarp();
-    const int el = sel[e];
-    for (int p0 = lane; p0 < NPAIR; p0 += 32) {
-      int p = p0, i = 0;
-      while (p >= NEN - i) { p -= NEN - i; ++i; }
-      const int j = i + p;
-      float H[DIM][DIM];
-#pragma unroll
-      for (int a = 0; a < DIM; ++a)
-#pragma unroll
-        for (int b = 0; b < DIM; ++b) {
-          const int r = a * NEN + i, c = b * NEN + j;
-          H[a][b] = r <= c ? M[r * LDM + c] : M[c * LDM + r];
-        }
-      float tr = 0.f;
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) tr += H[a][a];
-      const int ni = sconn[e * NEN + i], nj = sconn[e * NEN + j];
-      const int sij = slotmap[(int64_t)(i * NEN + j) * nelem + el] * DIM;
-      const int sji = slotmap[(int64_t)(j * NEN + i) * nelem + el] * DIM;
-      float V[DIM][DIM];
-#pragma unroll
-      for (int a = 0; a < DIM; ++a)
-#pragma unroll
-        for (int b = 0; b < DIM; ++b) {
-          V[a][b] = lam1 * H[a][b] + mu1 * H[b][a];
-          if (a == b) V[a][b] += mu1 * tr;
-        }
-#pragma unroll
-      for (int b = 0; b < DIM; ++b) {
-        float col[DIM];
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) col[a] = V[a][b];
-        add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sij + b) * n + ni * DIM], col);
-      }
-      if (i != j) {
+      __syncwarp();
+      const int ib = mt * NPB, ie = min(NEN, ib + NPB);
+      int npair = 0;
+      for (int i = ib; i < ie; ++i) npair += NEN - i;
+      for (int q0 = lane; q0 < npair; q0 += 32) {
+        int q = q0, i = ib;
+        while (q >= NEN - i) { q -= NEN - i; ++i; }
+        const int j = i + q;
+        const float* h = S + (i - ib) * DP * LDS + j * DP;
+        float H[DIM][DIM];
 #pragma unroll
         for (int a = 0; a < DIM; ++a)
-          add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sji + a) * n + nj * DIM], V[a]);
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) H[a][b] = h[a * LDS + b];
+        float tr = 0.f;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) tr += H[a][a];
+        const int ni = sconn[e * NEN + i], nj = sconn[e * NEN + j];
+        const int sij = slotmap[(int64_t)(i * NEN + j) * nelem + el] * DIM;
+        const int sji = slotmap[(int64_t)(j * NEN + i) * nelem + el] * DIM;
+        float V[DIM][DIM];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) {
+            V[a][b] = lam1 * H[a][b] + mu1 * H[b][a];
+            if (a == b) V[a][b] += mu1 * tr;
+          }
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) {
+          float col[DIM];
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) col[a] = V[a][b];
+          add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sij + b) * n + ni * DIM], col);
+        }
+        if (i != j) {
+#pragma unroll
+          for (int a = 0; a < DIM; ++a)
+            add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sji + a) * n + nj * DIM], V[a]);
+        }
       }
+      __syncwarp();
     }
-    __syncwarp();
   }
 }
 
 template <int ET>
 size_t smem_bytes_mma(int TE, int ngp) {
   constexpr ElemInfo info = gf_elem_info(ET);
-  const size_t nf = (size_t)(kThreads / 32) * MmaShape<ET>::RP * MmaShape<ET>::LDM +
+  const size_t nf = (size_t)(kThreads / 32) * 16 * MmaShape<ET>::LDS +
                     (size_t)ngp * info.dim * info.nen + ngp + (size_t)TE * info.nen * info.dim +
-                    (size_t)ngp * info.nen * info.dim * TE + (size_t)ngp * TE;
+                    (size_t)ngp * info.nen * info.dim * (TE + 1) + (size_t)ngp * TE;
   return nf * sizeof(float) + sizeof(int) * ((size_t)TE * info.nen + 2 * TE) + 16;
 }
 
 template <int ET>
 gf_status launch_mma(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K) {
-  // elements per CTA: a multiple of the 8 warps, as many as fit 200 KB (at most 64)
+  // elements per CTA: a multiple of the 8 warps, as many as fit 110 KB (two CTAs per SM)
   int TE = 64;
-  while (TE > 8 && smem_bytes_mma<ET>(TE, ctx->ngp) > 200 * 1024) TE -= 8;
+  while (TE > 8 && smem_bytes_mma<ET>(TE, ctx->ngp) > 110 * 1024) TE -= 8;
   const size_t sm = smem_bytes_mma<ET>(TE, ctx->ngp);
   if (sm > 227 * 1024)
     return gf_fail(ctx, GF_ERR_UNSUPPORTED, "TF32 engine: %zu bytes of shared memory", sm);
