@@ -5,10 +5,11 @@ on the Q8 512x512 workload, plus the time to solve it.
   python bench.py --impl reference ...     # the reference's CPU path on host cores
 
 One JSON line on rank 0.  `value` = elements assembled per second with inputs
-resident in HBM (device time of gf_assemble: K zero-fill + colour-scheduled fused
-integration/scatter kernels, FP32), L2 flushed between steps.  `e2e` = the same
-metric through the public C-ABI from pinned host buffers: mesh upload, pattern,
-colouring, assembly and download of the ELL matrix, every step.  For N > 1 each
+resident in HBM (device time of gf_assemble with the owner-computes schedule: the
+per-element geometry kernel and the owner kernel that writes every K entry once, FP32),
+L2 flushed between steps; the colour, atomic and TF32 tensor-core variants are timed
+beside it.  `e2e` = the same metric through the public C-ABI from pinned host buffers:
+mesh upload, pattern, assembly and download of the ELL matrix, every step.  For N > 1 each
 rank assembles its own replica of the workload (weak scaling; the assembly needs
 no exchange) and the time is the max over ranks.
 """
@@ -370,13 +371,16 @@ def run_gpu_arm(args):
 
     # the three scatter schedules side by side (median of a few steps each)
     variants = {}
-    for name, sc in (("owner", _lib.GF_SCATTER_OWNER), ("colour", _lib.GF_SCATTER_COLOR),
-                     ("atomic", _lib.GF_SCATTER_ATOMIC)):
+    runs = [("owner", _lib.GF_SCATTER_OWNER, 0), ("colour", _lib.GF_SCATTER_COLOR, 0),
+            ("atomic", _lib.GF_SCATTER_ATOMIC, 0)]
+    if esize == 4:   # the TF32 tensor-core engine assembles FP32 only
+        runs.append(("atomic_tf32", _lib.GF_SCATTER_ATOMIC, _lib.GF_ENGINE_TF32_MMA))
+    for name, sc, eng in runs:
         ts = []
         for _ in range(max(3, min(args.steps, 10))):
             flush.zero_()
             torch.cuda.synchronize()
-            ts.append(ctx.assemble(dtype, sc))
+            ts.append(ctx.assemble(dtype, sc, eng))
         variants[name] = {"value": m.nelem / float(np.median(ts)), "unit": UNIT,
                           "ms": float(np.median(ts)) * 1e3}
 
