@@ -113,10 +113,26 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   }
   __syncthreads();
 
-  // phase 1a (FP32 path only): flag elements with a large detJ spread
+  // phase 1a (FP32 path only): flag elements with a large detJ spread; |detJ| at every
+  // (element, Gauss point) in parallel first (swd as scratch), then the ratio per element
+  // (a thread per element alone would hold the CTA at the barrier when TE is small)
   if (!f64) {
-    for (int e = threadIdx.x; e < nt; e += kThreads)
-      sflag[e] = gf_distorted<NEN, DIM, TC>(sdN, ngp, sX + e * NEN * DIM);
+    for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
+      const int e = t % TE, g = t / TE;
+      if (e >= nt) continue;
+      float J[3][3], Ji[3][3];
+      gf_jacobian<NEN, DIM, float, TC>(sdN + g * DIM * NEN, sX + e * NEN * DIM, J);
+      swd[g * TE + e] = TC(fabsf(gf_det_inv<DIM, float>(J, Ji)));
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nt; e += kThreads) {
+      float dmin = 3.4e38f, dmax = 0.f;
+      for (int g = 0; g < ngp; ++g) {
+        dmin = fminf(dmin, float(swd[g * TE + e]));
+        dmax = fmaxf(dmax, float(swd[g * TE + e]));
+      }
+      sflag[e] = dmax > 10.f * dmin ? 1 : 0;
+    }
     __syncthreads();
   }
 
