@@ -342,8 +342,11 @@ def run_gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # "auto" resolves as the library's GF_SCATTER_AUTO does: atomic for Brick20, owner else
+    sname = args.scatter if args.scatter != "auto" else (
+        "atomic" if m.elem_type == mg.BRICK20 else "owner")
     scatter = {"owner": _lib.GF_SCATTER_OWNER, "colour": _lib.GF_SCATTER_COLOR,
-               "atomic": _lib.GF_SCATTER_ATOMIC, "auto": _lib.GF_SCATTER_AUTO}[args.scatter]
+               "atomic": _lib.GF_SCATTER_ATOMIC}[sname]
     for _ in range(args.warmup):
         ctx.assemble(dtype, scatter)
     barrier()
@@ -395,16 +398,18 @@ def run_gpu_arm(args):
     ngp = m.ngauss ** m.dim
     t_geo = float(np.mean([a for a, _ in split]))
     t_dom = float(np.mean([b for _, b in split]))
-    if args.scatter == "owner":
+    if sname == "owner":
         ninc = m.nelem * m.nen
         dom_bytes = (nnz * esize + m.nelem * ngp * (m.dim * m.dim + 1) * esize + m.nelem * esize
                      + ninc * (4 + 1 + 2 * m.nen) + (m.nnodes + 1) * 4)
         dom_name = "k_assemble_owner"
     else:
-        dom_bytes, dom_name = alg_bytes, "k_assemble (all colour passes) + K zero-fill"
+        dom_bytes = alg_bytes
+        dom_name = ("k_assemble (all colour passes)" if sname == "colour" else
+                    "k_assemble (atomic)") + " + K zero-fill"
     traffic = traffic_asm = None
     tfile = ROOT / "profiles" / "ncu_traffic.json"
-    if tfile.exists() and args.scatter == "owner":
+    if tfile.exists() and sname == "owner":
         tr = json.loads(tfile.read_text()).get(f"{cfg}/assemble")
         if tr is not None:
             traffic_asm = tr.get("bytes_per_assembly")
@@ -562,7 +567,7 @@ def run_gpu_arm(args):
             "roofline_spmv": {"bound": "hbm", "achieved": spmv_bytes / t_spmv / 1e9, "peak": hbm,
                               "unit": "GB/s", "frac": spmv_bytes / t_spmv / 1e9 / hbm,
                               "us_per_launch": t_spmv * 1e6, "algorithmic_bytes": spmv_bytes},
-            "scatter": args.scatter,
+            "scatter": sname,
             "scatter_variants": variants,
             "e2e": {"value": world * m.nelem / e2e_per, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -592,7 +597,7 @@ def main():
     ap.add_argument("--solvers", default=",".join(SOLVERS),
                     help="comma list of the solve block's entries (default: all)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--scatter", default="owner", choices=["owner", "colour", "atomic", "auto"])
+    ap.add_argument("--scatter", default="auto", choices=["owner", "colour", "atomic", "auto"])
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
