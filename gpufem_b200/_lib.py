@@ -83,6 +83,7 @@ SIGNATURES = {
     "gf_lp_collect": (I32, [P, I32, I32, D, I32]),
     "gf_lp_train": (I32, [P, I32, I32, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "gf_lp_apply": (I32, [P, P, P]),
+    "gf_lp_set_coarse": (I32, [P, I32]),
     "gf_lp_loss_grad": (I32, [P, P, P, C.POINTER(C.c_float), P]),
     "gf_twolevel_setup": (I32, [P, I32, C.POINTER(I32)]),
     "gf_twolevel_apply": (I32, [P, P, P]),

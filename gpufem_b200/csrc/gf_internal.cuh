@@ -355,6 +355,8 @@ gf_status gf_coarse_prepare(gf_ctx* ctx, int target_coarse);
 // z = D^-1 r + P Ac^-1 P^T r (FP64 vectors), rz_acc += r.z; launches only.
 void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z,
                      double* rz_acc, const int* done);
+// z += P Ac^-1 P^T r (the coarse term alone); launches only.
+void gf_coarse_add(gf_ctx* ctx, const double* r, double* z);
 // Two-level PCG steps (launches only, capturable).  Begin: x = 0, r = b, p = M r,
 // sc->rr = b.b, sc->rzn = r.M r.  Iterate (after the SpMV q = K p, p.q): x, r update,
 // then p = M r + beta p; the kernels return at once while sc->done != 0.
@@ -369,9 +371,10 @@ void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, doubl
 void gf_lp_mesh_changed(gf_ctx* ctx);
 gf_status gf_lp_prepare(gf_ctx* ctx);
 bool gf_lp_ready(const gf_ctx* ctx);
+bool gf_lp_coarse(const gf_ctx* ctx);  // learned preconditioner with the coarse correction
 // z = M(r): FP64 residual in, FP64 preconditioned vector out (r32: n floats of scratch)
 gf_status gf_lp_apply64(gf_ctx* ctx, const double* r64, float* r32_scratch, double* z);
 // Jacobi-PCG on the FP64 matrix recording (float(r_k), float(ustar - x_k)) every
 // `every` iterations into r_out / e_out (npairs slots of n floats); *recorded set.
 gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every, double tol,
-                        int maxit, float* r_out, float* e_out, int* recorded);
+                        int maxit, float* r_out, float* e_out, int* recorded, bool twolevel = false);

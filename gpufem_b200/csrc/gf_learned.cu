@@ -96,6 +96,7 @@ struct LpState {
   float* pr = nullptr;       // [npairs][n]
   float* pe = nullptr;       // [npairs][n]
   bool ready = false;        // diag / graph set up for the current matrix
+  bool coarse = false;       // with the two-level coarse correction (gf_lp_set_coarse)
 };
 
 namespace {
@@ -538,6 +539,7 @@ gf_status gf_lp_apply64(gf_ctx* ctx, const double* r64, float* r32_scratch, doub
 }
 
 bool gf_lp_ready(const gf_ctx* ctx) { return ctx->lp && ctx->lp->ready; }
+bool gf_lp_coarse(const gf_ctx* ctx) { return ctx->lp && ctx->lp->coarse; }
 
 // A new mesh or matrix invalidates the collected pairs and the diagonal; the
 // weights stay (they are mesh-independent).
@@ -557,7 +559,7 @@ gf_status gf_lp_collect_impl(gf_ctx* ctx, int npairs, int every, double tol, int
   const int n = s->n;
   // reference solution u* (tighter than the recorded run)
   gf_solve_opts o{};
-  o.solver = GF_SOLVER_PCG;
+  o.solver = s->coarse ? GF_SOLVER_TWOLEVEL_PCG : GF_SOLVER_PCG;
   o.matrix = GF_F64;
   o.tol = tol * 1e-3;
   o.max_iter = maxit * 4;
@@ -574,7 +576,7 @@ gf_status gf_lp_collect_impl(gf_ctx* ctx, int npairs, int every, double tol, int
   if ((st = gf_alloc(ctx, &s->pr, (size_t)npairs * n)) != GF_OK) { cudaFree(ustar); return st; }
   if ((st = gf_alloc(ctx, &s->pe, (size_t)npairs * n)) != GF_OK) { cudaFree(ustar); return st; }
   int got = 0;
-  st = gf_pcg_record(ctx, ustar, npairs, every, tol, maxit, s->pr, s->pe, &got);
+  st = gf_pcg_record(ctx, ustar, npairs, every, tol, maxit, s->pr, s->pe, &got, s->coarse);
   cudaFree(ustar);
   if (st != GF_OK && st != GF_ERR_NOT_CONVERGED) return st;
   s->npairs = got;
@@ -695,6 +697,13 @@ GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, fl
   GF_CUDA(ctx, cudaStreamSynchronize(cs));
   if (loss) *loss = (float)l;
   if (grad) GF_CUDA(ctx, cudaMemcpy(grad, s->g, sizeof(float) * P, cudaMemcpyDeviceToHost));
+  return GF_OK;
+}
+
+GF_API gf_status gf_lp_set_coarse(gf_ctx* ctx, int32_t on) {
+  if (!ctx) return GF_ERR_INVALID_ARG;
+  if (!ctx->lp) return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner not initialised (gf_lp_init)");
+  ctx->lp->coarse = on != 0;
   return GF_OK;
 }
 

@@ -1011,6 +1011,11 @@ __global__ void k_fcg_restart(FcgScalars* sc) {
   sc->done = sc->iter >= sc->maxit ? 3 : 0;
 }
 
+__global__ void k_sub_f32(int n, const double* __restrict__ a, float* __restrict__ b) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) b[i] = (float)((double)b[i] - a[i]);
+}
+
 __global__ void k_record_pair(int n, const double* __restrict__ r, const double* __restrict__ x,
                               const double* __restrict__ ustar, float* __restrict__ rout,
                               float* __restrict__ eout) {
@@ -1029,7 +1034,9 @@ gf_status run_fcg(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   gf_status st;
   if (!ctx->lp) return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner not initialised (gf_lp_init)");
   const bool learned = true;
+  const bool coarse = gf_lp_coarse(ctx);
   if ((st = gf_lp_prepare(ctx)) != GF_OK) return st;
+  if (coarse && (st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
   if (!ctx->d_fcg) {
     if (cudaMalloc(&ctx->d_fcg, sizeof(FcgScalars)) != cudaSuccess) {
       cudaGetLastError();
@@ -1058,8 +1065,15 @@ gf_status run_fcg(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   for (int kind = learned ? 0 : 1; kind < 2; ++kind) {
     GF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < check; ++k) {
-      if (kind == 0) gf_lp_apply64(ctx, r, r32, z);
-      else k_fcg_jacobi<<<nb, kT, 0, s>>>(n, r, dinv, z, sc);
+      // M: the network (kind 0) or Jacobi (kind 1), plus the coarse correction if enabled
+      if (kind == 0) {
+        gf_lp_apply64(ctx, r, r32, z);
+        if (coarse) gf_coarse_add(ctx, r, z);
+      } else if (coarse) {
+        gf_coarse_apply(ctx, r, dinv, z, nullptr, nullptr);
+      } else {
+        k_fcg_jacobi<<<nb, kT, 0, s>>>(n, r, dinv, z, sc);
+      }
       k_fcg_dots<<<red_grid(ctx, n), kT, 0, s>>>(n, z, r, rold, sc);
       k_fcg_dir<<<nb, kT, 0, s>>>(n, z, p, sc);
       k_fcg_spmv<<<mat_grid(ctx, L), L.threads, 0, s>>>(L, val, p, r, q, sc);
@@ -1134,7 +1148,7 @@ gf_status run_fcg(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
 }  // namespace
 
 gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every, double tol,
-                        int maxit, float* r_out, float* e_out, int* recorded) {
+                        int maxit, float* r_out, float* e_out, int* recorded, bool twolevel) {
   *recorded = 0;
   if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "recording needs the FP64 matrix");
   gf_status st;
@@ -1150,28 +1164,44 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
   MatLayout L;
   const void* vk = nullptr;
   if ((st = solver_matrix(ctx, GF_F64, &L, &vk)) != GF_OK) return st;
+  if (twolevel && (st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
   k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
-  k_cg_init<double><<<red_grid(ctx, n), kT, 0, s>>>(n, ctx->d_f, dinv, x, r, z, p, sc);
+  if (twolevel) gf_tl_begin(ctx, ctx->d_f, x, r, p, dinv, sc);
+  else k_cg_init<double><<<red_grid(ctx, n), kT, 0, s>>>(n, ctx->d_f, dinv, x, r, z, p, sc);
   k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
   GF_LAUNCH_CHECK(ctx, "k_cg_init");
-  k_record_pair<<<nb, kT, 0, s>>>(n, r, x, ustar, r_out, e_out);  // iteration 0: e = u*
-  GF_LAUNCH_CHECK(ctx, "k_record_pair");
+  // pair k: r_k, and the error e_k = u* - x_k; with the two-level iteration the coarse
+  // correction of r_k is taken off e_k (what a local correction still has to supply)
+  auto record = [&](int k) -> gf_status {
+    k_record_pair<<<nb, kT, 0, s>>>(n, r, x, ustar, r_out + (size_t)k * n, e_out + (size_t)k * n);
+    if (twolevel) {
+      GF_CUDA(ctx, cudaMemsetAsync(z, 0, sizeof(double) * n, s));
+      gf_coarse_add(ctx, r, z);
+      k_sub_f32<<<nb, kT, 0, s>>>(n, z, e_out + (size_t)k * n);
+    }
+    GF_LAUNCH_CHECK(ctx, "k_record_pair");
+    return GF_OK;
+  };
+  if ((st = record(0)) != GF_OK) return st;
   int got = 1;
   while (got < npairs) {
     for (int k = 0; k < every; ++k) {
       k_cg_spmv_dot<double, double><<<mat_grid(ctx, L), L.threads, 0, s>>>(
           L, (const double*)vk, p, q, sc);
-      k_cg_update<double><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
-      k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
+      if (twolevel) {
+        gf_tl_iterate(ctx, x, r, p, q, dinv, sc);
+      } else {
+        k_cg_update<double><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
+        k_cg_direction<double><<<nb, kT, 0, s>>>(n, z, p, sc);
+        ctx->launches += 2;
+      }
     }
-    ctx->launches += 3 * every;
+    ctx->launches += every;
     GF_CUDA(ctx, cudaMemcpyAsync(hs, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
     GF_CUDA(ctx, cudaStreamSynchronize(s));
     if (hs->done) break;
-    k_record_pair<<<nb, kT, 0, s>>>(n, r, x, ustar, r_out + (size_t)got * n,
-                                    e_out + (size_t)got * n);
-    GF_LAUNCH_CHECK(ctx, "k_record_pair");
+    if ((st = record(got)) != GF_OK) return st;
     ++got;
   }
   GF_CUDA(ctx, cudaStreamSynchronize(s));

@@ -602,14 +602,14 @@ k_prolong(int n, const int32_t* __restrict__ agg, const double* __restrict__ x,
           const double* __restrict__ cen, double sinv, const uint8_t* __restrict__ fixed,
           const double* __restrict__ dinv, const double* __restrict__ r,
           const double* __restrict__ zc, double* __restrict__ z, double* __restrict__ rz_acc,
-          const int* __restrict__ done) {
+          const int* __restrict__ done, int add) {
   constexpr int NM = DIM == 2 ? 3 : 6;
   __shared__ double sh[32];
   if (done && *done) return;
   double rz = 0.0;
   for (int i = blockIdx.x * kCT + threadIdx.x; i < n; i += gridDim.x * kCT) {
     const int a = i / DIM, c = i - a * DIM;
-    double zi = dinv[i] * r[i];
+    double zi = add ? z[i] : dinv ? dinv[i] * r[i] : 0.0;
     if (!fixed[i]) {
       const int A = agg[a];
       double d[DIM];
@@ -623,6 +623,7 @@ k_prolong(int n, const int32_t* __restrict__ agg, const double* __restrict__ x,
     z[i] = zi;
     rz += r[i] * zi;
   }
+  if (!rz_acc) return;
   const double s = cg_block_sum(rz, sh);
   if (threadIdx.x == 0) atomicAdd(rz_acc, s);
 }
@@ -951,8 +952,9 @@ gf_status gf_coarse_prepare(gf_ctx* ctx, int target) {
   return GF_OK;
 }
 
-void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z, double* rz_acc,
-                     const int* done) {
+// z = D^-1 r + P Ac^-1 P^T r (dinv null: the coarse term alone); add != 0: z += that.
+static void coarse_apply_impl(gf_ctx* ctx, const double* r, const double* dinv, double* z,
+                              double* rz_acc, const int* done, int add) {
   Coarse* c = static_cast<Coarse*>(ctx->coarse);
   cudaStream_t s = ctx->stream;
   const double sinv = 1.0 / c->s;
@@ -963,16 +965,25 @@ void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z
     k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, nullptr,
                                             nullptr, done);
     k_prolong<2><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
-                                    ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
+                                    ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done, add);
   } else {
     k_restrict<3><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
                                         ctx->d_fixed, r, c->rc, c->zc, done);
     k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, nullptr,
                                             nullptr, done);
     k_prolong<3><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
-                                    ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done);
+                                    ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done, add);
   }
   ctx->launches += 3;
+}
+
+void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z, double* rz_acc,
+                     const int* done) {
+  coarse_apply_impl(ctx, r, dinv, z, rz_acc, done, 0);
+}
+
+void gf_coarse_add(gf_ctx* ctx, const double* r, double* z) {
+  coarse_apply_impl(ctx, r, nullptr, z, nullptr, nullptr, 1);
 }
 
 template <int DIM>

@@ -201,6 +201,9 @@ class Context:
         w = np.ascontiguousarray(w, np.float32)
         self._c(lib.gf_lp_set_weights(self.h, _ptr(w)))
 
+    def lp_set_coarse(self, on: bool) -> None:
+        self._c(lib.gf_lp_set_coarse(self.h, 1 if on else 0))
+
     def lp_collect(self, npairs: int, every: int, tol: float = 1e-6, max_iter: int = 100000) -> None:
         self._c(lib.gf_lp_collect(self.h, npairs, every, tol, max_iter))
 

@@ -252,6 +252,12 @@ GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr
                              float* final_loss);
 /* z = M(r) on FP32 device vectors of n entries. */
 GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z);
+/* on != 0: the learned preconditioner works with the two-level coarse correction
+ * (gf_twolevel_setup): gf_lp_collect records its pairs from two-level PCG runs with the
+ * coarse correction of each residual taken off the error (the network learns what the
+ * coarse space misses), and GF_SOLVER_LEARNED_FCG applies M(r) + P Ac^-1 P^T r, falling
+ * back to two-level PCG.  Needs a mesh-built pattern. */
+GF_API gf_status gf_lp_set_coarse(gf_ctx* ctx, int32_t on);
 /* Loss of one (r, e) pair (FP32 device vectors) and its gradient w.r.t. every parameter
  * (host buffer of gf_lp_num_params floats, or NULL); weights unchanged. */
 GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, float* loss,

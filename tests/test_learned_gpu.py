@@ -101,3 +101,46 @@ def test_learned_fcg_requires_init():
     with pytest.raises(_lib.GpufemError) as ei:
         ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-8)
     assert ei.value.status == _lib.GF_ERR_STATE
+
+
+def test_coarse_mode_untrained_is_twolevel():
+    """With the coarse correction on, the untrained network (M = D^-1) gives
+    M = D^-1 + P Ac^-1 P^T: flexible CG takes two-level PCG's iteration count."""
+    m, ctx = brick8_problem(n=(8, 6, 6))
+    info_tl = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, tol=1e-10, max_iter=100000)
+    u_tl = ctx.solution()
+    ctx.lp_init(3, seed=3)
+    ctx.lp_set_coarse(True)
+    info = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
+    assert info.status == _lib.GF_OK and info.fallback == 0
+    assert abs(info.iterations - info_tl.iterations) <= 2, (info.iterations, info_tl.iterations)
+    assert np.linalg.norm(ctx.solution() - u_tl) <= 1e-7 * np.linalg.norm(u_tl)
+
+
+def test_coarse_mode_trained_and_fallback_converge():
+    m, ctx = brick8_problem(n=(8, 6, 6))
+    info_j = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-10, max_iter=100000)
+    u_pcg = ctx.solution()
+    ctx.lp_init(3, seed=3)
+    ctx.lp_set_coarse(True)
+    ctx.lp_collect(npairs=16, every=2, tol=1e-8)
+    ctx.lp_train(steps=50, batch=8, lr=1e-3, seed=2)
+    info = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
+    assert info.status == _lib.GF_OK and info.rel_residual <= 1e-9
+    assert np.linalg.norm(ctx.solution() - u_pcg) <= 1e-7 * np.linalg.norm(u_pcg)
+    # a bad network falls back to FCG with D^-1 + P Ac^-1 P^T, far fewer iterations than Jacobi
+    ctx.lp_set_weights(random_weights(3, seed=9, scale=3.0).astype(np.float32))
+    info = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
+    assert info.status == _lib.GF_OK and info.rel_residual <= 1e-9 and info.fallback == 1
+    assert np.linalg.norm(ctx.solution() - u_pcg) <= 1e-7 * np.linalg.norm(u_pcg)
+    ctx.lp_set_coarse(False)
+    info = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
+    assert info.status == _lib.GF_OK and info.fallback == 1
+
+
+def test_coarse_mode_needs_init():
+    from gpufem_b200.fem import Context
+    ctx = Context(0)
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.lp_set_coarse(True)
+    assert ei.value.status == _lib.GF_ERR_STATE
