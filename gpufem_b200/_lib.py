@@ -25,6 +25,7 @@ GF_ENGINE_CUDA_CORE, GF_ENGINE_TF32_MMA = 0, 1
 GF_BC_PENALTY, GF_BC_ELIMINATION = 0, 1
 GF_SOLVER_CG, GF_SOLVER_PCG, GF_SOLVER_MIXED_PCG, GF_SOLVER_LEARNED_FCG, GF_SOLVER_MIXED_PCG32 = 0, 1, 2, 3, 4
 GF_SOLVER_TWOLEVEL_PCG = 5
+GF_LP_LOSS_ERROR, GF_LP_LOSS_RESIDUAL = 0, 1
 
 
 class SolveOpts(C.Structure):
@@ -84,6 +85,8 @@ SIGNATURES = {
     "gf_lp_train": (I32, [P, I32, I32, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "gf_lp_apply": (I32, [P, P, P]),
     "gf_lp_set_coarse": (I32, [P, I32]),
+    "gf_lp_set_loss": (I32, [P, I32]),
+    "gf_lp_collect_random": (I32, [P, I32, C.c_uint64]),
     "gf_lp_loss_grad": (I32, [P, P, P, C.POINTER(C.c_float), P]),
     "gf_twolevel_setup": (I32, [P, I32, C.POINTER(I32)]),
     "gf_twolevel_apply": (I32, [P, P, P]),

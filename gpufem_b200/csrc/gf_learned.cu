@@ -4,8 +4,10 @@
 // src/SPRmatrix/SPRmatrix.cc:405-480).
 //
 // M(r) = D^-1 r + c * y(r),   rho = D^-1 r (Jacobi), c = rms(rho),
-// y = network(features) with per-node features [rho_a / c (dim), log(d_a / mean d) (dim)]:
-//   h0 = relu(W0 f + b0)                                   (2 dim -> 64)
+// v1 = D^-1 K rho, v2 = D^-1 K v1 (two matrix hops, so the network sees K itself),
+// y = network(features) with per-node features
+//   [rho_a / c (dim), v1_a / c (dim), v2_a / c (dim), log(d_a / mean d) (dim)]:
+//   h0 = relu(W0 f + b0)                                   (4 dim -> 64)
 //   h_{l+1} = relu(Ws_l h_l + Wn_l mean_{b in N(a)} h_l[b] + b_l),  l = 0, 1, 2   (64 -> 64)
 //   y = Wout h3 + bout                                     (64 -> dim)
 // N(a) = nodes sharing an element with a (the ELL node adjacency, self included).
@@ -14,8 +16,9 @@
 // The output scale c makes M(s r) = s M(r).
 //
 // Training pairs (r_k, e_k = u* - x_k) come from Jacobi-PCG runs on the context's
-// matrix (u* = a tighter PCG solution).  Loss per pair, with t = e - rho:
-//   L = sum_dofs d (c y - t)^2 / sum_dofs d e^2        (D-weighted relative error)
+// matrix (u* = a tighter PCG solution).  Loss per pair, z = M(r_k):
+//   GF_LP_LOSS_ERROR:    L = sum d (z - e)^2 / sum d e^2             (D-weighted error)
+//   GF_LP_LOSS_RESIDUAL: L = sum (K (e - z))^2 / d / sum (K e)^2 / d  (residual left by M)
 #include <cuda_bf16.h>
 
 #include <chrono>
@@ -38,7 +41,7 @@ struct LpOffsets {
 
 LpOffsets lp_offsets(int dim) {
   LpOffsets o{};
-  const int F = 2 * dim;
+  const int F = 4 * dim;
   int64_t p = 0;
   o.W0 = p; p += (int64_t)H * F;
   o.b0 = p; p += H;
@@ -57,7 +60,7 @@ struct LpScalars {
   double sumsq;   // sum rho^2
   double c;       // rms(rho)
   double loss;    // accumulated loss
-  double dsum;    // sum d e^2 (loss normaliser)
+  double dsum;    // loss normaliser (sum d e^2, or sum (K e)^2 / d)
 };
 
 }  // namespace
@@ -80,7 +83,12 @@ struct LpState {
   float* dlog = nullptr;     // log(d / mean d)
   float* dvec = nullptr;     // d (loss weight)
   // activations [N][H] (pre-activations kept for the ReLU masks)
-  float* feat = nullptr;     // [N][2 dim]
+  float* feat = nullptr;     // [N][4 dim]
+  float* v1 = nullptr;       // [n] D^-1 K rho
+  float* v2 = nullptr;       // [n] D^-1 K v1
+  float* lw = nullptr;       // [n] residual loss scratch: e - z, then D^-1 s
+  float* ls = nullptr;       // [n] s = K (e - z)
+  float* lt = nullptr;       // [n] K e, then K D^-1 s
   float* pre[kLayers + 1] = {};
   float* h[kLayers + 1] = {};
   float* agg[kLayers] = {};
@@ -97,6 +105,7 @@ struct LpState {
   float* pe = nullptr;       // [npairs][n]
   bool ready = false;        // diag / graph set up for the current matrix
   bool coarse = false;       // with the two-level coarse correction (gf_lp_set_coarse)
+  int loss = GF_LP_LOSS_ERROR;
 };
 
 namespace {
@@ -139,6 +148,7 @@ __global__ void k_lp_prep(int n, const float* __restrict__ r, const float* __res
 }
 
 __global__ void k_lp_features(int N, int dim, const float* __restrict__ rho,
+                              const float* __restrict__ v1, const float* __restrict__ v2,
                               const float* __restrict__ dlog, float* __restrict__ feat,
                               LpScalars* sc) {
   const int a = blockIdx.x * kLT + threadIdx.x;
@@ -147,10 +157,31 @@ __global__ void k_lp_features(int N, int dim, const float* __restrict__ rho,
   if (blockIdx.x == 0 && threadIdx.x == 0) sc->c = c;
   if (a >= N) return;
   const float ic = (float)(1.0 / c);
+  float* f = feat + (int64_t)a * 4 * dim;
   for (int k = 0; k < dim; ++k) {
-    feat[(int64_t)a * 2 * dim + k] = rho[a * dim + k] * ic;
-    feat[(int64_t)a * 2 * dim + dim + k] = dlog[a * dim + k];
+    f[k] = rho[a * dim + k] * ic;
+    f[dim + k] = v1[a * dim + k] * ic;
+    f[2 * dim + k] = v2[a * dim + k] * ic;
+    f[3 * dim + k] = dlog[a * dim + k];
   }
+}
+
+// y = scale .* (K x) on the column-major ELL (entry (row, slot) at row + slot n),
+// thread per row, FP64 accumulation; scale may be null.
+template <typename TK>
+__global__ void __launch_bounds__(kLT)
+k_lp_ellmv(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
+           const TK* __restrict__ val, const float* __restrict__ x,
+           const float* __restrict__ scale, float* __restrict__ y) {
+  const int row = blockIdx.x * kLT + threadIdx.x;
+  if (row >= n) return;
+  const int nz = rownnz[row];
+  double acc = 0.0;
+  for (int s = 0; s < nz; ++s) {
+    const int64_t o = (int64_t)s * n + row;
+    acc += (double)__ldg(val + o) * (double)__ldg(x + __ldg(col + o));
+  }
+  y[row] = (float)(scale ? acc * (double)scale[row] : acc);
 }
 
 // out[a][o] = act(b[o] + sum_k W1[o][k] A[a][k] (+ sum_k W2[o][k] B[a][k]))
@@ -324,6 +355,71 @@ __global__ void k_lp_loss_grad(int n, const float* __restrict__ e, const float* 
   if (threadIdx.x == 0) atomicAdd(loss_acc, l);
 }
 
+// Residual loss: w = e - z (z = rho + c y)
+__global__ void k_lp_rl_diff(int n, const float* __restrict__ e, const float* __restrict__ rho,
+                             const float* __restrict__ y, const LpScalars* __restrict__ sc,
+                             float* __restrict__ w) {
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  if (i < n) w[i] = (float)((double)e[i] - ((double)rho[i] + sc->c * (double)y[i]));
+}
+
+// normaliser: sum t^2 / d with t = K e
+__global__ void k_lp_rl_sums(int n, const float* __restrict__ t, const float* __restrict__ dinv,
+                             LpScalars* sc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  double s = 0.0;
+  if (i < n) s = (double)dinv[i] * t[i] * t[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->dsum, s);
+}
+
+// loss += sum s^2 / d / S; g = s / d (the SpMV after it forms K g)
+__global__ void k_lp_rl_loss(int n, const float* __restrict__ s_, const float* __restrict__ dinv,
+                             const LpScalars* __restrict__ sc, float* __restrict__ g,
+                             double* loss_acc) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  const double S = sc->dsum > 0 ? sc->dsum : 1.0;
+  double l = 0.0;
+  if (i < n) {
+    const double gi = (double)dinv[i] * s_[i];
+    l = gi * s_[i] / S;
+    g[i] = (float)gi;
+  }
+  l = lp_block_sum(l, sh);
+  if (threadIdx.x == 0) atomicAdd(loss_acc, l);
+}
+
+// dy = dL/dy = -2 c (K g) / S
+__global__ void k_lp_rl_dy(int n, const float* __restrict__ kg, const LpScalars* __restrict__ sc,
+                           float* __restrict__ dy) {
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  const double S = sc->dsum > 0 ? sc->dsum : 1.0;
+  if (i < n) dy[i] = (float)(-2.0 * sc->c * (double)kg[i] / S);
+}
+
+// Random training errors e = xi / sqrt(d), xi ~ N(0, 1): white in the D-norm, so the
+// error loss weighs every part of the spectrum of D^-1 K alike.  xi by the Box-Muller
+// transform of two uniforms from the splitmix64 mix of (seed, pair, index).
+__device__ inline uint64_t lp_mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_lp_random_error(int n, uint64_t seed, int pair, const float* __restrict__ dinv,
+                                  float* __restrict__ e) {
+  const int i = blockIdx.x * kLT + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t h = lp_mix64(seed ^ lp_mix64(((uint64_t)pair << 32) | (uint32_t)i));
+  const double u1 = ((h >> 11) + 1.0) * 0x1.0p-53;            // (0, 1]
+  const double u2 = (lp_mix64(h) >> 11) * 0x1.0p-53;           // [0, 1)
+  const double xi = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+  e[i] = (float)(xi * sqrt((double)dinv[i]));
+}
+
 __global__ void k_lp_adam(int64_t P, float* __restrict__ w, const float* __restrict__ g,
                           float* __restrict__ m, float* __restrict__ v,
                           __nv_bfloat16* __restrict__ wb, float lr, float b1, float b2,
@@ -392,6 +488,7 @@ inline int lp_grid(int64_t work) {
 static void lp_free_buffers(LpState* s) {
   auto f = [](auto*& p) { if (p) { cudaFree(p); p = nullptr; } };
   f(s->deg_inv); f(s->dinv); f(s->dinv64); f(s->dlog); f(s->dvec); f(s->feat);
+  f(s->v1); f(s->v2); f(s->lw); f(s->ls); f(s->lt);
   for (int l = 0; l <= kLayers; ++l) { f(s->pre[l]); f(s->h[l]); }
   for (int l = 0; l < kLayers; ++l) f(s->agg[l]);
   f(s->y); f(s->dy); f(s->rho); f(s->dh); f(s->dpre); f(s->tmp);
@@ -428,7 +525,8 @@ gf_status gf_lp_prepare(gf_ctx* ctx) {
     gf_status st;
 #define LPA(p, cnt) if ((st = lp_alloc(ctx, &(p), (size_t)(cnt))) != GF_OK) return st
     LPA(s->deg_inv, N); LPA(s->dinv, n); LPA(s->dinv64, n); LPA(s->dlog, n); LPA(s->dvec, n);
-    LPA(s->feat, (size_t)N * 2 * dim);
+    LPA(s->feat, (size_t)N * 4 * dim);
+    LPA(s->v1, n); LPA(s->v2, n); LPA(s->lw, n); LPA(s->ls, n); LPA(s->lt, n);
     for (int l = 0; l <= kLayers; ++l) { LPA(s->pre[l], (size_t)N * H); LPA(s->h[l], (size_t)N * H); }
     for (int l = 0; l < kLayers; ++l) LPA(s->agg[l], (size_t)N * H);
     LPA(s->y, n); LPA(s->dy, n); LPA(s->rho, n); LPA(s->dh, (size_t)N * H); LPA(s->dpre, (size_t)N * H);
@@ -458,6 +556,18 @@ gf_status gf_lp_prepare(gf_ctx* ctx) {
   return GF_OK;
 }
 
+// y = scale .* (K x) for FP32 device vectors (FP64 matrix values when present).
+static void lp_matvec(gf_ctx* ctx, const float* x, const float* scale, float* y) {
+  const int n = ctx->n;
+  if (ctx->has64)
+    k_lp_ellmv<double><<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(
+        n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, x, scale, y);
+  else
+    k_lp_ellmv<float><<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(
+        n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32, x, scale, y);
+  ctx->launches++;
+}
+
 // Network forward on FP32 residual r (device, n); fills rho, y and the activations.
 static void lp_forward(gf_ctx* ctx, const float* r) {
   LpState* s = ctx->lp;
@@ -466,14 +576,17 @@ static void lp_forward(gf_ctx* ctx, const float* r) {
   const LpOffsets& o = s->off;
   cudaMemsetAsync(&s->sc->sumsq, 0, sizeof(double), st);
   k_lp_prep<<<gf_blocks(n, kLT), kLT, 0, st>>>(n, r, s->dinv, s->rho, s->sc);
-  k_lp_features<<<gf_blocks(N, kLT), kLT, 0, st>>>(N, dim, s->rho, s->dlog, s->feat, s->sc);
+  lp_matvec(ctx, s->rho, s->dinv, s->v1);
+  lp_matvec(ctx, s->v1, s->dinv, s->v2);
+  k_lp_features<<<gf_blocks(N, kLT), kLT, 0, st>>>(N, dim, s->rho, s->v1, s->v2, s->dlog,
+                                                   s->feat, s->sc);
   const int gH = lp_grid((int64_t)N * H);
   if (dim == 2)
-    k_lp_dense<4, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
+    k_lp_dense<8, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
                                                 s->wb + o.b0, s->pre[0], s->h[0], 1);
   else
-    k_lp_dense<6, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
-                                                s->wb + o.b0, s->pre[0], s->h[0], 1);
+    k_lp_dense<12, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
+                                                 s->wb + o.b0, s->pre[0], s->h[0], 1);
   for (int l = 0; l < kLayers; ++l) {
     k_lp_aggregate<<<gH, kLT, 0, st>>>(N, ctx->d_adj_off, ctx->d_adj, s->deg_inv, s->h[l],
                                        s->agg[l], 0);
@@ -521,10 +634,35 @@ static void lp_backward(gf_ctx* ctx, const float* dy) {
   }
   k_lp_relu_grad<<<gH, kLT, 0, st>>>((int64_t)N * H, s->dh, s->pre[0], s->dpre);
   if (dim == 2)
-    k_lp_wgrad<4, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
+    k_lp_wgrad<8, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
   else
-    k_lp_wgrad<6, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
+    k_lp_wgrad<12, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
   ctx->launches += 3 + 6 * kLayers + 2;
+}
+
+// Forward, loss and backward of one training pair (r, e): adds the pair's loss to
+// sc->loss and its parameter gradient to s->g.
+static void lp_pair(gf_ctx* ctx, const float* r, const float* e) {
+  LpState* s = ctx->lp;
+  cudaStream_t cs = ctx->stream;
+  const int n = s->n, nb = gf_blocks(n, kLT);
+  cudaMemsetAsync(&s->sc->dsum, 0, sizeof(double), cs);
+  lp_forward(ctx, r);
+  if (s->loss == GF_LP_LOSS_RESIDUAL) {
+    k_lp_rl_diff<<<nb, kLT, 0, cs>>>(n, e, s->rho, s->y, s->sc, s->lw);
+    lp_matvec(ctx, s->lw, nullptr, s->ls);   // s = K (e - z)
+    lp_matvec(ctx, e, nullptr, s->lt);       // t = K e
+    k_lp_rl_sums<<<nb, kLT, 0, cs>>>(n, s->lt, s->dinv, s->sc);
+    k_lp_rl_loss<<<nb, kLT, 0, cs>>>(n, s->ls, s->dinv, s->sc, s->lw, &s->sc->loss);
+    lp_matvec(ctx, s->lw, nullptr, s->lt);   // K D^-1 s
+    k_lp_rl_dy<<<nb, kLT, 0, cs>>>(n, s->lt, s->sc, s->dy);
+    ctx->launches += 4;
+  } else {
+    k_lp_loss_sums<<<nb, kLT, 0, cs>>>(n, e, s->dvec, s->sc);
+    k_lp_loss_grad<<<nb, kLT, 0, cs>>>(n, e, s->rho, s->y, s->dvec, s->dy, s->sc, &s->sc->loss);
+    ctx->launches += 2;
+  }
+  lp_backward(ctx, s->dy);
 }
 
 // Preconditioner application for the solver: z = M(r) in FP64 from an FP64 residual.
@@ -588,6 +726,29 @@ gf_status gf_lp_collect_impl(gf_ctx* ctx, int npairs, int every, double tol, int
 // chunk boundaries; e = u* - x with u* from a tighter solve.
 gf_status gf_lp_collect_impl(gf_ctx* ctx, int npairs, int every, double tol, int maxit);
 
+// Random pairs: e_k white in the D-norm, r_k = K e_k.
+static gf_status lp_collect_random(gf_ctx* ctx, int npairs, uint64_t seed) {
+  LpState* s = ctx->lp;
+  const int n = s->n;
+  if (s->pr) cudaFree(s->pr);
+  if (s->pe) cudaFree(s->pe);
+  s->pr = s->pe = nullptr;
+  s->npairs = 0;
+  gf_status st;
+  if ((st = gf_alloc(ctx, &s->pr, (size_t)npairs * n)) != GF_OK) return st;
+  if ((st = gf_alloc(ctx, &s->pe, (size_t)npairs * n)) != GF_OK) return st;
+  for (int k = 0; k < npairs; ++k) {
+    float* e = s->pe + (int64_t)k * n;
+    k_lp_random_error<<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(n, seed, k, s->dinv, e);
+    ctx->launches++;
+    lp_matvec(ctx, e, nullptr, s->pr + (int64_t)k * n);
+  }
+  GF_CUDA(ctx, cudaGetLastError());
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  s->npairs = npairs;
+  return GF_OK;
+}
+
 extern "C" {
 
 GF_API int64_t gf_lp_num_params(int32_t dim) {
@@ -617,7 +778,7 @@ GF_API gf_status gf_lp_init(gf_ctx* ctx, int32_t dim, uint64_t seed) {
   std::mt19937_64 rng(seed);
   std::normal_distribution<float> nd(0.f, 1.f);
   const LpOffsets& o = s->off;
-  const int F = 2 * dim;
+  const int F = 4 * dim;
   for (int64_t k = 0; k < (int64_t)H * F; ++k) w[o.W0 + k] = nd(rng) * std::sqrt(2.f / F);
   for (int l = 0; l < kLayers; ++l)
     for (int64_t k = 0; k < (int64_t)H * H; ++k) {
@@ -684,13 +845,8 @@ GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, fl
   const int64_t P = s->off.total;
   cudaStream_t cs = ctx->stream;
   GF_CUDA(ctx, cudaMemsetAsync(s->g, 0, sizeof(float) * (P + H), cs));
-  GF_CUDA(ctx, cudaMemsetAsync(&s->sc->loss, 0, 2 * sizeof(double), cs));  // loss, dsum
-  lp_forward(ctx, r);
-  k_lp_loss_sums<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->dvec, s->sc);
-  k_lp_loss_grad<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->rho, s->y, s->dvec, s->dy,
-                                                        s->sc, &s->sc->loss);
-  ctx->launches += 2;
-  lp_backward(ctx, s->dy);
+  GF_CUDA(ctx, cudaMemsetAsync(&s->sc->loss, 0, sizeof(double), cs));
+  lp_pair(ctx, r, e);
   GF_CUDA(ctx, cudaGetLastError());
   double l = 0.0;
   GF_CUDA(ctx, cudaMemcpyAsync(&l, &s->sc->loss, sizeof(double), cudaMemcpyDeviceToHost, cs));
@@ -707,6 +863,15 @@ GF_API gf_status gf_lp_set_coarse(gf_ctx* ctx, int32_t on) {
   return GF_OK;
 }
 
+GF_API gf_status gf_lp_set_loss(gf_ctx* ctx, int32_t loss) {
+  if (!ctx) return GF_ERR_INVALID_ARG;
+  if (loss != GF_LP_LOSS_ERROR && loss != GF_LP_LOSS_RESIDUAL)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown loss %d", (int)loss);
+  if (!ctx->lp) return gf_fail(ctx, GF_ERR_STATE, "learned preconditioner not initialised (gf_lp_init)");
+  ctx->lp->loss = loss;
+  return GF_OK;
+}
+
 GF_API gf_status gf_lp_collect(gf_ctx* ctx, int32_t npairs, int32_t every, double tol,
                                int32_t max_iter) {
   if (!ctx || npairs <= 0 || every <= 0) return GF_ERR_INVALID_ARG;
@@ -714,6 +879,16 @@ GF_API gf_status gf_lp_collect(gf_ctx* ctx, int32_t npairs, int32_t every, doubl
   gf_status st = gf_lp_prepare(ctx);
   if (st != GF_OK) return st;
   return gf_lp_collect_impl(ctx, npairs, every, tol, max_iter > 0 ? max_iter : 100000);
+}
+
+GF_API gf_status gf_lp_collect_random(gf_ctx* ctx, int32_t npairs, uint64_t seed) {
+  if (!ctx || npairs <= 0) return GF_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gf_status st = gf_lp_prepare(ctx);
+  if (st != GF_OK) return st;
+  if (ctx->lp->coarse)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "random pairs have no coarse-corrected target");
+  return lp_collect_random(ctx, npairs, seed);
 }
 
 GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed,
@@ -736,13 +911,7 @@ GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr
       const int k = pick(rng);
       const float* r = s->pr + (int64_t)k * s->n;
       const float* e = s->pe + (int64_t)k * s->n;
-      GF_CUDA(ctx, cudaMemsetAsync(&s->sc->dsum, 0, sizeof(double), cs));
-      lp_forward(ctx, r);
-      k_lp_loss_sums<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->dvec, s->sc);
-      k_lp_loss_grad<<<gf_blocks(s->n, kLT), kLT, 0, cs>>>(s->n, e, s->rho, s->y, s->dvec,
-                                                            s->dy, s->sc, &s->sc->loss);
-      ctx->launches += 2;
-      lp_backward(ctx, s->dy);
+      lp_pair(ctx, r, e);
     }
     ++s->adam_t;
     const float b1 = 0.9f, b2 = 0.999f;

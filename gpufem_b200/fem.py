@@ -204,8 +204,15 @@ class Context:
     def lp_set_coarse(self, on: bool) -> None:
         self._c(lib.gf_lp_set_coarse(self.h, 1 if on else 0))
 
+    def lp_set_loss(self, loss: int) -> None:
+        """GF_LP_LOSS_ERROR or GF_LP_LOSS_RESIDUAL."""
+        self._c(lib.gf_lp_set_loss(self.h, loss))
+
     def lp_collect(self, npairs: int, every: int, tol: float = 1e-6, max_iter: int = 100000) -> None:
         self._c(lib.gf_lp_collect(self.h, npairs, every, tol, max_iter))
+
+    def lp_collect_random(self, npairs: int, seed: int = 0) -> None:
+        self._c(lib.gf_lp_collect_random(self.h, npairs, seed))
 
     def lp_train(self, steps: int, batch: int = 4, lr: float = 1e-3, seed: int = 0) -> float:
         loss = C.c_float()

@@ -230,12 +230,16 @@ GF_API gf_status gf_solution_view(gf_ctx* ctx, const double** u);
 
 /* ---- learned preconditioner (no counterpart in the reference) ---------------------------
  * M(r) = D^-1 r + c * y, c = rms(D^-1 r), y from a 3-layer message-passing network over
- * the node graph of K (nodes sharing an element): input layer (2*dim -> 64), three layers
- * h' = relu(Ws h + Wn mean_neighbours(h) + b) (hidden width 64), output layer (64 -> dim)
- * initialised to zero (an untrained network is Jacobi).  Weights are BF16 in use with an
- * FP32 master copy; activations and accumulation are FP32.  Used by GF_SOLVER_LEARNED_FCG.
- * Parameter layout: W0[64][2 dim], b0[64], then per layer Ws[64][64], Wn[64][64], b[64],
+ * the node graph of K (nodes sharing an element).  Per-node input features (4*dim):
+ * rho/c, v1/c, v2/c, log(d/geomean d) with rho = D^-1 r, v1 = D^-1 K rho, v2 = D^-1 K v1.
+ * Input layer (4*dim -> 64), three layers h' = relu(Ws h + Wn mean_neighbours(h) + b)
+ * (hidden width 64), output layer (64 -> dim) initialised to zero (an untrained network
+ * is Jacobi).  Weights are BF16 in use with an FP32 master copy; activations and
+ * accumulation are FP32.  Used by GF_SOLVER_LEARNED_FCG.
+ * Parameter layout: W0[64][4 dim], b0[64], then per layer Ws[64][64], Wn[64][64], b[64],
  * then Wout[dim][64], bout[dim]. */
+#define GF_LP_LOSS_ERROR 0    /* sum d (M(r) - e)^2 / sum d e^2 (default) */
+#define GF_LP_LOSS_RESIDUAL 1 /* sum (K (e - M(r)))^2 / d / sum (K e)^2 / d */
 GF_API int64_t gf_lp_num_params(int32_t dim);
 GF_API gf_status gf_lp_init(gf_ctx* ctx, int32_t dim, uint64_t seed);
 GF_API gf_status gf_lp_get_weights(gf_ctx* ctx, float* w);
@@ -245,9 +249,13 @@ GF_API gf_status gf_lp_set_weights(gf_ctx* ctx, const float* w);
  * to tol * 1e-3).  Replaces previously collected pairs. */
 GF_API gf_status gf_lp_collect(gf_ctx* ctx, int32_t npairs, int32_t every, double tol,
                                int32_t max_iter);
-/* Adam steps (lr, batch pairs per step) on the collected pairs; loss per pair
- * sum d (c y - (e - D^-1 r))^2 / sum d e^2 (d = diag K).  *final_loss = mean loss of the
- * last step. */
+/* Random training pairs: e_k = xi / sqrt(d) with xi standard normal (counter-based,
+ * from seed), r_k = K e_k.  Errors white in the D-norm make the error loss weigh every
+ * eigenmode of D^-1 K alike (a sparse-approximate-inverse objective).  Replaces
+ * previously collected pairs; GF_ERR_UNSUPPORTED with the coarse correction on. */
+GF_API gf_status gf_lp_collect_random(gf_ctx* ctx, int32_t npairs, uint64_t seed);
+/* Adam steps (lr, batch pairs per step) on the collected pairs with the loss chosen by
+ * gf_lp_set_loss (d = diag K).  *final_loss = mean loss of the last step. */
 GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed,
                              float* final_loss);
 /* z = M(r) on FP32 device vectors of n entries. */
@@ -258,6 +266,10 @@ GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z);
  * coarse space misses), and GF_SOLVER_LEARNED_FCG applies M(r) + P Ac^-1 P^T r, falling
  * back to two-level PCG.  Needs a mesh-built pattern. */
 GF_API gf_status gf_lp_set_coarse(gf_ctx* ctx, int32_t on);
+/* Training loss (GF_LP_LOSS_*) of gf_lp_train and gf_lp_loss_grad.  The residual loss
+ * weighs the error by K D^-1 K instead of D: it rewards reducing the rough part of the
+ * error, the part a local operator can reach. */
+GF_API gf_status gf_lp_set_loss(gf_ctx* ctx, int32_t loss);
 /* Loss of one (r, e) pair (FP32 device vectors) and its gradient w.r.t. every parameter
  * (host buffer of gf_lp_num_params floats, or NULL); weights unchanged. */
 GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, float* loss,

@@ -1,13 +1,16 @@
 """TEST INFRASTRUCTURE ONLY — numpy restatement of the learned preconditioner
-(forward, loss and backward), the checker for the CUDA kernels in
+(forward, losses and backward), the checker for the CUDA kernels in
 gpufem_b200/csrc/gf_learned.cu.  The reference has no learned preconditioner, so
 this oracle restates the network as include/gpufem_b200.h documents it.
 
 Network (hidden width 64, weights used as BF16, FP64 arithmetic here):
-  rho = r / d, c = rms(rho), f_a = [rho_a / c, log(d_a / geomean d)]
+  rho = r / d, v1 = (K rho) / d, v2 = (K v1) / d, c = rms(rho)
+  f_a = [rho_a / c, v1_a / c, v2_a / c, log(d_a / geomean d)]     (4 dim features)
   h0 = relu(W0 f + b0); h_{l+1} = relu(Ws_l h_l + Wn_l mean_{N(a)} h_l + b_l), l < 3
   y = Wout h3 + bout;  M(r) = rho + c y
-Loss: L = sum d (c y - (e - rho))^2 / sum d e^2.
+Losses for a pair (r, e), z = M(r):
+  "error":    L = sum d (z - e)^2 / sum d e^2
+  "residual": L = sum (K (e - z))^2 / d / sum (K e)^2 / d
 """
 from __future__ import annotations
 
@@ -18,7 +21,7 @@ LAYERS = 3
 
 
 def offsets(dim: int) -> dict:
-    F = 2 * dim
+    F = 4 * dim
     o, p = {}, 0
 
     def take(name, size):
@@ -49,7 +52,7 @@ def to_bf16(w: np.ndarray) -> np.ndarray:
 def unpack(w: np.ndarray, dim: int, bf16: bool = True) -> dict:
     o = offsets(dim)
     wb = to_bf16(w) if bf16 else np.asarray(w, np.float64)
-    F = 2 * dim
+    F = 4 * dim
     out = {}
     for name, (p, size) in o.items():
         if name == "total":
@@ -84,13 +87,17 @@ def _aggregate_t(adj, g):
     return np.stack([gs[nbrs].sum(axis=0) for nbrs in adj])
 
 
-def forward(w, dim, adj, d, r, bf16=True):
+def forward(w, dim, adj, d, r, K, bf16=True):
+    """z = M(r); K is the matrix (anything with K @ x), d its diagonal."""
     P = unpack(w, dim, bf16)
     N = len(adj)
     rho = r / d
+    v1 = (K @ rho) / d
+    v2 = (K @ v1) / d
     c = np.sqrt(np.mean(rho * rho)) + 1e-30
     logd = np.log(d) - np.mean(np.log(d))
-    f = np.concatenate([(rho / c).reshape(N, dim), logd.reshape(N, dim)], axis=1)
+    f = np.concatenate([(rho / c).reshape(N, dim), (v1 / c).reshape(N, dim),
+                        (v2 / c).reshape(N, dim), logd.reshape(N, dim)], axis=1)
     cache = {"f": f, "rho": rho, "c": c}
     pre0 = f @ P["W0"].T + P["b0"]
     h = np.maximum(pre0, 0)
@@ -106,14 +113,24 @@ def forward(w, dim, adj, d, r, bf16=True):
     return rho + c * y, cache
 
 
-def loss_and_grad(w, dim, adj, d, r, e, bf16=True):
+def loss_and_grad(w, dim, adj, d, r, e, K, loss="error", bf16=True):
     P = unpack(w, dim, bf16)
-    z, cache = forward(w, dim, adj, d, r, bf16)
-    rho, c, y = cache["rho"], cache["c"], cache["y"]
-    S = np.sum(d * e * e)
-    diff = c * y - (e - rho)
-    L = np.sum(d * diff * diff) / S
-    dy = (2.0 * d * c * diff / S).reshape(-1, dim)
+    z, cache = forward(w, dim, adj, d, r, K, bf16)
+    c = cache["c"]
+    if loss == "error":
+        S = np.sum(d * e * e)
+        diff = z - e
+        L = np.sum(d * diff * diff) / S
+        dz = 2.0 * d * diff / S
+    elif loss == "residual":
+        t = K @ e
+        S = np.sum(t * t / d)
+        s_ = K @ (e - z)
+        L = np.sum(s_ * s_ / d) / S
+        dz = -2.0 * (K @ (s_ / d)) / S
+    else:
+        raise ValueError(loss)
+    dy = (c * dz).reshape(-1, dim)
     o = offsets(dim)
     g = np.zeros(o["total"][0])
 

@@ -1,6 +1,7 @@
 """The numpy oracle of the learned preconditioner is self-consistent: analytic
-gradients agree with central finite differences (FP64, BF16 rounding off), the
-untrained network (zero output layer) is Jacobi, and M is scale-equivariant.  CPU."""
+gradients of both losses agree with central finite differences (FP64, BF16 rounding
+off), the untrained network (zero output layer) is Jacobi, and M is
+scale-equivariant.  CPU."""
 import numpy as np
 import pytest
 
@@ -13,9 +14,17 @@ def small_problem(seed=0):
     adj = G.node_adjacency(m.conn, m.nnodes)
     rng = np.random.default_rng(seed)
     d = np.exp(rng.normal(size=m.ndof))
+    # a symmetric matrix on the dof graph of the node adjacency, diagonal d
+    n = m.ndof
+    A = np.zeros((n, n))
+    for a, nbrs in enumerate(adj):
+        for b in nbrs:
+            A[3 * a:3 * a + 3, 3 * b:3 * b + 3] = rng.normal(scale=0.1, size=(3, 3))
+    K = 0.5 * (A + A.T)
+    K[np.arange(n), np.arange(n)] = d
     r = rng.normal(size=m.ndof)
     e = rng.normal(size=m.ndof)
-    return m, adj, d, r, e
+    return m, adj, d, r, e, K
 
 
 def random_weights(dim, seed=1, scale=0.3):
@@ -24,28 +33,29 @@ def random_weights(dim, seed=1, scale=0.3):
 
 
 def test_untrained_network_is_jacobi():
-    m, adj, d, r, _ = small_problem()
+    m, adj, d, r, _, K = small_problem()
     w = random_weights(3)
     p, size = G.offsets(3)["Wout"]
     w[p:p + size] = 0
     pb, sb = G.offsets(3)["bout"]
     w[pb:pb + sb] = 0
-    z, _ = G.forward(w, 3, adj, d, r)
+    z, _ = G.forward(w, 3, adj, d, r, K)
     assert np.allclose(z, r / d)
 
 
 def test_scale_equivariance():
-    m, adj, d, r, _ = small_problem()
+    m, adj, d, r, _, K = small_problem()
     w = random_weights(3)
-    z1, _ = G.forward(w, 3, adj, d, r)
-    z2, _ = G.forward(w, 3, adj, d, 7.5 * r)
+    z1, _ = G.forward(w, 3, adj, d, r, K)
+    z2, _ = G.forward(w, 3, adj, d, 7.5 * r, K)
     assert np.allclose(z2, 7.5 * z1, rtol=1e-12)
 
 
-def test_gradient_matches_finite_differences():
-    m, adj, d, r, e = small_problem()
+@pytest.mark.parametrize("loss", ["error", "residual"])
+def test_gradient_matches_finite_differences(loss):
+    m, adj, d, r, e, K = small_problem()
     w = random_weights(3, scale=0.2)
-    L, g, _ = G.loss_and_grad(w, 3, adj, d, r, e, bf16=False)
+    L, g, _ = G.loss_and_grad(w, 3, adj, d, r, e, K, loss, bf16=False)
     rng = np.random.default_rng(3)
     idx = rng.choice(w.size, 40, replace=False)
     o = G.offsets(3)
@@ -56,8 +66,8 @@ def test_gradient_matches_finite_differences():
         wp, wm = w.copy(), w.copy()
         wp[k] += h
         wm[k] -= h
-        Lp, _, _ = G.loss_and_grad(wp, 3, adj, d, r, e, bf16=False)
-        Lm, _, _ = G.loss_and_grad(wm, 3, adj, d, r, e, bf16=False)
+        Lp, _, _ = G.loss_and_grad(wp, 3, adj, d, r, e, K, loss, bf16=False)
+        Lm, _, _ = G.loss_and_grad(wm, 3, adj, d, r, e, K, loss, bf16=False)
         fd = (Lp - Lm) / (2 * h)
         assert abs(fd - g[k]) <= 1e-5 * max(1.0, abs(fd)), (k, fd, g[k])
 

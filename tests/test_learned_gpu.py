@@ -28,6 +28,15 @@ def diag_of(ctx):
     return np.array([v[np.nonzero(ci[: rn[r], r] == r)[0][0], r] for r in range(rn.size)])
 
 
+def csr_of(ctx):
+    import scipy.sparse as sp
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    W, n = ci.shape
+    mask = np.arange(W)[:, None] < rn[None, :]
+    rows = np.broadcast_to(np.arange(n)[None, :], (W, n))
+    return sp.csr_matrix((v[mask], (rows[mask], ci[mask])), shape=(n, n))
+
+
 def random_weights(dim, seed=2, scale=0.25):
     return np.random.default_rng(seed).normal(scale=scale, size=G.offsets(dim)["total"][0])
 
@@ -41,9 +50,12 @@ def test_untrained_network_is_jacobi():
     assert np.allclose(z, r / d, rtol=1e-6, atol=0)
 
 
-def test_forward_and_gradient_match_oracle():
+@pytest.mark.parametrize("loss", ["error", "residual"])
+def test_forward_and_gradient_match_oracle(loss):
     m, ctx = brick8_problem()
     ctx.lp_init(3, seed=1)
+    if loss == "residual":
+        ctx.lp_set_loss(_lib.GF_LP_LOSS_RESIDUAL)
     w = random_weights(3).astype(np.float32)
     ctx.lp_set_weights(w)
     assert np.array_equal(ctx.lp_get_weights(), w)
@@ -51,10 +63,11 @@ def test_forward_and_gradient_match_oracle():
     r = rng.normal(size=m.ndof).astype(np.float32)
     e = rng.normal(size=m.ndof).astype(np.float32)
     d = diag_of(ctx)
+    K = csr_of(ctx)
     adj = G.node_adjacency(m.conn, m.nnodes)
     z_gpu = ctx.lp_apply(r)
     L_ref, g_ref, z_ref = G.loss_and_grad(w.astype(np.float64), 3, adj, d, r.astype(np.float64),
-                                          e.astype(np.float64))
+                                          e.astype(np.float64), K, loss)
     assert np.linalg.norm(z_gpu - z_ref) <= 1e-4 * np.linalg.norm(z_ref)
     L_gpu, g_gpu = ctx.lp_loss_grad(r, e)
     assert abs(L_gpu - L_ref) <= 1e-4 * abs(L_ref)
@@ -65,10 +78,17 @@ def test_forward_and_gradient_match_oracle():
         assert np.linalg.norm(a - b) <= 1e-3 * max(np.linalg.norm(b), 1e-12), name
 
 
-def test_training_reduces_loss():
+@pytest.mark.parametrize("loss,pairs", [(_lib.GF_LP_LOSS_ERROR, "pcg"),
+                                        (_lib.GF_LP_LOSS_RESIDUAL, "pcg"),
+                                        (_lib.GF_LP_LOSS_ERROR, "random")])
+def test_training_reduces_loss(loss, pairs):
     m, ctx = brick8_problem(n=(6, 6, 6))
     ctx.lp_init(3, seed=3)
-    ctx.lp_collect(npairs=24, every=4, tol=1e-8)
+    ctx.lp_set_loss(loss)
+    if pairs == "random":
+        ctx.lp_collect_random(24, seed=11)
+    else:
+        ctx.lp_collect(npairs=24, every=4, tol=1e-8)
     l0 = ctx.lp_train(steps=1, batch=8, lr=1e-3, seed=1)
     l1 = ctx.lp_train(steps=150, batch=8, lr=1e-3, seed=2)
     assert np.isfinite(l1) and l1 < 0.9 * l0, (l0, l1)
@@ -101,6 +121,13 @@ def test_learned_fcg_requires_init():
     with pytest.raises(_lib.GpufemError) as ei:
         ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-8)
     assert ei.value.status == _lib.GF_ERR_STATE
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.lp_set_loss(_lib.GF_LP_LOSS_RESIDUAL)
+    assert ei.value.status == _lib.GF_ERR_STATE
+    ctx.lp_init(3, seed=1)
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.lp_set_loss(7)
+    assert ei.value.status == _lib.GF_ERR_INVALID_ARG
 
 
 def test_coarse_mode_untrained_is_twolevel():
@@ -136,6 +163,29 @@ def test_coarse_mode_trained_and_fallback_converge():
     ctx.lp_set_coarse(False)
     info = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
     assert info.status == _lib.GF_OK and info.fallback == 1
+
+
+def test_random_pairs_are_k_times_error():
+    """lp_collect_random: e white in the D-norm, r = K e.  With the zero network
+    (M = D^-1) the error loss of a pair is sum d (D^-1 K e - e)^2 / sum d e^2, which the
+    oracle evaluates from the same e; the sample mean of d e^2 is 1 per dof."""
+    m, ctx = brick8_problem(n=(5, 4, 4))
+    ctx.lp_init(3, seed=3)
+    ctx.lp_collect_random(4, seed=5)
+    L0 = ctx.lp_train(steps=1, batch=64, lr=1e-12, seed=1)
+    d = diag_of(ctx)
+    K = csr_of(ctx)
+    rng = np.random.default_rng(0)
+    vals = []
+    for _ in range(64):
+        e = rng.standard_normal(m.ndof) / np.sqrt(d)
+        z = (K @ e) / d
+        vals.append(np.sum(d * (z - e) ** 2) / np.sum(d * e * e))
+    assert abs(L0 - np.mean(vals)) <= 0.1 * np.mean(vals), (L0, np.mean(vals))
+    ctx.lp_set_coarse(True)
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.lp_collect_random(4, seed=5)
+    assert ei.value.status == _lib.GF_ERR_UNSUPPORTED
 
 
 def test_coarse_mode_needs_init():
