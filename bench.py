@@ -135,6 +135,22 @@ def cpu_model():
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's own CPU assembly on a bounded sample
 # ---------------------------------------------------------------------------
+class stdout_to_stderr:
+    """The reference's C code reports progress with printf: fd 1 goes to stderr while it
+    runs, so that stdout carries the bench's JSON line alone."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def reference_sample(config: str, steps: int, warmup: int):
     """Time the reference's StiffAlgoCPU (naive, OpenMP critical scatter, FP32 as
     shipped) on a down-scaled copy of the workload; elements/s per step.  Falls
@@ -199,7 +215,8 @@ def run_reference_arm(args):
         return
     steps = max(1, min(args.steps, 5))
     warm = max(1, min(args.warmup, 2))
-    cb = reference_sample(args.config, steps, warm)
+    with stdout_to_stderr():
+        cb = reference_sample(args.config, steps, warm)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": cb["seconds_per_step"] * 1e3, "higher_is_better": True,
@@ -350,14 +367,18 @@ def run_gpu_arm(args):
     for _ in range(args.warmup):
         ctx.assemble(dtype, scatter)
     barrier()
+    # L2 flushes go on the library's stream right before each timed call: its start event
+    # then waits on the flush kernel instead of on the host's first launch of the call
+    lib_stream = torch.cuda.ExternalStream(ctx.stream_handle())
     launches0 = ctx.launches()
     dev_s = []
     split = []   # (geometry kernel, scatter kernel) seconds of each step
     g_s, s_s = C.c_double(), C.c_double()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            flush.zero_()
             torch.cuda.synchronize()
+            with torch.cuda.stream(lib_stream):
+                flush.zero_()
             dev_s.append(ctx.assemble(dtype, scatter))
             _lib.lib.gf_last_assembly_split(ctx.h, C.byref(g_s), C.byref(s_s))
             split.append((g_s.value, s_s.value))
@@ -381,8 +402,9 @@ def run_gpu_arm(args):
     for name, sc, eng in runs:
         ts = []
         for _ in range(max(3, min(args.steps, 10))):
-            flush.zero_()
             torch.cuda.synchronize()
+            with torch.cuda.stream(lib_stream):
+                flush.zero_()
             ts.append(ctx.assemble(dtype, sc, eng))
         variants[name] = {"value": m.nelem / float(np.median(ts)), "unit": UNIT,
                           "ms": float(np.median(ts)) * 1e3}
@@ -421,9 +443,12 @@ def run_gpu_arm(args):
     xs = torch.randn(n, device="cuda", dtype=torch.float32 if esize == 4 else torch.float64)
     ys = torch.empty_like(xs)
     sp = []
+    torch.cuda.synchronize()
     for _ in range(10):
-        flush.zero_()
-        torch.cuda.synchronize()
+        # the flush runs on the library's stream just before the SpMV, so the SpMV's start
+        # event waits on the flush, not on the host's launch of the SpMV
+        with torch.cuda.stream(lib_stream):
+            flush.zero_()
         _lib.check(_lib.lib.gf_spmv(ctx.h, dtype, xs.data_ptr(), ys.data_ptr()), ctx.h)
         sp.append(_lib.lib.gf_last_device_seconds(ctx.h))
     t_spmv = float(np.median(sp))
@@ -528,7 +553,8 @@ def run_gpu_arm(args):
         if (rank == 0 and world == 1 and not args.no_cpu and p64 is not None
                 and cfg in ("q4_64", "q8_512")):
             # (the reference's assembly of the full 3-D meshes alone takes minutes)
-            rc = reference_cg_sample(m)
+            with stdout_to_stderr():
+                rc = reference_cg_sample(m)
             if rc is not None:
                 rc["extrapolated_seconds"] = rc["cg_us_per_iteration"] * 1e-6 * p64.iterations
                 rc["label"] = ("extrapolated: reference CPU_CG (unpreconditioned CG, FP32, OpenMP) "
@@ -542,7 +568,8 @@ def run_gpu_arm(args):
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = reference_sample(cfg, steps=2, warmup=1)
+        with stdout_to_stderr():
+            cb = reference_sample(cfg, steps=2, warmup=1)
         cpu_baseline = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if rank == 0:

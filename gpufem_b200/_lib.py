@@ -54,6 +54,7 @@ SIGNATURES = {
     "gf_last_assembly_split": (I32, [P, C.POINTER(D), C.POINTER(D)]),
     "gf_kernel_launches": (I64, [P]),
     "gf_sync": (I32, [P]),
+    "gf_stream": (I32, [P, C.POINTER(C.c_void_p)]),
     "gf_mesh_create": (I32, [P, I32, I32, P, I32, P, I32, D, P, D, I32]),
     "gf_mesh_set_modulus": (I32, [P, D, P]),
     "gf_mesh_color": (I32, [P, P, C.POINTER(I32)]),

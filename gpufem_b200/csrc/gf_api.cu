@@ -93,6 +93,12 @@ GF_API gf_status gf_sync(gf_ctx* ctx) {
   return GF_OK;
 }
 
+GF_API gf_status gf_stream(gf_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return GF_ERR_INVALID_ARG;
+  *stream = (void*)ctx->stream;
+  return GF_OK;
+}
+
 }  // extern "C"
 
 void gf_mesh_free(gf_ctx* ctx) {

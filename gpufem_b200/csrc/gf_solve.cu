@@ -108,6 +108,20 @@ __device__ inline double row_dot(int64_t o, int64_t stride, int nz, const int32_
   return (double)((a0 + a1) + (a2 + a3));
 }
 
+// x[2b], x[2b + 1] in one 8- or 16-byte load (x is 16-byte aligned: device allocations)
+template <typename Acc>
+__device__ inline void ldg_pair(const float* __restrict__ x, int b, Acc& x0, Acc& x1) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(x) + b);
+  x0 = (Acc)v.x;
+  x1 = (Acc)v.y;
+}
+template <typename Acc>
+__device__ inline void ldg_pair(const double* __restrict__ x, int b, Acc& x0, Acc& x1) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(x) + b);
+  x0 = (Acc)v.x;
+  x1 = (Acc)v.y;
+}
+
 // Node-block slices: thread t computes the DIM rows of node perm[t] (slice k = t / 32,
 // lane l = t % 32).  Per neighbour block it reads one coalesced column word, DIM x DIM
 // coalesced values and DIM consecutive entries of x (once for all DIM rows), and it
@@ -142,7 +156,8 @@ __device__ inline bool node_rows(const MatLayout& L, int t, const TK* __restrict
         if (p < w) {
           const TK* v = vp + p * SS;
           const TK u0 = __ldcs(v), u1 = __ldcs(v + 32), u2 = __ldcs(v + 64), u3 = __ldcs(v + 96);
-          const Acc x0 = (Acc)__ldg(x + (int64_t)bb[p] * 2), x1 = (Acc)__ldg(x + (int64_t)bb[p] * 2 + 1);
+          Acc x0, x1;
+          ldg_pair(x, bb[p], x0, x1);
           acc[0] += (Acc)u0 * x0 + (Acc)u1 * x1;
           acc[1] += (Acc)u2 * x0 + (Acc)u3 * x1;
         }
@@ -442,6 +457,9 @@ gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y) {
   const void* val = nullptr;
   gf_status st = solver_matrix(ctx, dtype, &L, &val);
   if (st != GF_OK) return st;
+  // 2-D node blocks read x in pairs (one 8- or 16-byte load per neighbour node)
+  if (L.bdim == 2 && ((uintptr_t)x % (dtype == GF_F64 ? 16 : 8)) != 0)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "x must be aligned to two entries");
   cudaEventRecord(ctx->ev0, ctx->stream);
   if (dtype == GF_F64)
     k_spmv<double, double, double><<<mat_grid(ctx, L), L.threads, 0, ctx->stream>>>(

@@ -265,6 +265,12 @@ class Context:
     def sync(self) -> None:
         self._c(lib.gf_sync(self.h))
 
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (torch.cuda.ExternalStream takes it)."""
+        h = C.c_void_p()
+        self._c(lib.gf_stream(self.h, C.byref(h)))
+        return int(h.value or 0)
+
 
 # ---------------------------------------------------------------------------
 # Reference-named mirror

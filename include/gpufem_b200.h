@@ -145,6 +145,9 @@ GF_API gf_status gf_last_assembly_split(const gf_ctx* ctx, double* geometry_seco
 GF_API int64_t gf_kernel_launches(const gf_ctx* ctx);
 /* Synchronise the context's stream. */
 GF_API gf_status gf_sync(gf_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work
+ * with the context's: work they enqueue on it runs between the context's calls. */
+GF_API gf_status gf_stream(gf_ctx* ctx, void** stream);
 
 /* ---- mesh (FemData::Init) --------------------------------------------------------
  * coords: nnodes*dim doubles, packed xy / xyz (dim = 2 for Q4/Q8, 3 for bricks).
@@ -218,7 +221,8 @@ GF_API gf_status gf_get_force(gf_ctx* ctx, double* f);
 GF_API gf_status gf_apply_constraints(gf_ctx* ctx, int32_t mode);
 
 /* ---- solve --------------------------------------------------------------------------- */
-/* y = K x on device pointers of dtype `dtype` (x, y: n entries). */
+/* y = K x on device pointers of dtype `dtype` (x, y: n entries; x 16-byte aligned, as
+ * every device allocation is: 2-D meshes read x in pairs, GF_ERR_INVALID_ARG otherwise). */
 GF_API gf_status gf_spmv(gf_ctx* ctx, int32_t dtype, const void* x, void* y);
 /* Host-buffer SpMV (n doubles in, n doubles out), computed in `dtype`. */
 GF_API gf_status gf_spmv_host(gf_ctx* ctx, int32_t dtype, const double* x, double* y);
