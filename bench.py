@@ -265,23 +265,26 @@ def _preconditioner_diagnostic(ctx, ustar):
     return out
 
 
-def learned_comparison(seed_base: int = 20260105, n_train: int = 6):
-    """Brick8 cubes with correlated log-normal E (sigma U(0.5, 2), correlation length
-    U(0.05, 0.3)) and nu U(0.2, 0.4), z = 0 clamped, pressure on z = 1.  The network is
-    trained on small seeded cubes (edge 12..20) and evaluated on held-out cubes (edge
-    24, 32, 40): time and iterations to reach relative residual 1e-8 (error against an FP64
-    PCG solution to 1e-12 reported), for FP64
-    Jacobi-PCG, mixed-precision PCG and learned FCG (with its Jacobi fallback)."""
+def learned_comparison(seed_base: int = 20260105, n_train: int = 48, n_test: int = 16):
+    """Brick8 cubes with edge n uniform in 16..48 elements, correlated log-normal E (sigma
+    U(0.5, 2), correlation length U(0.05, 0.3)) and nu U(0.2, 0.4), z = 0 clamped,
+    pressure on z = 1; n_train seeded training meshes and n_test held-out ones.  The
+    network is trained on pairs from Jacobi-PCG runs on the training meshes (one pass,
+    60 Adam steps per mesh) and compared on the held-out meshes: time and iterations to a
+    true relative residual of 1e-8, and the error against an FP64 PCG solution to 1e-12,
+    for FP64 Jacobi-PCG, mixed-precision PCG, learned FCG (with its Jacobi fallback) and
+    two-level PCG (no learning)."""
     from gpufem_b200 import _lib
     from gpufem_b200 import meshgen as mg
     from gpufem_b200.fem import Context
 
-    def make(nn, seed):
-        m = mg.clamp_and_load(mg.structured(mg.BRICK8, (nn,) * 3, jitter=0.1, seed=seed))
+    def make(seed):
         rs = np.random.default_rng(seed)
+        nn = int(rs.integers(16, 49))
+        m = mg.clamp_and_load(mg.structured(mg.BRICK8, (nn,) * 3, jitter=0.1, seed=seed))
         m.E = mg.lognormal_correlated(m, rs.uniform(0.5, 2.0), rs.uniform(0.05, 0.3), seed)
         m.nu = float(rs.uniform(0.2, 0.4))
-        return m
+        return nn, m
 
     def setup(ctx, m):
         ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
@@ -293,39 +296,44 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 6):
 
     ctx = Context(0)
     ctx.lp_init(3, seed=seed_base)
-    rng = np.random.default_rng(seed_base)
     t0 = time.perf_counter()
     losses = []
-    for epoch in range(2):
-        for k in range(n_train):
-            nn = int(rng.integers(12, 21))
-            m = make(nn, seed_base + 100 + k)
-            setup(ctx, m)
-            ctx.lp_collect(npairs=32, every=8, tol=1e-8)
-            losses.append(ctx.lp_train(steps=60, batch=8, lr=1e-3, seed=seed_base + epoch * 97 + k))
+    for k in range(n_train):
+        _, m = make(seed_base + 100 + k)
+        setup(ctx, m)
+        ctx.lp_collect(npairs=32, every=8, tol=1e-8)
+        losses.append(ctx.lp_train(steps=60, batch=8, lr=1e-3, seed=seed_base + k))
     train_s = time.perf_counter() - t0
     results = []
-    for nn, seed in ((24, seed_base + 901), (32, seed_base + 902), (40, seed_base + 903)):
-        m = make(nn, seed)
+    names = (("pcg_fp64", _lib.GF_SOLVER_PCG), ("mixed_pcg", _lib.GF_SOLVER_MIXED_PCG),
+             ("learned_fcg", _lib.GF_SOLVER_LEARNED_FCG), ("twolevel_pcg", _lib.GF_SOLVER_TWOLEVEL_PCG))
+    for k in range(n_test):
+        nn, m = make(seed_base + 900 + k)
         setup(ctx, m)
         ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-12, max_iter=400000, raise_on_error=False)
         ustar = ctx.solution()
         nrm = np.linalg.norm(ustar)
         row = {"edge": nn, "dofs": m.ndof}
-        for name, solver in (("pcg_fp64", _lib.GF_SOLVER_PCG), ("mixed_pcg", _lib.GF_SOLVER_MIXED_PCG),
-                             ("learned_fcg", _lib.GF_SOLVER_LEARNED_FCG)):
+        for name, solver in names:
             info = ctx.solve(solver, _lib.GF_F64, tol=1e-8, max_iter=400000, raise_on_error=False)
             err = float(np.linalg.norm(ctx.solution() - ustar) / nrm)
             row[name] = {"seconds": info.seconds, "iterations": info.iterations,
                          "rel_err_vs_reference": err, "status": info.status,
                          **({"fallback": info.fallback} if name == "learned_fcg" else {})}
-        if nn == 24:
+        if k == 0:
             row["diagnostic"] = _preconditioner_diagnostic(ctx, ustar)
         results.append(row)
     ctx.close()
-    return {"train_meshes": 2 * n_train, "train_seconds": train_s,
+
+    def ratio(a, b, key):
+        return float(np.median([r[a][key] / r[b][key] for r in results]))
+
+    summary = {f"median_{key}_ratio_{a}_over_pcg_fp64": ratio(a, "pcg_fp64", key)
+               for a in ("learned_fcg", "twolevel_pcg") for key in ("iterations", "seconds")}
+    summary["learned_fcg_fallbacks"] = int(sum(r["learned_fcg"]["fallback"] for r in results))
+    return {"train_meshes": n_train, "held_out_meshes": n_test, "train_seconds": train_s,
             "final_train_loss": losses[-1], "first_train_loss": losses[0],
-            "tol_rel_residual": 1e-8, "held_out": results}
+            "tol_rel_residual": 1e-8, "summary": summary, "held_out": results}
 
 
 # ---------------------------------------------------------------------------
