@@ -287,7 +287,7 @@ GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, fl
  * rows of constrained dofs zero.  P^T K P is assembled and inverted on the device (FP64,
  * regularised by 1e-10 * its largest diagonal entry; a zero diagonal entry becomes 1).  Built
  * for the current FP64 matrix and supports; rebuilt by the next TWOLEVEL_PCG solve after
- * either changes.  target_coarse 0 = 3072; at most 4096.  *ncoarse may be NULL. */
+ * either changes.  target_coarse 0 = n / 128 within [192, 3072]; at most 4096.  *ncoarse may be NULL. */
 GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse, int32_t* ncoarse);
 /* z = M r on HOST vectors of n doubles (builds the coarse space if needed). */
 GF_API gf_status gf_twolevel_apply(gf_ctx* ctx, const double* r, double* z);

@@ -27,6 +27,11 @@ MAX_COARSE = 4096
 DEFAULT_COARSE = 3072
 
 
+def default_target(n: int) -> int:
+    """The library's default coarse size for n dofs: n // 128 within [192, 3072]."""
+    return min(DEFAULT_COARSE, max(192, n // 128))
+
+
 def _lround(v: float) -> int:
     return int(math.floor(v + 0.5)) if v >= 0 else -int(math.floor(-v + 0.5))
 

@@ -41,7 +41,7 @@ def test_aggregates_and_apply_match_oracle(name, scale, target):
     ctx = _ctx(m)
     nc = ctx.twolevel_setup(target)
     agg, side = ctx.twolevel_aggregates()
-    agg_o, side_o = tl.aggregates(m.coords, target if target else tl.DEFAULT_COARSE)
+    agg_o, side_o = tl.aggregates(m.coords, target if target else tl.default_target(m.ndof))
     np.testing.assert_array_equal(agg, agg_o)
     assert side == side_o
     rn, ci, v = ctx.ell_download(_lib.GF_F64)
