@@ -180,3 +180,26 @@ def test_solver_caps_and_errors(Context):
     ctx.set_force(np.zeros(m.ndof))
     info = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-10)
     assert info.iterations == 0 and np.all(ctx.solution() == 0)
+
+
+@pytest.mark.parametrize("dtype", [_lib.GF_F64, _lib.GF_F32])
+def test_spmv_2d_node_blocks_vs_oracle_and_alignment(Context, oracle, dtype):
+    """2-D meshes read x in pairs: K x through gf_spmv against the oracle's ELL SpMV, and a
+    device x that is not aligned to two entries is refused before any launch."""
+    import torch
+    m = mg.workload("q8_512", scale=1 / 32)
+    ctx = Context(0)
+    ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+    ctx.assemble(dtype)
+    rn, ci, v = ctx.ell_download(dtype)
+    tdt = torch.float64 if dtype == _lib.GF_F64 else torch.float32
+    x = torch.randn(m.ndof + 1, dtype=tdt, device="cuda")
+    y = torch.empty(m.ndof, dtype=tdt, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib.gf_spmv(ctx.h, dtype, x.data_ptr(), y.data_ptr()), ctx.h)
+    xh = x[:m.ndof].cpu().numpy().astype(np.float64)
+    yo = oracle.spmv(rn, ci, v.astype(np.float64), xh)
+    tol = 1e-12 if dtype == _lib.GF_F64 else 1e-5
+    assert np.linalg.norm(y.cpu().numpy() - yo) <= tol * np.linalg.norm(yo)
+    st = _lib.lib.gf_spmv(ctx.h, dtype, x[1:].data_ptr(), y.data_ptr())
+    assert st == _lib.GF_ERR_INVALID_ARG
