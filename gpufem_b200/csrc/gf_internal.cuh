@@ -359,15 +359,17 @@ void gf_coarse_apply(gf_ctx* ctx, const double* r, const double* dinv, double* z
 void gf_coarse_add(gf_ctx* ctx, const double* r, double* z);
 // Two-level PCG steps (launches only, capturable).  Begin: x = 0, r = b, p = M r,
 // sc->rr = b.b, sc->rzn = r.M r.  Iterate (after the SpMV q = K p, p.q): x, r update,
-// then p = M r + beta p; the kernels return at once while sc->done != 0.
+// then p = M r + beta p; the kernels return at once while sc->done != 0.  p32 (or
+// null): n floats that receive an FP32 copy of every new p.
 void gf_tl_begin(gf_ctx* ctx, const double* b, double* x, double* r, double* p,
-                 const double* dinv, SolveScalars* sc);
+                 const double* dinv, SolveScalars* sc, float* p32 = nullptr);
 void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q,
-                   const double* dinv, SolveScalars* sc);
+                   const double* dinv, SolveScalars* sc, float* p32 = nullptr);
 // Reliable update: x = 0, r = scale * b, rr and rzn as in begin; then p = M r (restart)
 // or p = pscale * p (direction kept).  sc->rr and sc->rzn must be zero on entry.
 void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
-                 double* x, double* r, double* p, const double* dinv, SolveScalars* sc);
+                 double* x, double* r, double* p, const double* dinv, SolveScalars* sc,
+                 float* p32 = nullptr);
 void gf_lp_mesh_changed(gf_ctx* ctx);
 gf_status gf_lp_prepare(gf_ctx* ctx);
 bool gf_lp_ready(const gf_ctx* ctx);

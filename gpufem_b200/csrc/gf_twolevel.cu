@@ -683,20 +683,24 @@ k_tl_update(int n, const double* __restrict__ bq, double scale, double* __restri
 
 // z = D^-1 r + P zc on the fly.  MODE kTlFirst: p = z; kTlKeep: p = pscale p (a
 // reliable update that keeps the direction); kTlStep: p = z + beta p with
-// beta = rzn / rz, then the iteration count and the convergence test.
+// beta = rzn / rz, then the iteration count and the convergence test.  p32 (or null)
+// receives an FP32 copy of p for SpMVs on the FP32 matrix.
 constexpr int kTlFirst = 0, kTlKeep = 1, kTlStep = 2;
 template <int DIM, int MODE>
 __global__ void __launch_bounds__(kCT)
 k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ dinv,
                const uint8_t* __restrict__ fixed, const int32_t* __restrict__ agg,
                const double* __restrict__ xc, const double* __restrict__ cen, double sinv,
-               const double* __restrict__ zc, double* __restrict__ p, double pscale,
-               SolveScalars* sc) {
+               const double* __restrict__ zc, double* __restrict__ p, float* __restrict__ p32,
+               double pscale, SolveScalars* sc) {
   constexpr int NM = DIM == 2 ? 3 : 6;
   if (sc->done) return;
   if (MODE == kTlKeep) {
-    for (int64_t t = (int64_t)blockIdx.x * kCT + threadIdx.x; t < n; t += (int64_t)gridDim.x * kCT)
-      p[t] *= pscale;
+    for (int64_t t = (int64_t)blockIdx.x * kCT + threadIdx.x; t < n; t += (int64_t)gridDim.x * kCT) {
+      const double pn = p[t] * pscale;
+      p[t] = pn;
+      if (p32) p32[t] = (float)pn;
+    }
     return;
   }
   const double beta = MODE == kTlFirst ? 0.0 : sc->rzn / sc->rz;
@@ -716,7 +720,9 @@ k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ d
 #pragma unroll
       for (int m = 0; m < NM; ++m) zi += pr[m] * zc[A * NM + m];
     }
-    p[i] = MODE == kTlFirst ? zi : zi + beta * p[i];
+    const double pn = MODE == kTlFirst ? zi : zi + beta * p[i];
+    p[i] = pn;
+    if (p32) p32[i] = (float)pn;
   }
   if (MODE == kTlStep && blockIdx.x == 0 && threadIdx.x == 0) {
     sc->pq = 0.0;
@@ -995,7 +1001,8 @@ void gf_coarse_add(gf_ctx* ctx, const double* r, double* z) {
 
 template <int DIM>
 static void tl_launch(gf_ctx* ctx, int mode, const double* bq, double scale, double pscale,
-                      double* x, double* r, double* p, const double* dinv, SolveScalars* sc) {
+                      double* x, double* r, double* p, const double* dinv, SolveScalars* sc,
+                      float* p32) {
   Coarse* c = static_cast<Coarse*>(ctx->coarse);
   cudaStream_t s = ctx->stream;
   const int n = ctx->n;
@@ -1011,38 +1018,39 @@ static void tl_launch(gf_ctx* ctx, int mode, const double* bq, double scale, dou
   if (mode == kTlFirst)
     k_tl_direction<DIM, kTlFirst><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
                                                        ctx->d_coords64, c->cen, sinv, c->zc, p,
-                                                       1.0, sc);
+                                                       p32, 1.0, sc);
   else if (mode == kTlKeep)
     k_tl_direction<DIM, kTlKeep><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
                                                       ctx->d_coords64, c->cen, sinv, c->zc, p,
-                                                      pscale, sc);
+                                                      p32, pscale, sc);
   else
     k_tl_direction<DIM, kTlStep><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
                                                       ctx->d_coords64, c->cen, sinv, c->zc, p,
-                                                      1.0, sc);
+                                                      p32, 1.0, sc);
   ctx->launches += 4;
 }
 
 void gf_tl_begin(gf_ctx* ctx, const double* b, double* x, double* r, double* p,
-                 const double* dinv, SolveScalars* sc) {
-  gf_tl_reset(ctx, b, 1.0, true, 1.0, x, r, p, dinv, sc);
+                 const double* dinv, SolveScalars* sc, float* p32) {
+  gf_tl_reset(ctx, b, 1.0, true, 1.0, x, r, p, dinv, sc, p32);
 }
 
 void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
-                 double* x, double* r, double* p, const double* dinv, SolveScalars* sc) {
+                 double* x, double* r, double* p, const double* dinv, SolveScalars* sc,
+                 float* p32) {
   const int mode = restart ? kTlFirst : kTlKeep;
   if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
-    tl_launch<2>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc);
+    tl_launch<2>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc, p32);
   else
-    tl_launch<3>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc);
+    tl_launch<3>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc, p32);
 }
 
 void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q,
-                   const double* dinv, SolveScalars* sc) {
+                   const double* dinv, SolveScalars* sc, float* p32) {
   if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
-    tl_launch<2>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc);
+    tl_launch<2>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc, p32);
   else
-    tl_launch<3>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc);
+    tl_launch<3>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc, p32);
 }
 
 extern "C" GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse,
