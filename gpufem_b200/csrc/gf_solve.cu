@@ -286,6 +286,11 @@ k_cg_spmv_dot(MatLayout L, const TK* __restrict__ val, const V* __restrict__ p,
   if (threadIdx.x == 0) atomicAdd(&sc->pq, s);
 }
 
+__global__ void k_copy_f32(int n, const double* __restrict__ a, float* __restrict__ b) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
 // q = K32 p on the FP32 matrix from the FP32 copy p32 of the FP64 direction p: FP32
 // products and row sums (no FP64 conversion per matrix entry, which measured 81 against
 // 52 us on Q8 512), q and the p.q dot in FP64.
@@ -343,11 +348,16 @@ k_cg_update(int n, V* __restrict__ x, V* __restrict__ r, V* __restrict__ z,
 
 template <typename V>
 __global__ void __launch_bounds__(kT)
-k_cg_direction(int n, const V* __restrict__ z, V* __restrict__ p, SolveScalars* sc) {
+k_cg_direction(int n, const V* __restrict__ z, V* __restrict__ p, SolveScalars* sc,
+               float* __restrict__ p32 = nullptr) {
   if (sc->done) return;
   const V beta = (V)(sc->rzn / sc->rz);
   const int i = blockIdx.x * kT + threadIdx.x;
-  if (i < n) p[i] = z[i] + beta * p[i];
+  if (i < n) {
+    const V pn = z[i] + beta * p[i];
+    p[i] = pn;
+    if (p32) p32[i] = (float)pn;  // FP32 copy for the K32 SpMV (MIXED_PCG)
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     sc->pq = 0.0;
     sc->iter += 1;
@@ -706,7 +716,8 @@ __global__ void k_mixed_accumulate(int n, double sigma, V* __restrict__ x,
 template <typename V>
 __global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv, V pscale,
                               int restart, const V* __restrict__ dinv, V* __restrict__ r,
-                              V* __restrict__ z, V* __restrict__ p, SolveScalars* sc) {
+                              V* __restrict__ z, V* __restrict__ p, SolveScalars* sc,
+                              float* __restrict__ p32) {
   __shared__ double sh[32];
   double rz = 0.0, rr = 0.0;
   for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
@@ -714,7 +725,9 @@ __global__ void k_mixed_reset(int n, const double* __restrict__ r64, double inv,
     const V zi = ri * dinv[i];
     r[i] = ri;
     z[i] = zi;
-    p[i] = restart ? zi : p[i] * pscale;
+    const V pn = restart ? zi : p[i] * pscale;
+    p[i] = pn;
+    if (p32) p32[i] = (float)pn;
     rz += (double)ri * (double)zi;
     rr += (double)ri * (double)ri;
   }
@@ -767,8 +780,10 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   if (twolevel && sizeof(V) != sizeof(double))
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "two-level mixed solve runs on FP64 vectors");
   if (twolevel && (st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
-  // the two-level recursion never stores z: its room holds the FP32 copy of p
-  float* p32 = twolevel ? reinterpret_cast<float*>(z) : nullptr;
+  // FP32 copy of the FP64 direction for the K32 SpMV: the two-level recursion never
+  // stores z, so its room holds it; Jacobi uses the work area past dinv (10 n doubles)
+  float* p32 = sizeof(V) != sizeof(double) ? nullptr
+               : twolevel ? reinterpret_cast<float*>(z) : reinterpret_cast<float*>(v + 6 * (size_t)n);
   k_diag_inv<double, V><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_LAUNCH_CHECK(ctx, "k_diag_inv");
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u, 0, sizeof(double) * n, s));
@@ -789,6 +804,10 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       GF_LAUNCH_CHECK(ctx, "k_scale_to");
       k_cg_init<V><<<red_grid(ctx, n), kT, 0, s>>>(n, q, dinv, x, r, z, p, sc);
       GF_LAUNCH_CHECK(ctx, "k_cg_init");
+      if (p32) {
+        k_copy_f32<<<nb, kT, 0, s>>>(n, (const double*)p, p32);
+        GF_LAUNCH_CHECK(ctx, "k_copy_f32");
+      }
     }
     k_cg_init_fin<<<1, 1, 0, s>>>(sc, tol, maxit);
     GF_LAUNCH_CHECK(ctx, "k_cg_init_fin");
@@ -803,9 +822,13 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
         gf_tl_iterate(ctx, (double*)x, (double*)r, (double*)p, (const double*)q,
                       (const double*)dinv, sc, p32);
       } else {
-        k_cg_spmv_dot<float, V><<<mat_grid(ctx, L32), L32.threads, 0, s>>>(L32, val32, p, q, sc);
+        if (p32)
+          k_cg_spmv_dot_x32<<<mat_grid(ctx, L32), L32.threads, 0, s>>>(
+              L32, val32, p32, (const double*)p, (double*)q, sc);
+        else
+          k_cg_spmv_dot<float, V><<<mat_grid(ctx, L32), L32.threads, 0, s>>>(L32, val32, p, q, sc);
         k_cg_update<V><<<red_grid(ctx, n), kT, 0, s>>>(n, x, r, z, p, q, dinv, sc);
-        k_cg_direction<V><<<nb, kT, 0, s>>>(n, z, p, sc);
+        k_cg_direction<V><<<nb, kT, 0, s>>>(n, z, p, sc, p32);
       }
     }
     const int64_t per_chunk = twolevel ? ctx->launches - l0 + check : 3 * (int64_t)check;
@@ -871,7 +894,7 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       else
         k_mixed_reset<V><<<red_grid(ctx, n), kT, 0, s>>>(n, r64, 1.0 / sigma_new,
                                                          (V)(sigma / sigma_new), restart ? 1 : 0,
-                                                         dinv, r, z, p, sc);
+                                                         dinv, r, z, p, sc, p32);
       ce = cudaGetLastError();
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "k_mixed_reset"); break; }
       ctx->launches += twolevel ? 1 : 2;  // gf_tl_reset counts its own
@@ -1210,8 +1233,6 @@ gf_status gf_pcg_record(gf_ctx* ctx, const double* ustar, int npairs, int every,
   const void* vk = nullptr;
   if ((st = solver_matrix(ctx, GF_F64, &L, &vk)) != GF_OK) return st;
   if (twolevel && (st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
-  // the two-level recursion never stores z: its room holds the FP32 copy of p
-  float* p32 = twolevel ? reinterpret_cast<float*>(z) : nullptr;
   k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, dinv);
   GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
   if (twolevel) gf_tl_begin(ctx, ctx->d_f, x, r, p, dinv, sc);
