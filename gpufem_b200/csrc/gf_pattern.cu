@@ -49,7 +49,9 @@ __global__ void k_fill_incidence(int64_t total, int nen, const int32_t* __restri
 
 // Warp per node: collect the nodes of all incident elements, then for each
 // first occurrence compute its rank among distinct values.  mode 0 counts,
-// mode 1 writes adj[adj_off[node] + rank].
+// mode 1 writes adj[adj_off[node] + rank].  With at most 32 candidates (every 2-D
+// element type) a lane holds one: __match_any_sync finds the first occurrences and
+// shuffles rank them, in registers; more candidates go through shared memory.
 template <int MODE>
 __global__ void k_node_adjacency(int nnodes, int nen, const int32_t* __restrict__ conn,
                                  const int32_t* __restrict__ inc_off,
@@ -65,6 +67,24 @@ __global__ void k_node_adjacency(int nnodes, int nen, const int32_t* __restrict_
   uint8_t* fl = firstf[warp];
   const int e0 = inc_off[node], e1 = inc_off[node + 1];
   const int C = (e1 - e0) * nen;
+  if (C <= 32) {
+    const bool act = lane < C;
+    const int v = act ? conn[(int64_t)inc[e0 + lane / nen] * nen + lane % nen] : 0x7fffffff;
+    const unsigned same = __match_any_sync(0xffffffffu, v);
+    const bool first = act && (__ffs(same) - 1) == lane;
+    const unsigned firsts = __ballot_sync(0xffffffffu, first);
+    if (MODE == 0) {
+      if (lane == 0) nadj[node] = __popc(firsts);
+    } else {
+      int rank = 0;
+      for (int q = 0; q < 32; ++q) {
+        const int vq = __shfl_sync(0xffffffffu, v, q);
+        rank += ((firsts >> q) & 1u) && vq < v ? 1 : 0;
+      }
+      if (first) adj[adj_off[node] + rank] = v;
+    }
+    return;
+  }
   if (C > kCandCap) {
     if (lane == 0) atomicExch(errflag, 1);
     return;
