@@ -213,20 +213,65 @@ k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
     double da[DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) da[c] = (x[(int64_t)ra + c] - cA[c]) * sinv;
+    double pa[DIM][NM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      p_row<DIM>(c, da, pa[c]);
+      if (fixed[ra + c]) {
+#pragma unroll
+        for (int m = 0; m < NM; ++m) pa[c][m] = 0.0;
+      }
+    }
+    // K_ab P_b summed over consecutive neighbours b of one aggregate (the columns are
+    // sorted, so neighbours in one box come in runs); P_a^T times the sum is added once
+    // per run: into registers for B = A, else into the table (or Ac)
+    int curB = -1;
+    double S[DIM][NM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c)
+#pragma unroll
+      for (int m = 0; m < NM; ++m) S[c][m] = 0.0;
+    auto flush = [&](int Bx) {
+      if (Bx == A) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+          for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int m2 = 0; m2 < NM; ++m2) acc[m][m2] += pa[c][m] * S[c][m2];
+      } else if (Bx >= 0) {
+        const int sl = tab_slot(ids, Bx);
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+#pragma unroll
+          for (int m2 = 0; m2 < NM; ++m2) {
+            double v = 0.0;
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) v += pa[c][m] * S[c][m2];
+            if (v == 0.0) continue;
+            if (sl >= 0) atomicAdd(&tab[sl][m * NM + m2], v);
+            else atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + Bx * NM + m2], v);
+          }
+        }
+      }
+    };
     const int nzb = rownnz[ra] / DIM;
     for (int p = 0; p < nzb; ++p) {
       const int b = colidx[(int64_t)(p * DIM) * n + ra] / DIM;
       const int B = agg[b];
+      if (B != curB) {
+        flush(curB);
+        curB = B;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+          for (int m = 0; m < NM; ++m) S[c][m] = 0.0;
+      }
       double db[DIM];
 #pragma unroll
       for (int c = 0; c < DIM; ++c)
         db[c] = (x[(int64_t)b * DIM + c] - cen[(int64_t)B * DIM + c]) * sinv;
-      // KPb[c][m] = sum_c2 K_ab[c][c2] P_b[c2][m]
-      double KPb[DIM][NM];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c)
-#pragma unroll
-        for (int m = 0; m < NM; ++m) KPb[c][m] = 0.0;
+      // S[c][m] += sum_c2 K_ab[c][c2] P_b[c2][m]
 #pragma unroll
       for (int c2 = 0; c2 < DIM; ++c2) {
         if (fixed[b * DIM + c2]) continue;
@@ -234,43 +279,13 @@ k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
         p_row<DIM>(c2, db, pr);
 #pragma unroll
         for (int c = 0; c < DIM; ++c) {
-          const double k = K[(int64_t)(p * DIM + c2) * n + ra + c];
+          const double kv = K[(int64_t)(p * DIM + c2) * n + ra + c];
 #pragma unroll
-          for (int m = 0; m < NM; ++m) KPb[c][m] += k * pr[m];
-        }
-      }
-      double pa[DIM][NM];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        p_row<DIM>(c, da, pa[c]);
-        if (fixed[ra + c]) {
-#pragma unroll
-          for (int m = 0; m < NM; ++m) pa[c][m] = 0.0;
-        }
-      }
-      if (B == A) {
-#pragma unroll
-        for (int c = 0; c < DIM; ++c)
-#pragma unroll
-          for (int m = 0; m < NM; ++m)
-#pragma unroll
-            for (int m2 = 0; m2 < NM; ++m2) acc[m][m2] += pa[c][m] * KPb[c][m2];
-      } else {
-        const int sl = tab_slot(ids, B);
-#pragma unroll
-        for (int m = 0; m < NM; ++m) {
-#pragma unroll
-          for (int m2 = 0; m2 < NM; ++m2) {
-            double v = 0.0;
-#pragma unroll
-            for (int c = 0; c < DIM; ++c) v += pa[c][m] * KPb[c][m2];
-            if (v == 0.0) continue;
-            if (sl >= 0) atomicAdd(&tab[sl][m * NM + m2], v);
-            else atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
-          }
+          for (int m = 0; m < NM; ++m) S[c][m] += kv * pr[m];
         }
       }
     }
+    flush(curB);
   }
   // the (A, A) block: warp sums, then one pass over the warps' partials
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
