@@ -64,3 +64,10 @@ def test_twolevel_pcg_matches_jacobi_pcg(oracle, name, scale):
     u, it_2 = pc.pcg(f, 1e-12)
     assert np.linalg.norm(u - ustar) <= 1e-8 * np.linalg.norm(ustar)
     assert it_2 * 2 < it_j, (it_2, it_j)
+
+
+@pytest.mark.parametrize("n,expect", [(0, 192), (8450, 192), (46875, 366), (206763, 1615),
+                                      (393216, 3072), (1576962, 3072)])
+def test_default_coarse_target(n, expect):
+    """The library's default coarse size: n / 128 within [192, 3072]."""
+    assert tl.default_target(n) == expect
