@@ -55,3 +55,21 @@ def test_no_gpu_reports_cuda_error_without_crashing():
     # null-context calls fail cleanly
     assert _lib.lib.gf_assemble(None, 0, 0, 0) == _lib.GF_ERR_INVALID_ARG
     assert _lib.lib.gf_solve(None, None, None) == _lib.GF_ERR_INVALID_ARG
+
+
+def test_every_context_entry_point_rejects_a_null_context():
+    """Each gf_status entry point whose first parameter is the context returns
+    GF_ERR_INVALID_ARG for a null context (zero / null for the other arguments)."""
+    from gpufem_b200 import _lib
+    txt = (ROOT / "include" / "gpufem_b200.h").read_text()
+    checked = 0
+    for name, args in re.findall(r"GF_API\s+gf_status\s+(gf_\w+)\s*\(([^)]*)\)", txt):
+        first = args.split(",")[0].strip()
+        if not re.match(r"(const\s+)?gf_ctx\s*\*\s*\w+$", first):
+            continue
+        _, argtypes = _lib.SIGNATURES[name]
+        vals = [t(0) if t in (C.c_double, C.c_float, C.c_int32, C.c_int64, C.c_uint64) else None
+                for t in argtypes]
+        assert getattr(_lib.lib, name)(*vals) == _lib.GF_ERR_INVALID_ARG, name
+        checked += 1
+    assert checked >= 35
