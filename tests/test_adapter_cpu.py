@@ -1,8 +1,9 @@
-"""The reference-side strategy (tests/adapter/StiffAlgoCUDA.h) compiles and links against
-the reference's own headers and CPU library (the oracle build of its sources) and
-libgpufem_b200, and runs: it reads a neutral file with the reference's FileIO,
-initialises the reference's FemData and calls CalcGlobalStiffness.  Without a GPU the
-C-ABI reports GF_ERR_CUDA at gf_create and the strategy's calls fail cleanly."""
+"""The reference-side classes (tests/adapter/StiffAlgoCUDA.h, ELLmatrixCUDA.h) compile and
+link against the reference's own headers and CPU library (the oracle build of its
+sources) and libgpufem_b200, and run: the driver reads a neutral file with the
+reference's FileIO, initialises the reference's FemData, calls CalcGlobalStiffness and
+uses K through the SPRmatrix interface.  Without a GPU the C-ABI reports GF_ERR_CUDA at
+gf_create and every call fails cleanly."""
 import os
 import subprocess
 from pathlib import Path
@@ -39,8 +40,10 @@ def test_strategy_builds_against_reference_and_runs(tmp_path):
     create = int(lines["create"])
     if create == _lib.GF_OK:      # a GPU: the strategy assembled the reference's mesh
         assert int(lines["assemble"].split()[0]) == _lib.GF_OK
-        n, w = map(int, lines["ell"].split())
-        assert n == m.ndof and w > 0
+        n, nnz = map(int, lines["ell"].split())
+        assert n == m.ndof and nnz > 0
+        assert float(lines["k00"]) > 0 and float(lines["rigid"]) < 1e-4
     else:
         assert create == _lib.GF_ERR_CUDA
         assert int(lines["assemble"].split()[0]) == _lib.GF_ERR_INVALID_ARG
+        assert lines["ell"].split() == ["0", "0"]
