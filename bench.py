@@ -32,8 +32,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "elems/s assembled"
-SOLVERS = ["reference", "pcg_fp64", "mixed_pcg", "mixed_pcg32", "twolevel_pcg", "twolevel_pcg_k32",
-           "learned"]
+SOLVERS = ["pcg_fp64", "mixed_pcg", "mixed_pcg32", "twolevel_pcg", "twolevel_pcg_k32", "learned"]
 UNIT = "elements/s"
 WORKLOADS = {
     # name: (description, dtype of the timed assembly)
@@ -151,13 +150,12 @@ class stdout_to_stderr:
         return False
 
 
-def reference_sample(config: str, steps: int, warmup: int):
+def reference_sample(config: str, steps: int, warmup: int, scale: float = 1.0):
     """Time the reference's StiffAlgoCPU (naive, OpenMP critical scatter, FP32 as
-    shipped) on a down-scaled copy of the workload; elements/s per step.  Falls
+    shipped) on the workload mesh (scale 1: the full mesh); elements/s per step.  Falls
     back to the single-threaded C oracle port when the reference build is absent."""
     from gpufem_b200 import meshgen as mg
     from oracle.oracle import Oracle, Reference
-    scale = {"q8_512": 1 / 4, "q4_64": 1.0, "brick8_128": 1 / 4, "brick20_64": 1 / 4}[config]
     m = mg.workload(config, scale=scale)
     cores = os.cpu_count() or 1
     times = []
@@ -170,8 +168,10 @@ def reference_sample(config: str, steps: int, warmup: int):
             if i >= warmup:
                 times.append(t)
         s.close()
-        sample = (f"{mg.NAMES[m.elem_type]} {'x'.join(map(str, m.n))} ({m.nelem} elements, "
-                  f"scalar E): reference StiffAlgoCPU naive, FP32, {cores} OpenMP threads")
+        sample = (f"{mg.NAMES[m.elem_type]} {'x'.join(map(str, m.n))} ({m.nelem} elements): "
+                  f"reference StiffAlgoCPU naive, FP32, {cores} OpenMP threads, {steps} steps "
+                  f"after {warmup} warm-up; E scalar (the reference's FemData holds one "
+                  f"modulus; Ke scales linearly in E, so the work per element is the same)")
     else:
         kind = "port"
         cores = 1
@@ -184,7 +184,7 @@ def reference_sample(config: str, steps: int, warmup: int):
                 times.append(time.perf_counter() - t0)
         sample = (f"{mg.NAMES[m.elem_type]} {'x'.join(map(str, m.n))} ({m.nelem} elements): "
                   f"C oracle port, FP64, 1 thread")
-    t = float(np.median(times))
+    t = float(np.mean(times))   # whole-run throughput, as the GPU arm reports it
     return {"value": m.nelem / t, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
             "cpu": cpu_model(), "seconds_per_step": t}
 
@@ -209,23 +209,207 @@ def reference_cg_sample(m, iters: int = 20):
             "cg_iterations_timed": iters, "threads": cores, "cpu": cpu_model()}
 
 
+def workload_config(cfg: str, m, world: int) -> dict:
+    """The `config` object both arms print for workload `cfg` (mesh-derived only)."""
+    return {"workload": cfg, "description": WORKLOADS[cfg], "elements": m.nelem,
+            "nodes": m.nnodes, "dofs": m.ndof, "parallelism": f"replicas x{world}"}
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_info()
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 5))
-    warm = max(1, min(args.warmup, 2))
+    from gpufem_b200 import meshgen as mg
+    steps, warm = args.steps, args.warmup
     with stdout_to_stderr():
         cb = reference_sample(args.config, steps, warm)
+    m = mg.workload(args.config)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": cb["seconds_per_step"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.config, "description": WORKLOADS[args.config]},
+            "config": workload_config(args.config, m, args.gpus),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def host_recheck(ctx, u_hi, u_lo):
+    """Host-side check of the device-certified solution u* = u_hi + u_lo on the full
+    system: the oracle's double-double residual (C restatement, one thread) and the
+    reference's own FP64 ELLmatrix::Axy (ELLmatrix.cc:194-204, FP64 build, all cores) on
+    the downloaded K64.  The FP64 residual of fl(u*) cannot fall below the FP64 rounding
+    of K u (about eps * || |K| |u| || / ||f||), which is reported beside it."""
+    from gpufem_b200 import _lib
+    from oracle.oracle import Oracle, Reference
+    t0 = time.perf_counter()
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    f = ctx.get_force()
+    fn = float(np.linalg.norm(f))
+    out = {"download_seconds": time.perf_counter() - t0}
+    _, nrm = Oracle().residual_dd(rn, ci, v, f, u_hi, u_lo)
+    out["oracle_dd_rel_residual"] = nrm / fn
+    if Reference.available("fp64"):
+        cores = os.cpu_count() or 1
+        with stdout_to_stderr():
+            y, t = Reference("fp64").ell_axy(rn, ci, v, u_hi, nthreads=cores)
+        out["reference_axy_fp64_rel_residual"] = float(np.linalg.norm(f - y) / fn)
+        out["reference_axy_seconds"] = t
+        ku = np.zeros(rn.size)
+        au = np.abs(u_hi)
+        for j in range(ci.shape[0]):       # || |K| |u| || by slots, for the FP64 floor
+            live = np.nonzero(j < rn)[0]
+            ku[live] += np.abs(v[j, live]) * au[ci[j, live]]
+        out["fp64_roundoff_floor"] = float(np.finfo(np.float64).eps * np.linalg.norm(ku) / fn)
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
+# ---------------------------------------------------------------------------
+# solves to an error target against a certified solution
+# ---------------------------------------------------------------------------
+SOLVER_TABLE = {
+    # name: (solver, matrix dtype, uses the two-level set-up, label)
+    "pcg_fp64": ("GF_SOLVER_PCG", "GF_F64", False, "FP64 Jacobi-PCG"),
+    "mixed_pcg": ("GF_SOLVER_MIXED_PCG", "GF_F32", False,
+                  "Jacobi-PCG on K32, FP64 vectors, FP64 reliable updates on K64"),
+    "mixed_pcg32": ("GF_SOLVER_MIXED_PCG32", "GF_F32", False,
+                    "Jacobi-PCG on K32, FP32 vectors, FP64 reliable updates on K64"),
+    "twolevel_pcg": ("GF_SOLVER_TWOLEVEL_PCG", "GF_F64", True,
+                     "FP64 PCG, M = Jacobi + rigid-body modes of box aggregates"),
+    "twolevel_pcg_k32": ("GF_SOLVER_TWOLEVEL_PCG", "GF_F32", True,
+                         "two-level PCG with K32 SpMVs, FP64 vectors, reliable updates on K64"),
+}
+
+
+def time_to_error(ctx, solver, matrix, ustar, target, max_iter=400000):
+    """Solve with stopping tolerances target x (1, 0.3, 0.1, ...) until the relative
+    error against the certified solution is <= target; the run that first meets it is
+    the result (its device time and iterations).  Returns the result and every run."""
+    from gpufem_b200 import _lib
+    nrm = float(np.linalg.norm(ustar))
+    runs = []
+    for fac in (1.0, 0.3, 0.1, 0.03, 0.01, 3e-3, 1e-3, 3e-4, 1e-4, 3e-5, 1e-5):
+        tol = max(target * fac, 1e-14)
+        info = ctx.solve(solver, matrix, tol=tol, max_iter=max_iter, inner_tol=1e-4,
+                         raise_on_error=False)
+        err = float(np.linalg.norm(ctx.solution() - ustar) / nrm)
+        runs.append({"tol": tol, "seconds": info.seconds, "iterations": info.iterations,
+                     "rel_err": err, "rel_residual": info.rel_residual, "status": info.status,
+                     "outer": info.outer, "fallback": info.fallback})
+        if (err <= target and info.status == _lib.GF_OK) or tol <= 1e-14:
+            break
+    best = dict(runs[-1])
+    best["met"] = bool(best["rel_err"] <= target and best["status"] == _lib.GF_OK)
+    best["runs"] = runs
+    return best
+
+
+def solve_study(ctx, target, solvers, asm_seconds):
+    """Every solver on the context's constrained system (K64 and K32, f set), to a
+    relative error <= target against u* = the double-double refined solution (two-level
+    FP64 PCG corrections, residual certified by gf_residual_dd and rechecked on the host).
+    Totals add the assembly (asm_seconds: {"f64": s, "f32": s}), the solver layout build,
+    the two-level set-up where used, and the solve."""
+    from gpufem_b200 import _lib
+    out = {"target_rel_error": target}
+    # the solver layout (sliced copies of K64 and K32) is built by the first product;
+    # build it once here so that every solve below is timed alike
+    x = np.zeros(ctx.n)
+    t0 = time.perf_counter()
+    ctx.spmv(x, _lib.GF_F64)
+    ctx.spmv(x, _lib.GF_F32)
+    layout_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    nc = ctx.twolevel_setup(0)
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    u_hi, u_lo, rinfo = ctx.refine_dd(_lib.GF_SOLVER_TWOLEVEL_PCG, inner_tol=1e-9, target=1e-17)
+    out["reference_solution"] = {
+        "how": "double-double iterative refinement: r = f - K64 (u_hi + u_lo) by "
+               "gf_residual_dd, corrections by FP64 two-level PCG to 1e-9",
+        "rel_residual_dd": rinfo["rel_residual_history"][-1],
+        "rel_residual_history": rinfo["rel_residual_history"],
+        "last_correction_rel": rinfo["correction_history"][-1] if rinfo["correction_history"]
+        else None,
+        "seconds": time.perf_counter() - t0}
+    out["layout_seconds"] = layout_s
+    out["twolevel_setup_seconds"] = setup_s
+    out["coarse_unknowns"] = nc
+    ustar = u_hi
+    rank, world, _ = dist_info()
+    if rank == 0 and world == 1:
+        out["reference_solution"]["host_recheck"] = host_recheck(ctx, u_hi, u_lo)
+    base = None
+    for name in solvers:
+        sv, mt, tl, label = SOLVER_TABLE[name]
+        mt_v = getattr(_lib, mt)
+        r = time_to_error(ctx, getattr(_lib, sv), mt_v, ustar, target)
+        asm = asm_seconds["f64"] + (asm_seconds.get("convert", 0.0) if mt_v == _lib.GF_F32 else 0)
+        r["label"] = label
+        r["total_seconds"] = asm + layout_s + (setup_s if tl else 0.0) + r["seconds"]
+        r["total_includes"] = ("FP64 assembly" + (" + FP32 copy" if mt_v == _lib.GF_F32 else "")
+                               + " + solver layout" + (" + two-level set-up" if tl else "")
+                               + " + solve")
+        out[name] = r
+        if name == "pcg_fp64":
+            base = r["total_seconds"]
+    if base:
+        out["speedup_total_vs_pcg_fp64"] = {k: base / out[k]["total_seconds"]
+                                            for k in solvers if k != "pcg_fp64"}
+    return out
+
+
+def north_star_study(args, flush):
+    """Brick20 64^3 (the north-star workload): FP32 and FP64 assembly in every schedule,
+    then every solver to FP64-oracle relative error 1e-6 with totals against FP64
+    Jacobi-PCG."""
+    import torch
+    from gpufem_b200 import _lib
+    from gpufem_b200 import meshgen as mg
+    from gpufem_b200.fem import Context
+    m = mg.workload("brick20_64")
+    ctx = Context(0)
+    lib_stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+    n, W, nnz = ctx.build_pattern()
+    ctx.color(None)
+    ctx.set_supports(m.supports)
+    ctx.set_force(m.f)
+
+    def timed(dtype, scatter, engine=0, reps=3):
+        ctx.assemble(dtype, scatter, engine)
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            with torch.cuda.stream(lib_stream):
+                flush.zero_()
+            ts.append(ctx.assemble(dtype, scatter, engine))
+        return float(np.median(ts))
+
+    asm = {}
+    for dname, dt in (("f32", _lib.GF_F32), ("f64", _lib.GF_F64)):
+        for sname, sc in (("auto", _lib.GF_SCATTER_AUTO), ("owner", _lib.GF_SCATTER_OWNER),
+                          ("atomic", _lib.GF_SCATTER_ATOMIC), ("colour", _lib.GF_SCATTER_COLOR)):
+            t = timed(dt, sc)
+            asm[f"{dname}_{sname}"] = {"ms": t * 1e3, "elements_per_s": m.nelem / t}
+    # the system solved: FP64 assembly (AUTO), its FP32 rounding, elimination BCs
+    t_f64 = asm["f64_auto"]["ms"] * 1e-3
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_AUTO)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.convert_f64_to_f32()
+    ctx.sync()
+    t_conv = time.perf_counter() - t0
+    ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
+    solvers = [x for x in args.solvers.split(",") if x in SOLVER_TABLE]
+    study = solve_study(ctx, 1e-6, solvers, {"f64": t_f64, "convert": t_conv})
+    ctx.close()
+    return {"workload": "brick20_64", "description": WORKLOADS["brick20_64"],
+            "elements": m.nelem, "dofs": n, "nnz": nnz, "ell_width": W,
+            "assembly": asm, "fp32_copy_seconds": t_conv, "solve": study,
+            "l2": "flushed (256 MB write) before each timed assembly"}
 
 
 # ---------------------------------------------------------------------------
@@ -401,6 +585,24 @@ def run_gpu_arm(args):
     per_step = total / args.steps
     value = world * m.nelem / per_step
 
+    # the same metric with the symbolic phase inside each step: pattern build (node
+    # incidence, adjacency, ELL columns) + assembly, host wall time around both with the
+    # device synchronised, as the reference's timed StiffAlgoCPU inserts its entries
+    pat_t = []
+    for _ in range(max(3, min(args.steps, 10))):
+        torch.cuda.synchronize()
+        with torch.cuda.stream(lib_stream):
+            flush.zero_()
+        ctx.sync()
+        t0 = time.perf_counter()
+        ctx.build_pattern()
+        ctx.assemble(dtype, scatter)
+        ctx.sync()
+        pat_t.append(time.perf_counter() - t0)
+    with_pattern = {"value": world * m.nelem / float(np.median(pat_t)), "unit": UNIT,
+                    "ms_per_step": float(np.median(pat_t)) * 1e3,
+                    "includes": "gf_ell_build_pattern + gf_assemble, host wall time"}
+
     # the three scatter schedules side by side (median of a few steps each)
     variants = {}
     runs = [("owner", _lib.GF_SCATTER_OWNER, 0), ("colour", _lib.GF_SCATTER_COLOR, 0),
@@ -497,74 +699,35 @@ def run_gpu_arm(args):
     h2d = m.coords.nbytes + m.conn.nbytes + (m.E.nbytes if m.E is not None else 0)
     d2h = n * 4 + n * W * 4 + n * W * esize
 
-    # solve: every solver on the same problem, to a true relative residual of 1e-8
+    # solve: every solver on the same problem, to a relative error against the certified
+    # solution (1e-8 for the 2-D workloads, 1e-6 for the 3-D ones)
     solve = None
     solvers = [x for x in args.solvers.split(",") if x]
     unknown = set(solvers) - set(SOLVERS)
     if unknown:
         raise SystemExit(f"unknown solver(s) {sorted(unknown)}; choose from {SOLVERS}")
-    if not args.no_solve and any(x != "learned" for x in solvers):
+    if not args.no_solve and any(x in SOLVER_TABLE for x in solvers):
         ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
         ctx.set_supports(m.supports)
         ctx.set_force(m.f)
-        ctx.assemble(_lib.GF_F64, scatter)
+        t_f64 = ctx.assemble(_lib.GF_F64, scatter)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         ctx.convert_f64_to_f32()     # symmetric FP32 copy for the mixed solvers
+        ctx.sync()
+        t_conv = time.perf_counter() - t0
         ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
-        solve = {"tol": 1e-8}
-        ustar = nrm = None
-        if "reference" in solvers:
-            # FP64 PCG stops on its recursive residual; on this system (log-normal E) the
-            # true residual it can reach is ~5e-10, so the comparison runs at 1e-8
-            ref = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-12, max_iter=400000,
-                            raise_on_error=False)
-            ustar = ctx.solution()
-            nrm = np.linalg.norm(ustar)
-            solve["reference_solution"] = {"solver": "FP64 Jacobi-PCG to 1e-12",
-                                           "rel_residual": ref.rel_residual,
-                                           "iterations": ref.iterations, "seconds": ref.seconds}
-
-        def record(name, info, **extra):
-            d = {"seconds": info.seconds, "iterations": info.iterations, "status": info.status,
-                 "rel_residual": info.rel_residual, **extra}
-            if ustar is not None:
-                d["rel_err_vs_reference"] = float(np.linalg.norm(ctx.solution() - ustar) / nrm)
-            solve[name] = d
-
-        p64 = None
-        if "pcg_fp64" in solvers:
-            p64 = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-8, max_iter=400000,
-                            raise_on_error=False)
-            record("pcg_fp64", p64)
-        for name, solver in (("mixed_pcg", _lib.GF_SOLVER_MIXED_PCG),
-                             ("mixed_pcg32", _lib.GF_SOLVER_MIXED_PCG32)):
-            if name in solvers:
-                mix = ctx.solve(solver, tol=1e-8, max_iter=400000, inner_tol=1e-4,
-                                raise_on_error=False)
-                record(name, mix, outer=mix.outer, fp64_fallback=mix.fallback)
-        if "twolevel_pcg" in solvers or "twolevel_pcg_k32" in solvers:
-            # two-level PCG: coarse-space build (aggregation, P^T K P, inverse; host wall
-            # time, synchronised) timed apart from the solves that use it
-            t0 = time.perf_counter()
-            nc = ctx.twolevel_setup(0)
-            tl_setup = time.perf_counter() - t0
-        if "twolevel_pcg" in solvers:
-            tl = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, tol=1e-8, max_iter=400000,
-                           raise_on_error=False)
-            record("twolevel_pcg", tl, setup_seconds=tl_setup,
-                   seconds_with_setup=tl_setup + tl.seconds, coarse_unknowns=nc,
-                   label="FP64 PCG, M = Jacobi + rigid-body modes of box aggregates")
-        if "twolevel_pcg_k32" in solvers:
-            tl32 = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, _lib.GF_F32, tol=1e-8, max_iter=400000,
-                             raise_on_error=False)
-            record("twolevel_pcg_k32", tl32, outer=tl32.outer, fp64_fallback=tl32.fallback,
-                   label="two-level PCG with K32 SpMVs, FP64 vectors, reliable updates on K64")
-        if (rank == 0 and world == 1 and not args.no_cpu and p64 is not None
+        target = 1e-8 if m.dim == 2 else 1e-6
+        solve = solve_study(ctx, target, [x for x in solvers if x in SOLVER_TABLE],
+                            {"f64": t_f64, "convert": t_conv})
+        if (rank == 0 and world == 1 and not args.no_cpu and "pcg_fp64" in solve
                 and cfg in ("q4_64", "q8_512")):
             # (the reference's assembly of the full 3-D meshes alone takes minutes)
             with stdout_to_stderr():
                 rc = reference_cg_sample(m)
             if rc is not None:
-                rc["extrapolated_seconds"] = rc["cg_us_per_iteration"] * 1e-6 * p64.iterations
+                its = solve["pcg_fp64"]["iterations"]
+                rc["extrapolated_seconds"] = rc["cg_us_per_iteration"] * 1e-6 * its
                 rc["label"] = ("extrapolated: reference CPU_CG (unpreconditioned CG, FP32, OpenMP) "
                                "time per iteration on the full system x the FP64 Jacobi-PCG "
                                "iteration count above; assembly timed once on the full mesh")
@@ -573,6 +736,12 @@ def run_gpu_arm(args):
     learned = None
     if not args.no_solve and rank == 0 and "learned" in solvers:
         learned = learned_comparison()
+
+    north_star = None
+    if (not args.no_solve and not args.no_north_star and rank == 0 and world == 1
+            and cfg == "q8_512"):
+        ctx.close()                  # free the Q8 matrices before the Brick20 64^3 study
+        north_star = north_star_study(args, flush)
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -586,9 +755,11 @@ def run_gpu_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if esize == 4 else "f64", "data": "synthetic",
-            "config": {"workload": cfg, "description": WORKLOADS[cfg], "elements": m.nelem,
-                       "dofs": n, "nnz": nnz, "ell_width": W, "l2": "flushed (256 MB write) "
-                       "between timed steps", "parallelism": f"replicas x{world}"},
+            "config": workload_config(cfg, m, world),
+            "matrix": {"dofs": n, "nnz": nnz, "ell_width": W},
+            "timing": "device time (CUDA events on the library's stream); L2 flushed (256 MB "
+                      "write) before every timed step",
+            "value_with_pattern": with_pattern,
             "roofline": {"bound": "hbm", "achieved": dom_bytes / t_dom / 1e9, "peak": hbm,
                          "unit": "GB/s", "frac": dom_bytes / t_dom / 1e9 / hbm,
                          "traffic": traffic, "kernel": dom_name,
@@ -610,6 +781,7 @@ def run_gpu_arm(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "solve": solve,
+            "north_star": north_star,
             "learned": learned,
             "cpu_baseline": cpu_baseline,
         }
@@ -632,9 +804,11 @@ def main():
     ap.add_argument("--solvers", default=",".join(SOLVERS),
                     help="comma list of the solve block's entries (default: all)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-north-star", action="store_true",
+                    help="skip the Brick20 64^3 assembly + solve study of the default run")
     ap.add_argument("--scatter", default="auto", choices=["owner", "colour", "atomic", "auto"])
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
+    if args.warmup < 3:     # both arms: at least 3 warm-up steps
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)

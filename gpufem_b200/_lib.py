@@ -65,6 +65,7 @@ SIGNATURES = {
     "gf_ell_convert_f64_to_f32": (I32, [P]),
     "gf_ell_view": (I32, [P, I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(P), C.POINTER(P),
                           C.POINTER(P)]),
+    "gf_ell_version": (I32, [P, I32, C.POINTER(I64)]),
     "gf_ell_download": (I32, [P, I32, P, P, P]),
     "gf_ell_upload": (I32, [P, I32, I32, P, P, P]),
     "gf_ell_diagonal": (I32, [P, I32, P]),
@@ -77,6 +78,7 @@ SIGNATURES = {
     "gf_spmv_host": (I32, [P, I32, P, P]),
     "gf_solve": (I32, [P, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     "gf_get_solution": (I32, [P, P]),
+    "gf_residual_dd": (I32, [P, P, P, P, C.POINTER(D)]),
     "gf_solution_view": (I32, [P, C.POINTER(P)]),
     "gf_lp_num_params": (I64, [I32]),
     "gf_lp_init": (I32, [P, I32, C.c_uint64]),

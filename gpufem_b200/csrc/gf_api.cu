@@ -525,6 +525,14 @@ GF_API gf_status gf_ell_convert_f64_to_f32(gf_ctx* ctx) {
   return GF_OK;
 }
 
+GF_API gf_status gf_ell_version(gf_ctx* ctx, int32_t dtype, int64_t* version) {
+  if (!ctx || !version) return GF_ERR_INVALID_ARG;
+  if (dtype != GF_F64 && dtype != GF_F32)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown dtype %d", dtype);
+  *version = dtype == GF_F64 ? ctx->kver64 : ctx->kver32;
+  return GF_OK;
+}
+
 GF_API gf_status gf_ell_view(gf_ctx* ctx, int32_t dtype, int32_t* n, int32_t* width,
                              const int32_t** rownnz, const int32_t** colidx,
                              const void** values) {

@@ -233,6 +233,44 @@ k_residual64(MatLayout L, const double* __restrict__ val, const double* __restri
   if (threadIdx.x == 0) atomicAdd(acc, s);
 }
 
+// r = f - K (u_hi + u_lo) on the column-major ELL in double-double arithmetic (the
+// compensated dot product "Dot2" of Ogita, Rump and Oishi, SIAM J. Sci. Comput. 26(6),
+// 2005: each product split exactly with an FMA, each sum with TwoSum), rounded to FP64
+// once at the end; also sum of r_i^2.  The residual of a solution held as an unevaluated
+// sum u_hi + u_lo is then exact to about 2^-104 relative to max |K_ij (u_hi + u_lo)_j|,
+// well below the FP64 rounding of K u itself (which bounds an FP64 residual).
+__global__ void __launch_bounds__(kT)
+k_residual_dd(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ colidx,
+              const double* __restrict__ val, const double* __restrict__ uh,
+              const double* __restrict__ ul, const double* __restrict__ f,
+              double* __restrict__ r, double* __restrict__ acc) {
+  __shared__ double sh[32];
+  double rr = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = f[i], c = 0.0;
+    const int len = rownnz[i];
+    for (int j = 0; j < len; ++j) {
+      const size_t o = (size_t)j * n + i;
+      const double k = val[o];
+      const int col = colidx[o];
+      const double h = uh[col];
+      // explicit round-to-nearest operations: no FMA contraction may merge these steps
+      const double p = __dmul_rn(k, h);
+      const double pe = fma(k, h, -p);   // k h = p + pe exactly
+      const double t = __dsub_rn(s, p);  // TwoSum(s, -p) = t + te exactly
+      const double bp = __dsub_rn(t, s);
+      const double te = __dadd_rn(__dsub_rn(s, __dsub_rn(t, bp)), __dsub_rn(-p, bp));
+      s = t;
+      c += te - pe - k * ul[col];
+    }
+    const double v = s + c;
+    r[i] = v;
+    rr += v * v;
+  }
+  double b = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(acc, b);
+}
+
 // ---- CG kernels ------------------------------------------------------------
 template <typename V>
 __global__ void __launch_bounds__(kT)
@@ -1475,6 +1513,40 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
 }
 
 // ---------------------------------------------------------------------------
+// Compensated residual for iterative refinement (gf_residual_dd).
+// ---------------------------------------------------------------------------
+extern "C" GF_API gf_status gf_residual_dd(gf_ctx* ctx, const double* u_hi, const double* u_lo,
+                                           double* r, double* rel_residual) {
+  if (!ctx || !u_hi || !u_lo || !r) return GF_ERR_INVALID_ARG;
+  if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "no FP64 matrix");
+  if (!ctx->d_f) return gf_fail(ctx, GF_ERR_STATE, "no force vector");
+  cudaSetDevice(ctx->device);
+  gf_status st;
+  if (!ctx->d_red && (st = gf_alloc(ctx, &ctx->d_red, 4)) != GF_OK) return st;
+  if (!ctx->h_pinned && cudaMallocHost(&ctx->h_pinned, 256) != cudaSuccess) {
+    cudaGetLastError();
+    return gf_fail(ctx, GF_ERR_OOM, "pinned scalars");
+  }
+  cudaStream_t s = ctx->stream;
+  const int n = ctx->n;
+  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_red, 0, 2 * sizeof(double), s));
+  k_residual_dd<<<std::min(gf_blocks(n, kT), 8 * ctx->sm_count), kT, 0, s>>>(
+      n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, u_hi, u_lo, ctx->d_f, r, ctx->d_red);
+  GF_LAUNCH_CHECK(ctx, "k_residual_dd");
+  if (rel_residual) {
+    double ff = 0.0;
+    for (double v : ctx->h_f) ff += v * v;
+    double* h = (double*)ctx->h_pinned + 16;
+    GF_CUDA(ctx, cudaMemcpyAsync(h, ctx->d_red, sizeof(double), cudaMemcpyDeviceToHost, s));
+    GF_CUDA(ctx, cudaStreamSynchronize(s));
+    *rel_residual = ff > 0.0 ? std::sqrt(*h / ff) : std::sqrt(*h);
+  } else {
+    GF_CUDA(ctx, cudaStreamSynchronize(s));
+  }
+  return GF_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free Jacobi-PCG (gf_pcg_noalloc).
 //
 // For callers that may not allocate device memory themselves or through this
@@ -1502,6 +1574,23 @@ static_assert(sizeof(SolveScalars) <= 16 * sizeof(double), "scalar block");
 
 static __device__ __align__(256) double
     g_pcg_noalloc_scratch[(size_t)kNoAllocVecs * GF_PCG_NOALLOC_MAX_N + kNoAllocScalarDoubles];
+
+// Checks the caller's ELL before any kernel trusts it: every row length within
+// [0, width] and every stored column (slot < row length) within [0, n).  It reads only
+// in-bounds words (slots below min(row length, width)); a bad row sets *bad.
+__global__ void k_noalloc_ell_check(int n, int width, const int32_t* __restrict__ rownnz,
+                                    const int32_t* __restrict__ colidx, int* bad) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int len = rownnz[i];
+    bool ok = len >= 0 && len <= width;
+    const int m = ok ? len : 0;
+    for (int j = 0; j < m && ok; ++j) {
+      const int c = colidx[(size_t)j * n + i];
+      ok = c >= 0 && c < n;
+    }
+    if (!ok) atomicExch(bad, 1);
+  }
+}
 
 static std::mutex g_pcg_noalloc_mu;
 static double* g_pcg_noalloc_addr[kNoAllocMaxDevices] = {};
@@ -1553,7 +1642,18 @@ extern "C" GF_API gf_status gf_pcg_noalloc(int32_t n, int32_t width, const int32
     cudaGetLastError();
     return e == cudaSuccess ? GF_OK : GF_ERR_CUDA;
   };
-  cudaError_t e = cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s);
+  // validate the ELL (row lengths, column range) into a flag word of the scalar block
+  int* bad = reinterpret_cast<int*>(S + kNoAllocVecs * M + 17);
+  cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int), s);
+  if (e != cudaSuccess) return fail(e);
+  k_noalloc_ell_check<<<std::min(nb, 4 * 148), kT, 0, s>>>(n, width, rownnz, colidx, bad);
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+  int hbad = 0;
+  e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(e);
+  if (hbad) return GF_ERR_INVALID_ARG;
+  e = cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s);
   if (e != cudaSuccess) return fail(e);
   k_diag_inv<double, double><<<nb, kT, 0, s>>>(n, rownnz, colidx, values, dinv);
   k_cg_init<double><<<nb, kT, 0, s>>>(n, b, dinv, x, r, z, p, sc);

@@ -184,6 +184,58 @@ class Context:
         self._c(lib.gf_get_solution(self.h, _ptr(u)))
         return u
 
+    def residual_dd(self, u_hi: np.ndarray, u_lo: np.ndarray):
+        """r = f - K64 (u_hi + u_lo) in double-double on the device (gf_residual_dd);
+        returns (r rounded to FP64, ||r|| / ||f||)."""
+        import torch
+        dev = lambda a: torch.tensor(np.ascontiguousarray(a, np.float64), device="cuda")
+        uh, ul = dev(u_hi), dev(u_lo)
+        r = torch.empty_like(uh)
+        rel = C.c_double()
+        torch.cuda.synchronize()
+        self._c(lib.gf_residual_dd(self.h, C.c_void_p(uh.data_ptr()), C.c_void_p(ul.data_ptr()),
+                                   C.c_void_p(r.data_ptr()), C.byref(rel)))
+        return r.cpu().numpy(), rel.value
+
+    def refine_dd(self, solver: int = _lib.GF_SOLVER_PCG, matrix: int = _lib.GF_F64,
+                  inner_tol: float = 1e-8, target: float = 1e-16, max_steps: int = 8,
+                  max_iter: int = 400000):
+        """Iterative refinement of K64 u = f with the solution held in double-double:
+        r = f - K (u_hi + u_lo) exactly enough (gf_residual_dd), K d = r solved by `solver`
+        to `inner_tol`, (u_hi, u_lo) += d by exact two-sums, until ||r|| / ||f|| <= target
+        or the residual stops falling.  The context's force vector is restored afterwards.
+        Returns (u_hi, u_lo, info) with the residual history, the relative size of the last
+        correction and the inner iterations."""
+        f = self.get_force()
+        u_hi = np.zeros(self.n)
+        u_lo = np.zeros(self.n)
+        hist, inner, corr = [], [], []
+        try:
+            for _ in range(max_steps + 1):
+                r, rel = self.residual_dd(u_hi, u_lo)
+                hist.append(rel)
+                if rel <= target or (len(hist) > 2 and rel >= 0.5 * hist[-2]):
+                    break
+                if len(hist) > max_steps:
+                    break
+                self.set_force(r)
+                info = self.solve(solver, matrix, tol=inner_tol, max_iter=max_iter,
+                                  raise_on_error=False)
+                d = self.solution()
+                inner.append(int(info.iterations))
+                s = u_hi + d                      # TwoSum(u_hi, d) = s + e exactly
+                bb = s - u_hi
+                e = (u_hi - (s - bb)) + (d - bb)
+                lo = u_lo + e
+                u_hi = s + lo                     # renormalise (FastTwoSum, |s| >= |lo|)
+                u_lo = lo - (u_hi - s)
+                nu = np.linalg.norm(u_hi)
+                corr.append(float(np.linalg.norm(d) / nu) if nu > 0 else 0.0)
+        finally:
+            self.set_force(f)
+        return u_hi, u_lo, {"rel_residual_history": hist, "inner_iterations": inner,
+                            "correction_history": corr}
+
     # ---- learned preconditioner ------------------------------------------
     def lp_init(self, dim: int, seed: int = 0) -> None:
         self._c(lib.gf_lp_init(self.h, dim, seed))

@@ -195,6 +195,11 @@ GF_API gf_status gf_ell_convert_f64_to_f32(gf_ctx* ctx);
 GF_API gf_status gf_ell_view(gf_ctx* ctx, int32_t dtype, int32_t* n, int32_t* width,
                              const int32_t** rownnz, const int32_t** colidx,
                              const void** values);
+/* Version of the values of the matrix of `dtype`: a per-context counter that grows every
+ * time those values change (assembly, constraints, conversion, upload).  No counterpart in
+ * the reference, whose ELLmatrix lives in host memory: a host-side cache of the device
+ * matrix (the reference-side ELLmatrixCUDA adapter) compares it to tell that it is stale. */
+GF_API gf_status gf_ell_version(gf_ctx* ctx, int32_t dtype, int64_t* version);
 /* Copy to host: rownnz[n], colidx[n*width], values[n*width] (dtype-sized). */
 GF_API gf_status gf_ell_download(gf_ctx* ctx, int32_t dtype, int32_t* rownnz,
                                  int32_t* colidx, void* values);
@@ -229,6 +234,15 @@ GF_API gf_status gf_spmv_host(gf_ctx* ctx, int32_t dtype, const double* x, doubl
 GF_API gf_status gf_solve(gf_ctx* ctx, const gf_solve_opts* opts, gf_solve_info* info);
 /* Solution of the last solve (n doubles). */
 GF_API gf_status gf_get_solution(gf_ctx* ctx, double* u);
+/* r = f - K64 (u_hi + u_lo) in double-double arithmetic (compensated products and sums,
+ * rounded to FP64 once), for iterative refinement of a solution held as an unevaluated sum
+ * of two doubles; the residual r = b - A x that SPRmatrix::CPU_CG (SPRmatrix.cc:405-480)
+ * starts from, computed accurately enough to certify solutions whose true residual is
+ * below FP64 roundoff of K u.  u_hi, u_lo and r are DEVICE pointers (n doubles, on this
+ * context's device); f is the context's force vector.  rel_residual (host, may be NULL)
+ * receives ||r|| / ||f||. */
+GF_API gf_status gf_residual_dd(gf_ctx* ctx, const double* u_hi, const double* u_lo, double* r,
+                                double* rel_residual);
 /* Device pointer of the FP64 solution. */
 GF_API gf_status gf_solution_view(gf_ctx* ctx, const double** u);
 
@@ -304,7 +318,9 @@ GF_API gf_status gf_twolevel_aggregates(gf_ctx* ctx, int32_t* node_agg, double* 
  * gf_ell_view describes it, b and x of n doubles) and `stream` is the caller's CUDA stream
  * (NULL = legacy default stream).  Its work vectors live in one fixed __device__ array
  * sized for n <= GF_PCG_NOALLOC_MAX_N (about 10.5 MB, held by every GPU that loads the
- * library until the process exits); larger n returns GF_ERR_INVALID_ARG.  All calls share
+ * library until the process exits); larger n returns GF_ERR_INVALID_ARG, and so does an
+ * ELL whose row lengths fall outside [0, width] or whose stored columns fall outside
+ * [0, n) (checked on the device before the solve starts).  All calls share
  * that array: calls whose GPU work overlaps (other streams, other threads) race.  The first
  * call on a device looks up the array's address (cudaGetSymbolAddress) and should come
  * before any stream capture.  Returns when done; *iterations and *rel_residual (true FP64

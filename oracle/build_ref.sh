@@ -17,10 +17,14 @@
 # the METIS dual-graph restatement: oracle/ref_stubs.cc; the C-ABI driver the
 # tests call: oracle/ref_driver.cc.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or GPUFEM_REFERENCE_ROOT in the environment)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${GPUFEM_REFERENCE_ROOT:-}}"
+if [ -z "$REF" ]; then
+  echo "build_ref.sh: give the reference root as an argument or in GPUFEM_REFERENCE_ROOT" >&2
+  exit 2
+fi
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src/FEM" ]; then
   echo "build_ref.sh: reference sources not found at $REF; skipping" >&2

@@ -23,6 +23,9 @@
  *   or_eliminate      symmetric elimination (no reference counterpart; the
  *                     reference's SUB mode is a no-op, fem.cc:147-165)
  *   or_spmv           ELLmatrix::Axy (ELLmatrix.cc:194-204)
+ *   or_residual_dd    r = f - K (u_hi + u_lo) over the same ELL walk as Axy, in
+ *                     double-double (Dot2 of Ogita, Rump and Oishi 2005: products
+ *                     split exactly by fma, sums by TwoSum); no reference counterpart
  *   or_cg             SPRmatrix::CPU_CG (src/SPRmatrix/SPRmatrix.cc:405-480),
  *                     optionally Jacobi-preconditioned (no reference counterpart)
  *   or_greedy_color   femColor::MakeGreedyColoring over METIS_MeshToDual
@@ -390,6 +393,28 @@ void or_spmv(int n, int W, const int* rownnz, const int* colidx, const double* v
     }
     y[i] = s;
   }
+}
+
+/* r = f - K (u_hi + u_lo), accumulated in double-double and rounded once; returns r.r */
+double or_residual_dd(int n, int W, const int* rownnz, const int* colidx, const double* vals,
+                      const double* f, const double* uh, const double* ul, double* r) {
+  (void)W;
+  double rr = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double s = f[i], c = 0.0;
+    for (int j = 0; j < rownnz[i]; ++j) {
+      int64_t o = (int64_t)j * n + i;
+      double k = vals[o], h = uh[colidx[o]];
+      double p = k * h, pe = fma(k, h, -p);
+      double t = s - p, bp = t - s;
+      double te = (s - (t - bp)) + (-p - bp);
+      s = t;
+      c += te - pe - k * ul[colidx[o]];
+    }
+    r[i] = s + c;
+    rr += r[i] * r[i];
+  }
+  return rr;
 }
 
 /* CG from x0 = 0 until r.r <= eps^2 r0.r0 or maxit; Jacobi when precond != 0.

@@ -35,9 +35,16 @@ def build_oracle(force: bool = False) -> Path:
     return LIB
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
-    """Compile the reference CPU path into oracle/_ref (no-op without sources)."""
-    if not Path(ref_root, "src", "FEM").exists():
+def reference_root(ref_root: str | None = None) -> str | None:
+    """Where the reference sources lie: the argument, else $GPUFEM_REFERENCE_ROOT."""
+    return ref_root or os.environ.get("GPUFEM_REFERENCE_ROOT") or None
+
+
+def build_reference(ref_root: str | None = None) -> bool:
+    """Compile the reference CPU path into oracle/_ref (no-op without sources).
+    The source tree is `ref_root`, else $GPUFEM_REFERENCE_ROOT."""
+    ref_root = reference_root(ref_root)
+    if ref_root is None or not Path(ref_root, "src", "FEM").exists():
         return False
     subprocess.run(["bash", str(HERE / "build_ref.sh"), ref_root], check=True)
     return (REF_DIR / "libref_fp64.so").exists()
@@ -63,6 +70,8 @@ class Oracle:
         L.or_penalty.argtypes = [i32, i32, v, v, v, v]
         L.or_eliminate.argtypes = [i32, i32, v, v, v, v, v]
         L.or_spmv.argtypes = [i32, i32, v, v, v, v, v]
+        L.or_residual_dd.argtypes = [i32, i32, v, v, v, v, v, v, v]
+        L.or_residual_dd.restype = d
         L.or_cg.argtypes = [i32, i32, v, v, v, v, v, i32, d, i32]
         L.or_cg.restype = i32
         L.or_greedy_color.argtypes = [i32, i32, i32, v, v]
@@ -144,6 +153,17 @@ class Oracle:
                          _p(np.ascontiguousarray(x, np.float64)), _p(y))
         return y
 
+    def residual_dd(self, rownnz, colidx, vals, f, u_hi, u_lo):
+        """r = f - K (u_hi + u_lo) in double-double, rounded once; returns (r, ||r||)."""
+        W, n = colidx.shape
+        r = np.zeros(n)
+        rr = self.lib.or_residual_dd(n, W, _p(rownnz), _p(np.ascontiguousarray(colidx)),
+                                     _p(np.ascontiguousarray(vals, np.float64)),
+                                     _p(np.ascontiguousarray(f, np.float64)),
+                                     _p(np.ascontiguousarray(u_hi, np.float64)),
+                                     _p(np.ascontiguousarray(u_lo, np.float64)), _p(r))
+        return r, float(np.sqrt(rr))
+
     def cg(self, rownnz, colidx, vals, b, maxit=10000, eps=1e-10, precond=True):
         W, n = colidx.shape
         x = np.zeros(n)
@@ -200,8 +220,25 @@ class Reference:
         L.ref_mat_get.argtypes = [v, i32, i32]
         L.ref_mat_cg.argtypes = [v, v, v, i32, d]
         L.ref_mat_axy.argtypes = [v, v, v]
+        L.ref_ell_axy_external.argtypes = [i32, i32, v, v, v, v, v, i32]
+        L.ref_ell_axy_external.restype = d
         L.ref_binsearch_step.argtypes = [v, i32, i32, i32, i32]
         L.ref_binsearch_step.restype = i32
+
+    def ell_axy(self, rownnz, colidx, vals, x, nthreads: int = 0):
+        """The reference's ELLmatrix::Axy on a caller's column-major ELL (colidx, vals of
+        shape (width, n)); FP64 build only.  Returns (y, seconds)."""
+        if self.tag != "fp64":
+            raise ValueError("ell_axy takes FP64 arrays: use the fp64 build")
+        W, n = colidx.shape
+        rownnz = np.ascontiguousarray(rownnz, np.int32)
+        colidx = np.ascontiguousarray(colidx, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(n)
+        t = self.lib.ref_ell_axy_external(n, W, _p(rownnz), _p(colidx), _p(vals), _p(x), _p(y),
+                                          nthreads)
+        return y, t
 
     @staticmethod
     def available(tag: str = "fp64") -> bool:

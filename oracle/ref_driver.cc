@@ -210,6 +210,34 @@ void ref_axy(void* h, const double* x, double* y, int nthreads) {
   for (int i = 0; i < n; ++i) y[i] = (double)yr[i];
 }
 
+// The reference's ELLmatrix::Axy (ELLmatrix.cc:194-204, OpenMP over rows) on a caller's
+// column-major ELL (entry (row, slot) at slot * n + row, as ELLmatrix stores it): the
+// arrays are lent to an ELLmatrix object for the one call, so the product is the
+// reference's own code on the caller's matrix.  Values and vectors are fem_float (double
+// in the FP64 build).  Returns wall seconds.
+double ref_ell_axy_external(int n, int width, int32_t* rownnz, int32_t* colidx, real* vals,
+                            real* x, real* y, int nthreads) {
+  ELLmatrix* m = new ELLmatrix(n);
+  real* own_data = m->m_matdata;
+  int* own_col = m->m_colidx;
+  int* own_nnz = m->m_rownnz;
+  const int own_w = m->m_maxrowlen;
+  m->m_matdata = vals;
+  m->m_colidx = colidx;
+  m->m_rownnz = rownnz;
+  m->m_maxrowlen = width;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  double t0 = omp_get_wtime();
+  m->Axy(x, y);
+  double t1 = omp_get_wtime();
+  m->m_matdata = own_data;
+  m->m_colidx = own_col;
+  m->m_rownnz = own_nnz;
+  m->m_maxrowlen = own_w;
+  delete m;
+  return t1 - t0;
+}
+
 // ---- raw ELLmatrix access for the reference's known-answer tests ----------
 void* ref_mat_new(int n) { return SPRmatrix::CreateMatrix(n, SPRmatrix::ELL); }
 void ref_mat_free(void* m) { delete (SPRmatrix*)m; }

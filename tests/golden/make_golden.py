@@ -11,7 +11,7 @@ ELL matrix (rownnz, column indices, values) in FP64 and FP32, the penalty-modifi
 matrix diagonal, and the CG solution with the reference's solver.
 
 Usage (needs the reference sources, i.e. this runs only where they are mounted):
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py REFERENCE_ROOT   (or GPUFEM_REFERENCE_ROOT set)
 """
 from __future__ import annotations
 
@@ -24,7 +24,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from gpufem_b200 import meshgen as mg  # noqa: E402
-from oracle.oracle import Reference, build_reference  # noqa: E402
+from oracle.oracle import Reference, build_reference, reference_root  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
@@ -75,7 +75,10 @@ def run(open_fn):
     return out
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str | None = None) -> None:
+    ref_root = reference_root(ref_root)
+    if ref_root is None:
+        raise SystemExit("give the reference root as an argument or in GPUFEM_REFERENCE_ROOT")
     if not (Reference.available("fp64") and Reference.available("fp32")):
         if not build_reference(ref_root):
             raise SystemExit("reference sources not available")

@@ -73,3 +73,11 @@ def test_every_context_entry_point_rejects_a_null_context():
         assert getattr(_lib.lib, name)(*vals) == _lib.GF_ERR_INVALID_ARG, name
         checked += 1
     assert checked >= 35
+
+
+def test_noalloc_maximum_matches_header():
+    """The Python binding's copy of GF_PCG_NOALLOC_MAX_N equals the header's."""
+    from gpufem_b200 import _lib
+    hdr = (ROOT / "include" / "gpufem_b200.h").read_text()
+    m = re.search(r"#define\s+GF_PCG_NOALLOC_MAX_N\s+(\d+)", hdr)
+    assert m and int(m.group(1)) == _lib.GF_PCG_NOALLOC_MAX_N

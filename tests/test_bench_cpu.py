@@ -32,6 +32,14 @@ def test_reference_arm_prints_one_json_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("reference", "port")
     assert d["cpu_baseline"]["cores"] >= 1 and d["config"]["workload"] == "q4_64"
+    # same steps and warm-up as the GPU arm (which takes at least 3 warm-up steps), and
+    # the full workload mesh in the same config object the GPU arm prints
+    assert d["steps"] == 1 and d["warmup"] == 3
+    assert d["config"]["elements"] == 64 * 64 and d["config"]["dofs"] == 65 * 65 * 2
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from gpufem_b200 import meshgen as mg
+    assert d["config"] == bench.workload_config("q4_64", mg.workload("q4_64"), 1)
 
 
 def test_reference_arm_other_ranks_print_nothing():

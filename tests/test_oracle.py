@@ -226,3 +226,49 @@ def test_oracle_vs_live_reference_coloured(oracle, et, n, ng):
     assert row_rel_err(ell_to_dense(rn, ci, v), ell_to_dense(ro, co, vo)) <= 1e-12
     _, nc = oracle.greedy_color(et, m.nnodes, m.conn)
     assert s.num_colors() == nc
+
+
+def test_residual_dd_is_exact_to_double_double():
+    """or_residual_dd against exact rational arithmetic on a small ELL system whose
+    solution is held as u_hi + u_lo: the FP64 residual f - K u_hi loses the u_lo part and
+    the rounding of K u; the compensated one keeps both."""
+    from fractions import Fraction
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(7)
+    n, W = 40, 5
+    rownnz = rng.integers(1, W + 1, n).astype(np.int32)
+    colidx = np.zeros((W, n), np.int32)
+    vals = np.zeros((W, n))
+    for i in range(n):
+        cols = np.sort(rng.choice(n, rownnz[i], replace=False))
+        colidx[: rownnz[i], i] = cols
+        vals[: rownnz[i], i] = rng.standard_normal(rownnz[i]) * 10.0 ** rng.integers(-3, 4)
+    uh = rng.standard_normal(n)
+    ul = uh * 1e-17 * rng.standard_normal(n)
+    f = np.zeros(n)
+    for i in range(n):   # f close to K u so that the residual cancels heavily
+        f[i] = sum(vals[j, i] * uh[colidx[j, i]] for j in range(rownnz[i]))
+    r, nrm = Oracle().residual_dd(rownnz, colidx, vals, f, uh, ul)
+    for i in range(n):
+        exact = Fraction(f[i]) - sum(Fraction(vals[j, i]) * (Fraction(uh[colidx[j, i]])
+                                                              + Fraction(ul[colidx[j, i]]))
+                                     for j in range(rownnz[i]))
+        scale = max(abs(Fraction(vals[j, i]) * Fraction(uh[colidx[j, i]]))
+                    for j in range(rownnz[i]))
+        assert abs(Fraction(r[i]) - exact) <= Fraction(2.0 ** -100) * scale + abs(exact) * Fraction(2.0 ** -52)
+    assert np.isclose(nrm, np.linalg.norm(r))
+
+
+def test_reference_axy_on_external_ell_matches_oracle_spmv():
+    """The reference's own ELLmatrix::Axy lent a caller's ELL (ref_ell_axy_external)
+    equals the oracle's SpMV on an assembled matrix."""
+    from oracle.oracle import Oracle, Reference
+    if not Reference.available("fp64"):
+        pytest.skip("reference oracle build absent")
+    from gpufem_b200 import meshgen as mg
+    m = mg.clamp_and_load(mg.structured(mg.BRICK8, (3, 3, 2), jitter=0.1, seed=2))
+    O = Oracle()
+    rn, ci, v = O.assemble(m.elem_type, m.ngauss, m.coords, m.conn, m.E0, m.nu)
+    x = np.random.default_rng(1).standard_normal(m.ndof)
+    y, _ = Reference("fp64").ell_axy(rn, ci, v, x, nthreads=2)
+    assert np.allclose(y, O.spmv(rn, ci, v, x), rtol=1e-13, atol=1e-9 * np.abs(v).max())

@@ -203,3 +203,33 @@ def test_spmv_2d_node_blocks_vs_oracle_and_alignment(Context, oracle, dtype):
     assert np.linalg.norm(y.cpu().numpy() - yo) <= tol * np.linalg.norm(yo)
     st = _lib.lib.gf_spmv(ctx.h, dtype, x[1:].data_ptr(), y.data_ptr())
     assert st == _lib.GF_ERR_INVALID_ARG
+
+
+def test_residual_dd_and_refinement_vs_oracle(Context, oracle):
+    """gf_residual_dd equals the oracle's double-double residual for a solution held as
+    u_hi + u_lo, and refinement drives the true residual far below what an FP64 residual
+    can show (the FP64 residual of the refined solution is bounded below by roundoff)."""
+    m = mg.workload("q8_512", scale=1 / 32)
+    ctx = Context(0)
+    ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+    ctx.set_supports(m.supports)
+    ctx.set_force(m.f)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+    ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
+    rn, ci, v = ctx.ell_download(_lib.GF_F64)
+    f = ctx.get_force()
+    ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-10, max_iter=100000)
+    uh = ctx.solution()
+    ul = uh * 1e-17 * np.random.default_rng(3).standard_normal(uh.size)
+    r_dev, rel_dev = ctx.residual_dd(uh, ul)
+    r_or, nrm = oracle.residual_dd(rn, ci, v, f, uh, ul)
+    scale = np.abs(v).max() * np.abs(uh).max()
+    assert np.abs(r_dev - r_or).max() <= 1e-14 * np.abs(r_or).max() + 1e-28 * scale
+    assert rel_dev == pytest.approx(nrm / np.linalg.norm(f), rel=1e-10)
+    u_hi, u_lo, info = ctx.refine_dd(_lib.GF_SOLVER_PCG, inner_tol=1e-9, target=1e-18)
+    hist = info["rel_residual_history"]
+    assert hist[0] == pytest.approx(1.0) and hist[-1] <= 1e-16, hist
+    _, nrm = oracle.residual_dd(rn, ci, v, f, u_hi, u_lo)
+    assert nrm / np.linalg.norm(f) <= 1e-16
+    ustar, _ = oracle.cg(rn, ci, v, f, maxit=200000, eps=1e-13, precond=True)
+    assert np.linalg.norm(u_hi - ustar) <= 1e-9 * np.linalg.norm(ustar)
