@@ -212,6 +212,8 @@ class Context:
         hist, inner, corr = [], [], []
         try:
             for _ in range(max_steps + 1):
+                if hist:
+                    self.set_force(f)             # the residual is always against f
                 r, rel = self.residual_dd(u_hi, u_lo)
                 hist.append(rel)
                 if rel <= target or (len(hist) > 2 and rel >= 0.5 * hist[-2]):
