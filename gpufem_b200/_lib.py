@@ -45,6 +45,10 @@ I64 = C.c_int64
 D = C.c_double
 
 # name -> (restype, argtypes); kept in the order of include/gpufem_b200.h
+# callbacks of the sharded solve (gf_dist_pcg): collectives enqueued on the given stream
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p)
+HALO_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+
 SIGNATURES = {
     "gf_create": (I32, [C.POINTER(P), I32]),
     "gf_destroy": (I32, [P]),
@@ -77,6 +81,9 @@ SIGNATURES = {
     "gf_spmv": (I32, [P, I32, P, P]),
     "gf_spmv_host": (I32, [P, I32, P, P]),
     "gf_solve": (I32, [P, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+    "gf_dist_set_halo": (I32, [P, I32, I32, P, I32, P]),
+    # the callbacks pass as plain pointers: C.cast(ALLREDUCE_FN(f), C.c_void_p)
+    "gf_dist_pcg": (I32, [P, C.POINTER(SolveOpts), P, P, P, C.POINTER(SolveInfo)]),
     "gf_get_solution": (I32, [P, P]),
     "gf_residual_dd": (I32, [P, P, P, P, C.POINTER(D)]),
     "gf_solution_view": (I32, [P, C.POINTER(P)]),

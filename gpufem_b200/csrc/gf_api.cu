@@ -60,12 +60,14 @@ GF_API gf_status gf_destroy(gf_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   gf_lp_free(ctx);
   gf_coarse_free(ctx);
+  gf_dist_free(ctx);
   gf_solver_free(ctx);
   gf_pattern_free(ctx);
   gf_mesh_free(ctx);
   gf_pfree(ctx, ctx->d_f);
   gf_pfree(ctx, ctx->d_fixed);
   if (ctx->d_geo) cudaFree(ctx->d_geo);
+  gf_free(ctx->d_asm_err);
   gf_pool_clear(ctx);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);

@@ -36,38 +36,6 @@ namespace {
 
 constexpr int kThreads = 256;
 
-// Adds DIM values to DIM consecutive rows of one ELL slot column (the rows of one
-// node).  Atomic FP32 uses vector reductions where the address allows: one
-// red.global.add.v2.f32 for a 2-D node (its two rows start 8-byte aligned because n
-// is even), a v2 plus a scalar reduction for a 3-D node; FP64 and the colour schedule
-// (plain read-modify-write) go per value.
-__device__ inline void red_v2_f32(float* p, float a, float b) {
-  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
-}
-
-template <int DIM, typename T, bool ATOMIC>
-__device__ inline void add_rows(T* p, const T (&v)[DIM]) {
-  if constexpr (ATOMIC && sizeof(T) == 4 && DIM >= 2) {
-    float* q = reinterpret_cast<float*>(p);
-    if ((reinterpret_cast<uintptr_t>(q) & 7) == 0) {
-      red_v2_f32(q, (float)v[0], (float)v[1]);
-      if (DIM == 3) atomicAdd(q + 2, (float)v[DIM - 1]);
-    } else if (DIM == 3) {
-      atomicAdd(q, (float)v[0]);
-      red_v2_f32(q + 1, (float)v[1], (float)v[DIM - 1]);
-    } else {
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) atomicAdd(q + c, (float)v[c]);
-    }
-  } else if constexpr (ATOMIC) {
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) atomicAdd(p + c, v[c]);
-  } else {
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) p[c] += v[c];
-  }
-}
-
 template <int ET, typename TC, bool ATOMIC>
 __global__ void __launch_bounds__(kThreads)
 k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
@@ -206,264 +174,6 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   }
 }
 
-// ---- TF32 tensor-core engine (GF_ENGINE_TF32_MMA, FP32) ---------------------------
-// The node-pair blocks of one element are blocks of one Gram matrix: with rows
-// r = a*NEN + i (component a of node i) and k over the Gauss points,
-//   M[r][c] = sum_k w_k G[r][k] G[c][k],   H_ij[a][b] = M[a*NEN+i][b*NEN+j],
-// where G[r][k] = g_i[a] at point k and w_k = w detJ E.  A warp forms M for one element
-// with mma.sync.m16n8k8 TF32 tiles (rows and k padded with zeros to multiples of 16 and 8)
-// over the upper triangle (column tile >= row tile), in three TF32 products
-// (hi*hi + hi*lo + lo*hi, each operand split as x = hi + lo) so that M keeps close to
-// FP32 accuracy, writes it to its shared-memory buffer, and then its lanes form the
-// blocks of the pairs i <= j and scatter them as the CUDA-core kernel does.
-__device__ inline uint32_t f2tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-__device__ inline void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
-  hi = f2tf32(x);
-  lo = f2tf32(x - __uint_as_float(hi));
-}
-
-__device__ inline void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-constexpr int kMmaMaxKS = (GF_MAX_GP + 7) / 8;  // k-steps of 8 Gauss points
-
-template <int ET>
-struct MmaShape {
-  static constexpr ElemInfo info = gf_elem_info(ET);
-  static constexpr int DP = info.dim == 3 ? 4 : 2;   // rows per node (3-D padded to 4)
-  static constexpr int NPB = 16 / DP;                // nodes per 16-row strip
-  static constexpr int RP = (info.nen * DP + 15) / 16 * 16;  // padded rows / columns of M
-  static constexpr int LDS = RP + 4;                 // row stride of a strip in shared memory
-};
-
-template <int ET, bool ATOMIC>
-__global__ void __launch_bounds__(kThreads)
-k_assemble_mma(const int32_t* __restrict__ elems, int count, int TE, int ngp,
-               const int32_t* __restrict__ conn, const double* __restrict__ coords,
-               const float* __restrict__ Eel, const uint16_t* __restrict__ slotmap, int nelem,
-               int n, const AsmTables* __restrict__ tab, float lam1, float mu1,
-               float* __restrict__ K) {
-  constexpr ElemInfo info = gf_elem_info(ET);
-  constexpr int NEN = info.nen, DIM = info.dim;
-  constexpr int DP = MmaShape<ET>::DP, NPB = MmaShape<ET>::NPB;
-  constexpr int RP = MmaShape<ET>::RP, LDS = MmaShape<ET>::LDS;
-  constexpr int NPAIR = NEN * (NEN + 1) / 2;
-  constexpr int NW = kThreads / 32;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float* sM = reinterpret_cast<float*>(smem_raw);                // NW * 16 * LDS
-  float* sdN = sM + NW * 16 * LDS;                               // ngp*DIM*NEN
-  float* sw = sdN + ngp * DIM * NEN;                             // ngp
-  float* sX = sw + ngp;                                          // TE*NEN*DIM
-  // G with an odd element stride SE = TE + 1: the fragment loads of one warp (one element,
-  // rows and Gauss points varying across lanes) then fall into different banks
-  const int SE = TE + 1;
-  float* sG = sX + TE * NEN * DIM;                               // ngp*NEN*DIM*SE
-  float* swd = sG + ngp * NEN * DIM * SE;                        // ngp*TE
-  int* sconn = reinterpret_cast<int*>(swd + ngp * TE);           // TE*NEN
-  int* sel = sconn + TE * NEN;                                   // TE
-  int* sflag = sel + TE;                                         // TE
-
-  const int tile0 = blockIdx.x * TE;
-  const int nt = min(TE, count - tile0);
-  for (int k = threadIdx.x; k < ngp * DIM * NEN; k += kThreads) sdN[k] = tab->dN32[k];
-  for (int k = threadIdx.x; k < ngp; k += kThreads) sw[k] = tab->w32[k];
-  for (int e = threadIdx.x; e < TE; e += kThreads) {
-    sel[e] = e < nt ? elems[tile0 + e] : -1;
-    sflag[e] = 0;
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k < nt * NEN; k += kThreads) {
-    const int e = k / NEN, i = k % NEN;
-    const int node = conn[(int64_t)sel[e] * NEN + i];
-    const int node0 = conn[(int64_t)sel[e] * NEN];
-    sconn[k] = node;
-#pragma unroll
-    for (int c = 0; c < DIM; ++c)
-      sX[k * DIM + c] = float(coords[(int64_t)node * DIM + c] - coords[(int64_t)node0 * DIM + c]);
-  }
-  __syncthreads();
-  // distortion flag (max/min |detJ| > 10): |detJ| at every (element, Gauss point) in
-  // parallel first (a CTA holds only a few elements here), then the ratio per element
-  for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
-    const int e = t % TE, g = t / TE;
-    if (e >= nt) continue;
-    float J[3][3], Ji[3][3];
-    gf_jacobian<NEN, DIM, float, float>(sdN + g * DIM * NEN, sX + e * NEN * DIM, J);
-    swd[g * TE + e] = fabsf(gf_det_inv<DIM, float>(J, Ji));
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nt; e += kThreads) {
-    float dmin = 3.4e38f, dmax = 0.f;
-    for (int g = 0; g < ngp; ++g) {
-      dmin = fminf(dmin, swd[g * TE + e]);
-      dmax = fmaxf(dmax, swd[g * TE + e]);
-    }
-    sflag[e] = dmax > 10.f * dmin ? 1 : 0;
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < TE * ngp; t += kThreads) {
-    const int e = t % TE, g = t / TE;
-    if (e >= nt) continue;
-    const float detJ = gf_gradients<NEN, DIM, float>(sdN + g * DIM * NEN, sX + e * NEN * DIM,
-                                                     sflag[e], sG + (g * NEN * DIM) * SE + e, SE);
-    swd[g * TE + e] = sw[g] * detJ * Eel[sel[e]];
-  }
-  __syncthreads();
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gid = lane >> 2, tig = lane & 3;
-  const int KS = (ngp + 7) >> 3;
-  float* S = sM + warp * 16 * LDS;  // this warp's strip of M: 16 rows x RP columns
-  // G[r][k] of element e, rows node-major (r = i*DP + a; 0 for a >= DIM, i >= NEN, k >= ngp)
-  auto Gv = [&](int r, int k, int e) -> float {
-    const int i = r / DP, a = r - i * DP;
-    if (a >= DIM || i >= NEN || k >= ngp) return 0.f;
-    return sG[((k * NEN + i) * DIM + a) * SE + e];
-  };
-  for (int e = warp; e < nt; e += NW) {
-    const int el = sel[e];
-    // strip mt: rows of nodes NPB*mt .. NPB*mt + NPB-1 against the columns of every node
-    // j >= NPB*mt; then the blocks of the pairs (i, j >= i) with i in the strip
-    for (int mt = 0; mt < RP / 16; ++mt) {
-      const int r0 = mt * 16 + gid, r1 = r0 + 8;
-      uint32_t ah[kMmaMaxKS][4], al[kMmaMaxKS][4];
-#pragma unroll
-      for (int ks = 0; ks < kMmaMaxKS; ++ks) {
-        if (ks >= KS) break;
-        const int k0 = ks * 8 + tig, k1 = k0 + 4;
-        const float w0 = k0 < ngp ? swd[k0 * TE + e] : 0.f;
-        const float w1 = k1 < ngp ? swd[k1 * TE + e] : 0.f;
-        split_tf32(Gv(r0, k0, e) * w0, ah[ks][0], al[ks][0]);
-        split_tf32(Gv(r1, k0, e) * w0, ah[ks][1], al[ks][1]);
-        split_tf32(Gv(r0, k1, e) * w1, ah[ks][2], al[ks][2]);
-        split_tf32(Gv(r1, k1, e) * w1, ah[ks][3], al[ks][3]);
-      }
-      for (int ntl = 2 * mt; ntl < RP / 8; ++ntl) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        const int c = ntl * 8 + gid;
-#pragma unroll
-        for (int ks = 0; ks < kMmaMaxKS; ++ks) {
-          if (ks >= KS) break;
-          uint32_t bh0, bl0, bh1, bl1;
-          split_tf32(Gv(c, ks * 8 + tig, e), bh0, bl0);
-          split_tf32(Gv(c, ks * 8 + tig + 4, e), bh1, bl1);
-          mma_tf32(acc, al[ks], bh0, bh1);
-          mma_tf32(acc, ah[ks], bl0, bl1);
-          mma_tf32(acc, ah[ks], bh0, bh1);
-        }
-        float* m0 = S + gid * LDS + ntl * 8 + 2 * tig;
-        float* m1 = m0 + 8 * LDS;
-        m0[0] = acc[0];
-        m0[1] = acc[1];
-        m1[0] = acc[2];
-        m1[1] = acc[3];
-      }
-      __syncwarp();
-      const int ib = mt * NPB, ie = min(NEN, ib + NPB);
-      int npair = 0;
-      for (int i = ib; i < ie; ++i) npair += NEN - i;
-      for (int q0 = lane; q0 < npair; q0 += 32) {
-        int q = q0, i = ib;
-        while (q >= NEN - i) { q -= NEN - i; ++i; }
-        const int j = i + q;
-        const float* h = S + (i - ib) * DP * LDS + j * DP;
-        float H[DIM][DIM];
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int b = 0; b < DIM; ++b) H[a][b] = h[a * LDS + b];
-        float tr = 0.f;
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) tr += H[a][a];
-        const int ni = sconn[e * NEN + i], nj = sconn[e * NEN + j];
-        const int sij = slotmap[(int64_t)(i * NEN + j) * nelem + el] * DIM;
-        const int sji = slotmap[(int64_t)(j * NEN + i) * nelem + el] * DIM;
-        float V[DIM][DIM];
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int b = 0; b < DIM; ++b) {
-            V[a][b] = lam1 * H[a][b] + mu1 * H[b][a];
-            if (a == b) V[a][b] += mu1 * tr;
-          }
-#pragma unroll
-        for (int b = 0; b < DIM; ++b) {
-          float col[DIM];
-#pragma unroll
-          for (int a = 0; a < DIM; ++a) col[a] = V[a][b];
-          add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sij + b) * n + ni * DIM], col);
-        }
-        if (i != j) {
-#pragma unroll
-          for (int a = 0; a < DIM; ++a)
-            add_rows<DIM, float, ATOMIC>(&K[(int64_t)(sji + a) * n + nj * DIM], V[a]);
-        }
-      }
-      __syncwarp();
-    }
-  }
-}
-
-template <int ET>
-size_t smem_bytes_mma(int TE, int ngp) {
-  constexpr ElemInfo info = gf_elem_info(ET);
-  const size_t nf = (size_t)(kThreads / 32) * 16 * MmaShape<ET>::LDS +
-                    (size_t)ngp * info.dim * info.nen + ngp + (size_t)TE * info.nen * info.dim +
-                    (size_t)ngp * info.nen * info.dim * (TE + 1) + (size_t)ngp * TE;
-  return nf * sizeof(float) + sizeof(int) * ((size_t)TE * info.nen + 2 * TE) + 16;
-}
-
-template <int ET>
-gf_status launch_mma(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K) {
-  // elements per CTA: a multiple of the 8 warps, as many as fit 110 KB (two CTAs per SM)
-  int TE = 64;
-  while (TE > 8 && smem_bytes_mma<ET>(TE, ctx->ngp) > 110 * 1024) TE -= 8;
-  const size_t sm = smem_bytes_mma<ET>(TE, ctx->ngp);
-  if (sm > 227 * 1024)
-    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "TF32 engine: %zu bytes of shared memory", sm);
-  auto kc = k_assemble_mma<ET, false>;
-  auto ka = k_assemble_mma<ET, true>;
-  GF_CUDA(ctx, cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const float lam1 = (float)ctx->lam1, mu1 = (float)ctx->mu1;
-  if (scatter == GF_SCATTER_ATOMIC) {
-    const int count = ctx->nelem;
-    ka<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
-        ctx->d_allperm, count, TE, ctx->ngp, ctx->d_conn, ctx->d_coords64, ctx->d_Eel32,
-        ctx->d_slotmap, ctx->nelem, ctx->n, d_tab, lam1, mu1, K);
-    GF_LAUNCH_CHECK(ctx, "k_assemble_mma(atomic)");
-  } else {
-    for (int c = 0; c < ctx->ncolors; ++c) {
-      const int c0 = ctx->color_off[c], count = ctx->color_off[c + 1] - c0;
-      if (count == 0) continue;
-      kc<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
-          ctx->d_perm + c0, count, TE, ctx->ngp, ctx->d_conn, ctx->d_coords64, ctx->d_Eel32,
-          ctx->d_slotmap, ctx->nelem, ctx->n, d_tab, lam1, mu1, K);
-      GF_LAUNCH_CHECK(ctx, "k_assemble_mma(colour)");
-    }
-  }
-  return GF_OK;
-}
-
-gf_status launch_mma_dispatch(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K) {
-  switch (ctx->elem_type) {
-    case GF_Q4: return launch_mma<GF_Q4>(ctx, scatter, d_tab, K);
-    case GF_Q8: return launch_mma<GF_Q8>(ctx, scatter, d_tab, K);
-    case GF_BRICK8: return launch_mma<GF_BRICK8>(ctx, scatter, d_tab, K);
-    default: return launch_mma<GF_BRICK20>(ctx, scatter, d_tab, K);
-  }
-}
-
 template <int ET, typename TC>
 size_t smem_bytes(int TE, int ngp) {
   constexpr ElemInfo info = gf_elem_info(ET);
@@ -522,6 +232,7 @@ gf_status launch_dispatch(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* 
 }  // namespace
 
 gf_status gf_assemble_owner(gf_ctx* ctx, int dtype, const AsmTables* d_tab);
+gf_status gf_assemble_tc(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K, int* d_err);
 
 gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out) {
   if (ctx->d_asmtab) {
@@ -565,6 +276,10 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   } else {
     if (!ctx->d_K32 && (st = gf_palloc(ctx, &ctx->d_K32, (size_t)total)) != GF_OK) return st;
   }
+  if (mma) {
+    if (!ctx->d_asm_err && (st = gf_alloc(ctx, &ctx->d_asm_err, 1)) != GF_OK) return st;
+    GF_CUDA(ctx, cudaMemsetAsync(ctx->d_asm_err, 0, sizeof(int), ctx->stream));
+  }
   cudaEventRecord(ctx->ev0, ctx->stream);
   if (scatter == GF_SCATTER_OWNER) {
     // owner-computes: every K entry (padding included) is written exactly once
@@ -574,13 +289,19 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
     st = launch_dispatch<double>(ctx, scatter, d_tab, ctx->d_K64);
   } else {
     cudaMemsetAsync(ctx->d_K32, 0, sizeof(float) * total, ctx->stream);
-    st = mma ? launch_mma_dispatch(ctx, scatter, d_tab, ctx->d_K32)
+    st = mma ? gf_assemble_tc(ctx, scatter, d_tab, ctx->d_K32, ctx->d_asm_err)
              : launch_dispatch<float>(ctx, scatter, d_tab, ctx->d_K32);
   }
   cudaEventRecord(ctx->ev1, ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (st != GF_OK) return st;
   if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "assembly");
+  if (mma) {
+    int herr = 0;
+    GF_CUDA(ctx, cudaMemcpy(&herr, ctx->d_asm_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr)
+      return gf_fail(ctx, GF_ERR_CUDA, "tensor-core assembly: an MMA completion wait timed out");
+  }
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   ctx->last_seconds = ms * 1e-3;

@@ -14,6 +14,42 @@ struct AsmTables {
   float w32[GF_MAX_GP];
 };
 
+// Adds DIM values to DIM consecutive rows of one ELL slot column (the rows of one
+// node).  Atomic FP32 uses vector reductions where the address allows: one
+// red.global.add.v2.f32 for a 2-D node (its two rows start 8-byte aligned because n
+// is even), a v2 plus a scalar reduction for a 3-D node; FP64 and the colour schedule
+// (plain read-modify-write) go per value.
+__device__ inline void red_v2_f32(float* p, float a, float b) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
+
+template <int DIM, typename T, bool ATOMIC>
+__device__ inline void add_rows(T* p, const T (&v)[DIM]) {
+  if constexpr (ATOMIC && sizeof(T) == 4 && DIM == 3) {
+    // the pair of rows that starts 8-byte aligned takes the vector reduction; the choice is
+    // made by selecting addresses, not by branching, since neighbouring lanes hold nodes of
+    // both parities and a branch would run both paths for the whole warp
+    float* q = reinterpret_cast<float*>(p);
+    const bool al = (reinterpret_cast<uintptr_t>(q) & 7) == 0;
+    red_v2_f32(al ? q : q + 1, al ? (float)v[0] : (float)v[1], al ? (float)v[1] : (float)v[2]);
+    atomicAdd(al ? q + 2 : q, al ? (float)v[2] : (float)v[0]);
+  } else if constexpr (ATOMIC && sizeof(T) == 4 && DIM == 2) {
+    float* q = reinterpret_cast<float*>(p);
+    if ((reinterpret_cast<uintptr_t>(q) & 7) == 0) {
+      red_v2_f32(q, (float)v[0], (float)v[1]);
+    } else {
+      atomicAdd(q, (float)v[0]);
+      atomicAdd(q + 1, (float)v[1]);
+    }
+  } else if constexpr (ATOMIC) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) atomicAdd(p + c, v[c]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) p[c] += v[c];
+  }
+}
+
 template <int DIM, typename R>
 __device__ inline R gf_det_inv(const R (&J)[3][3], R (&Ji)[3][3]) {
   if (DIM == 2) {

@@ -191,6 +191,7 @@ struct gf_ctx {
   double* d_Eel = nullptr;       // per-element modulus
   float* d_Eel32 = nullptr;
   void* d_asmtab = nullptr;      // shape-derivative tables (gf_assemble.cu)
+  int* d_asm_err = nullptr;      // tensor-core assembly: set when an MMA wait timed out
 
   // colouring
   int ncolors = 0;
@@ -256,6 +257,7 @@ struct gf_ctx {
   // learned preconditioner
   LpState* lp = nullptr;
   void* coarse = nullptr;  // two-level preconditioner (gf_twolevel.cu)
+  void* dist = nullptr;    // sharded PCG: halo lists and device vectors (gf_solve.cu)
   int coarse_target = 0;   // requested coarse unknowns (0: default)
 };
 
@@ -339,6 +341,7 @@ gf_status gf_constraints_apply(gf_ctx* ctx, int mode);
 gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y);
 gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info);
 void gf_solver_free(gf_ctx* ctx);
+void gf_dist_free(gf_ctx* ctx);
 void gf_mesh_free(gf_ctx* ctx);
 void gf_pattern_free(gf_ctx* ctx);
 

@@ -12,7 +12,9 @@
 //   y = Wout h3 + bout                                     (64 -> dim)
 // N(a) = nodes sharing an element with a (the ELL node adjacency, self included).
 // Weights are kept in FP32 (Adam master copy) and used as BF16; activations and
-// accumulation are FP32.  Wout starts at zero, so an untrained network is Jacobi.
+// accumulation are FP32.  The dense layers (and their data gradients) run on the tcgen05
+// tensor cores (k_lp_mm_tc): activations split into TF32 hi + lo, BF16 weights exact in
+// TF32, FP32 accumulation in TMEM.  Wout starts at zero, so an untrained network is Jacobi.
 // The output scale c makes M(s r) = s M(r).
 //
 // Training pairs (r_k, e_k = u* - x_k) come from Jacobi-PCG runs on the context's
@@ -28,6 +30,7 @@
 #include <vector>
 
 #include "gf_internal.cuh"
+#include "gf_tc.cuh"
 
 namespace {
 
@@ -103,6 +106,8 @@ struct LpState {
   int npairs = 0;
   float* pr = nullptr;       // [npairs][n]
   float* pe = nullptr;       // [npairs][n]
+  int* err = nullptr;        // set by a tensor-core layer whose MMA wait timed out
+  int mm_grid = 0;           // CTAs of the tensor-core layers (resident CTAs per SM x SMs)
   bool ready = false;        // diag / graph set up for the current matrix
   bool coarse = false;       // with the two-level coarse correction (gf_lp_set_coarse)
   int loss = GF_LP_LOSS_ERROR;
@@ -184,59 +189,153 @@ k_lp_ellmv(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict_
   y[row] = (float)(scale ? acc * (double)scale[row] : acc);
 }
 
-// out[a][o] = act(b[o] + sum_k W1[o][k] A[a][k] (+ sum_k W2[o][k] B[a][k]))
-// Thread per (node, output channel); weights staged in shared memory as FP32.
-template <int CIN, int COUT, bool TWO>
-__global__ void __launch_bounds__(kLT)
-k_lp_dense(int N, const float* __restrict__ A, const float* __restrict__ B,
-           const __nv_bfloat16* __restrict__ W1, const __nv_bfloat16* __restrict__ W2,
-           const __nv_bfloat16* __restrict__ bias, float* __restrict__ pre,
-           float* __restrict__ out, int relu) {
-  __shared__ float sW1[COUT][CIN + 1];
-  __shared__ float sW2[TWO ? COUT : 1][TWO ? CIN + 1 : 1];
-  __shared__ float sb[COUT];
-  for (int k = threadIdx.x; k < COUT * CIN; k += kLT) {
-    sW1[k / CIN][k % CIN] = __bfloat162float(W1[k]);
-    if (TWO) sW2[k / CIN][k % CIN] = __bfloat162float(W2[k]);
-  }
-  for (int k = threadIdx.x; k < COUT; k += kLT) sb[k] = __bfloat162float(bias[k]);
-  __syncthreads();
-  const int64_t total = (int64_t)N * COUT;
-  for (int64_t t = blockIdx.x * (int64_t)kLT + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * kLT) {
-    const int a = (int)(t / COUT), o = (int)(t % COUT);
-    const float* Aa = A + (int64_t)a * CIN;
-    float acc = sb[o];
-#pragma unroll 16
-    for (int k = 0; k < CIN; ++k) acc += sW1[o][k] * __ldg(Aa + k);
-    if (TWO) {
-      const float* Ba = B + (int64_t)a * CIN;
-#pragma unroll 16
-      for (int k = 0; k < CIN; ++k) acc += sW2[o][k] * __ldg(Ba + k);
-    }
-    if (pre) pre[t] = acc;
-    out[t] = (relu && acc < 0.f) ? 0.f : acc;
-  }
+// ---- dense layers on the tcgen05 tensor cores ----------------------------------------
+// out[a][o] = act(bias[o] + sum_k W1[o][k] X1[a][k] (+ sum_k W2[o][k] X2[a][k]))   (WT = false)
+// out[a][o] (+)= sum_k W1[k][o] X1[a][k]                                        (WT = true:
+//   the data gradient of a layer whose weight is [KD][NO] row-major, read transposed)
+// as D = X W^T on the tensor cores: a CTA takes tiles of 128 nodes (M = 128 TMEM lanes, a
+// thread per node in the epilogue), N = NO padded to 16 output channels, K = KD padded to 8
+// input channels per part (X1, then X2).  X is split into TF32 hi + lo parts and the BF16
+// weights are exact in TF32, so the two products X_lo W^T + X_hi W^T give FP32 accuracy
+// with FP32 accumulation in TMEM.
+constexpr int kMmThreads = 128;
+constexpr int kMmWaitIters = 1 << 20;
+
+__host__ __device__ constexpr int mm_pad16(int x) { return x < 16 ? 16 : (x + 15) / 16 * 16; }
+__host__ __device__ constexpr int mm_pad8(int x) { return (x + 7) / 8 * 8; }
+__host__ __device__ constexpr int mm_tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : 128; }
+
+template <int KD, int NO, bool TWO>
+__host__ __device__ constexpr size_t mm_smem_bytes() {
+  constexpr int KDP = mm_pad8(KD), NOP = mm_pad16(NO), P = TWO ? 2 : 1;
+  return (size_t)2 * 128 * KDP * 4          // X hi, lo (one part at a time)
+         + (size_t)P * NOP * KDP * 4        // W parts
+         + (size_t)NOP * 4 + 16;            // bias, mbarrier, TMEM address
 }
 
-// out[a][k] (+)= sum_o W[o][k] G[a][o]   (transpose of the dense layer, data gradient)
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(kLT)
-k_lp_dense_t(int N, const float* __restrict__ G, const __nv_bfloat16* __restrict__ W,
-             float* __restrict__ out, int accumulate) {
-  __shared__ float sW[COUT][CIN + 1];
-  for (int k = threadIdx.x; k < COUT * CIN; k += kLT) sW[k / CIN][k % CIN] = __bfloat162float(W[k]);
-  __syncthreads();
-  const int64_t total = (int64_t)N * CIN;
-  for (int64_t t = blockIdx.x * (int64_t)kLT + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * kLT) {
-    const int a = (int)(t / CIN), k = (int)(t % CIN);
-    const float* Ga = G + (int64_t)a * COUT;
-    float acc = 0.f;
-#pragma unroll 16
-    for (int o = 0; o < COUT; ++o) acc += sW[o][k] * __ldg(Ga + o);
-    out[t] = accumulate ? out[t] + acc : acc;
+template <int KD, int NO, bool TWO, bool WT>
+__global__ void __launch_bounds__(kMmThreads)
+k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
+           const __nv_bfloat16* __restrict__ W1, const __nv_bfloat16* __restrict__ W2,
+           const __nv_bfloat16* __restrict__ bias, float* __restrict__ pre,
+           float* __restrict__ out, int relu, int accumulate, int* __restrict__ err) {
+  constexpr int KDP = mm_pad8(KD), NOP = mm_pad16(NO), P = TWO ? 2 : 1;
+  constexpr int NCH = KDP / 4;                 // 16-byte K chunks per row
+  constexpr uint32_t COLS = mm_tmem_cols(NOP);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  float* xh = reinterpret_cast<float*>(smem);
+  float* xl = xh + 128 * KDP;
+  float* wt = xl + 128 * KDP;                  // [P][KDP/4][NOP][4]
+  float* sb = wt + P * NOP * KDP;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sb + NOP);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  for (int q = tid; q < P * NOP * KDP; q += kMmThreads) {
+    const int p = q / (NOP * KDP), rem = q % (NOP * KDP);
+    const int n = rem / KDP, k = rem % KDP;
+    float v = 0.f;
+    if (n < NO && k < KD) {
+      const __nv_bfloat16* W = p == 0 ? W1 : W2;
+      v = __bfloat162float(WT ? W[(int64_t)k * NO + n] : W[(int64_t)n * KD + k]);
+    }
+    wt[p * NOP * KDP + (k >> 2) * NOP * 4 + n * 4 + (k & 3)] = v;
   }
+  for (int q = tid; q < NOP; q += kMmThreads)
+    sb[q] = (bias && q < NO) ? __bfloat162float(bias[q]) : 0.f;
+  if (warp == 0) tc_alloc(tslot, COLS);
+  if (tid == 0) tc_mbar_init(mbar);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  constexpr uint32_t idesc = tc_idesc_tf32(128, NOP);
+  uint32_t phase = 0;
+  bool ok = true;
+  const int ntiles = (N + 127) / 128;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int a0 = tile * 128;
+    for (int p = 0; p < P && ok; ++p) {
+      const float* X = p == 0 ? X1 : X2;
+      for (int q = tid; q < 128 * NCH; q += kMmThreads) {
+        const int r = q & 127, c = q >> 7;   // consecutive threads: consecutive 16-byte rows
+        const int a = a0 + r;
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = 4 * c + u;
+          v[u] = (a < N && k < KD) ? __ldg(X + (int64_t)a * KD + k) : 0.f;
+        }
+        float4 h, l;
+        float* hp = &h.x;
+        float* lp = &l.x;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const uint32_t hb = tc_tf32_round(v[u]);
+          hp[u] = __uint_as_float(hb);
+          lp[u] = __uint_as_float(tc_tf32_round(v[u] - __uint_as_float(hb)));
+        }
+        *reinterpret_cast<float4*>(xh + c * 512 + r * 4) = h;
+        *reinterpret_cast<float4*>(xl + c * 512 + r * 4) = l;
+      }
+      tc_fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      if (tid == 0) {
+        const uint32_t ah = tc_smem_u32(xh), al = tc_smem_u32(xl);
+        const uint32_t bw = tc_smem_u32(wt + p * NOP * KDP);
+        for (int ks = 0; ks < KDP / 8; ++ks) {
+          const uint64_t db = tc_desc(bw + ks * 2 * NOP * 16, NOP * 16, 128);
+          tc_mma_tf32(tmem, tc_desc(al + ks * 2 * 128 * 16, 128 * 16, 128), db, idesc,
+                      (p > 0 || ks > 0) ? 1u : 0u);
+          tc_mma_tf32(tmem, tc_desc(ah + ks * 2 * 128 * 16, 128 * 16, 128), db, idesc, 1u);
+        }
+        tc_commit(mbar);
+      }
+      // the X tiles are rewritten by the next part or tile only after these MMAs finished
+      const bool done = tc_mbar_wait(mbar, phase, kMmWaitIters);
+      phase ^= 1u;
+      if (!done && lane == 0) atomicExch(err, 1);
+      ok = __syncthreads_and(done);
+      tc_fence_after();
+    }
+    if (!ok) break;
+    // epilogue: a thread per node (TMEM lane), its NO output channels
+    const int a = a0 + warp * 32 + lane;
+    float acc[NOP];
+    if constexpr (NOP >= 32) {
+#pragma unroll
+      for (int c0 = 0; c0 < NOP; c0 += 32) {
+        float t[32];
+        tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, t);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[c0 + j] = t[j];
+      }
+    } else {
+      float t[16];
+      tc_ld16(tmem + ((uint32_t)(warp * 32) << 16), t);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) acc[j] = t[j];
+    }
+    tc_wait_ld();
+    if (a < N) {
+      float* o = out + (int64_t)a * NO;
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        const float v = acc[c] + sb[c];
+        if (pre) pre[(int64_t)a * NO + c] = v;
+        const float y = (relu && v < 0.f) ? 0.f : v;
+        o[c] = accumulate ? o[c] + y : y;
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tc_dealloc(tmem, COLS);
 }
 
 // Weight gradient: dW[o][k] += sum_a G[a][o] A[a][k]; db[o] += sum_a G[a][o].
@@ -502,7 +601,7 @@ void gf_lp_free(gf_ctx* ctx) {
   if (!s) return;
   lp_free_buffers(s);
   auto f = [](auto*& p) { if (p) { cudaFree(p); p = nullptr; } };
-  f(s->w); f(s->wb); f(s->g); f(s->m); f(s->v); f(s->sc);
+  f(s->w); f(s->wb); f(s->g); f(s->m); f(s->v); f(s->sc); f(s->err);
   delete s;
   ctx->lp = nullptr;
 }
@@ -568,6 +667,58 @@ static void lp_matvec(gf_ctx* ctx, const float* x, const float* scale, float* y)
   ctx->launches++;
 }
 
+// Tensor-core dense layer on the context stream (see k_lp_mm_tc).
+template <int KD, int NO, bool TWO, bool WT>
+static void lp_mm(gf_ctx* ctx, const float* X1, const float* X2, const __nv_bfloat16* W1,
+                  const __nv_bfloat16* W2, const __nv_bfloat16* bias, float* pre, float* out,
+                  int relu, int accumulate) {
+  LpState* s = ctx->lp;
+  const int ntiles = (s->N + 127) / 128;
+  const int grid = std::max(1, std::min(ntiles, s->mm_grid));
+  k_lp_mm_tc<KD, NO, TWO, WT><<<grid, kMmThreads, mm_smem_bytes<KD, NO, TWO>(), ctx->stream>>>(
+      s->N, X1, X2, W1, W2, bias, pre, out, relu, accumulate, s->err);
+  ctx->launches++;
+}
+
+template <int KD, int NO, bool TWO, bool WT>
+static gf_status lp_mm_attr(gf_ctx* ctx, int* per_sm) {
+  auto k = k_lp_mm_tc<KD, NO, TWO, WT>;
+  const int sm = (int)mm_smem_bytes<KD, NO, TWO>();
+  GF_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  GF_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
+  *per_sm = std::min(*per_sm, tc_ctas_per_sm(k, kMmThreads, (size_t)sm, (int)mm_tmem_cols(mm_pad16(NO))));
+  return GF_OK;
+}
+
+// One-time set-up of the tensor-core layers of a dim-dimensional network.
+static gf_status lp_mm_setup(gf_ctx* ctx, int dim) {
+  LpState* s = ctx->lp;
+  int per_sm = 512 / 64;   // TMEM: 64 columns per CTA
+  gf_status st;
+  if (dim == 2) {
+    if ((st = lp_mm_attr<8, H, false, false>(ctx, &per_sm)) != GF_OK) return st;
+    if ((st = lp_mm_attr<H, 2, false, false>(ctx, &per_sm)) != GF_OK) return st;
+    if ((st = lp_mm_attr<2, H, false, true>(ctx, &per_sm)) != GF_OK) return st;
+  } else {
+    if ((st = lp_mm_attr<12, H, false, false>(ctx, &per_sm)) != GF_OK) return st;
+    if ((st = lp_mm_attr<H, 3, false, false>(ctx, &per_sm)) != GF_OK) return st;
+    if ((st = lp_mm_attr<3, H, false, true>(ctx, &per_sm)) != GF_OK) return st;
+  }
+  if ((st = lp_mm_attr<H, H, true, false>(ctx, &per_sm)) != GF_OK) return st;
+  if ((st = lp_mm_attr<H, H, false, true>(ctx, &per_sm)) != GF_OK) return st;
+  s->mm_grid = ctx->sm_count * per_sm;
+  return GF_OK;
+}
+
+// Timeout flag of the tensor-core layers (read after a synchronisation).
+static gf_status lp_check_err(gf_ctx* ctx) {
+  int h = 0;
+  GF_CUDA(ctx, cudaMemcpy(&h, ctx->lp->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) return gf_fail(ctx, GF_ERR_CUDA, "learned network: an MMA completion wait timed out");
+  return GF_OK;
+}
+
 // Network forward on FP32 residual r (device, n); fills rho, y and the activations.
 static void lp_forward(gf_ctx* ctx, const float* r) {
   LpState* s = ctx->lp;
@@ -582,26 +733,24 @@ static void lp_forward(gf_ctx* ctx, const float* r) {
                                                    s->feat, s->sc);
   const int gH = lp_grid((int64_t)N * H);
   if (dim == 2)
-    k_lp_dense<8, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
-                                                s->wb + o.b0, s->pre[0], s->h[0], 1);
+    lp_mm<8, H, false, false>(ctx, s->feat, nullptr, s->wb + o.W0, nullptr, s->wb + o.b0,
+                              s->pre[0], s->h[0], 1, 0);
   else
-    k_lp_dense<12, H, false><<<gH, kLT, 0, st>>>(N, s->feat, nullptr, s->wb + o.W0, nullptr,
-                                                 s->wb + o.b0, s->pre[0], s->h[0], 1);
+    lp_mm<12, H, false, false>(ctx, s->feat, nullptr, s->wb + o.W0, nullptr, s->wb + o.b0,
+                               s->pre[0], s->h[0], 1, 0);
   for (int l = 0; l < kLayers; ++l) {
     k_lp_aggregate<<<gH, kLT, 0, st>>>(N, ctx->d_adj_off, ctx->d_adj, s->deg_inv, s->h[l],
                                        s->agg[l], 0);
-    k_lp_dense<H, H, true><<<gH, kLT, 0, st>>>(N, s->h[l], s->agg[l], s->wb + o.Ws[l],
-                                               s->wb + o.Wn[l], s->wb + o.bl[l], s->pre[l + 1],
-                                               s->h[l + 1], 1);
+    lp_mm<H, H, true, false>(ctx, s->h[l], s->agg[l], s->wb + o.Ws[l], s->wb + o.Wn[l],
+                             s->wb + o.bl[l], s->pre[l + 1], s->h[l + 1], 1, 0);
   }
-  const int gy = lp_grid((int64_t)N * dim);
   if (dim == 2)
-    k_lp_dense<H, 2, false><<<gy, kLT, 0, st>>>(N, s->h[kLayers], nullptr, s->wb + o.Wout,
-                                                nullptr, s->wb + o.bout, nullptr, s->y, 0);
+    lp_mm<H, 2, false, false>(ctx, s->h[kLayers], nullptr, s->wb + o.Wout, nullptr,
+                              s->wb + o.bout, nullptr, s->y, 0, 0);
   else
-    k_lp_dense<H, 3, false><<<gy, kLT, 0, st>>>(N, s->h[kLayers], nullptr, s->wb + o.Wout,
-                                                nullptr, s->wb + o.bout, nullptr, s->y, 0);
-  ctx->launches += 5 + 2 * kLayers;
+    lp_mm<H, 3, false, false>(ctx, s->h[kLayers], nullptr, s->wb + o.Wout, nullptr,
+                              s->wb + o.bout, nullptr, s->y, 0, 0);
+  ctx->launches += 3 + kLayers;
 }
 
 // Backward from dy ([N][dim] == n floats) into s->g (accumulated).
@@ -615,10 +764,12 @@ static void lp_backward(gf_ctx* ctx, const float* dy) {
   // output layer
   if (dim == 2) {
     k_lp_wgrad<H, 2><<<gw, kLT, 0, st>>>(N, dy, s->h[kLayers], s->g + o.Wout, s->g + o.bout);
-    k_lp_dense_t<H, 2><<<gH, kLT, 0, st>>>(N, dy, s->wb + o.Wout, s->dh, 0);
+    lp_mm<2, H, false, true>(ctx, dy, nullptr, s->wb + o.Wout, nullptr, nullptr, nullptr,
+                             s->dh, 0, 0);
   } else {
     k_lp_wgrad<H, 3><<<gw, kLT, 0, st>>>(N, dy, s->h[kLayers], s->g + o.Wout, s->g + o.bout);
-    k_lp_dense_t<H, 3><<<gH, kLT, 0, st>>>(N, dy, s->wb + o.Wout, s->dh, 0);
+    lp_mm<3, H, false, true>(ctx, dy, nullptr, s->wb + o.Wout, nullptr, nullptr, nullptr,
+                             s->dh, 0, 0);
   }
   for (int l = kLayers - 1; l >= 0; --l) {
     k_lp_relu_grad<<<gH, kLT, 0, st>>>((int64_t)N * H, s->dh, s->pre[l + 1], s->dpre);
@@ -627,10 +778,12 @@ static void lp_backward(gf_ctx* ctx, const float* dy) {
     k_lp_wgrad<H, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->agg[l], s->g + o.Wn[l],
                                          s->g + o.total);  // scratch slot past the params
     // dh_l = Ws^T dpre + aggregate^T(Wn^T dpre)
-    k_lp_dense_t<H, H><<<gH, kLT, 0, st>>>(N, s->dpre, s->wb + o.Wn[l], s->tmp, 0);
+    lp_mm<H, H, false, true>(ctx, s->dpre, nullptr, s->wb + o.Wn[l], nullptr, nullptr, nullptr,
+                             s->tmp, 0, 0);
     k_lp_aggregate<<<gH, kLT, 0, st>>>(N, ctx->d_adj_off, ctx->d_adj, s->deg_inv, s->tmp,
                                        s->dh, 1);
-    k_lp_dense_t<H, H><<<gH, kLT, 0, st>>>(N, s->dpre, s->wb + o.Ws[l], s->dh, 1);
+    lp_mm<H, H, false, true>(ctx, s->dpre, nullptr, s->wb + o.Ws[l], nullptr, nullptr, nullptr,
+                             s->dh, 0, 1);
   }
   k_lp_relu_grad<<<gH, kLT, 0, st>>>((int64_t)N * H, s->dh, s->pre[0], s->dpre);
   if (dim == 2)
@@ -773,6 +926,9 @@ GF_API gf_status gf_lp_init(gf_ctx* ctx, int32_t dim, uint64_t seed) {
   if ((st = lp_alloc(ctx, &s->m, (size_t)P)) != GF_OK) return st;
   if ((st = lp_alloc(ctx, &s->v, (size_t)P)) != GF_OK) return st;
   if ((st = lp_alloc(ctx, &s->sc, 1)) != GF_OK) return st;
+  if ((st = lp_alloc(ctx, &s->err, 1)) != GF_OK) return st;
+  GF_CUDA(ctx, cudaMemset(s->err, 0, sizeof(int)));
+  if ((st = lp_mm_setup(ctx, dim)) != GF_OK) return st;
   // He-style init for hidden layers; output layer zero (untrained = Jacobi)
   std::vector<float> w(P, 0.f);
   std::mt19937_64 rng(seed);
@@ -825,11 +981,16 @@ GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z) {
   gf_status st = gf_lp_prepare(ctx);
   if (st != GF_OK) return st;
   LpState* s = ctx->lp;
+  cudaEventRecord(ctx->ev0, ctx->stream);
   lp_forward(ctx, r);
   k_lp_output<float><<<gf_blocks(s->n, kLT), kLT, 0, ctx->stream>>>(s->n, s->rho, s->y, s->sc, z);
   GF_LAUNCH_CHECK(ctx, "k_lp_output");
+  cudaEventRecord(ctx->ev1, ctx->stream);
   GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return GF_OK;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->last_seconds = ms * 1e-3;   // device time of one application (gf_last_device_seconds)
+  return lp_check_err(ctx);
 }
 
 // Loss and gradient for one (r, e) pair of FP32 device vectors; the gradient of
@@ -851,6 +1012,7 @@ GF_API gf_status gf_lp_loss_grad(gf_ctx* ctx, const float* r, const float* e, fl
   double l = 0.0;
   GF_CUDA(ctx, cudaMemcpyAsync(&l, &s->sc->loss, sizeof(double), cudaMemcpyDeviceToHost, cs));
   GF_CUDA(ctx, cudaStreamSynchronize(cs));
+  if ((st = lp_check_err(ctx)) != GF_OK) return st;
   if (loss) *loss = (float)l;
   if (grad) GF_CUDA(ctx, cudaMemcpy(grad, s->g, sizeof(float) * P, cudaMemcpyDeviceToHost));
   return GF_OK;
@@ -925,6 +1087,7 @@ GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr
     last = l / batch;
     if (!std::isfinite(last)) return gf_fail(ctx, GF_ERR_STALLED, "training diverged at step %d", it);
   }
+  if ((st = lp_check_err(ctx)) != GF_OK) return st;
   if (final_loss) *final_loss = (float)last;
   return GF_OK;
 }

@@ -1513,6 +1513,290 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
 }
 
 // ---------------------------------------------------------------------------
+// Sharded Jacobi-PCG (gf_dist_set_halo, gf_dist_pcg).
+//
+// The context holds one rank's local mesh: its owned nodes first, then a halo of the
+// nodes its elements share with other ranks, and the local K whose owned rows are exact.
+// PCG runs over the owned dofs with every vector and scalar on the device; per iteration
+// the library packs the send values of p, the caller's halo callback exchanges them
+// (point-to-point, enqueued on the context stream), the library unpacks the received
+// values into the halo part of p, multiplies, and the caller's all-reduce callback sums
+// p.q, then (r.z, r.r) over the ranks, again enqueued on the stream.  The host reads the
+// stop flag once per check_every iterations; every rank takes the same steps because the
+// flag comes from all-reduced scalars.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct DistScalars {
+  double pq;      // all-reduced p.q
+  double rzn;     // all-reduced r.z (new), then r.r: adjacent for one all-reduce
+  double rr;
+  double rz;      // r.z of the previous iteration
+  double rr0, tol2;
+  int iter, maxit, done, pad;
+};
+
+struct DistState {
+  int n_owned = 0, n_send = 0, n_recv = 0;
+  int32_t* d_send = nullptr;   // local dofs packed for the neighbours (owned)
+  int32_t* d_recv = nullptr;   // local dofs filled from the neighbours (halo)
+  double* d_sbuf = nullptr;
+  double* d_rbuf = nullptr;
+  double* d_vec = nullptr;     // x, r, z, dinv (n_owned each), p, q (n local each)
+  DistScalars* d_sc = nullptr;
+};
+
+__global__ void k_dist_init(int no, int n, const double* __restrict__ f,
+                            const double* __restrict__ dinv, double* __restrict__ x,
+                            double* __restrict__ r, double* __restrict__ z, double* __restrict__ p,
+                            DistScalars* sc) {
+  __shared__ double sh[32];
+  double rz = 0.0, rr = 0.0;
+  for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
+    if (i < no) {
+      const double b = f[i], zi = b * dinv[i];
+      x[i] = 0.0;
+      r[i] = b;
+      z[i] = zi;
+      p[i] = zi;
+      rz += b * zi;
+      rr += b * b;
+    } else {
+      p[i] = 0.0;
+    }
+  }
+  const double s1 = block_sum(rz, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
+  const double s2 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
+__global__ void k_dist_init_fin(DistScalars* sc, double tol, int maxit) {
+  sc->rz = sc->rzn;
+  sc->rr0 = sc->rr;
+  sc->tol2 = tol * tol * sc->rr;
+  sc->iter = 0;
+  sc->maxit = maxit;
+  sc->pq = 0.0;
+  sc->done = (sc->rr <= 0.0 || sc->rr <= sc->tol2) ? 1 : (maxit <= 0 ? 3 : 0);
+}
+
+__global__ void k_dist_gather(int m, const int32_t* __restrict__ idx, const double* __restrict__ v,
+                              double* __restrict__ out) {
+  const int k = blockIdx.x * kT + threadIdx.x;
+  if (k < m) out[k] = v[idx[k]];
+}
+
+__global__ void k_dist_scatter(int m, const int32_t* __restrict__ idx, const double* __restrict__ in,
+                               double* __restrict__ v) {
+  const int k = blockIdx.x * kT + threadIdx.x;
+  if (k < m) v[idx[k]] = in[k];
+}
+
+// q = K_local p over every local row; p.q over the owned rows only.  Block 0 clears the
+// r.z / r.r slots that the update kernel accumulates into next.
+__global__ void __launch_bounds__(kT)
+k_dist_spmv_dot(MatLayout L, const double* __restrict__ val, const double* __restrict__ p,
+                double* __restrict__ q, int no, DistScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->rzn = 0.0;
+    sc->rr = 0.0;
+  }
+  double pq = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L.count; t += gridDim.x * blockDim.x)
+    mat_rows(L, t, val, p, [&](int row, double v) {
+      q[row] = v;
+      if (row < no) pq += p[row] * v;
+    });
+  const double s = block_sum(pq, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->pq, s);
+}
+
+__global__ void __launch_bounds__(kT)
+k_dist_update(int no, double* __restrict__ x, double* __restrict__ r, double* __restrict__ z,
+              const double* __restrict__ p, const double* __restrict__ q,
+              const double* __restrict__ dinv, DistScalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const double pq = sc->pq;
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 2;
+    return;
+  }
+  const double alpha = sc->rz / pq;
+  double rz = 0.0, rr = 0.0;
+  for (int i = blockIdx.x * kT + threadIdx.x; i < no; i += gridDim.x * kT) {
+    x[i] += alpha * p[i];
+    const double ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    const double zi = ri * dinv[i];
+    z[i] = zi;
+    rz += ri * zi;
+    rr += ri * ri;
+  }
+  const double s1 = block_sum(rz, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rzn, s1);
+  const double s2 = block_sum(rr, sh);
+  if (threadIdx.x == 0) atomicAdd(&sc->rr, s2);
+}
+
+// p = z + beta p on the owned dofs; a single thread also advances the scalars (after every
+// block has read rz: it runs as the last block of the grid, see k_dist_scalars)
+__global__ void k_dist_direction(int no, const double* __restrict__ z, double* __restrict__ p,
+                                 const DistScalars* sc) {
+  if (sc->done) return;
+  const double beta = sc->rzn / sc->rz;
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i < no) p[i] = z[i] + beta * p[i];
+}
+
+__global__ void k_dist_scalars(DistScalars* sc) {
+  if (sc->done) return;
+  sc->rz = sc->rzn;
+  sc->pq = 0.0;
+  sc->iter += 1;
+  if (sc->rr <= sc->tol2) sc->done = 1;
+  else if (sc->iter >= sc->maxit) sc->done = 3;
+}
+
+}  // namespace
+
+void gf_dist_free(gf_ctx* ctx) {
+  DistState* d = static_cast<DistState*>(ctx->dist);
+  if (!d) return;
+  gf_free(d->d_send);
+  gf_free(d->d_recv);
+  gf_free(d->d_sbuf);
+  gf_free(d->d_rbuf);
+  gf_free(d->d_vec);
+  gf_free(d->d_sc);
+  delete d;
+  ctx->dist = nullptr;
+}
+
+extern "C" GF_API gf_status gf_dist_set_halo(gf_ctx* ctx, int32_t n_owned, int32_t n_send,
+                                             const int32_t* send_dofs, int32_t n_recv,
+                                             const int32_t* recv_dofs) {
+  if (!ctx) return GF_ERR_INVALID_ARG;
+  if (!ctx->has_pattern) return gf_fail(ctx, GF_ERR_STATE, "no local matrix");
+  const int n = ctx->n;
+  if (n_owned <= 0 || n_owned > n || n_send < 0 || n_recv < 0 ||
+      (n_send > 0 && !send_dofs) || (n_recv > 0 && !recv_dofs))
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "halo description");
+  for (int k = 0; k < n_send; ++k)
+    if (send_dofs[k] < 0 || send_dofs[k] >= n_owned)
+      return gf_fail(ctx, GF_ERR_INVALID_ARG, "send dof %d is not an owned dof", send_dofs[k]);
+  for (int k = 0; k < n_recv; ++k)
+    if (recv_dofs[k] < n_owned || recv_dofs[k] >= n)
+      return gf_fail(ctx, GF_ERR_INVALID_ARG, "receive dof %d is not a halo dof", recv_dofs[k]);
+  cudaSetDevice(ctx->device);
+  gf_dist_free(ctx);
+  DistState* d = new DistState();
+  ctx->dist = d;
+  d->n_owned = n_owned;
+  d->n_send = n_send;
+  d->n_recv = n_recv;
+  gf_status st;
+  if ((st = gf_alloc(ctx, &d->d_send, (size_t)std::max(n_send, 1))) != GF_OK) return st;
+  if ((st = gf_alloc(ctx, &d->d_recv, (size_t)std::max(n_recv, 1))) != GF_OK) return st;
+  if ((st = gf_alloc(ctx, &d->d_sbuf, (size_t)std::max(n_send, 1))) != GF_OK) return st;
+  if ((st = gf_alloc(ctx, &d->d_rbuf, (size_t)std::max(n_recv, 1))) != GF_OK) return st;
+  if ((st = gf_alloc(ctx, &d->d_vec, (size_t)4 * n_owned + 2 * (size_t)n)) != GF_OK) return st;
+  if ((st = gf_alloc(ctx, &d->d_sc, 1)) != GF_OK) return st;
+  if (n_send)
+    GF_CUDA(ctx, cudaMemcpy(d->d_send, send_dofs, sizeof(int32_t) * n_send, cudaMemcpyHostToDevice));
+  if (n_recv)
+    GF_CUDA(ctx, cudaMemcpy(d->d_recv, recv_dofs, sizeof(int32_t) * n_recv, cudaMemcpyHostToDevice));
+  return GF_OK;
+}
+
+extern "C" GF_API gf_status gf_dist_pcg(gf_ctx* ctx, const gf_solve_opts* o,
+                                        gf_allreduce_fn allreduce, gf_halo_fn halo, void* user,
+                                        gf_solve_info* info) {
+  if (!ctx || !o || !info || !allreduce) return GF_ERR_INVALID_ARG;
+  DistState* d = static_cast<DistState*>(ctx->dist);
+  if (!d) return gf_fail(ctx, GF_ERR_STATE, "no halo description (gf_dist_set_halo)");
+  if (!ctx->has64) return gf_fail(ctx, GF_ERR_STATE, "no FP64 local matrix");
+  if ((d->n_send || d->n_recv) && !halo)
+    return gf_fail(ctx, GF_ERR_INVALID_ARG, "a halo exchange callback is required");
+  if (!(o->tol > 0.0)) return gf_fail(ctx, GF_ERR_INVALID_ARG, "tol must be > 0");
+  cudaSetDevice(ctx->device);
+  *info = gf_solve_info{};
+  gf_status st;
+  if ((st = ensure_work(ctx)) != GF_OK) return st;
+  const int n = ctx->n, no = d->n_owned;
+  const int maxit = o->max_iter > 0 ? o->max_iter : 10000;
+  const int check = o->check_every > 0 ? std::min(o->check_every, 256) : 16;
+  cudaStream_t s = ctx->stream;
+  double *x = d->d_vec, *r = x + no, *z = r + no, *dinv = z + no, *p = dinv + no, *q = p + n;
+  DistScalars* sc = d->d_sc;
+  MatLayout L;
+  const void* val = nullptr;
+  if ((st = solver_matrix(ctx, GF_F64, &L, &val)) != GF_OK) return st;
+  auto coll = [&](int32_t rc, const char* what) -> gf_status {
+    if (rc != 0) return gf_fail(ctx, GF_ERR_STATE, "%s callback returned %d", what, (int)rc);
+    return GF_OK;
+  };
+  cudaEventRecord(ctx->ev0, s);
+  k_diag_inv<double, double><<<gf_blocks(no, kT), kT, 0, s>>>(no, ctx->d_rownnz, ctx->d_colidx,
+                                                               ctx->d_K64, dinv);
+  GF_LAUNCH_CHECK(ctx, "k_diag_inv");
+  GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(DistScalars), s));
+  k_dist_init<<<red_grid(ctx, n), kT, 0, s>>>(no, n, ctx->d_f, dinv, x, r, z, p, sc);
+  GF_LAUNCH_CHECK(ctx, "k_dist_init");
+  if ((st = coll(allreduce(&sc->rzn, 2, (void*)s, user), "all-reduce")) != GF_OK) return st;
+  k_dist_init_fin<<<1, 1, 0, s>>>(sc, o->tol, maxit);
+  GF_LAUNCH_CHECK(ctx, "k_dist_init_fin");
+  DistScalars hs{};
+  int iters = 0;
+  for (;;) {
+    for (int k = 0; k < check; ++k) {
+      if (d->n_send) {
+        k_dist_gather<<<gf_blocks(d->n_send, kT), kT, 0, s>>>(d->n_send, d->d_send, p, d->d_sbuf);
+        GF_LAUNCH_CHECK(ctx, "k_dist_gather");
+      }
+      if (d->n_send || d->n_recv)
+        if ((st = coll(halo(d->d_sbuf, d->d_rbuf, (void*)s, user), "halo")) != GF_OK) return st;
+      if (d->n_recv) {
+        k_dist_scatter<<<gf_blocks(d->n_recv, kT), kT, 0, s>>>(d->n_recv, d->d_recv, d->d_rbuf, p);
+        GF_LAUNCH_CHECK(ctx, "k_dist_scatter");
+      }
+      k_dist_spmv_dot<<<mat_grid(ctx, L), L.threads, 0, s>>>(L, (const double*)val, p, q, no, sc);
+      GF_LAUNCH_CHECK(ctx, "k_dist_spmv_dot");
+      if ((st = coll(allreduce(&sc->pq, 1, (void*)s, user), "all-reduce")) != GF_OK) return st;
+      k_dist_update<<<red_grid(ctx, no), kT, 0, s>>>(no, x, r, z, p, q, dinv, sc);
+      GF_LAUNCH_CHECK(ctx, "k_dist_update");
+      if ((st = coll(allreduce(&sc->rzn, 2, (void*)s, user), "all-reduce")) != GF_OK) return st;
+      k_dist_direction<<<gf_blocks(no, kT), kT, 0, s>>>(no, z, p, sc);
+      GF_LAUNCH_CHECK(ctx, "k_dist_direction");
+      k_dist_scalars<<<1, 1, 0, s>>>(sc);
+      GF_LAUNCH_CHECK(ctx, "k_dist_scalars");
+    }
+    GF_CUDA(ctx, cudaMemcpyAsync(&hs, sc, sizeof(DistScalars), cudaMemcpyDeviceToHost, s));
+    GF_CUDA(ctx, cudaStreamSynchronize(s));
+    iters = hs.iter;
+    if (hs.done) break;
+  }
+  GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_u, x, sizeof(double) * no, cudaMemcpyDeviceToDevice, s));
+  GF_CUDA(ctx, cudaMemsetAsync(ctx->d_u + no, 0, sizeof(double) * (n - no), s));
+  cudaEventRecord(ctx->ev1, s);
+  GF_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  info->seconds = ctx->last_seconds = ms * 1e-3;
+  info->iterations = iters;
+  info->outer = 1;
+  info->rel_residual = hs.rr0 > 0.0 ? std::sqrt(hs.rr / hs.rr0) : 0.0;  // recursive, all ranks
+  info->status = status_of(hs.done);
+  if (hs.done != 1)
+    gf_fail(ctx, (gf_status)info->status, "sharded PCG stopped with code %d after %d iterations",
+            hs.done, iters);
+  return (gf_status)info->status;
+}
+
+// ---------------------------------------------------------------------------
 // Compensated residual for iterative refinement (gf_residual_dd).
 // ---------------------------------------------------------------------------
 extern "C" GF_API gf_status gf_residual_dd(gf_ctx* ctx, const double* u_hi, const double* u_lo,

@@ -21,6 +21,7 @@ this module splits the same problem by nodes:
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass, field
 from typing import Callable, Dict, List, Optional
 
@@ -120,6 +121,15 @@ def build_shard(mesh: mg.Mesh, owner: np.ndarray, rank: int) -> Shard:
         if theirs.size:
             sh.send[s] = g2l[theirs]
     return sh
+
+
+class _DeviceArray:
+    """A device buffer of doubles described by __cuda_array_interface__ (zero-copy view)."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f8",
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None, "stream": None}
 
 
 class TorchComm:
@@ -246,6 +256,63 @@ class ShardedSolver:
 
     def solve(self, tol: float = 1e-8, max_iter: int = 100000) -> SolveResult:
         return self.pcg.solve(self.b, tol, max_iter)
+
+    def solve_device(self, tol: float = 1e-8, max_iter: int = 100000, check_every: int = 16):
+        """The same Jacobi-PCG inside the library (gf_dist_pcg): vectors, dots and scalars
+        on the device, the halo exchange and the all-reduces enqueued by torch.distributed
+        (NCCL) on the library's stream from the library's callbacks, no host
+        synchronisation per iteration.  Returns (owned-dof solution as a numpy array,
+        SolveInfo)."""
+        import torch
+        import torch.distributed as dist
+        from . import _lib
+        sh, ctx = self.shard, self.ctx
+        if not hasattr(self, "_dist_cb"):
+            send_r, recv_r = sorted(sh.send), sorted(sh.recv)
+            send = [sh.dofs(sh.send[r]) for r in send_r]
+            recv = [sh.dofs(sh.recv[r]) for r in recv_r]
+            sd = np.concatenate(send).astype(np.int32) if send else np.zeros(0, np.int32)
+            rd = np.concatenate(recv).astype(np.int32) if recv else np.zeros(0, np.int32)
+            _lib.check(_lib.lib.gf_dist_set_halo(ctx.h, sh.n_owned, sd.size,
+                                                 sd.ctypes.data_as(C.c_void_p), rd.size,
+                                                 rd.ctypes.data_as(C.c_void_p)), ctx.h)
+            soff = np.concatenate([[0], np.cumsum([a.size for a in send])]).astype(int)
+            roff = np.concatenate([[0], np.cumsum([a.size for a in recv])]).astype(int)
+            stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=self.device)
+
+            def dev(ptr, count):
+                return torch.as_tensor(_DeviceArray(ptr, count), device=self.device)
+
+            def allreduce(ptr, count, _stream, _user):
+                try:
+                    with torch.cuda.stream(stream):
+                        dist.all_reduce(dev(ptr, count))
+                    return 0
+                except Exception:   # reported to the library as a failed collective
+                    return 1
+
+            def halo(sptr, rptr, _stream, _user):
+                try:
+                    sb, rb = dev(sptr, int(soff[-1])), dev(rptr, int(roff[-1]))
+                    ops = [dist.P2POp(dist.isend, sb[soff[k]:soff[k + 1]], r)
+                           for k, r in enumerate(send_r)]
+                    ops += [dist.P2POp(dist.irecv, rb[roff[k]:roff[k + 1]], r)
+                            for k, r in enumerate(recv_r)]
+                    with torch.cuda.stream(stream):
+                        for req in dist.batch_isend_irecv(ops):
+                            req.wait()
+                    return 0
+                except Exception:
+                    return 1
+
+            self._dist_cb = (_lib.ALLREDUCE_FN(allreduce), _lib.HALO_FN(halo))
+        o = _lib.SolveOpts(solver=_lib.GF_SOLVER_PCG, matrix=_lib.GF_F64, max_iter=max_iter,
+                           tol=tol, check_every=check_every)
+        info = _lib.SolveInfo()
+        st = _lib.lib.gf_dist_pcg(ctx.h, C.byref(o), C.cast(self._dist_cb[0], C.c_void_p),
+                                  C.cast(self._dist_cb[1], C.c_void_p), None, C.byref(info))
+        _lib.check(st, ctx.h)
+        return ctx.solution()[:sh.n_owned], info
 
     def gather(self, x) -> np.ndarray:
         """Full solution on every rank (all-gather of owned dofs; for checks)."""

@@ -135,7 +135,7 @@ GF_API gf_status gf_create(gf_ctx** ctx, int32_t device);
 GF_API gf_status gf_destroy(gf_ctx* ctx);
 GF_API const char* gf_last_error(const gf_ctx* ctx);
 GF_API const char* gf_version(void);
-/* Device time (seconds) of the last timed phase: assemble, spmv or solve. */
+/* Device time (seconds) of the last timed phase: assemble, spmv, solve or lp_apply. */
 GF_API double gf_last_device_seconds(const gf_ctx* ctx);
 /* The last gf_assemble split by kernel (device seconds): for GF_SCATTER_OWNER the
  * geometry kernel and the owner kernel; for the other schedules 0 and the whole. */
@@ -276,7 +276,8 @@ GF_API gf_status gf_lp_collect_random(gf_ctx* ctx, int32_t npairs, uint64_t seed
  * gf_lp_set_loss (d = diag K).  *final_loss = mean loss of the last step. */
 GF_API gf_status gf_lp_train(gf_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed,
                              float* final_loss);
-/* z = M(r) on FP32 device vectors of n entries. */
+/* z = M(r) on FP32 device vectors of n entries; gf_last_device_seconds then gives the
+ * device time of this one application. */
 GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z);
 /* on != 0: the learned preconditioner works with the two-level coarse correction
  * (gf_twolevel_setup): gf_lp_collect records its pairs from two-level PCG runs with the
@@ -307,6 +308,31 @@ GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse, int32_t* 
 GF_API gf_status gf_twolevel_apply(gf_ctx* ctx, const double* r, double* z);
 /* Aggregate (0-based, in box order) of every node, and the box side s. */
 GF_API gf_status gf_twolevel_aggregates(gf_ctx* ctx, int32_t* node_agg, double* box_side);
+
+/* ---- sharded solve ----------------------------------------------------------------------
+ * No counterpart in the reference (it runs one device).  One context per rank holds the
+ * rank's local mesh — its owned nodes first, then a halo of the nodes its elements share
+ * with other ranks — assembled as usual, so the owned rows of K are exact.  gf_dist_pcg is
+ * Jacobi-PCG over the owned dofs (x0 = 0, stop when r.r <= tol^2 b.b summed over ranks)
+ * with every vector and scalar on the device and no host synchronisation per iteration:
+ * the caller's callbacks enqueue the collectives on the context's stream (`stream`,
+ * a cudaStream_t) and return at once (non-zero return = failure).
+ *   gf_allreduce_fn: sum `count` doubles at the device address in place over all ranks.
+ *   gf_halo_fn: send the packed owned values `send` (n_send doubles, in the order of
+ *     send_dofs) to the ranks that hold them as halo, and receive the halo values `recv`
+ *     (n_recv doubles, in the order of recv_dofs).
+ * Every rank must call gf_dist_pcg with the same options; all ranks then make the same
+ * callbacks in the same order and stop at the same iteration.  The solution (owned dofs;
+ * halo dofs 0) is read with gf_get_solution; info->rel_residual is the recursive one. */
+typedef int32_t (*gf_allreduce_fn)(double* values, int32_t count, void* stream, void* user);
+typedef int32_t (*gf_halo_fn)(const double* send, double* recv, void* stream, void* user);
+/* send_dofs: owned local dofs whose values the neighbours need, packed per neighbour as
+ * the caller's halo callback expects; recv_dofs: halo local dofs filled from them. */
+GF_API gf_status gf_dist_set_halo(gf_ctx* ctx, int32_t n_owned, int32_t n_send,
+                                  const int32_t* send_dofs, int32_t n_recv,
+                                  const int32_t* recv_dofs);
+GF_API gf_status gf_dist_pcg(gf_ctx* ctx, const gf_solve_opts* opts, gf_allreduce_fn allreduce,
+                             gf_halo_fn halo, void* user, gf_solve_info* info);
 
 /* ---- allocation-free solve -------------------------------------------------------------
  * No counterpart in the reference.  FP64 Jacobi-PCG (x0 = 0, stop when the recursive

@@ -1,7 +1,7 @@
-"""The TF32 tensor-core engine (GF_ENGINE_TF32_MMA): element Gram matrices on
-mma.sync tiles in three TF32 products, against the oracle and the reference's golden
-vectors with the FP32 tolerance (row-relative 1e-6), on the colour and atomic
-schedules."""
+"""The TF32 tensor-core engine (GF_ENGINE_TF32_MMA): element Gram matrices on the
+tcgen05 tensor cores (TMEM accumulators, three TF32 products of split operands), against
+the oracle and the reference's golden vectors with the FP32 tolerance (row-relative
+1e-6), on the colour and atomic schedules."""
 import numpy as np
 import pytest
 
