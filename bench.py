@@ -394,6 +394,14 @@ def north_star_study(args, flush):
                           ("atomic", _lib.GF_SCATTER_ATOMIC), ("colour", _lib.GF_SCATTER_COLOR)):
             t = timed(dt, sc)
             asm[f"{dname}_{sname}"] = {"ms": t * 1e3, "elements_per_s": m.nelem / t}
+    # the tcgen05 engine (FP32): element Gram matrices on the tensor cores, scattered by
+    # atomics, or stored and gathered by the owner kernel (split: tensor kernel, gather)
+    for sname, sc in (("atomic", _lib.GF_SCATTER_ATOMIC), ("owner", _lib.GF_SCATTER_OWNER)):
+        t = timed(_lib.GF_F32, sc, _lib.GF_ENGINE_TF32_MMA)
+        g_s, s_s = C.c_double(), C.c_double()
+        _lib.lib.gf_last_assembly_split(ctx.h, C.byref(g_s), C.byref(s_s))
+        asm[f"f32_tcgen05_{sname}"] = {"ms": t * 1e3, "elements_per_s": m.nelem / t,
+                                       "split_ms": [g_s.value * 1e3, s_s.value * 1e3]}
     # the system solved: FP64 assembly (AUTO), its FP32 rounding, elimination BCs
     t_f64 = asm["f64_auto"]["ms"] * 1e-3
     ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_AUTO)
@@ -506,6 +514,17 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 48, n_test: int
                          **({"fallback": info.fallback} if name == "learned_fcg" else {})}
         if k == 0:
             row["diagnostic"] = _preconditioner_diagnostic(ctx, ustar)
+        # device time of one network application (features, three message-passing layers,
+        # output) against one FP64 SpMV of the same matrix (median of 5 each)
+        rr = np.random.default_rng(k).standard_normal(m.ndof)
+        ta, ts = [], []
+        for _ in range(5):
+            ctx.lp_apply(rr)
+            ta.append(_lib.lib.gf_last_device_seconds(ctx.h))
+            ctx.spmv(rr, _lib.GF_F64)
+            ts.append(_lib.lib.gf_last_device_seconds(ctx.h))
+        row["application_us"] = float(np.median(ta)) * 1e6
+        row["spmv_fp64_us"] = float(np.median(ts)) * 1e6
         results.append(row)
     ctx.close()
 
@@ -515,6 +534,8 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 48, n_test: int
     summary = {f"median_{key}_ratio_{a}_over_pcg_fp64": ratio(a, "pcg_fp64", key)
                for a in ("learned_fcg", "twolevel_pcg") for key in ("iterations", "seconds")}
     summary["learned_fcg_fallbacks"] = int(sum(r["learned_fcg"]["fallback"] for r in results))
+    big = max(results, key=lambda r: r["dofs"])
+    summary["largest_mesh_application_over_spmv"] = big["application_us"] / big["spmv_fp64_us"]
     return {"train_meshes": n_train, "held_out_meshes": n_test, "train_seconds": train_s,
             "final_train_loss": losses[-1], "first_train_loss": losses[0],
             "tol_rel_residual": 1e-8, "summary": summary, "held_out": results}
@@ -607,8 +628,9 @@ def run_gpu_arm(args):
     variants = {}
     runs = [("owner", _lib.GF_SCATTER_OWNER, 0), ("colour", _lib.GF_SCATTER_COLOR, 0),
             ("atomic", _lib.GF_SCATTER_ATOMIC, 0)]
-    if esize == 4:   # the TF32 tensor-core engine assembles FP32 only
-        runs.append(("atomic_tf32", _lib.GF_SCATTER_ATOMIC, _lib.GF_ENGINE_TF32_MMA))
+    if esize == 4:   # the tcgen05 tensor-core engine assembles FP32 only
+        runs += [("atomic_tcgen05", _lib.GF_SCATTER_ATOMIC, _lib.GF_ENGINE_TF32_MMA),
+                 ("owner_tcgen05", _lib.GF_SCATTER_OWNER, _lib.GF_ENGINE_TF32_MMA)]
     for name, sc, eng in runs:
         ts = []
         for _ in range(max(3, min(args.steps, 10))):

@@ -233,6 +233,7 @@ gf_status launch_dispatch(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* 
 
 gf_status gf_assemble_owner(gf_ctx* ctx, int dtype, const AsmTables* d_tab);
 gf_status gf_assemble_tc(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K, int* d_err);
+gf_status gf_assemble_owner_gram(gf_ctx* ctx, const float* gram, float* K);
 
 gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out) {
   if (ctx->d_asmtab) {
@@ -264,9 +265,6 @@ gf_status gf_asm_tables(gf_ctx* ctx, const AsmTables** out) {
 
 gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
   const bool mma = engine == GF_ENGINE_TF32_MMA;
-  if (mma && scatter == GF_SCATTER_OWNER)
-    return gf_fail(ctx, GF_ERR_UNSUPPORTED,
-                   "the TF32 engine runs the element-wise schedules (colour, atomic)");
   gf_status st;
   const AsmTables* d_tab = nullptr;
   if ((st = gf_asm_tables(ctx, &d_tab)) != GF_OK) return st;
@@ -280,8 +278,24 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
     if (!ctx->d_asm_err && (st = gf_alloc(ctx, &ctx->d_asm_err, 1)) != GF_OK) return st;
     GF_CUDA(ctx, cudaMemsetAsync(ctx->d_asm_err, 0, sizeof(int), ctx->stream));
   }
+  if (mma && scatter == GF_SCATTER_OWNER) {
+    // element Gram matrices from the tensor cores, RAW x RAW floats per element
+    const size_t raw = (size_t)ctx->nen * ctx->dim;
+    const size_t need = (size_t)ctx->nelem * raw * raw * sizeof(float);
+    if (ctx->gram_bytes < need) {
+      gf_free(ctx->d_gram);
+      ctx->gram_bytes = 0;
+      if ((st = gf_alloc(ctx, &ctx->d_gram, need / sizeof(float))) != GF_OK) return st;
+      ctx->gram_bytes = need;
+    }
+  }
   cudaEventRecord(ctx->ev0, ctx->stream);
-  if (scatter == GF_SCATTER_OWNER) {
+  if (mma && scatter == GF_SCATTER_OWNER) {
+    // tensor cores: every element's Gram matrix to HBM; owner gather: K written once
+    st = gf_assemble_tc(ctx, scatter, d_tab, ctx->d_gram, ctx->d_asm_err);
+    cudaEventRecord(ctx->evm, ctx->stream);
+    if (st == GF_OK) st = gf_assemble_owner_gram(ctx, ctx->d_gram, ctx->d_K32);
+  } else if (scatter == GF_SCATTER_OWNER) {
     // owner-computes: every K entry (padding included) is written exactly once
     st = gf_assemble_owner(ctx, dtype, d_tab);
   } else if (dtype == GF_F64) {

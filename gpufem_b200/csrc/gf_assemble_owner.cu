@@ -417,6 +417,129 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
       __stcs(&K[(int64_t)s * n + row0 + r], tile[(size_t)s * RB + r]);
 }
 
+// ---------------------------------------------------------------------------
+// Owner gather of element Gram matrices (FP32, the tensor-core engine's owner schedule).
+// The tcgen05 kernel has stored M_e = G W G^T of every element (RAW x RAW floats, rows and
+// columns (node, component), w = Gauss weight * detJ * E folded in); a CTA owns NB nodes as
+// above and, per (owned node a = local node i of incident element e, group of JG element
+// nodes j), reads the 3 x 3 (2 x 2) blocks P = M_e[(i, .), (j, .)] and adds
+// V = lam1 P + mu1 P^T + mu1 tr(P) I into its row tile; the tile is then stored once.
+// M is read once in total (block (i, j) of M_e belongs to the owner of node i alone).
+template <int ET, int JG>
+__global__ void __launch_bounds__(kOT)
+k_assemble_owner_gram(int nnodes, int n, int W, int NB, const int32_t* __restrict__ inc_off,
+                      const int32_t* __restrict__ inc, const uint8_t* __restrict__ inc_loc,
+                      const uint16_t* __restrict__ inc_slot, const float* __restrict__ gram,
+                      float lam1, float mu1, float* __restrict__ K) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  constexpr int NEN = info.nen, DIM = info.dim, RAW = NEN * DIM;
+  constexpr int NJ = NEN / JG;
+  static_assert(NEN % JG == 0, "node groups must tile the element");
+  const int RB = NB * DIM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* tile = reinterpret_cast<float*>(smem_raw);           // [W][RB]
+  int* soff = reinterpret_cast<int*>(tile + (size_t)W * RB);   // [NB + 1]
+  uint8_t* sal = reinterpret_cast<uint8_t*>(soff + NB + 1);    // [tasks] owning node
+
+  const int a0 = blockIdx.x * NB;
+  const int a1 = min(a0 + NB, nnodes);
+  {
+    float4* t4 = reinterpret_cast<float4*>(tile);   // W * RB is a multiple of 4 (launcher)
+    for (int k = threadIdx.x; k < W * RB / 4; k += kOT) t4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  for (int k = threadIdx.x; k <= a1 - a0; k += kOT) soff[k] = inc_off[a0 + k];
+  __syncthreads();
+  const int q0 = soff[0];
+  const int T = soff[a1 - a0] - q0;
+  for (int t = threadIdx.x; t < T; t += kOT) {
+    int lo = 0, hi = a1 - a0;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (soff[mid] - q0 <= t) lo = mid; else hi = mid;
+    }
+    sal[t] = (uint8_t)lo;
+  }
+  __syncthreads();
+  for (int w = threadIdx.x; w < T * NJ; w += kOT) {
+    const int t = w / NJ;
+    const int j0 = (w - t * NJ) * JG;
+    const int al = sal[t];
+    const int q = q0 + t;
+    const int e = inc[q];
+    const int i = inc_loc[q];
+    const float* Mi = gram + (int64_t)e * RAW * RAW + (int64_t)(i * DIM) * RAW;
+    const uint16_t* slots = inc_slot + (int64_t)q * NEN;
+    // the DIM rows of this item, JG * DIM floats each, in 16-byte loads (RAW, JG * DIM and
+    // j0 * DIM are multiples of 4, so every segment starts 16-byte aligned)
+    constexpr int SEG = JG * DIM;
+    static_assert(SEG % 4 == 0 && RAW % 4 == 0, "16-byte segments");
+    float seg[DIM][SEG];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int u = 0; u < SEG / 4; ++u) {
+        const float4 v4 = __ldg(reinterpret_cast<const float4*>(Mi + a * RAW + j0 * DIM) + u);
+        seg[a][4 * u] = v4.x;
+        seg[a][4 * u + 1] = v4.y;
+        seg[a][4 * u + 2] = v4.z;
+        seg[a][4 * u + 3] = v4.w;
+      }
+#pragma unroll
+    for (int jj = 0; jj < JG; ++jj) {
+      const int j = j0 + jj;
+      float P[DIM][DIM];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) P[a][b] = seg[a][jj * DIM + b];
+      float tr = 0.f;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) tr += P[a][a];
+      const int p = slots[j];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) {
+          float v = lam1 * P[a][b] + mu1 * P[b][a];
+          if (a == b) v += mu1 * tr;
+          atomicAdd(&tile[(size_t)(p * DIM + b) * RB + al * DIM + a], v);
+        }
+    }
+  }
+  __syncthreads();
+  const int rows = (a1 - a0) * DIM;
+  const int64_t row0 = (int64_t)a0 * DIM;
+  for (int s = threadIdx.x >> 5; s < W; s += kOT >> 5)
+    for (int r = threadIdx.x & 31; r < rows; r += 32)
+      __stcs(&K[(int64_t)s * n + row0 + r], tile[(size_t)s * RB + r]);
+}
+
+template <int ET>
+gf_status launch_owner_gram(gf_ctx* ctx, const float* gram, float* K) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  const int W = ctx->W;
+  auto bytes = [&](int NB) {
+    return sizeof(float) * (size_t)W * NB * info.dim + sizeof(int) * (NB + 1) +
+           (size_t)NB * ctx->maxval + 16;
+  };
+  // node blocks of a multiple of 4 nodes, so that the row tile (W x NB x dim floats) is a
+  // whole number of 16-byte chunks
+  int NB = std::min(128, std::max(16, (ctx->nnodes + 2 * ctx->sm_count - 1) / (2 * ctx->sm_count)));
+  NB = NB / 4 * 4;
+  while (NB > 4 && bytes(NB) > kOwnerSmemLimit) NB -= 4;
+  if (bytes(NB) > kOwnerSmemLimit)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "owner gather: a row block does not fit");
+  constexpr int JG = info.nen <= 8 ? info.nen : 4;   // JG * dim floats: 16-byte segments
+  auto kern = k_assemble_owner_gram<ET, JG>;
+  GF_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)bytes(NB)));
+  kern<<<(ctx->nnodes + NB - 1) / NB, kOT, bytes(NB), ctx->stream>>>(
+      ctx->nnodes, ctx->n, W, NB, ctx->d_inc_off, ctx->d_inc, ctx->d_inc_loc, ctx->d_inc_slot,
+      gram, (float)ctx->lam1, (float)ctx->mu1, K);
+  GF_LAUNCH_CHECK(ctx, "k_assemble_owner_gram");
+  return GF_OK;
+}
+
 template <int ET, typename TC>
 size_t owner_smem_bytes(int NB, int W, int ngp, int maxval) {
   constexpr ElemInfo info = gf_elem_info(ET);
@@ -515,5 +638,13 @@ gf_status gf_assemble_owner(gf_ctx* ctx, int dtype, const AsmTables* d_tab) {
   return owner_dispatch<float>(ctx, ctx->d_K32, d_tab);
 }
 
-
-
+// Launches the owner gather of the element Gram matrices `gram` (stored by the tensor-core
+// kernel) into the FP32 matrix K on the context's stream (no sync).
+gf_status gf_assemble_owner_gram(gf_ctx* ctx, const float* gram, float* K) {
+  switch (ctx->elem_type) {
+    case GF_Q4: return launch_owner_gram<GF_Q4>(ctx, gram, K);
+    case GF_Q8: return launch_owner_gram<GF_Q8>(ctx, gram, K);
+    case GF_BRICK8: return launch_owner_gram<GF_BRICK8>(ctx, gram, K);
+    default: return launch_owner_gram<GF_BRICK20>(ctx, gram, K);
+  }
+}

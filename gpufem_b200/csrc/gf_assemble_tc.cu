@@ -58,11 +58,6 @@ struct TcShape {
   static constexpr int EPW = WPE > 1 ? 1 : 32 / RPE;         // elements per warp
   static constexpr int EPG = WPE > 1 ? 4 / WPE : 4 * EPW;    // elements per 128-row group
   static constexpr int LW = RPE * WPE;                       // columns of one element
-  // threads per (element, Gauss point) when the gradients are formed: 3-D elements split
-  // their nodes in two so that more of the CTA's 128 threads share that phase
-  static constexpr int NSPLIT = DIM == 3 ? 2 : 1;
-  static constexpr int NCH = NEN / NSPLIT;                   // nodes per thread
-  static_assert(NEN % NSPLIT == 0, "node split");
 };
 
 // Row (TMEM lane) of component a of node i of element slot e within a group.
@@ -83,7 +78,7 @@ __host__ __device__ constexpr int tc_col(int j, int b) {
 template <int ET>
 struct TcSmem {
   // byte offsets within the dynamic shared memory of one CTA
-  size_t tile, a_hi, a_lo, b_hi, b_lo, dN, w, X, wd, wt, ji, slot, conn, sel, flag, neg, mbar,
+  size_t tile, a_hi, a_lo, dN, w, X, wd, wt, ji, slot, conn, sel, flag, neg, mbar,
       tslot, total;
 };
 
@@ -96,8 +91,6 @@ __host__ __device__ TcSmem<ET> tc_smem(int ngp) {
   size_t o = 0;
   L.a_hi = o; o += L.tile;
   L.a_lo = o; o += L.tile;
-  L.b_hi = o; o += L.tile;
-  L.b_lo = o; o += L.tile;
   L.dN = o; o += (size_t)ngp * S::DIM * S::NEN * 4;
   L.w = o; o += (size_t)ngp * 4;
   L.X = o; o += (size_t)S::EPG * S::NEN * S::DIM * 4;
@@ -116,7 +109,10 @@ __host__ __device__ TcSmem<ET> tc_smem(int ngp) {
   return L;
 }
 
-template <int ET, bool ATOMIC>
+// MODE 0: colour schedule (plain read-modify-write of K), 1: atomic schedule
+// (red.global.add into K), 2: store each element's Gram matrix M (RAW x RAW, row-major,
+// rows and columns (node, component)) to `out` for the owner gather (gf_assemble_owner.cu).
+template <int ET, int MODE>
 __global__ void __launch_bounds__(kTcThreads)
 k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
               const int32_t* __restrict__ conn, const double* __restrict__ coords,
@@ -125,12 +121,11 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
               float* __restrict__ K, int* __restrict__ err) {
   using S = TcShape<ET>;
   constexpr int NEN = S::NEN, DIM = S::DIM, EPG = S::EPG;
+  constexpr bool ATOMIC = MODE == 1, GRAM = MODE == 2;
   extern __shared__ __align__(1024) unsigned char smem[];
   const TcSmem<ET> L = tc_smem<ET>(ngp);
   float* aH = reinterpret_cast<float*>(smem + L.a_hi);
   float* aL = reinterpret_cast<float*>(smem + L.a_lo);
-  float* bH = reinterpret_cast<float*>(smem + L.b_hi);
-  float* bL = reinterpret_cast<float*>(smem + L.b_lo);
   float* sdN = reinterpret_cast<float*>(smem + L.dN);
   float* sw = reinterpret_cast<float*>(smem + L.w);
   float* sX = reinterpret_cast<float*>(smem + L.X);
@@ -153,7 +148,7 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
   // TMEM columns, the MMA-completion barrier
   for (int k = tid; k < ngp * DIM * NEN; k += kTcThreads) sdN[k] = tab->dN32[k];
   for (int k = tid; k < ngp; k += kTcThreads) sw[k] = tab->w32[k];
-  for (size_t k = tid; k < 4 * L.tile / 4; k += kTcThreads) aH[k] = 0.f;  // a_hi..b_lo
+  for (size_t k = tid; k < 2 * L.tile / 4; k += kTcThreads) aH[k] = 0.f;  // a_hi, a_lo
   if (warp == 0) tc_alloc(tslot, kTcCols);
   if (tid == 0) tc_mbar_init(mbar);
   tc_fence_before();
@@ -188,10 +183,11 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
     __syncthreads();
     // slot indices of the group's node pairs, [e][pair] (for the atomic schedule the group's
     // elements are consecutive, so a pair's EPG entries are contiguous in the [pair][element] map)
-    for (int t = tid; t < ne * NEN * NEN; t += kTcThreads) {
-      const int pr = t / ne, e = t % ne;
-      sslot[e * NEN * NEN + pr] = slotmap[(int64_t)pr * nelem + sel[e]];
-    }
+    if constexpr (!GRAM)
+      for (int t = tid; t < ne * NEN * NEN; t += kTcThreads) {
+        const int pr = t / ne, e = t % ne;
+        sslot[e * NEN * NEN + pr] = slotmap[(int64_t)pr * nelem + sel[e]];
+      }
     for (int t = tid; t < ne * ngp; t += kTcThreads) {
       const int e = t / ngp, g = t % ngp;
       float J[3][3], Ji[3][3];
@@ -212,75 +208,56 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
       sflag[e] = dmax > 10.f * dmin ? 1 : 0;
     }
     __syncthreads();
-    for (int t = tid; t < ne * ngp * S::NSPLIT; t += kTcThreads) {
-      const int h = t % S::NSPLIT, eg = t / S::NSPLIT;
-      const int e = eg / ngp, g = eg % ngp;
-      const int i0 = h * S::NCH;
-      const float* dN = sdN + g * DIM * NEN;
-      const float* X = sX + e * NEN * DIM;
-      float gr[S::NCH][DIM];
-      float detJ;
+    // per (element, Gauss point): the weight W = w detJ E and J^-1 scaled by sqrt|W| (FP64
+    // J and J^-1 for a distorted element), so that a row of A is sqrt|W| J^-1 dN
+    for (int t = tid; t < ne * ngp; t += kTcThreads) {
+      const int e = t / ngp, g = t % ngp;
+      float* ji = sji + t * DIM * DIM;
+      float detJ = swd[t];
       if (sflag[e]) {
         double J[3][3], Ji[3][3];
-        gf_jacobian<NEN, DIM, double, float>(dN, X, J);
+        gf_jacobian<NEN, DIM, double, float>(sdN + g * DIM * NEN, sX + e * NEN * DIM, J);
         detJ = (float)gf_det_inv<DIM, double>(J, Ji);
 #pragma unroll
-        for (int ii = 0; ii < S::NCH; ++ii)
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            double s = 0.0;
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) s += Ji[c][a] * double(dN[a * NEN + i0 + ii]);
-            gr[ii][c] = (float)s;
-          }
-      } else {
-        float Ji[3][3];
-        const float* ji = sji + (e * ngp + g) * DIM * DIM;
-#pragma unroll
-        for (int q = 0; q < DIM * DIM; ++q) Ji[q / DIM][q % DIM] = ji[q];
-        detJ = swd[e * ngp + g];
-#pragma unroll
-        for (int ii = 0; ii < S::NCH; ++ii)
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            float s = 0.f;
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) s += Ji[c][a] * dN[a * NEN + i0 + ii];
-            gr[ii][c] = s;
-          }
+        for (int q = 0; q < DIM * DIM; ++q) ji[q] = (float)Ji[q / DIM][q % DIM];
       }
       const float w = sw[g] * detJ * Eel[sel[e]];
       const float sq = sqrtf(fabsf(w));
       if (w < 0.f) atomicOr(sneg, 1);
-      const int kb = (g >> 2) * 512 + (g & 3);   // (k/4) * 128 rows * 4 + k % 4, in floats
 #pragma unroll
-      for (int ii = 0; ii < S::NCH; ++ii)
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          const float v = gr[ii][c] * sq;
-          const uint32_t hi = tc_tf32_round(v);
-          const uint32_t lo = tc_tf32_round(v - __uint_as_float(hi));
-          const int o = kb + tc_row<ET>(e, i0 + ii, c) * 4;
-          aH[o] = __uint_as_float(hi);
-          aL[o] = __uint_as_float(lo);
-        }
-      if (h == 0) swt[e * ngp + g] = w;
+      for (int q = 0; q < DIM * DIM; ++q) ji[q] *= sq;
+      swt[t] = w;
     }
     __syncthreads();
-    const bool need_b = *sneg != 0;
-    if (need_b) {   // B = A with the columns of negative weights negated
-      for (int t = tid; t < ne * ngp; t += kTcThreads) {
-        const int e = t / ngp, g = t % ngp;
-        const float sgn = swt[e * ngp + g] < 0.f ? -1.f : 1.f;
-        const int kb = (g >> 2) * 512 + (g & 3);
+    // operand tiles: a thread per (element, row (i, c), 4 Gauss points) forms
+    // A[(i,c)][k] = sum_b (sqrt|W| J^-1)[c][b] dN_i/dxi_b at k, splits it into TF32 hi + lo
+    // and stores each as one 16-byte chunk (consecutive threads: consecutive rows, so the
+    // stores are conflict-free); Gauss points past ngp give zeros
+    {
+      const int KC = (ngp + 7) / 8 * 2;           // 4-point chunks of the padded K
+      const int nrow = ne * S::RAW;
+      for (int t = tid; t < nrow * KC; t += kTcThreads) {
+        const int kc = t / nrow, rem = t - kc * nrow;
+        const int e = rem / S::RAW, r = rem - e * S::RAW;
+        const int i = r / DIM, c = r - i * DIM;
+        float hv[4], lv[4];
 #pragma unroll
-        for (int i = 0; i < NEN; ++i)
+        for (int u = 0; u < 4; ++u) {
+          const int g = 4 * kc + u;
+          float v = 0.f;
+          if (g < ngp) {
+            const float* ji = sji + (e * ngp + g) * DIM * DIM + c * DIM;
+            const float* dN = sdN + g * DIM * NEN + i;
 #pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            const int o = kb + tc_row<ET>(e, i, c) * 4;
-            bH[o] = sgn * aH[o];
-            bL[o] = sgn * aL[o];
+            for (int b = 0; b < DIM; ++b) v += ji[b] * dN[b * NEN];
           }
+          const uint32_t hb = tc_tf32_round(v);
+          hv[u] = __uint_as_float(hb);
+          lv[u] = __uint_as_float(tc_tf32_round(v - hv[u]));
+        }
+        const int o = kc * 512 + tc_row<ET>(e, i, c) * 4;
+        *reinterpret_cast<float4*>(aH + o) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+        *reinterpret_cast<float4*>(aL + o) = make_float4(lv[0], lv[1], lv[2], lv[3]);
       }
     }
     // make the generic-proxy tile writes visible to the tensor cores
@@ -289,10 +266,13 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
     __syncthreads();
     tc_fence_after();
 
-    // ---- 2. M = A B^T on the tensor cores ---------------------------------------------
-    if (tid == 0) {
+    // ---- 2. M = A A^T on the tensor cores ---------------------------------------------
+    // (a group with a negative weight, i.e. an inverted element, forms M on the CUDA cores
+    // in step 3 instead: M = A S A^T with S the signs of the weights)
+    const bool neg = *sneg != 0;
+    if (tid == 0 && !neg) {
       const uint32_t ah = tc_smem_u32(aH), al = tc_smem_u32(aL);
-      const uint32_t bh = need_b ? tc_smem_u32(bH) : ah, bl = need_b ? tc_smem_u32(bL) : al;
+      const uint32_t bh = ah, bl = al;
       const uint32_t lbo = 128 * 16, sbo = 128;   // next K chunk of 4; next 8-row group
       for (int ks = 0; ks < KP / 8; ++ks) {
         const uint32_t off = (uint32_t)ks * 2 * lbo;
@@ -303,8 +283,8 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
       }
       tc_commit(mbar);
     }
-    const bool done = tc_mbar_wait(mbar, phase, kTcMaxWaitIters);
-    phase ^= 1u;
+    const bool done = neg || tc_mbar_wait(mbar, phase, kTcMaxWaitIters);
+    if (!neg) phase ^= 1u;
     if (!done) {   // the tensor-core work did not complete in time: report and stop
       if (lane == 0) atomicExch(err, 1);
       ok = false;
@@ -316,7 +296,34 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
     // ---- 3. rows of M -> node-pair blocks -> ELL ---------------------------------------
     {
       float v[S::LW];
-      if constexpr (S::WPE > 1) {
+      if (neg) {
+        // M[r][c] = sum_k sign(w_k) A[r][k] A[c][k] with A = hi + lo from the tiles: this
+        // lane's row r against the columns of its own element
+        int e0l, i0l;
+        if constexpr (S::WPE > 1) {
+          e0l = warp / S::WPE;
+          i0l = (warp % S::WPE) * S::NPW + lane / DIM;
+        } else {
+          e0l = warp * S::EPW + lane / S::RPE;
+          i0l = (lane % S::RPE) / DIM;
+        }
+        const int rr = warp * 32 + lane;
+#pragma unroll
+        for (int j = 0; j < NEN; ++j)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) {
+            const int cc = tc_row<ET>(e0l < EPG ? e0l : 0, j, b);
+            double acc = 0.0;   // FP64 products and sum of the split operands (hi + lo exact)
+            if (e0l < ne && i0l < NEN)
+              for (int g = 0; g < ngp; ++g) {
+                const int kb = (g >> 2) * 512 + (g & 3);
+                const double sg = swt[e0l * ngp + g] < 0.f ? -1.0 : 1.0;
+                acc += sg * ((double)aH[kb + rr * 4] + (double)aL[kb + rr * 4]) *
+                       ((double)aH[kb + cc * 4] + (double)aL[kb + cc * 4]);
+              }
+            v[tc_col<ET>(j, b)] = (float)acc;
+          }
+      } else if constexpr (S::WPE > 1) {
         const int e = warp / S::WPE;
         float t0[32], t1[32];
         const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(e * S::LW);
@@ -340,7 +347,7 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
           v[c] = x;
         }
       }
-      tc_wait_ld();
+      if (!neg) tc_wait_ld();
 
       // this lane's (element, node, component)
       int e, i, a;
@@ -354,6 +361,22 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
         a = (lane % S::RPE) % DIM;
       }
       const bool valid = i < NEN && (S::WPE > 1 ? lane < S::NPW * DIM : true) && e < ne;
+      if constexpr (GRAM) {
+        // this lane's row of M, (node i, component a), as RAW contiguous floats
+        if (valid) {
+          constexpr int RAW = S::RAW;
+          float* dst = K + (int64_t)sel[e] * RAW * RAW + (int64_t)(i * DIM + a) * RAW;
+#pragma unroll
+          for (int q = 0; q < RAW / 4; ++q) {
+            float4 w4;
+            w4.x = v[tc_col<ET>((4 * q) / DIM, (4 * q) % DIM)];
+            w4.y = v[tc_col<ET>((4 * q + 1) / DIM, (4 * q + 1) % DIM)];
+            w4.z = v[tc_col<ET>((4 * q + 2) / DIM, (4 * q + 2) % DIM)];
+            w4.w = v[tc_col<ET>((4 * q + 3) / DIM, (4 * q + 3) % DIM)];
+            __stcs(reinterpret_cast<float4*>(dst) + q, w4);
+          }
+        }
+      } else {
       const int ni = valid ? sconn[e * NEN + i] : 0;
 #pragma unroll
       for (int j = 0; j < NEN; ++j) {
@@ -396,6 +419,7 @@ k_assemble_tc(const int32_t* __restrict__ elems, int count, int ngp,
           add_rows<DIM, float, ATOMIC>(&K[(int64_t)(slot * DIM + a) * n + (int64_t)ni * DIM], col);
         }
       }
+      }
     }
     tc_fence_before();
     __syncthreads();
@@ -414,8 +438,12 @@ gf_status launch_tc(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K, 
   // at most 4 CTAs per SM (4 x 128 TMEM columns = the SM's 512): each asks for at least a
   // quarter of the SM's 228 KB of shared memory, less the 1 KB the system reserves per CTA
   const size_t sm = std::max(L.total, (size_t)56 * 1024);
-  auto kc = k_assemble_tc<ET, false>;
-  auto ka = k_assemble_tc<ET, true>;
+  auto kc = k_assemble_tc<ET, 0>;
+  auto ka = k_assemble_tc<ET, 1>;
+  auto kg = k_assemble_tc<ET, 2>;
+  GF_CUDA(ctx, cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GF_CUDA(ctx, cudaFuncSetAttribute(kg, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
   GF_CUDA(ctx, cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   // the whole unified L1/shared array as shared memory, so that the occupancy query and the
@@ -425,11 +453,20 @@ gf_status launch_tc(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K, 
   GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributePreferredSharedMemoryCarveout,
                                     (int)cudaSharedmemCarveoutMaxShared));
   // resident CTAs per SM: registers, shared memory and the 512 TMEM columns of an SM
-  const int per_sm = tc_ctas_per_sm(ka, kTcThreads, sm, kTcCols);
+  const int per_sm = tc_ctas_per_sm(scatter == GF_SCATTER_OWNER    ? kg
+                                    : scatter == GF_SCATTER_ATOMIC ? ka : kc,
+                                    kTcThreads, sm, kTcCols);
   const int grid_cap = ctx->sm_count * per_sm;
   const float lam1 = (float)ctx->lam1, mu1 = (float)ctx->mu1;
   constexpr int EPG = TcShape<ET>::EPG;
-  if (scatter == GF_SCATTER_ATOMIC) {
+  if (scatter == GF_SCATTER_OWNER) {   // Gram matrices to K (the `K` argument) for the gather
+    const int count = ctx->nelem;
+    const int grid = std::min(grid_cap, (count + EPG - 1) / EPG);
+    kg<<<grid, kTcThreads, sm, ctx->stream>>>(ctx->d_allperm, count, ctx->ngp, ctx->d_conn,
+                                              ctx->d_coords64, ctx->d_Eel32, nullptr,
+                                              ctx->nelem, ctx->n, d_tab, lam1, mu1, K, d_err);
+    GF_LAUNCH_CHECK(ctx, "k_assemble_tc(gram)");
+  } else if (scatter == GF_SCATTER_ATOMIC) {
     const int count = ctx->nelem;
     const int grid = std::min(grid_cap, (count + EPG - 1) / EPG);
     ka<<<grid, kTcThreads, sm, ctx->stream>>>(ctx->d_allperm, count, ctx->ngp, ctx->d_conn,
@@ -452,8 +489,10 @@ gf_status launch_tc(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K, 
 
 }  // namespace
 
-// FP32 assembly with the tcgen05 tensor-core engine (colour or atomic schedule); d_err
-// (device int, zeroed by the caller) is set if an MMA-completion wait timed out.
+// FP32 assembly with the tcgen05 tensor-core engine (colour or atomic schedule: into K;
+// owner schedule: each element's Gram matrix into K as nelem x RAW x RAW floats, which
+// gf_assemble_owner_gram then gathers); d_err (device int, zeroed by the caller) is set if
+// an MMA-completion wait timed out.
 gf_status gf_assemble_tc(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K, int* d_err) {
   switch (ctx->elem_type) {
     case GF_Q4: return launch_tc<GF_Q4>(ctx, scatter, d_tab, K, d_err);

@@ -192,6 +192,8 @@ struct gf_ctx {
   float* d_Eel32 = nullptr;
   void* d_asmtab = nullptr;      // shape-derivative tables (gf_assemble.cu)
   int* d_asm_err = nullptr;      // tensor-core assembly: set when an MMA wait timed out
+  float* d_gram = nullptr;       // tensor-core owner schedule: element Gram matrices
+  size_t gram_bytes = 0;
 
   // colouring
   int ncolors = 0;

@@ -231,7 +231,8 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  for (int q = tid; q < P * NOP * KDP; q += kMmThreads) {
+#pragma unroll 8
+  for (int q = tid; q < P * NOP * KDP; q += kMmThreads) {   // unrolled: the loads overlap
     const int p = q / (NOP * KDP), rem = q % (NOP * KDP);
     const int n = rem / KDP, k = rem % KDP;
     float v = 0.f;
@@ -257,6 +258,7 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
     const int a0 = tile * 128;
     for (int p = 0; p < P && ok; ++p) {
       const float* X = p == 0 ? X1 : X2;
+#pragma unroll 4
       for (int q = tid; q < 128 * NCH; q += kMmThreads) {
         const int r = q & 127, c = q >> 7;   // consecutive threads: consecutive 16-byte rows
         const int a = a0 + r;
@@ -403,7 +405,8 @@ k_lp_aggregate(int N, const int32_t* __restrict__ adj_off, const int32_t* __rest
     const int a = (int)(t / H), c = (int)(t % H);
     float s = 0.f;
     const int q1 = adj_off[a + 1];
-    for (int q = adj_off[a]; q < q1; ++q) {
+#pragma unroll 8
+    for (int q = adj_off[a]; q < q1; ++q) {   // unrolled: the neighbours' gathers overlap
       const int b = __ldg(adj + q);
       const float v = __ldg(h + (int64_t)b * H + c);
       s += backward ? v * __ldg(deg_inv + b) : v;
