@@ -544,6 +544,65 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 48, n_test: int
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def run_sharded_arm(args):
+    """--sharded: the workload split into node slabs over the ranks (one halo layer of
+    elements each, gpufem_b200.shard).  Every rank assembles its local mesh (owner
+    schedule, FP32 K for the metric; FP64 K for the solve) and all ranks run the
+    device-resident sharded Jacobi-PCG (gf_dist_pcg, NCCL on the library stream) to a
+    relative residual of 1e-8.  value = workload elements / max-over-ranks assembly time
+    (strong scaling: the total work is fixed)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from gpufem_b200 import _lib
+    from gpufem_b200 import meshgen as mg
+    from gpufem_b200 import shard as sd
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    if not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        dist.init_process_group("nccl", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=300))
+    cfg = args.config
+    m = mg.workload(cfg)
+    solver = sd.ShardedSolver(m, rank, world, device=local, scatter=_lib.GF_SCATTER_OWNER)
+    ctx = solver.ctx
+    # assembly throughput of the local meshes (FP32, owner schedule), max over ranks
+    for _ in range(args.warmup):
+        ctx.assemble(_lib.GF_F32, _lib.GF_SCATTER_OWNER)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ts = [ctx.assemble(_lib.GF_F32, _lib.GF_SCATTER_OWNER) for _ in range(args.steps)]
+    t = torch.tensor([float(sum(ts))], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    per_step = float(t.item()) / args.steps
+    # the solve: the FP64 system the solver holds (assembled and constrained at set-up)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+    ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
+    solver.solve_device(tol=1e-8, max_iter=400000)          # warm: solver layout built
+    x, info = solver.solve_device(tol=1e-8, max_iter=400000)
+    st = torch.tensor([info.seconds], device="cuda", dtype=torch.float64)
+    dist.all_reduce(st, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        line = {"metric": METRIC, "value": m.nelem / per_step, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": dict(workload_config(cfg, m, world), parallelism=f"node slabs x{world}"),
+                "sharded_solve": {"solver": "gf_dist_pcg (Jacobi-PCG, FP64, NCCL halo exchange "
+                                            "and all-reduces on the library stream)",
+                                  "iterations": info.iterations, "seconds_max_over_ranks":
+                                  float(st.item()), "us_per_iteration":
+                                  float(st.item()) / max(1, info.iterations) * 1e6,
+                                  "status": info.status},
+                "local_dofs": solver.shard.n_local, "owned_dofs": solver.shard.n_owned}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_gpu_arm(args):
     import torch
     rank, world, local = dist_info()
@@ -557,7 +616,7 @@ def run_gpu_arm(args):
     from gpufem_b200.fem import Context
 
     cfg = args.config
-    m = mg.workload(cfg)
+    m = mg.workload(cfg, scale=args.scale)
     dtype = _lib.GF_F64 if cfg == "q4_64" else _lib.GF_F32
     esize = 8 if dtype == _lib.GF_F64 else 4
     ctx = Context(local)
@@ -777,7 +836,8 @@ def run_gpu_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if esize == 4 else "f64", "data": "synthetic",
-            "config": workload_config(cfg, m, world),
+            "config": dict(workload_config(cfg, m, world),
+                           **({"scale": args.scale} if args.scale != 1.0 else {})),
             "matrix": {"dofs": n, "nnz": nnz, "ell_width": W},
             "timing": "device time (CUDA events on the library's stream); L2 flushed (256 MB "
                       "write) before every timed step",
@@ -826,6 +886,12 @@ def main():
     ap.add_argument("--solvers", default=",".join(SOLVERS),
                     help="comma list of the solve block's entries (default: all)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="mesh edge scale of the workload (1 = the full workload; smaller "
+                         "cases for profiler captures)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="split the workload over the ranks (node slabs) and solve with the "
+                         "device-resident sharded PCG instead of running replicas")
     ap.add_argument("--no-north-star", action="store_true",
                     help="skip the Brick20 64^3 assembly + solve study of the default run")
     ap.add_argument("--scatter", default="auto", choices=["owner", "colour", "atomic", "auto"])
@@ -834,6 +900,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.sharded:
+        run_sharded_arm(args)
     else:
         run_gpu_arm(args)
 

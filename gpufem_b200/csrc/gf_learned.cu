@@ -205,10 +205,17 @@ __host__ __device__ constexpr int mm_pad16(int x) { return x < 16 ? 16 : (x + 15
 __host__ __device__ constexpr int mm_pad8(int x) { return (x + 7) / 8 * 8; }
 __host__ __device__ constexpr int mm_tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : 128; }
 
+// X hi/lo tiles, reused after the MMAs as the output staging tile [128][NO + 1]
+template <int KD, int NO>
+__host__ __device__ constexpr size_t mm_xbytes() {
+  return (size_t)2 * 128 * mm_pad8(KD) * 4 > (size_t)128 * (NO + 1) * 4
+             ? (size_t)2 * 128 * mm_pad8(KD) * 4 : (size_t)128 * (NO + 1) * 4;
+}
+
 template <int KD, int NO, bool TWO>
 __host__ __device__ constexpr size_t mm_smem_bytes() {
   constexpr int KDP = mm_pad8(KD), NOP = mm_pad16(NO), P = TWO ? 2 : 1;
-  return (size_t)2 * 128 * KDP * 4          // X hi, lo (one part at a time)
+  return (mm_xbytes<KD, NO>() + 15) / 16 * 16  // X hi, lo / output staging
          + (size_t)P * NOP * KDP * 4        // W parts
          + (size_t)NOP * 4 + 16;            // bias, mbarrier, TMEM address
 }
@@ -225,7 +232,8 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
   extern __shared__ __align__(1024) unsigned char smem[];
   float* xh = reinterpret_cast<float*>(smem);
   float* xl = xh + 128 * KDP;
-  float* wt = xl + 128 * KDP;                  // [P][KDP/4][NOP][4]
+  float* stage = xh;                           // [128][NO + 1] after the MMAs
+  float* wt = reinterpret_cast<float*>(smem + (mm_xbytes<KD, NO>() + 15) / 16 * 16);
   float* sb = wt + P * NOP * KDP;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sb + NOP);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
@@ -260,13 +268,29 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
       const float* X = p == 0 ? X1 : X2;
 #pragma unroll 4
       for (int q = tid; q < 128 * NCH; q += kMmThreads) {
-        const int r = q & 127, c = q >> 7;   // consecutive threads: consecutive 16-byte rows
+        // a warp takes 8 rows x 4 chunks (when NCH >= 4): 64 contiguous bytes of each of 8
+        // rows in global memory, a 4-way bank conflict at most in shared memory
+        int r, c;
+        if constexpr (NCH % 4 == 0) {
+          const int ln = q & 31, wq = q >> 5;
+          r = (wq & 15) * 8 + (ln & 7);
+          c = (wq >> 4) * 4 + (ln >> 3);
+        } else {
+          r = q & 127;
+          c = q >> 7;
+        }
         const int a = a0 + r;
         float v[4];
+        if constexpr (KD % 4 == 0) {
+          float4 x4 = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (a < N && 4 * c < KD) x4 = __ldg(reinterpret_cast<const float4*>(X + (int64_t)a * KD) + c);
+          v[0] = x4.x; v[1] = x4.y; v[2] = x4.z; v[3] = x4.w;
+        } else {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int k = 4 * c + u;
-          v[u] = (a < N && k < KD) ? __ldg(X + (int64_t)a * KD + k) : 0.f;
+          for (int u = 0; u < 4; ++u) {
+            const int k = 4 * c + u;
+            v[u] = (a < N && k < KD) ? __ldg(X + (int64_t)a * KD + k) : 0.f;
+          }
         }
         float4 h, l;
         float* hp = &h.x;
@@ -321,17 +345,25 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
       for (int j = 0; j < 16; ++j) acc[j] = t[j];
     }
     tc_wait_ld();
-    if (a < N) {
-      float* o = out + (int64_t)a * NO;
+    (void)a;
+    // stage the tile's outputs in shared memory (row stride NO + 1: conflict-free), then
+    // store them with consecutive threads on consecutive channels (coalesced)
+    const int rr = warp * 32 + lane;
 #pragma unroll
-      for (int c = 0; c < NO; ++c) {
-        const float v = acc[c] + sb[c];
-        if (pre) pre[(int64_t)a * NO + c] = v;
+    for (int c = 0; c < NO; ++c) stage[rr * (NO + 1) + c] = acc[c] + sb[c];
+    tc_fence_before();
+    __syncthreads();
+    for (int q = tid; q < 128 * NO; q += kMmThreads) {
+      const int r = q / NO, c = q - r * NO;
+      const int an = a0 + r;
+      if (an < N) {
+        const float v = stage[r * (NO + 1) + c];
+        const int64_t o = (int64_t)an * NO + c;
+        if (pre) pre[o] = v;
         const float y = (relu && v < 0.f) ? 0.f : v;
-        o[c] = accumulate ? o[c] + y : y;
+        out[o] = accumulate ? out[o] + y : y;
       }
     }
-    tc_fence_before();
     __syncthreads();
   }
   tc_fence_before();

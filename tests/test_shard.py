@@ -185,8 +185,10 @@ def test_sharded_device_pcg_one_rank_matches_single_gpu_solve():
     ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-8, max_iter=100000)
     info = ctx.solve(_lib.GF_SOLVER_PCG, _lib.GF_F64, tol=1e-8, max_iter=100000)
     u1 = ctx.solution()
-    assert info_d2.status == _lib.GF_OK and abs(info_d2.iterations - info.iterations) <= 2
-    # (dot products are summed by atomics, so two runs agree to rounding, not bitwise)
+    # (dot products are summed by atomics, so two runs agree to rounding, not bitwise; over
+    # ~13,000 iterations that moves the stopping iteration by a few)
+    assert info_d2.status == _lib.GF_OK
+    assert abs(info_d2.iterations - info.iterations) <= max(2, info.iterations // 1000)
     assert np.linalg.norm(x - x2) <= 1e-6 * np.linalg.norm(x)
     assert np.linalg.norm(u - u1) <= 1e-6 * np.linalg.norm(u1)
     per_it_d = info_d2.seconds / info_d2.iterations

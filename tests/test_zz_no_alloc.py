@@ -79,7 +79,8 @@ def test_pcg_noalloc_iteration_cap_zero_rhs_and_null_outputs():
                                  C.byref(rel))
     torch.cuda.synchronize()
     assert st == _lib.GF_ERR_NOT_CONVERGED and it.value == 3
-    assert 1e-8 < rel.value < 1.0
+    # (the CG residual norm is not monotone: after 3 steps it may sit just above 1)
+    assert TOL < rel.value < 10.0
     # a zero right-hand side: converged at once, x = 0
     z = torch.zeros_like(b)
     x.fill_(float("nan"))
