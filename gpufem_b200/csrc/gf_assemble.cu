@@ -198,8 +198,8 @@ gf_status launch_et(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* K) {
   const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
   auto kc = k_assemble<ET, TC, false>;
   auto ka = k_assemble<ET, TC, true>;
-  GF_CUDA(ctx, cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GF_CUDA(ctx, gf_smem_attr(kc, (int)sm));
+  GF_CUDA(ctx, gf_smem_attr(ka, (int)sm));
   if (scatter == GF_SCATTER_ATOMIC) {
     const int count = ctx->nelem;
     ka<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
@@ -289,6 +289,7 @@ gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine) {
       ctx->gram_bytes = need;
     }
   }
+  if (scatter != GF_SCATTER_OWNER && (st = gf_slotmap_ensure(ctx)) != GF_OK) return st;
   cudaEventRecord(ctx->ev0, ctx->stream);
   if (mma && scatter == GF_SCATTER_OWNER) {
     // tensor cores: every element's Gram matrix to HBM; owner gather: K written once

@@ -125,22 +125,33 @@ k_elem_geometry(int nelem, int ngp, int EB, const int32_t* __restrict__ conn,
 
 // Thread per element (element types with at most 24 coordinates): the element's
 // local coordinates stay in registers (FP64, plus their FP32 rounding) and the Gauss
-// rule is a compile-time table; same arithmetic and output as k_elem_geometry.  Each
-// warp stages its 32 elements' output in shared memory and stores it as one
-// contiguous, coalesced block.
+// rule is a compile-time table; same arithmetic and output as k_elem_geometry.  With
+// NODE (the input of k_assemble_owner_node) an element's block starts every PS values,
+// PS = PER rounded up to 8 (zero padding: 32-byte aligned blocks for vector loads), and
+// the stored w detJ is multiplied by the element's modulus (the product the owner
+// kernel would otherwise form per Gauss point).  Each warp stages its 32 elements'
+// output in shared memory and stores it as one contiguous, coalesced block.
 template <int ET, typename TC, int NG1>
+constexpr int geo_stride(bool node) {
+  constexpr int PER = GpTable<ET, NG1>::NGP * (gf_elem_info(ET).dim * gf_elem_info(ET).dim + 1);
+  return node ? (PER + 7) / 8 * 8 : PER;
+}
+
+template <int ET, typename TC, int NG1, bool NODE>
 __global__ void __launch_bounds__(kOT)
 k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
-                   const double* __restrict__ coords, TC* __restrict__ geo) {
+                   const double* __restrict__ coords, const TC* __restrict__ Eel,
+                   TC* __restrict__ geo) {
   constexpr ElemInfo info = gf_elem_info(ET);
   constexpr int NEN = info.nen, DIM = info.dim, GS = DIM * DIM + 1;
   constexpr int NGP = GpTable<ET, NG1>::NGP;
   constexpr int PER = NGP * GS;  // output values per element
+  constexpr int PS = geo_stride<ET, TC, NG1>(NODE);
   constexpr GpTable<ET, NG1> Tab = gf_gp_table<ET, NG1>();
   // 1-D weights (1, 1) or (5/9, 8/9, 5/9), multiplied in the reference's tensor order
   constexpr double w1[3] = {NG1 == 2 ? 1.0 : 5.0 / 9.0, NG1 == 2 ? 1.0 : 8.0 / 9.0, 5.0 / 9.0};
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TC* stage = reinterpret_cast<TC*>(smem_raw) + (size_t)(threadIdx.x >> 5) * 32 * PER;
+  TC* stage = reinterpret_cast<TC*>(smem_raw) + (size_t)(threadIdx.x >> 5) * 32 * PS;
   const bool f64 = sizeof(TC) == 8;
   const int lane = threadIdx.x & 31;
   const int e0 = (blockIdx.x * kOT + threadIdx.x) & ~31;  // first element of the warp
@@ -185,7 +196,10 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
       }
       use64 = dmax > 10.f * dmin;
     }
-    TC* out = stage + lane * PER;
+    TC* out = stage + lane * PS;
+#pragma unroll
+    for (int k = PER; k < PS; ++k) out[k] = TC(0);
+    const TC Ee = NODE ? Eel[e] : TC(1);
 #pragma unroll
     for (int g = 0; g < NGP; ++g) {
       const int gi = DIM == 2 ? g / NG1 : g / (NG1 * NG1);
@@ -208,7 +222,7 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
         for (int a = 0; a < DIM; ++a)
 #pragma unroll
           for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
-        out[g * GS + DIM * DIM] = TC(wg * d);
+        out[g * GS + DIM * DIM] = NODE ? TC(wg * d) * Ee : TC(wg * d);
       } else {
         float J[3][3], Ji[3][3];
 #pragma unroll
@@ -225,15 +239,15 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
         for (int a = 0; a < DIM; ++a)
 #pragma unroll
           for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
-        out[g * GS + DIM * DIM] = TC((float)wg * d);
+        out[g * GS + DIM * DIM] = NODE ? TC((float)wg * d) * Ee : TC((float)wg * d);
       }
     }
   }
   __syncwarp();
   // the warp's elements are consecutive: their outputs form one contiguous block
   const int nw = min(32, nelem - e0);
-  TC* dst = geo + (int64_t)e0 * PER;
-  for (int k = lane; k < nw * PER; k += 32) dst[k] = stage[k];
+  TC* dst = geo + (int64_t)e0 * PS;
+  for (int k = lane; k < nw * PS; k += 32) dst[k] = stage[k];
 }
 
 // Block rows H_j, j in [J0, J0 + JG), of one task with the Gauss rule known at compile
@@ -418,6 +432,201 @@ k_assemble_owner(int nnodes, int n, int W, int NB, int ngp,
 }
 
 // ---------------------------------------------------------------------------
+// 2-D FP32 owner kernel, thread per owned node.  A CTA owns NB consecutive nodes, one
+// thread each, and keeps their 2 NB rows as a shared-memory tile [slot][row].  The CTA
+// first orders its nodes by degree (incident elements), highest first, so that the
+// nodes of a warp walk the same number of elements.  A thread then walks its node's
+// incident elements in incidence order and adds the node's block row of each Ke into
+// its own two tile rows (row pair = the thread's position, mapped back to the node's rows
+// by the store) with plain read-modify-writes: no other thread touches them, so no
+// atomics are needed and the sum over elements has a fixed order.  Per Gauss
+// point, g_i = w detJ E J^-T dN_i (dN_i from shared memory: i is known at run time) and
+// g_j = J^-T dN_j (dN_j instruction constants) form H_j += g_i g_j^T, two entries per
+// packed FMA (fma.rn.f32x2: two IEEE single-precision FMAs in one instruction).  J^-1
+// and w detJ E are read as 32-byte loads (element stride PS, a multiple of 8 floats):
+// the lanes of a warp read 32 different elements, so the number of load requests, not
+// the bytes, sets the load cost.  The tile is stored once, two rows per 8-byte store.
+constexpr int kDegBuckets = 32;
+
+// 8 consecutive floats from a 32-byte aligned address of read-only data
+__device__ __forceinline__ void ldg8(const float* p, float (&v)[8]) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]),
+        "=f"(v[7])
+      : "l"(p));
+}
+
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
+template <int ET, int NG1, int NB>
+size_t owner_node_smem_bytes(int W) {
+  constexpr int NEN = gf_elem_info(ET).nen;
+  return sizeof(float) * (size_t)W * 2 * NB + sizeof(float2) * NG1 * NG1 * NEN +
+         sizeof(int) * (3 * NB + 1 + (NB / 32 + 1) * kDegBuckets);
+}
+
+// One task of k_assemble_owner_node: the owned node's block row of the element whose
+// geometry block is gv (local index i of the node, incidence entry q), added into the
+// node's two tile rows.
+template <int ET, int NG1, int RB>
+__device__ __forceinline__ void owner_node_task(const float* gv, int i, int64_t q,
+                                                const uint16_t* __restrict__ inc_slot,
+                                                const float2* sdN, float lam1, float mu1,
+                                                float* myrows) {
+  constexpr int NEN = gf_elem_info(ET).nen, GS = 5, NGP = NG1 * NG1;
+  constexpr GpTable<ET, NG1> Tab = gf_gp_table<ET, NG1>();
+  float2 H[NEN][2];   // H[j][a] = (H_j[a][0], H_j[a][1])
+#pragma unroll
+  for (int j = 0; j < NEN; ++j) H[j][0] = H[j][1] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int g = 0; g < NGP; ++g) {
+    const float j00 = gv[g * GS], j01 = gv[g * GS + 1];
+    const float j10 = gv[g * GS + 2], j11 = gv[g * GS + 3];
+    const float wd = gv[g * GS + 4];   // w detJ E
+    const float2 dn = sdN[g * NEN + i];
+    const float gi0 = fmaf(j01, dn.y, j00 * dn.x) * wd;
+    const float gi1 = fmaf(j11, dn.y, j10 * dn.x) * wd;
+    const float2 g0 = make_float2(gi0, gi0), g1 = make_float2(gi1, gi1);
+#pragma unroll
+    for (int j = 0; j < NEN; ++j) {
+      const float d0 = Tab.d32[(g * 2) * NEN + j], d1 = Tab.d32[(g * 2 + 1) * NEN + j];
+      const float2 gj = make_float2(fmaf(j01, d1, j00 * d0), fmaf(j11, d1, j10 * d0));
+      H[j][0] = fma2(g0, gj, H[j][0]);
+      H[j][1] = fma2(g1, gj, H[j][1]);
+    }
+  }
+  // neighbour slots of the element's nodes (16 or 8 bytes, aligned: q * NEN * 2 bytes)
+  uint32_t sw[NEN / 2];
+  if constexpr (NEN == 8) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(inc_slot + q * NEN));
+    sw[0] = v.x; sw[1] = v.y; sw[2] = v.z; sw[3] = v.w;
+  } else {
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(inc_slot + q * NEN));
+    sw[0] = v.x; sw[1] = v.y;
+  }
+#pragma unroll
+  for (int j = 0; j < NEN; ++j) {
+    const int p = (int)((sw[j >> 1] >> (16 * (j & 1))) & 0xFFFFu);
+    const float h00 = H[j][0].x, h01 = H[j][0].y, h10 = H[j][1].x, h11 = H[j][1].y;
+    const float tr = h00 + h11;
+    // V = lam1 H + mu1 H^T + mu1 tr(H) I; column b of V is rows (2 al, 2 al + 1) of
+    // tile column 2 p + b: two adjacent floats
+    float2* c0 = reinterpret_cast<float2*>(myrows + (size_t)(2 * p) * RB);
+    float2* c1 = reinterpret_cast<float2*>(myrows + (size_t)(2 * p + 1) * RB);
+    float2 x0 = *c0, x1 = *c1;
+    x0.x += fmaf(mu1, tr, fmaf(mu1, h00, lam1 * h00));
+    x0.y += fmaf(mu1, h01, lam1 * h10);
+    x1.x += fmaf(mu1, h10, lam1 * h01);
+    x1.y += fmaf(mu1, tr, fmaf(mu1, h11, lam1 * h11));
+    *c0 = x0;
+    *c1 = x1;
+  }
+}
+
+template <int PS>
+__device__ __forceinline__ void load_geo(const float* ge, float (&gv)[PS]) {
+#pragma unroll
+  for (int c = 0; c < PS / 8; ++c) {
+    float v[8];
+    ldg8(ge + 8 * c, v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) gv[8 * c + k] = v[k];
+  }
+}
+
+template <int ET, int NG1, int NB>
+__global__ void __launch_bounds__(NB)
+k_assemble_owner_node(int nnodes, int n, int W, const int32_t* __restrict__ inc_off,
+                      const int32_t* __restrict__ inc, const uint8_t* __restrict__ inc_loc,
+                      const uint16_t* __restrict__ inc_slot, const float* __restrict__ geo,
+                      const AsmTables* __restrict__ tab, float lam1, float mu1,
+                      float* __restrict__ K) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  static_assert(info.dim == 2, "2-D elements");
+  constexpr int NEN = info.nen, GS = 5, NGP = NG1 * NG1, RB = 2 * NB, NW = NB / 32;
+  constexpr int PS = geo_stride<ET, float, NG1>(true);
+  constexpr GpTable<ET, NG1> Tab = gf_gp_table<ET, NG1>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* tile = reinterpret_cast<float*>(smem_raw);                // [W][RB]
+  float2* sdN = reinterpret_cast<float2*>(tile + (size_t)W * RB);  // [NGP][NEN]
+  int* soff = reinterpret_cast<int*>(sdN + NGP * NEN);             // [NB + 1]
+  int* sord = soff + NB + 1;                                       // [NB] node of a thread
+  int* spos = sord + NB;                                           // [NB] thread of a node
+  int* wcnt = spos + NB;                                           // [NW + 1][kDegBuckets]
+
+  const int t = threadIdx.x;
+  const int a0 = blockIdx.x * NB;
+  const int na = min(NB, nnodes - a0);
+  {
+    float4* t4 = reinterpret_cast<float4*>(tile);   // W * RB is a multiple of 4
+    for (int k = t; k < W * RB / 4; k += NB) t4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  for (int k = t; k < NGP * NEN; k += NB) {
+    const int g = k / NEN, i = k - g * NEN;
+    sdN[k] = make_float2(tab->dN32[(g * 2) * NEN + i], tab->dN32[(g * 2 + 1) * NEN + i]);
+  }
+  for (int k = t; k <= na; k += NB) soff[k] = inc_off[a0 + k];
+  for (int k = t; k < NW * kDegBuckets; k += NB) wcnt[k] = 0;
+  __syncthreads();
+  // stable counting sort of the CTA's nodes by degree, highest first: a node's position
+  // is the count of nodes of higher degree plus the nodes of its degree before it (per
+  // warp with a match mask, then over the warps).  The node at position t is summed by
+  // thread t into tile row pair t, so a warp's 8-byte tile accesses fall on distinct
+  // banks; the store maps the pairs back to the nodes' rows.
+  const int warp = t >> 5, lane = t & 31;
+  const int bkt = t < na ? min(soff[t + 1] - soff[t], kDegBuckets - 1) : -1;
+  const unsigned same = __match_any_sync(0xffffffffu, bkt);
+  const int wrank = __popc(same & ((1u << lane) - 1u));
+  if (bkt >= 0 && wrank == 0) wcnt[warp * kDegBuckets + bkt] = __popc(same);
+  __syncthreads();
+  if (t == 0) {
+    int acc = 0;
+    for (int b = kDegBuckets - 1; b >= 0; --b)
+      for (int w = 0; w < NW; ++w) {
+        const int c = wcnt[w * kDegBuckets + b];
+        wcnt[w * kDegBuckets + b] = acc;
+        acc += c;
+      }
+  }
+  __syncthreads();
+  if (bkt >= 0) {
+    const int pos = wcnt[warp * kDegBuckets + bkt] + wrank;
+    sord[pos] = t;
+    spos[t] = pos;
+  }
+  __syncthreads();
+
+  const int al = t < na ? sord[t] : 0;
+  const int q0 = soff[al];
+  const int deg = t < na ? soff[al + 1] - q0 : 0;
+  float* myrows = tile + 2 * t;
+  for (int k = 0; k < deg; ++k) {
+    float gv[PS];
+    load_geo(geo + (int64_t)__ldg(inc + q0 + k) * PS, gv);
+    owner_node_task<ET, NG1, RB>(gv, __ldg(inc_loc + q0 + k), q0 + k, inc_slot, sdN, lam1, mu1,
+                                 myrows);
+  }
+  __syncthreads();
+  // store: warp w takes slots w, w + NB/32, ...; lanes stride the block's row pairs
+  // (n is even and a0 * 2 is a multiple of 4, so every pair starts 8-byte aligned)
+  const int pairs = na;
+  const int64_t row0 = (int64_t)a0 * 2;
+  for (int sl = t >> 5; sl < W; sl += NB >> 5) {
+    const float2* src = reinterpret_cast<const float2*>(tile + (size_t)sl * RB);
+    float2* dst = reinterpret_cast<float2*>(K + (int64_t)sl * n + row0);
+    for (int r = t & 31; r < pairs; r += 32) __stcs(dst + r, src[spos[r]]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Owner gather of element Gram matrices (FP32, the tensor-core engine's owner schedule).
 // The tcgen05 kernel has stored M_e = G W G^T of every element (RAW x RAW floats, rows and
 // columns (node, component), w = Gauss weight * detJ * E folded in); a CTA owns NB nodes as
@@ -531,8 +740,7 @@ gf_status launch_owner_gram(gf_ctx* ctx, const float* gram, float* K) {
     return gf_fail(ctx, GF_ERR_UNSUPPORTED, "owner gather: a row block does not fit");
   constexpr int JG = info.nen <= 8 ? info.nen : 4;   // JG * dim floats: 16-byte segments
   auto kern = k_assemble_owner_gram<ET, JG>;
-  GF_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)bytes(NB)));
+  GF_CUDA(ctx, gf_smem_attr(kern, (int)bytes(NB)));
   kern<<<(ctx->nnodes + NB - 1) / NB, kOT, bytes(NB), ctx->stream>>>(
       ctx->nnodes, ctx->n, W, NB, ctx->d_inc_off, ctx->d_inc, ctx->d_inc_loc, ctx->d_inc_slot,
       gram, (float)ctx->lam1, (float)ctx->mu1, K);
@@ -561,31 +769,73 @@ constexpr bool owner_compile_time_gauss() {
   return gf_elem_info(ET).dim == 2;
 }
 
+// Geometry buffer of at least `bytes` bytes (kept across assemblies).
+static gf_status owner_geo_buffer(gf_ctx* ctx, size_t bytes) {
+  if (ctx->geo_bytes >= bytes) return GF_OK;
+  if (ctx->d_geo) cudaFree(ctx->d_geo);
+  ctx->d_geo = nullptr;
+  ctx->geo_bytes = 0;
+  if (cudaMalloc(&ctx->d_geo, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return gf_fail(ctx, GF_ERR_OOM, "geometry buffer (%zu bytes)", bytes);
+  }
+  ctx->geo_bytes = bytes;
+  return GF_OK;
+}
+
+// 2-D FP32: per-element geometry with a 16-byte element stride, then the thread-per-node
+// owner kernel (CTAs of kOwnerNodeNB nodes: with a 42-slot Q8 row tile, 43 KB of shared
+// memory, four CTAs per SM).
+constexpr int kOwnerNodeNB = 128;
+
+template <int ET>
+gf_status launch_owner_node(gf_ctx* ctx, float* K, const AsmTables* d_tab) {
+  constexpr int NB = kOwnerNodeNB;
+  const int W = ctx->W;
+  const int PS = ctx->ngauss == 2 ? geo_stride<ET, float, 2>(true) : geo_stride<ET, float, 3>(true);
+  gf_status st = owner_geo_buffer(ctx, (size_t)ctx->nelem * PS * sizeof(float));
+  if (st != GF_OK) return st;
+  float* geo = static_cast<float*>(ctx->d_geo);
+  const size_t gsm = sizeof(float) * (size_t)kOT * PS;
+  auto gk = ctx->ngauss == 2 ? k_elem_geometry_pe<ET, float, 2, true>
+                             : k_elem_geometry_pe<ET, float, 3, true>;
+  GF_CUDA(ctx, gf_smem_attr(gk, (int)gsm));
+  gk<<<gf_blocks(ctx->nelem, kOT), kOT, gsm, ctx->stream>>>(ctx->nelem, ctx->d_conn,
+                                                           ctx->d_coords64, ctx->d_Eel32, geo);
+  GF_LAUNCH_CHECK(ctx, "k_elem_geometry_pe");
+  cudaEventRecord(ctx->evm, ctx->stream);
+  auto kern = ctx->ngauss == 2 ? k_assemble_owner_node<ET, 2, NB> : k_assemble_owner_node<ET, 3, NB>;
+  const size_t sm = ctx->ngauss == 2 ? owner_node_smem_bytes<ET, 2, NB>(W)
+                                     : owner_node_smem_bytes<ET, 3, NB>(W);
+  if (sm > 200 * 1024)
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "owner scatter: a row block does not fit");
+  GF_CUDA(ctx, gf_smem_attr(kern, (int)sm));
+  kern<<<(ctx->nnodes + NB - 1) / NB, NB, sm, ctx->stream>>>(
+      ctx->nnodes, ctx->n, W, ctx->d_inc_off, ctx->d_inc, ctx->d_inc_loc, ctx->d_inc_slot,
+      geo, d_tab, (float)ctx->lam1, (float)ctx->mu1, K);
+  GF_LAUNCH_CHECK(ctx, "k_assemble_owner_node");
+  return GF_OK;
+}
+
 template <int ET, typename TC>
 gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   constexpr ElemInfo info = gf_elem_info(ET);
+  if constexpr (info.dim == 2 && sizeof(TC) == 4) return launch_owner_node<ET>(ctx, K, d_tab);
   const int W = ctx->W, ngp = ctx->ngp;
-  const size_t need = (size_t)ctx->nelem * ngp * (info.dim * info.dim + 1) * sizeof(TC);
-  if (ctx->geo_bytes < need) {
-    if (ctx->d_geo) cudaFree(ctx->d_geo);
-    ctx->d_geo = nullptr;
-    ctx->geo_bytes = 0;
-    if (cudaMalloc(&ctx->d_geo, need) != cudaSuccess) {
-      cudaGetLastError();
-      return gf_fail(ctx, GF_ERR_OOM, "geometry buffer (%zu bytes)", need);
-    }
-    ctx->geo_bytes = need;
-  }
+  const int PER = ngp * (info.dim * info.dim + 1);
+  gf_status st = owner_geo_buffer(ctx, (size_t)ctx->nelem * PER * sizeof(TC));
+  if (st != GF_OK) return st;
   TC* geo = static_cast<TC*>(ctx->d_geo);
   // per-element kernel where its output staging fits (Q4, Q8; Brick8 with 2x2x2 Gauss)
   const size_t gsm = sizeof(TC) * (size_t)kOT * ngp * (info.dim * info.dim + 1);
   bool per_element = false;
   if constexpr (info.nen * info.dim <= 24) {
     if (gsm <= 100 * 1024) {
-      auto gk = ctx->ngauss == 2 ? k_elem_geometry_pe<ET, TC, 2> : k_elem_geometry_pe<ET, TC, 3>;
-      GF_CUDA(ctx, cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+      auto gk = ctx->ngauss == 2 ? k_elem_geometry_pe<ET, TC, 2, false>
+                                 : k_elem_geometry_pe<ET, TC, 3, false>;
+      GF_CUDA(ctx, gf_smem_attr(gk, (int)gsm));
       gk<<<gf_blocks(ctx->nelem, kOT), kOT, gsm, ctx->stream>>>(ctx->nelem, ctx->d_conn,
-                                                               ctx->d_coords64, geo);
+                                                               ctx->d_coords64, nullptr, geo);
       per_element = true;
     }
   }
@@ -609,7 +859,7 @@ gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   auto kern = k_assemble_owner<ET, TC, JG, 0>;
   if constexpr (owner_compile_time_gauss<ET, TC>())
     kern = ctx->ngauss == 2 ? k_assemble_owner<ET, TC, JG, 2> : k_assemble_owner<ET, TC, JG, 3>;
-  GF_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GF_CUDA(ctx, gf_smem_attr(kern, (int)sm));
   const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
   kern<<<(ctx->nnodes + NB - 1) / NB, kOT, sm, ctx->stream>>>(
       ctx->nnodes, ctx->n, W, NB, ngp, ctx->d_inc_off, ctx->d_inc, ctx->d_inc_loc,

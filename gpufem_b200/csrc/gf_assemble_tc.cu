@@ -441,17 +441,20 @@ gf_status launch_tc(gf_ctx* ctx, int scatter, const AsmTables* d_tab, float* K, 
   auto kc = k_assemble_tc<ET, 0>;
   auto ka = k_assemble_tc<ET, 1>;
   auto kg = k_assemble_tc<ET, 2>;
-  GF_CUDA(ctx, cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  GF_CUDA(ctx, cudaFuncSetAttribute(kg, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    (int)cudaSharedmemCarveoutMaxShared));
-  GF_CUDA(ctx, cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GF_CUDA(ctx, gf_smem_attr(kg, (int)sm));
+  GF_CUDA(ctx, gf_func_attr(reinterpret_cast<const void*>(kg),
+                            cudaFuncAttributePreferredSharedMemoryCarveout,
+                            (int)cudaSharedmemCarveoutMaxShared));
+  GF_CUDA(ctx, gf_smem_attr(kc, (int)sm));
+  GF_CUDA(ctx, gf_smem_attr(ka, (int)sm));
   // the whole unified L1/shared array as shared memory, so that the occupancy query and the
   // launch see the same carve-out
-  GF_CUDA(ctx, cudaFuncSetAttribute(kc, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    (int)cudaSharedmemCarveoutMaxShared));
-  GF_CUDA(ctx, cudaFuncSetAttribute(ka, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    (int)cudaSharedmemCarveoutMaxShared));
+  GF_CUDA(ctx, gf_func_attr(reinterpret_cast<const void*>(kc),
+                            cudaFuncAttributePreferredSharedMemoryCarveout,
+                            (int)cudaSharedmemCarveoutMaxShared));
+  GF_CUDA(ctx, gf_func_attr(reinterpret_cast<const void*>(ka),
+                            cudaFuncAttributePreferredSharedMemoryCarveout,
+                            (int)cudaSharedmemCarveoutMaxShared));
   // resident CTAs per SM: registers, shared memory and the 512 TMEM columns of an SM
   const int per_sm = tc_ctas_per_sm(scatter == GF_SCATTER_OWNER    ? kg
                                     : scatter == GF_SCATTER_ATOMIC ? ka : kc,

@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "gpufem_b200.h"
@@ -328,6 +331,31 @@ void gf_pfree(gf_ctx* ctx, T*& p) {
   if (p) { gf_pool_put(ctx, p); p = nullptr; }
 }
 
+// Kernel attributes that persist for the process (per device): the dynamic shared-memory
+// limit and the carveout are set on a kernel's first launch (or when a launch needs more
+// shared memory than set so far), not before every launch, which would cost host time
+// between a call's timing events.
+inline cudaError_t gf_func_attr(const void* fn, cudaFuncAttribute attr, int value) {
+  static std::mutex mu;
+  static std::map<std::pair<std::pair<const void*, int>, int>, int> set;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_pair(std::make_pair(fn, dev), (int)attr);
+  std::lock_guard<std::mutex> lock(mu);
+  const auto it = set.find(key);
+  const bool grow_only = attr == cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (it != set.end() && (grow_only ? it->second >= value : it->second == value))
+    return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(fn, attr, value);
+  if (e == cudaSuccess) set[key] = value;
+  return e;
+}
+template <typename K>
+inline cudaError_t gf_smem_attr(K kernel, size_t bytes) {
+  return gf_func_attr(reinterpret_cast<const void*>(kernel),
+                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 inline int gf_blocks(int64_t work, int threads) {
   int64_t b = (work + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -337,10 +365,12 @@ inline int gf_blocks(int64_t work, int threads) {
 
 // internal entry points across translation units
 gf_status gf_pattern_build(gf_ctx* ctx);
+gf_status gf_slotmap_ensure(gf_ctx* ctx);
 gf_status gf_color_build(gf_ctx* ctx, const int32_t* user_colors);
 gf_status gf_assemble_launch(gf_ctx* ctx, int dtype, int scatter, int engine);
 gf_status gf_constraints_apply(gf_ctx* ctx, int mode);
 gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y);
+gf_status gf_matvec_f32(gf_ctx* ctx, const float* x, const float* scale, float* y);
 gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info);
 void gf_solver_free(gf_ctx* ctx);
 void gf_dist_free(gf_ctx* ctx);

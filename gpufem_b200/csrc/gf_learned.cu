@@ -171,24 +171,6 @@ __global__ void k_lp_features(int N, int dim, const float* __restrict__ rho,
   }
 }
 
-// y = scale .* (K x) on the column-major ELL (entry (row, slot) at row + slot n),
-// thread per row, FP64 accumulation; scale may be null.
-template <typename TK>
-__global__ void __launch_bounds__(kLT)
-k_lp_ellmv(int n, const int32_t* __restrict__ rownnz, const int32_t* __restrict__ col,
-           const TK* __restrict__ val, const float* __restrict__ x,
-           const float* __restrict__ scale, float* __restrict__ y) {
-  const int row = blockIdx.x * kLT + threadIdx.x;
-  if (row >= n) return;
-  const int nz = rownnz[row];
-  double acc = 0.0;
-  for (int s = 0; s < nz; ++s) {
-    const int64_t o = (int64_t)s * n + row;
-    acc += (double)__ldg(val + o) * (double)__ldg(x + __ldg(col + o));
-  }
-  y[row] = (float)(scale ? acc * (double)scale[row] : acc);
-}
-
 // ---- dense layers on the tcgen05 tensor cores ----------------------------------------
 // out[a][o] = act(bias[o] + sum_k W1[o][k] X1[a][k] (+ sum_k W2[o][k] X2[a][k]))   (WT = false)
 // out[a][o] (+)= sum_k W1[k][o] X1[a][k]                                        (WT = true:
@@ -205,11 +187,15 @@ __host__ __device__ constexpr int mm_pad16(int x) { return x < 16 ? 16 : (x + 15
 __host__ __device__ constexpr int mm_pad8(int x) { return (x + 7) / 8 * 8; }
 __host__ __device__ constexpr int mm_tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : 128; }
 
-// X hi/lo tiles, reused after the MMAs as the output staging tile [128][NO + 1]
+// row stride of the output staging tile: NO + 4 floats when rows are moved as 16-byte
+// vectors (NO a multiple of 4), else NO + 1 (conflict-free scalar accesses)
+__host__ __device__ constexpr int mm_stage_stride(int no) { return no % 4 == 0 ? no + 4 : no + 1; }
+
+// X hi/lo tiles, reused after the MMAs as the output staging tile [128][stride]
 template <int KD, int NO>
 __host__ __device__ constexpr size_t mm_xbytes() {
-  return (size_t)2 * 128 * mm_pad8(KD) * 4 > (size_t)128 * (NO + 1) * 4
-             ? (size_t)2 * 128 * mm_pad8(KD) * 4 : (size_t)128 * (NO + 1) * 4;
+  return (size_t)2 * 128 * mm_pad8(KD) * 4 > (size_t)128 * mm_stage_stride(NO) * 4
+             ? (size_t)2 * 128 * mm_pad8(KD) * 4 : (size_t)128 * mm_stage_stride(NO) * 4;
 }
 
 template <int KD, int NO, bool TWO>
@@ -266,8 +252,13 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
     const int a0 = tile * 128;
     for (int p = 0; p < P && ok; ++p) {
       const float* X = p == 0 ? X1 : X2;
-#pragma unroll 4
-      for (int q = tid; q < 128 * NCH; q += kMmThreads) {
+      // every thread issues all its loads of the tile before using any (NCH 16-byte
+      // chunks per row, 128 * NCH / 128 = NCH per thread), so the tile arrives in one
+      // round of memory latency
+      float4 xv[NCH];
+#pragma unroll
+      for (int u = 0; u < NCH; ++u) {
+        const int q = tid + u * kMmThreads;
         // a warp takes 8 rows x 4 chunks (when NCH >= 4): 64 contiguous bytes of each of 8
         // rows in global memory, a 4-way bank conflict at most in shared memory
         int r, c;
@@ -280,26 +271,40 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
           c = q >> 7;
         }
         const int a = a0 + r;
-        float v[4];
         if constexpr (KD % 4 == 0) {
-          float4 x4 = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (a < N && 4 * c < KD) x4 = __ldg(reinterpret_cast<const float4*>(X + (int64_t)a * KD) + c);
-          v[0] = x4.x; v[1] = x4.y; v[2] = x4.z; v[3] = x4.w;
+          xv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (a < N && 4 * c < KD)
+            xv[u] = __ldg(reinterpret_cast<const float4*>(X + (int64_t)a * KD) + c);
         } else {
+          float* v = &xv[u].x;
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int k = 4 * c + u;
-            v[u] = (a < N && k < KD) ? __ldg(X + (int64_t)a * KD + k) : 0.f;
+          for (int w = 0; w < 4; ++w) {
+            const int k = 4 * c + w;
+            v[w] = (a < N && k < KD) ? __ldg(X + (int64_t)a * KD + k) : 0.f;
           }
         }
+      }
+#pragma unroll
+      for (int u = 0; u < NCH; ++u) {
+        const int q = tid + u * kMmThreads;
+        int r, c;
+        if constexpr (NCH % 4 == 0) {
+          const int ln = q & 31, wq = q >> 5;
+          r = (wq & 15) * 8 + (ln & 7);
+          c = (wq >> 4) * 4 + (ln >> 3);
+        } else {
+          r = q & 127;
+          c = q >> 7;
+        }
+        const float* v = &xv[u].x;
         float4 h, l;
         float* hp = &h.x;
         float* lp = &l.x;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const uint32_t hb = tc_tf32_round(v[u]);
-          hp[u] = __uint_as_float(hb);
-          lp[u] = __uint_as_float(tc_tf32_round(v[u] - __uint_as_float(hb)));
+        for (int w = 0; w < 4; ++w) {
+          const uint32_t hb = tc_tf32_round(v[w]);
+          hp[w] = __uint_as_float(hb);
+          lp[w] = __uint_as_float(tc_tf32_round(v[w] - __uint_as_float(hb)));
         }
         *reinterpret_cast<float4*>(xh + c * 512 + r * 4) = h;
         *reinterpret_cast<float4*>(xl + c * 512 + r * 4) = l;
@@ -346,22 +351,54 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
     }
     tc_wait_ld();
     (void)a;
-    // stage the tile's outputs in shared memory (row stride NO + 1: conflict-free), then
-    // store them with consecutive threads on consecutive channels (coalesced)
+    // stage the tile's outputs in shared memory, then store them with consecutive threads
+    // on consecutive channels (coalesced; 16-byte vectors when NO is a multiple of 4)
     const int rr = warp * 32 + lane;
+    constexpr int SS = mm_stage_stride(NO);
+    if constexpr (NO % 4 == 0) {
 #pragma unroll
-    for (int c = 0; c < NO; ++c) stage[rr * (NO + 1) + c] = acc[c] + sb[c];
+      for (int c = 0; c < NO; c += 4)
+        *reinterpret_cast<float4*>(stage + rr * SS + c) =
+            make_float4(acc[c] + sb[c], acc[c + 1] + sb[c + 1], acc[c + 2] + sb[c + 2],
+                        acc[c + 3] + sb[c + 3]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) stage[rr * SS + c] = acc[c] + sb[c];
+    }
     tc_fence_before();
     __syncthreads();
-    for (int q = tid; q < 128 * NO; q += kMmThreads) {
-      const int r = q / NO, c = q - r * NO;
-      const int an = a0 + r;
-      if (an < N) {
-        const float v = stage[r * (NO + 1) + c];
-        const int64_t o = (int64_t)an * NO + c;
-        if (pre) pre[o] = v;
-        const float y = (relu && v < 0.f) ? 0.f : v;
-        out[o] = accumulate ? out[o] + y : y;
+    if constexpr (NO % 4 == 0) {
+      constexpr int NV = NO / 4;
+      for (int q = tid; q < 128 * NV; q += kMmThreads) {
+        const int r = q / NV, c = (q - r * NV) * 4;
+        const int an = a0 + r;
+        if (an < N) {
+          const float4 v = *reinterpret_cast<const float4*>(stage + r * SS + c);
+          const int64_t o = (int64_t)an * NO + c;
+          if (pre) *reinterpret_cast<float4*>(pre + o) = v;
+          float4 y = v;
+          if (relu) {
+            y.x = fmaxf(y.x, 0.f); y.y = fmaxf(y.y, 0.f);
+            y.z = fmaxf(y.z, 0.f); y.w = fmaxf(y.w, 0.f);
+          }
+          if (accumulate) {
+            const float4 o4 = *reinterpret_cast<const float4*>(out + o);
+            y.x += o4.x; y.y += o4.y; y.z += o4.z; y.w += o4.w;
+          }
+          *reinterpret_cast<float4*>(out + o) = y;
+        }
+      }
+    } else {
+      for (int q = tid; q < 128 * NO; q += kMmThreads) {
+        const int r = q / NO, c = q - r * NO;
+        const int an = a0 + r;
+        if (an < N) {
+          const float v = stage[r * SS + c];
+          const int64_t o = (int64_t)an * NO + c;
+          if (pre) pre[o] = v;
+          const float y = (relu && v < 0.f) ? 0.f : v;
+          out[o] = accumulate ? out[o] + y : y;
+        }
       }
     }
     __syncthreads();
@@ -426,24 +463,36 @@ k_lp_wgrad(int N, const float* __restrict__ G, const float* __restrict__ A,
 
 // forward:  out[a] = deg_inv[a] * sum_{b in N(a)} h[b]
 // backward: out[b] = sum_{a in N(b)} deg_inv[a] * g[a]   (the node graph is symmetric)
-// Thread per (node, channel); channel fastest so a warp reads 128 contiguous bytes.
+// 16 threads per node, 4 channels (16 bytes) each, neighbours summed in adjacency order.
+// A CTA walks a contiguous range of per_cta nodes, 16 at a time: mesh numberings keep
+// neighbours close, so the rows that the next nodes read again were just read and are
+// still in L1.
+constexpr int kAggNodes = kLT / 16;
+
 __global__ void __launch_bounds__(kLT)
-k_lp_aggregate(int N, const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
-               const float* __restrict__ deg_inv, const float* __restrict__ h,
-               float* __restrict__ out, int backward) {
-  const int64_t total = (int64_t)N * H;
-  for (int64_t t = blockIdx.x * (int64_t)kLT + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * kLT) {
-    const int a = (int)(t / H), c = (int)(t % H);
-    float s = 0.f;
+k_lp_aggregate(int N, int per_cta, const int32_t* __restrict__ adj_off,
+               const int32_t* __restrict__ adj, const float* __restrict__ deg_inv,
+               const float* __restrict__ h, float* __restrict__ out, int backward) {
+  const int sub = threadIdx.x >> 4, c4 = threadIdx.x & 15;
+  const int a_end = min(N, (blockIdx.x + 1) * per_cta);
+  for (int a = blockIdx.x * per_cta + sub; a < a_end; a += kAggNodes) {
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
     const int q1 = adj_off[a + 1];
-#pragma unroll 8
+#pragma unroll 4
     for (int q = adj_off[a]; q < q1; ++q) {   // unrolled: the neighbours' gathers overlap
       const int b = __ldg(adj + q);
-      const float v = __ldg(h + (int64_t)b * H + c);
-      s += backward ? v * __ldg(deg_inv + b) : v;
+      float4 v = __ldg(reinterpret_cast<const float4*>(h + (int64_t)b * H) + c4);
+      if (backward) {
+        const float w = __ldg(deg_inv + b);
+        v.x *= w; v.y *= w; v.z *= w; v.w *= w;
+      }
+      s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
     }
-    out[t] = backward ? s : s * deg_inv[a];
+    if (!backward) {
+      const float w = deg_inv[a];
+      s.x *= w; s.y *= w; s.z *= w; s.w *= w;
+    }
+    reinterpret_cast<float4*>(out + (int64_t)a * H)[c4] = s;
   }
 }
 
@@ -667,6 +716,10 @@ gf_status gf_lp_prepare(gf_ctx* ctx) {
     LPA(s->tmp, (size_t)N * H);
 #undef LPA
   }
+  {
+    gf_status st = gf_sell_prepare(ctx, ctx->has64 ? GF_F64 : GF_F32);  // feature products
+    if (st != GF_OK) return st;
+  }
   cudaStream_t st_ = ctx->stream;
   k_lp_degree<<<gf_blocks(N, kLT), kLT, 0, st_>>>(N, ctx->d_adj_off, s->deg_inv);
   ctx->launches++;
@@ -690,15 +743,20 @@ gf_status gf_lp_prepare(gf_ctx* ctx) {
   return GF_OK;
 }
 
-// y = scale .* (K x) for FP32 device vectors (FP64 matrix values when present).
+// y = scale .* (K x) for FP32 device vectors (FP64 matrix values when present), on the
+// solver's node-block layout (prepared by gf_lp_prepare, so this only enqueues).
 static void lp_matvec(gf_ctx* ctx, const float* x, const float* scale, float* y) {
-  const int n = ctx->n;
-  if (ctx->has64)
-    k_lp_ellmv<double><<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(
-        n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64, x, scale, y);
-  else
-    k_lp_ellmv<float><<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(
-        n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K32, x, scale, y);
+  gf_matvec_f32(ctx, x, scale, y);
+}
+
+// Neighbour aggregation (see k_lp_aggregate) on the context stream.
+static void lp_aggregate(gf_ctx* ctx, const float* h, float* out, int backward) {
+  LpState* s = ctx->lp;
+  const int N = s->N;
+  const int grid = std::max(1, std::min((N + kAggNodes - 1) / kAggNodes, ctx->sm_count * 8));
+  const int per_cta = (N + grid - 1) / grid;
+  k_lp_aggregate<<<grid, kLT, 0, ctx->stream>>>(N, per_cta, ctx->d_adj_off, ctx->d_adj,
+                                                s->deg_inv, h, out, backward);
   ctx->launches++;
 }
 
@@ -719,9 +777,10 @@ template <int KD, int NO, bool TWO, bool WT>
 static gf_status lp_mm_attr(gf_ctx* ctx, int* per_sm) {
   auto k = k_lp_mm_tc<KD, NO, TWO, WT>;
   const int sm = (int)mm_smem_bytes<KD, NO, TWO>();
-  GF_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  GF_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    (int)cudaSharedmemCarveoutMaxShared));
+  GF_CUDA(ctx, gf_smem_attr(k, sm));
+  GF_CUDA(ctx, gf_func_attr(reinterpret_cast<const void*>(k),
+                            cudaFuncAttributePreferredSharedMemoryCarveout,
+                            (int)cudaSharedmemCarveoutMaxShared));
   *per_sm = std::min(*per_sm, tc_ctas_per_sm(k, kMmThreads, (size_t)sm, (int)mm_tmem_cols(mm_pad16(NO))));
   return GF_OK;
 }
@@ -754,8 +813,9 @@ static gf_status lp_check_err(gf_ctx* ctx) {
   return GF_OK;
 }
 
-// Network forward on FP32 residual r (device, n); fills rho, y and the activations.
-static void lp_forward(gf_ctx* ctx, const float* r) {
+// Network forward on FP32 residual r (device, n); fills rho, y and the activations (the
+// pre-activations too when `train`: the backward pass needs them).
+static void lp_forward(gf_ctx* ctx, const float* r, bool train) {
   LpState* s = ctx->lp;
   cudaStream_t st = ctx->stream;
   const int N = s->N, n = s->n, dim = s->dim;
@@ -766,18 +826,16 @@ static void lp_forward(gf_ctx* ctx, const float* r) {
   lp_matvec(ctx, s->v1, s->dinv, s->v2);
   k_lp_features<<<gf_blocks(N, kLT), kLT, 0, st>>>(N, dim, s->rho, s->v1, s->v2, s->dlog,
                                                    s->feat, s->sc);
-  const int gH = lp_grid((int64_t)N * H);
   if (dim == 2)
     lp_mm<8, H, false, false>(ctx, s->feat, nullptr, s->wb + o.W0, nullptr, s->wb + o.b0,
-                              s->pre[0], s->h[0], 1, 0);
+                              train ? s->pre[0] : nullptr, s->h[0], 1, 0);
   else
     lp_mm<12, H, false, false>(ctx, s->feat, nullptr, s->wb + o.W0, nullptr, s->wb + o.b0,
-                               s->pre[0], s->h[0], 1, 0);
+                               train ? s->pre[0] : nullptr, s->h[0], 1, 0);
   for (int l = 0; l < kLayers; ++l) {
-    k_lp_aggregate<<<gH, kLT, 0, st>>>(N, ctx->d_adj_off, ctx->d_adj, s->deg_inv, s->h[l],
-                                       s->agg[l], 0);
+    lp_aggregate(ctx, s->h[l], s->agg[l], 0);
     lp_mm<H, H, true, false>(ctx, s->h[l], s->agg[l], s->wb + o.Ws[l], s->wb + o.Wn[l],
-                             s->wb + o.bl[l], s->pre[l + 1], s->h[l + 1], 1, 0);
+                             s->wb + o.bl[l], train ? s->pre[l + 1] : nullptr, s->h[l + 1], 1, 0);
   }
   if (dim == 2)
     lp_mm<H, 2, false, false>(ctx, s->h[kLayers], nullptr, s->wb + o.Wout, nullptr,
@@ -785,7 +843,7 @@ static void lp_forward(gf_ctx* ctx, const float* r) {
   else
     lp_mm<H, 3, false, false>(ctx, s->h[kLayers], nullptr, s->wb + o.Wout, nullptr,
                               s->wb + o.bout, nullptr, s->y, 0, 0);
-  ctx->launches += 3 + kLayers;
+  ctx->launches += 3;
 }
 
 // Backward from dy ([N][dim] == n floats) into s->g (accumulated).
@@ -815,8 +873,7 @@ static void lp_backward(gf_ctx* ctx, const float* dy) {
     // dh_l = Ws^T dpre + aggregate^T(Wn^T dpre)
     lp_mm<H, H, false, true>(ctx, s->dpre, nullptr, s->wb + o.Wn[l], nullptr, nullptr, nullptr,
                              s->tmp, 0, 0);
-    k_lp_aggregate<<<gH, kLT, 0, st>>>(N, ctx->d_adj_off, ctx->d_adj, s->deg_inv, s->tmp,
-                                       s->dh, 1);
+    lp_aggregate(ctx, s->tmp, s->dh, 1);
     lp_mm<H, H, false, true>(ctx, s->dpre, nullptr, s->wb + o.Ws[l], nullptr, nullptr, nullptr,
                              s->dh, 0, 1);
   }
@@ -825,7 +882,7 @@ static void lp_backward(gf_ctx* ctx, const float* dy) {
     k_lp_wgrad<8, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
   else
     k_lp_wgrad<12, H><<<gw, kLT, 0, st>>>(N, s->dpre, s->feat, s->g + o.W0, s->g + o.b0);
-  ctx->launches += 3 + 6 * kLayers + 2;
+  ctx->launches += 3 + 5 * kLayers + 2;
 }
 
 // Forward, loss and backward of one training pair (r, e): adds the pair's loss to
@@ -835,7 +892,7 @@ static void lp_pair(gf_ctx* ctx, const float* r, const float* e) {
   cudaStream_t cs = ctx->stream;
   const int n = s->n, nb = gf_blocks(n, kLT);
   cudaMemsetAsync(&s->sc->dsum, 0, sizeof(double), cs);
-  lp_forward(ctx, r);
+  lp_forward(ctx, r, true);
   if (s->loss == GF_LP_LOSS_RESIDUAL) {
     k_lp_rl_diff<<<nb, kLT, 0, cs>>>(n, e, s->rho, s->y, s->sc, s->lw);
     lp_matvec(ctx, s->lw, nullptr, s->ls);   // s = K (e - z)
@@ -858,7 +915,7 @@ gf_status gf_lp_apply64(gf_ctx* ctx, const double* r64, float* r32_scratch, doub
   LpState* s = ctx->lp;
   const int n = s->n;
   k_lp_cast_f32<<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(n, r64, r32_scratch);
-  lp_forward(ctx, r32_scratch);
+  lp_forward(ctx, r32_scratch, false);
   k_lp_output<double><<<gf_blocks(n, kLT), kLT, 0, ctx->stream>>>(n, s->rho, s->y, s->sc, z);
   ctx->launches += 2;
   return GF_OK;
@@ -1017,7 +1074,7 @@ GF_API gf_status gf_lp_apply(gf_ctx* ctx, const float* r, float* z) {
   if (st != GF_OK) return st;
   LpState* s = ctx->lp;
   cudaEventRecord(ctx->ev0, ctx->stream);
-  lp_forward(ctx, r);
+  lp_forward(ctx, r, false);
   k_lp_output<float><<<gf_blocks(s->n, kLT), kLT, 0, ctx->stream>>>(s->n, s->rho, s->y, s->sc, z);
   GF_LAUNCH_CHECK(ctx, "k_lp_output");
   cudaEventRecord(ctx->ev1, ctx->stream);

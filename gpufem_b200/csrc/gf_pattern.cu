@@ -121,6 +121,105 @@ __global__ void k_node_adjacency(int nnodes, int nen, const int32_t* __restrict_
   }
 }
 
+// Warp per node, for meshes whose nodes all see at most 32 element-node slots (every
+// 2-D mesh with at most 32 / nen elements per node): one pass gives the node's incident
+// elements in ascending order (written back to inc), its local index in each, the rank
+// of every element node among the node's distinct neighbours (= the neighbour's slot in
+// the sorted adjacency list, inc_slot), the node's own slot (diagpos), the neighbour
+// count and the sorted list itself, at adj_tmp[inc_off[node] * nen + rank] (a node's list
+// has at most as many entries as it has element-node slots).  The same quantities as
+// k_node_adjacency + k_incidence_finish + k_diagpos, without their searches.
+__global__ void k_node_pattern(int nnodes, int nen, const int32_t* __restrict__ conn,
+                               const int32_t* __restrict__ inc_off, int32_t* __restrict__ inc,
+                               int32_t* __restrict__ nadj, int32_t* __restrict__ adj_tmp,
+                               uint8_t* __restrict__ inc_loc, uint16_t* __restrict__ inc_slot,
+                               int32_t* __restrict__ diagpos) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int node = blockIdx.x * kWarpsPerBlock + warp;
+  if (node >= nnodes) return;   // whole warp
+  const int e0 = inc_off[node], deg = inc_off[node + 1] - e0;
+  const int C = deg * nen;      // <= 32 (the caller checked max degree * nen)
+  // ascending order of the incident elements (distinct ids): rank by comparison
+  const int el = lane < deg ? inc[e0 + lane] : 0x7fffffff;
+  int er = 0;
+  for (int q = 0; q < deg; ++q) er += __shfl_sync(kFull, el, q) < el ? 1 : 0;
+  // element of candidate slot `lane`: the one of rank lane / nen
+  const int kq = lane / nen, j = lane - kq * nen;
+  int myel = 0;
+  for (int q = 0; q < deg; ++q) {
+    const int rq = __shfl_sync(kFull, er, q);
+    const int eq = __shfl_sync(kFull, el, q);
+    if (rq == kq) myel = eq;
+  }
+  __syncwarp();
+  if (lane < deg) inc[e0 + er] = el;
+  const bool act = lane < C;
+  const int v = act ? conn[(int64_t)myel * nen + j] : 0x7fffffff;
+  const unsigned same = __match_any_sync(kFull, v);
+  const bool first = act && (__ffs(same) - 1) == lane;
+  const unsigned firsts = __ballot_sync(kFull, first);
+  int rank = 0;   // distinct neighbours below v
+  for (int q = 0; q < C; ++q) {
+    const int vq = __shfl_sync(kFull, v, q);
+    rank += ((firsts >> q) & 1u) && vq < v ? 1 : 0;
+  }
+  if (lane == 0) {
+    nadj[node] = __popc(firsts);
+    if (C == 0) diagpos[node] = 0;
+  }
+  if (first) adj_tmp[(int64_t)e0 * nen + rank] = v;
+  if (act) {
+    inc_slot[(int64_t)(e0 + kq) * nen + j] = (uint16_t)rank;
+    if (v == node) {
+      inc_loc[e0 + kq] = (uint8_t)j;
+      diagpos[node] = rank;
+    }
+  }
+}
+
+// Thread per row after k_node_pattern: rownnz and the row's columns from the node's sorted
+// list in adj_tmp (slots past the row's length hold col = row; all threads walk the
+// slots together, so each slot's column of colidx is written by consecutive threads).
+template <int DIM>
+__global__ void k_rows_from_lists(int n, int W, int nen, const int32_t* __restrict__ inc_off,
+                                  const int32_t* __restrict__ nadj,
+                                  const int32_t* __restrict__ adj_tmp,
+                                  int32_t* __restrict__ rownnz, int32_t* __restrict__ colidx) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  const int node = row / DIM;
+  const int len = nadj[node] * DIM;
+  const int32_t* list = adj_tmp + (int64_t)inc_off[node] * nen;
+  rownnz[row] = len;
+  for (int s = 0; s < W; ++s) {
+    const int b = s < len ? __ldg(list + s / DIM) : 0;
+    colidx[(int64_t)s * n + row] = s < len ? b * DIM + s % DIM : row;
+  }
+}
+
+// Warp per 32 consecutive nodes: their sorted lists from adj_tmp into adj, one node at a
+// time (lane k copies entry k), so the stores into each list coalesce.
+__global__ void k_adj_fill(int nnodes, int nen, const int32_t* __restrict__ inc_off,
+                           const int32_t* __restrict__ nadj, const int32_t* __restrict__ adj_off,
+                           const int32_t* __restrict__ adj_tmp, int32_t* __restrict__ adj) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+  if (base >= nnodes) return;   // whole warp
+  const int mine = base + lane;
+  const int m = mine < nnodes ? nadj[mine] : 0;
+  const int64_t src = mine < nnodes ? (int64_t)inc_off[mine] * nen : 0;
+  const int dst = mine < nnodes ? adj_off[mine] : 0;
+#pragma unroll 4
+  for (int i = 0; i < 32; ++i) {
+    const int mi = __shfl_sync(kFull, m, i);
+    const int64_t si = __shfl_sync(kFull, src, i);
+    const int di = __shfl_sync(kFull, dst, i);
+    if (lane < mi) adj[di + lane] = __ldg(adj_tmp + si + lane);
+  }
+}
+
 __global__ void k_rownnz(int nnodes, int dim, const int32_t* __restrict__ nadj,
                          int32_t* __restrict__ rownnz) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -128,20 +227,20 @@ __global__ void k_rownnz(int nnodes, int dim, const int32_t* __restrict__ nadj,
     for (int c = 0; c < dim; ++c) rownnz[a * dim + c] = nadj[a] * dim;
 }
 
-__global__ void k_colidx(int n, int W, int dim, const int32_t* __restrict__ rownnz,
-                         const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
-                         int32_t* __restrict__ colidx) {
-  const int64_t total = (int64_t)n * W;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int row = (int)(i % n);
-    const int slot = (int)(i / n);
-    int col = row;
-    if (slot < rownnz[row]) {
-      const int node = row / dim;
-      col = adj[adj_off[node] + slot / dim] * dim + slot % dim;
-    }
-    colidx[i] = col;
+// Thread per row: the columns of row (node a, component c) are the dofs of a's sorted
+// adjacency list; slots past the row's length hold col = row.  All threads walk the
+// slots together, so each slot's column of colidx is written by consecutive threads.
+template <int DIM>
+__global__ void k_colidx(int n, int W, const int32_t* __restrict__ adj_off,
+                         const int32_t* __restrict__ adj, int32_t* __restrict__ colidx) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  const int node = row / DIM;
+  const int q0 = adj_off[node];
+  const int len = (adj_off[node + 1] - q0) * DIM;
+  for (int s = 0; s < W; ++s) {
+    const int b = s < len ? __ldg(adj + q0 + s / DIM) : 0;
+    colidx[(int64_t)s * n + row] = s < len ? b * DIM + s % DIM : row;
   }
 }
 
@@ -235,12 +334,13 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   gf_status st;
 
   int32_t *d_cnt = nullptr, *d_inc_off = nullptr, *d_fill = nullptr, *d_inc = nullptr;
-  int32_t *d_nadj = nullptr, *d_err = nullptr, *d_max = nullptr;
+  int32_t *d_nadj = nullptr, *d_err = nullptr, *d_max = nullptr, *d_adjtmp = nullptr;
   char* d_tmp = nullptr;
   size_t tmp_bytes = 0, b1 = 0, b2 = 0, b3 = 0;
   auto cleanup = [&]() {
     gf_pfree(ctx, d_cnt); gf_pfree(ctx, d_inc_off); gf_pfree(ctx, d_fill); gf_pfree(ctx, d_inc);
     gf_pfree(ctx, d_nadj); gf_pfree(ctx, d_err); gf_pfree(ctx, d_max); gf_pfree(ctx, d_tmp);
+    gf_pfree(ctx, d_adjtmp);
   };
 #define GF_TRY(x)             \
   do {                        \
@@ -258,7 +358,7 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   GF_TRY(gf_palloc(ctx, &d_inc, (size_t)total));
   GF_TRY(gf_palloc(ctx, &d_nadj, (size_t)nnodes + 1));
   GF_TRY(gf_palloc(ctx, &d_err, 1));
-  GF_TRY(gf_palloc(ctx, &d_max, 1));
+  GF_TRY(gf_palloc(ctx, &d_max, 2));
   GF_TRY(gf_palloc(ctx, &ctx->d_adj_off, (size_t)nnodes + 1));
   GF_TRYC(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (nnodes + 1), s));
   GF_TRYC(cudaMemsetAsync(d_nadj, 0, sizeof(int32_t) * (nnodes + 1), s));
@@ -277,9 +377,25 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
                           cudaMemcpyDeviceToDevice, s));
   k_fill_incidence<<<gf_blocks(total, 256), 256, 0, s>>>(total, nen, ctx->d_conn, d_fill, d_inc);
   ctx->launches++;
+  // the most elements around one node decides the adjacency path
+  GF_TRYC(cub::DeviceReduce::Max(d_tmp, tmp_bytes, d_cnt, d_max + 1, nnodes, s));
+  int32_t h_maxval = 0;
+  GF_TRYC(cudaMemcpyAsync(&h_maxval, d_max + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GF_TRYC(cudaStreamSynchronize(s));
+  const bool fused = (int64_t)h_maxval * nen <= 32;
   const int ablocks = (nnodes + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  k_node_adjacency<0><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
-      nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, nullptr, nullptr, d_err);
+  if (fused) {
+    GF_TRY(gf_palloc(ctx, &d_adjtmp, (size_t)total * nen));
+    GF_TRY(gf_palloc(ctx, &ctx->d_inc_loc, (size_t)total));
+    GF_TRY(gf_palloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
+    GF_TRY(gf_palloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
+    k_node_pattern<<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
+        nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, d_adjtmp, ctx->d_inc_loc,
+        ctx->d_inc_slot, ctx->d_diagpos);
+  } else {
+    k_node_adjacency<0><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
+        nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, nullptr, nullptr, d_err);
+  }
   ctx->launches++;
   GF_TRYC(cudaGetLastError());
   GF_TRYC(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_nadj, ctx->d_adj_off, nnodes + 1, s));
@@ -307,32 +423,41 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   GF_TRY(gf_palloc(ctx, &ctx->d_adj, (size_t)h_tot));
   GF_TRY(gf_palloc(ctx, &ctx->d_rownnz, (size_t)n));
   GF_TRY(gf_palloc(ctx, &ctx->d_colidx, (size_t)slots));
-  GF_TRY(gf_palloc(ctx, &ctx->d_slotmap, (size_t)nelem * nen * nen));
-  GF_TRY(gf_palloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
-  k_node_adjacency<1><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
-      nnodes, nen, ctx->d_conn, d_inc_off, d_inc, nullptr, ctx->d_adj_off, ctx->d_adj, d_err);
-  ctx->launches++;
-  k_rownnz<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, dim, d_nadj, ctx->d_rownnz);
-  ctx->launches++;
-  k_colidx<<<ctx->sm_count * 16, 256, 0, s>>>(n, ctx->W, dim, ctx->d_rownnz, ctx->d_adj_off,
-                                              ctx->d_adj, ctx->d_colidx);
-  ctx->launches++;
-  k_slotmap<<<gf_blocks(total, 256), 256, 0, s>>>(nelem, nen, ctx->d_conn, ctx->d_adj_off,
-                                                  ctx->d_adj, ctx->d_slotmap, d_err);
-  ctx->launches++;
-  k_diagpos<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_adj_off, ctx->d_adj,
-                                                   ctx->d_diagpos);
-  ctx->launches++;
-  // incidence kept for the owner-computes scatter
-  GF_TRY(gf_palloc(ctx, &ctx->d_inc_loc, (size_t)total));
-  GF_TRY(gf_palloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
-  k_incidence_finish<<<gf_blocks(nnodes, 128), 128, 0, s>>>(
-      nnodes, nen, ctx->d_conn, d_inc_off, d_inc, ctx->d_adj_off, ctx->d_adj, ctx->d_inc_loc,
-      ctx->d_inc_slot, d_err);
-  ctx->launches++;
-  GF_TRYC(cub::DeviceReduce::Max(d_tmp, tmp_bytes, d_cnt, d_max, nnodes, s));
-  int32_t h_maxval = 0;
-  GF_TRYC(cudaMemcpyAsync(&h_maxval, d_max, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  if (fused) {
+    k_adj_fill<<<gf_blocks((nnodes + 31) / 32, 8), 256, 0, s>>>(
+        nnodes, nen, d_inc_off, d_nadj, ctx->d_adj_off, d_adjtmp, ctx->d_adj);
+    if (dim == 2)
+      k_rows_from_lists<2><<<gf_blocks(n, 256), 256, 0, s>>>(
+          n, ctx->W, nen, d_inc_off, d_nadj, d_adjtmp, ctx->d_rownnz, ctx->d_colidx);
+    else
+      k_rows_from_lists<3><<<gf_blocks(n, 256), 256, 0, s>>>(
+          n, ctx->W, nen, d_inc_off, d_nadj, d_adjtmp, ctx->d_rownnz, ctx->d_colidx);
+    ctx->launches += 2;
+  } else {
+    GF_TRY(gf_palloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
+    k_node_adjacency<1><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
+        nnodes, nen, ctx->d_conn, d_inc_off, d_inc, nullptr, ctx->d_adj_off, ctx->d_adj, d_err);
+    k_rownnz<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, dim, d_nadj, ctx->d_rownnz);
+    if (dim == 2)
+      k_colidx<2><<<gf_blocks(n, 256), 256, 0, s>>>(n, ctx->W, ctx->d_adj_off, ctx->d_adj,
+                                                    ctx->d_colidx);
+    else
+      k_colidx<3><<<gf_blocks(n, 256), 256, 0, s>>>(n, ctx->W, ctx->d_adj_off, ctx->d_adj,
+                                                    ctx->d_colidx);
+    ctx->launches += 3;
+  }
+  if (!fused) {
+    k_diagpos<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_adj_off, ctx->d_adj,
+                                                     ctx->d_diagpos);
+    ctx->launches++;
+    // incidence kept for the owner-computes scatter
+    GF_TRY(gf_palloc(ctx, &ctx->d_inc_loc, (size_t)total));
+    GF_TRY(gf_palloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
+    k_incidence_finish<<<gf_blocks(nnodes, 128), 128, 0, s>>>(
+        nnodes, nen, ctx->d_conn, d_inc_off, d_inc, ctx->d_adj_off, ctx->d_adj, ctx->d_inc_loc,
+        ctx->d_inc_slot, d_err);
+    ctx->launches++;
+  }
   GF_TRYC(cudaGetLastError());
   GF_TRYC(cudaMemcpyAsync(&h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_TRYC(cudaStreamSynchronize(s));
@@ -350,6 +475,38 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   return GF_OK;
 #undef GF_TRY
 #undef GF_TRYC
+}
+
+// Element slot map of the colour and atomic schedules (the owner schedule reads the
+// per-node incidence slots instead), built on the first assembly that needs it.
+gf_status gf_slotmap_ensure(gf_ctx* ctx) {
+  if (ctx->d_slotmap) return GF_OK;
+  if (!ctx->has_pattern) return gf_fail(ctx, GF_ERR_STATE, "no pattern");
+  const int nelem = ctx->nelem, nen = ctx->nen;
+  const int64_t total = (int64_t)nelem * nen;
+  cudaStream_t s = ctx->stream;
+  gf_status st;
+  int32_t* d_err = nullptr;
+  if ((st = gf_palloc(ctx, &d_err, 1)) != GF_OK) return st;
+  if ((st = gf_palloc(ctx, &ctx->d_slotmap, (size_t)total * nen)) != GF_OK) {
+    gf_pfree(ctx, d_err);
+    return st;
+  }
+  int32_t h_err = 0;
+  cudaMemsetAsync(d_err, 0, sizeof(int32_t), s);
+  k_slotmap<<<gf_blocks(total, 256), 256, 0, s>>>(nelem, nen, ctx->d_conn, ctx->d_adj_off,
+                                                  ctx->d_adj, ctx->d_slotmap, d_err);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  gf_pfree(ctx, d_err);
+  if (e != cudaSuccess || h_err) {
+    gf_pfree(ctx, ctx->d_slotmap);
+    return e != cudaSuccess ? gf_cuda_fail(ctx, e, "slot map")
+                            : gf_fail(ctx, GF_ERR_CUDA, "slot map lookup failed");
+  }
+  return GF_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -217,6 +217,18 @@ k_spmv(MatLayout L, const TK* __restrict__ val, const TX* __restrict__ x, TY* __
     mat_rows(L, t, val, x, [&](int row, double v) { y[row] = (TY)v; });
 }
 
+// y = scale .* (K x) for FP32 x and y (scale may be null), FP64 accumulation with FP64
+// values
+template <typename TK>
+__global__ void __launch_bounds__(kT)
+k_spmv_rowscale(MatLayout L, const TK* __restrict__ val, const float* __restrict__ x,
+                const float* __restrict__ scale, float* __restrict__ y) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L.count; t += gridDim.x * blockDim.x)
+    mat_rows(L, t, val, x, [&](int row, double v) {
+      y[row] = (float)(scale ? v * (double)__ldg(scale + row) : v);
+    });
+}
+
 // r = f - K u (FP64), and r.r
 __global__ void __launch_bounds__(kT)
 k_residual64(MatLayout L, const double* __restrict__ val, const double* __restrict__ u,
@@ -523,6 +535,25 @@ gf_status solver_matrix(gf_ctx* ctx, int dtype, MatLayout* L, const void** val) 
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// y = scale .* (K x) on FP32 vectors over the solver's matrix layout (FP64 values when the
+// context has them).  Enqueue only: inside a stream capture the layout must already be
+// prepared (gf_sell_prepare), which makes solver_matrix a lookup.
+gf_status gf_matvec_f32(gf_ctx* ctx, const float* x, const float* scale, float* y) {
+  MatLayout L;
+  const void* val = nullptr;
+  const int dt = ctx->has64 ? GF_F64 : GF_F32;
+  gf_status st = solver_matrix(ctx, dt, &L, &val);
+  if (st != GF_OK) return st;
+  if (dt == GF_F64)
+    k_spmv_rowscale<double><<<mat_grid(ctx, L), L.threads, 0, ctx->stream>>>(
+        L, (const double*)val, x, scale, y);
+  else
+    k_spmv_rowscale<float><<<mat_grid(ctx, L), L.threads, 0, ctx->stream>>>(
+        L, (const float*)val, x, scale, y);
+  ctx->launches++;
+  return GF_OK;
+}
+
 gf_status gf_spmv_launch(gf_ctx* ctx, int dtype, const void* x, void* y) {
   MatLayout L;
   const void* val = nullptr;

@@ -107,10 +107,38 @@ def test_learned_fcg_converges_and_matches_pcg():
     assert np.linalg.norm(u - u_pcg) <= 1e-7 * np.linalg.norm(u_pcg)
 
 
+def negating_weights(dim):
+    """Weights whose network gives y = -2 rho / c, i.e. M(r) = -D^-1 r (z.r < 0 at the
+    first step, whatever the rounding of the dot products): the first 2 dim hidden
+    channels carry +-rho / c through the ReLUs unchanged, every other weight is 0; all
+    values are exact in BF16."""
+    o = G.offsets(dim)
+    w = np.zeros(o["total"][0])
+    F = 4 * dim
+    W0 = np.zeros((G.H, F))
+    Ws = np.zeros((G.H, G.H))
+    Wout = np.zeros((dim, G.H))
+    for k in range(dim):
+        W0[2 * k, k], W0[2 * k + 1, k] = 1.0, -1.0
+        Ws[2 * k, 2 * k] = Ws[2 * k + 1, 2 * k + 1] = 1.0
+        Wout[k, 2 * k], Wout[k, 2 * k + 1] = -2.0, 2.0
+    w[o["W0"][0]:o["W0"][0] + o["W0"][1]] = W0.ravel()
+    for l in range(G.LAYERS):
+        w[o[f"Ws{l}"][0]:o[f"Ws{l}"][0] + o[f"Ws{l}"][1]] = Ws.ravel()
+    w[o["Wout"][0]:o["Wout"][0] + o["Wout"][1]] = Wout.ravel()
+    return w
+
+
 def test_fallback_to_jacobi_when_learned_preconditioner_is_bad():
     m, ctx = brick8_problem(n=(6, 6, 6))
     ctx.lp_init(3, seed=3)
-    ctx.lp_set_weights(random_weights(3, seed=9, scale=3.0).astype(np.float32))
+    w = negating_weights(3).astype(np.float32)
+    # (the oracle confirms the construction: M(r) = -D^-1 r)
+    r = np.random.default_rng(4).normal(size=m.ndof)
+    z_ref, _ = G.forward(w.astype(np.float64), 3, G.node_adjacency(m.conn, m.nnodes),
+                         diag_of(ctx), r, csr_of(ctx))
+    assert np.allclose(z_ref, -r / diag_of(ctx), rtol=1e-12, atol=0)
+    ctx.lp_set_weights(w)
     info = ctx.solve(_lib.GF_SOLVER_LEARNED_FCG, tol=1e-10, max_iter=100000)
     assert info.status == _lib.GF_OK and info.rel_residual <= 1e-9
     assert info.fallback == 1
