@@ -457,6 +457,54 @@ def _preconditioner_diagnostic(ctx, ustar):
     return out
 
 
+def learned_application(edge: int = 48, ctx_lp=None, reps: int = 7):
+    """Device time of one learned-preconditioner application (features with two products
+    with K, three message-passing layers, output) on the largest training-set mesh, a
+    Brick8 cube of edge 48 (117,649 nodes, 352,947 dofs; correlated log-normal E), against
+    one FP64 SpMV of the same matrix; L2 flushed before each call, median of `reps`.
+    Uses the network of ctx_lp (trained) when given, else a seeded untrained one."""
+    import torch
+    from gpufem_b200 import _lib
+    from gpufem_b200 import meshgen as mg
+    from gpufem_b200.fem import Context
+    m = mg.clamp_and_load(mg.structured(mg.BRICK8, (edge,) * 3, jitter=0.1, seed=48))
+    m.E = mg.lognormal_correlated(m, 1.0, 0.2, 48)
+    ctx = Context(0)
+    ctx.mesh_create(m.elem_type, m.coords, m.conn, m.ngauss, m.E0, m.E, m.nu)
+    ctx.set_supports(m.supports)
+    ctx.set_force(m.f)
+    ctx.assemble(_lib.GF_F64, _lib.GF_SCATTER_OWNER)
+    ctx.apply_constraints(_lib.GF_BC_ELIMINATION)
+    ctx.lp_init(3, seed=1)
+    if ctx_lp is not None:
+        ctx.lp_set_weights(ctx_lp.lp_get_weights())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ls = torch.cuda.ExternalStream(ctx.stream_handle())
+    r = torch.randn(m.ndof, device="cuda", dtype=torch.float32)
+    z = torch.empty_like(r)
+    x = torch.randn(m.ndof, device="cuda", dtype=torch.float64)
+    y = torch.empty_like(x)
+    ta, ts = [], []
+    for _ in range(reps + 1):
+        torch.cuda.synchronize()
+        with torch.cuda.stream(ls):
+            flush.zero_()
+        _lib.check(_lib.lib.gf_lp_apply(ctx.h, C.c_void_p(r.data_ptr()), C.c_void_p(z.data_ptr())),
+                   ctx.h)
+        ta.append(_lib.lib.gf_last_device_seconds(ctx.h))
+        torch.cuda.synchronize()
+        with torch.cuda.stream(ls):
+            flush.zero_()
+        _lib.check(_lib.lib.gf_spmv(ctx.h, _lib.GF_F64, C.c_void_p(x.data_ptr()),
+                                    C.c_void_p(y.data_ptr())), ctx.h)
+        ts.append(_lib.lib.gf_last_device_seconds(ctx.h))
+    ctx.close()
+    a, sp = float(np.median(ta[1:])), float(np.median(ts[1:]))
+    return {"mesh": f"Brick8 {edge}^3", "nodes": m.nnodes, "dofs": m.ndof,
+            "application_us": a * 1e6, "spmv_fp64_us": sp * 1e6, "application_over_spmv": a / sp,
+            "timing": "device time, L2 flushed before each call, median of %d" % reps}
+
+
 def learned_comparison(seed_base: int = 20260105, n_train: int = 48, n_test: int = 16):
     """Brick8 cubes with edge n uniform in 16..48 elements, correlated log-normal E (sigma
     U(0.5, 2), correlation length U(0.05, 0.3)) and nu U(0.2, 0.4), z = 0 clamped,
@@ -526,6 +574,8 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 48, n_test: int
         row["application_us"] = float(np.median(ta)) * 1e6
         row["spmv_fp64_us"] = float(np.median(ts)) * 1e6
         results.append(row)
+
+    app48 = learned_application(ctx_lp=ctx)
     ctx.close()
 
     def ratio(a, b, key):
@@ -534,8 +584,7 @@ def learned_comparison(seed_base: int = 20260105, n_train: int = 48, n_test: int
     summary = {f"median_{key}_ratio_{a}_over_pcg_fp64": ratio(a, "pcg_fp64", key)
                for a in ("learned_fcg", "twolevel_pcg") for key in ("iterations", "seconds")}
     summary["learned_fcg_fallbacks"] = int(sum(r["learned_fcg"]["fallback"] for r in results))
-    big = max(results, key=lambda r: r["dofs"])
-    summary["largest_mesh_application_over_spmv"] = big["application_us"] / big["spmv_fp64_us"]
+    summary["application_brick8_48"] = app48
     return {"train_meshes": n_train, "held_out_meshes": n_test, "train_seconds": train_s,
             "final_train_loss": losses[-1], "first_train_loss": losses[0],
             "tol_rel_residual": 1e-8, "summary": summary, "held_out": results}
@@ -631,9 +680,8 @@ def run_gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # "auto" resolves as the library's GF_SCATTER_AUTO does: atomic for Brick20, owner else
-    sname = args.scatter if args.scatter != "auto" else (
-        "atomic" if m.elem_type == mg.BRICK20 else "owner")
+    # "auto" resolves as the library's GF_SCATTER_AUTO does: atomic in 3-D, owner in 2-D
+    sname = args.scatter if args.scatter != "auto" else ("atomic" if m.dim == 3 else "owner")
     scatter = {"owner": _lib.GF_SCATTER_OWNER, "colour": _lib.GF_SCATTER_COLOR,
                "atomic": _lib.GF_SCATTER_ATOMIC}[sname]
     for _ in range(args.warmup):
@@ -705,17 +753,21 @@ def run_gpu_arm(args):
     hbm, peak_kind = peaks()
     alg_bytes = nnz * esize + m.nnodes * m.dim * esize + m.nelem * (m.nen * 4 + esize)
     achieved = alg_bytes / per_step / 1e9
-    # dominant kernel (owner schedule: k_assemble_owner): K values written once, plus
-    # what it must read — J^-1 and w*detJ per element and Gauss point, the moduli, and
-    # per incidence the element id, local node index and nen neighbour slots
+    # dominant kernel (owner schedule: k_assemble_owner_node for 2-D FP32, else
+    # k_assemble_owner): K values written once, plus what it must read — J^-1 and w*detJ
+    # per element and Gauss point (the 2-D FP32 kernel reads w*detJ*E, the modulus folded
+    # in; the other reads the moduli apart), and per incidence the element id, local node
+    # index and nen neighbour slots
     ngp = m.ngauss ** m.dim
     t_geo = float(np.mean([a for a, _ in split]))
     t_dom = float(np.mean([b for _, b in split]))
     if sname == "owner":
         ninc = m.nelem * m.nen
-        dom_bytes = (nnz * esize + m.nelem * ngp * (m.dim * m.dim + 1) * esize + m.nelem * esize
+        node_kernel = m.dim == 2 and esize == 4
+        dom_bytes = (nnz * esize + m.nelem * ngp * (m.dim * m.dim + 1) * esize
+                     + (0 if node_kernel else m.nelem * esize)
                      + ninc * (4 + 1 + 2 * m.nen) + (m.nnodes + 1) * 4)
-        dom_name = "k_assemble_owner"
+        dom_name = "k_assemble_owner_node" if node_kernel else "k_assemble_owner"
     else:
         dom_bytes = alg_bytes
         dom_name = ("k_assemble (all colour passes)" if sname == "colour" else
@@ -726,7 +778,7 @@ def run_gpu_arm(args):
         tr = json.loads(tfile.read_text()).get(f"{cfg}/assemble")
         if tr is not None:
             traffic_asm = tr.get("bytes_per_assembly")
-            traffic = tr.get("kernels", {}).get("k_assemble_owner")
+            traffic = tr.get("kernels", {}).get(dom_name)
 
     # SpMV roofline: node-block slices, i.e. the values, one int32 column per dim x dim
     # block, x read once and y written once
@@ -892,6 +944,9 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="split the workload over the ranks (node slabs) and solve with the "
                          "device-resident sharded PCG instead of running replicas")
+    ap.add_argument("--learned-application", action="store_true",
+                    help="time only one learned-preconditioner application against one FP64 "
+                         "SpMV on the Brick8 48^3 mesh (untrained network) and print it")
     ap.add_argument("--no-north-star", action="store_true",
                     help="skip the Brick20 64^3 assembly + solve study of the default run")
     ap.add_argument("--scatter", default="auto", choices=["owner", "colour", "atomic", "auto"])
@@ -902,6 +957,8 @@ def main():
         run_reference_arm(args)
     elif args.sharded:
         run_sharded_arm(args)
+    elif args.learned_application:
+        print(json.dumps(learned_application()), flush=True)
     else:
         run_gpu_arm(args)
 

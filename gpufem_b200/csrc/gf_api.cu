@@ -501,8 +501,8 @@ GF_API gf_status gf_assemble(gf_ctx* ctx, int32_t dtype, int32_t scatter, int32_
   if (engine != GF_ENGINE_CUDA_CORE && engine != GF_ENGINE_TF32_MMA)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown engine %d", engine);
   if (scatter == GF_SCATTER_AUTO)  // fastest measured schedule per element type (B200)
-    scatter = (ctx->elem_type == GF_BRICK20 && engine != GF_ENGINE_TF32_MMA) ? GF_SCATTER_ATOMIC
-                                                                               : GF_SCATTER_OWNER;
+    scatter = (ctx->dim == 3 && engine != GF_ENGINE_TF32_MMA) ? GF_SCATTER_ATOMIC
+                                                              : GF_SCATTER_OWNER;
   if (engine == GF_ENGINE_TF32_MMA && dtype != GF_F32)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "the TF32 engine assembles FP32 only");
   cudaSetDevice(ctx->device);

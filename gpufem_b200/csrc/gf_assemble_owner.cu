@@ -137,8 +137,13 @@ constexpr int geo_stride(bool node) {
   return node ? (PER + 7) / 8 * 8 : PER;
 }
 
+template <int ET, typename TC, int NG1>
+constexpr int geo_stage_stride(bool node) {
+  return geo_stride<ET, TC, NG1>(node) | 1;
+}
+
 template <int ET, typename TC, int NG1, bool NODE>
-__global__ void __launch_bounds__(kOT)
+__global__ void __launch_bounds__(kOT, gf_elem_info(ET).dim == 2 ? 3 : 1)
 k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
                    const double* __restrict__ coords, const TC* __restrict__ Eel,
                    TC* __restrict__ geo) {
@@ -151,7 +156,10 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
   // 1-D weights (1, 1) or (5/9, 8/9, 5/9), multiplied in the reference's tensor order
   constexpr double w1[3] = {NG1 == 2 ? 1.0 : 5.0 / 9.0, NG1 == 2 ? 1.0 : 8.0 / 9.0, 5.0 / 9.0};
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TC* stage = reinterpret_cast<TC*>(smem_raw) + (size_t)(threadIdx.x >> 5) * 32 * PS;
+  // staging rows of SPS = PS rounded up to odd: a warp's 32 element rows, written a value
+  // at a time, then fall on distinct banks
+  constexpr int SPS = geo_stage_stride<ET, TC, NG1>(NODE);
+  TC* stage = reinterpret_cast<TC*>(smem_raw) + (size_t)(threadIdx.x >> 5) * 32 * SPS;
   const bool f64 = sizeof(TC) == 8;
   const int lane = threadIdx.x & 31;
   const int e0 = (blockIdx.x * kOT + threadIdx.x) & ~31;  // first element of the warp
@@ -175,55 +183,21 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
         }
       }
     }
+    // FP32 J^-1 and w detJ straight into the staging block, with the distortion test over
+    // the same Jacobians; an element that fails it is redone in FP64 (rare)
+    TC* out = stage + lane * SPS;
+#pragma unroll
+    for (int k = PER; k < PS; ++k) out[k] = TC(0);
+    const TC Ee = NODE ? Eel[e] : TC(1);
     bool use64 = f64;
     if (!f64) {
       float dmin = 3.4e38f, dmax = 0.f;
 #pragma unroll
       for (int g = 0; g < NGP; ++g) {
-        float J[3][3], Ji[3][3];
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            float s = 0.f;
-#pragma unroll
-            for (int i = 0; i < NEN; ++i) s += Tab.d32[(g * DIM + a) * NEN + i] * Xf[i][c];
-            J[a][c] = s;
-          }
-        const float d = fabsf(gf_det_inv<DIM, float>(J, Ji));
-        dmin = fminf(dmin, d);
-        dmax = fmaxf(dmax, d);
-      }
-      use64 = dmax > 10.f * dmin;
-    }
-    TC* out = stage + lane * PS;
-#pragma unroll
-    for (int k = PER; k < PS; ++k) out[k] = TC(0);
-    const TC Ee = NODE ? Eel[e] : TC(1);
-#pragma unroll
-    for (int g = 0; g < NGP; ++g) {
-      const int gi = DIM == 2 ? g / NG1 : g / (NG1 * NG1);
-      const int gj = DIM == 2 ? g % NG1 : (g / NG1) % NG1;
-      const int gk = DIM == 2 ? 0 : g % NG1;
-      const double wg = w1[gi] * w1[gj] * (DIM == 2 ? 1.0 : w1[gk]);
-      if (use64) {
-        double J[3][3], Ji[3][3];
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            double s = 0.0;
-#pragma unroll
-            for (int i = 0; i < NEN; ++i) s += Tab.d64[(g * DIM + a) * NEN + i] * X[i][c];
-            J[a][c] = s;
-          }
-        const double d = gf_det_inv<DIM, double>(J, Ji);
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
-        out[g * GS + DIM * DIM] = NODE ? TC(wg * d) * Ee : TC(wg * d);
-      } else {
+        const int gi = DIM == 2 ? g / NG1 : g / (NG1 * NG1);
+        const int gj = DIM == 2 ? g % NG1 : (g / NG1) % NG1;
+        const int gk = DIM == 2 ? 0 : g % NG1;
+        const double wg = w1[gi] * w1[gj] * (DIM == 2 ? 1.0 : w1[gk]);
         float J[3][3], Ji[3][3];
 #pragma unroll
         for (int a = 0; a < DIM; ++a)
@@ -240,6 +214,34 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
 #pragma unroll
           for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
         out[g * GS + DIM * DIM] = NODE ? TC((float)wg * d) * Ee : TC((float)wg * d);
+        dmin = fminf(dmin, fabsf(d));
+        dmax = fmaxf(dmax, fabsf(d));
+      }
+      use64 = dmax > 10.f * dmin;
+    }
+    if (use64) {
+#pragma unroll
+      for (int g = 0; g < NGP; ++g) {
+        const int gi = DIM == 2 ? g / NG1 : g / (NG1 * NG1);
+        const int gj = DIM == 2 ? g % NG1 : (g / NG1) % NG1;
+        const int gk = DIM == 2 ? 0 : g % NG1;
+        const double wg = w1[gi] * w1[gj] * (DIM == 2 ? 1.0 : w1[gk]);
+        double J[3][3], Ji[3][3];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) {
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < NEN; ++i) s += Tab.d64[(g * DIM + a) * NEN + i] * X[i][c];
+            J[a][c] = s;
+          }
+        const double d = gf_det_inv<DIM, double>(J, Ji);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) out[g * GS + a * DIM + c] = TC(Ji[a][c]);
+        out[g * GS + DIM * DIM] = NODE ? TC(wg * d) * Ee : TC(wg * d);
       }
     }
   }
@@ -247,7 +249,10 @@ k_elem_geometry_pe(int nelem, const int32_t* __restrict__ conn,
   // the warp's elements are consecutive: their outputs form one contiguous block
   const int nw = min(32, nelem - e0);
   TC* dst = geo + (int64_t)e0 * PS;
-  for (int k = lane; k < nw * PS; k += 32) dst[k] = stage[k];
+  for (int k = lane; k < nw * PS; k += 32) {
+    const int el = k / PS;
+    dst[k] = stage[el * SPS + (k - el * PS)];
+  }
 }
 
 // Block rows H_j, j in [J0, J0 + JG), of one task with the Gauss rule known at compile
@@ -796,7 +801,9 @@ gf_status launch_owner_node(gf_ctx* ctx, float* K, const AsmTables* d_tab) {
   gf_status st = owner_geo_buffer(ctx, (size_t)ctx->nelem * PS * sizeof(float));
   if (st != GF_OK) return st;
   float* geo = static_cast<float*>(ctx->d_geo);
-  const size_t gsm = sizeof(float) * (size_t)kOT * PS;
+  const size_t gsm = sizeof(float) * (size_t)kOT *
+                    (ctx->ngauss == 2 ? geo_stage_stride<ET, float, 2>(true)
+                                      : geo_stage_stride<ET, float, 3>(true));
   auto gk = ctx->ngauss == 2 ? k_elem_geometry_pe<ET, float, 2, true>
                              : k_elem_geometry_pe<ET, float, 3, true>;
   GF_CUDA(ctx, gf_smem_attr(gk, (int)gsm));
@@ -827,7 +834,7 @@ gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   if (st != GF_OK) return st;
   TC* geo = static_cast<TC*>(ctx->d_geo);
   // per-element kernel where its output staging fits (Q4, Q8; Brick8 with 2x2x2 Gauss)
-  const size_t gsm = sizeof(TC) * (size_t)kOT * ngp * (info.dim * info.dim + 1);
+  const size_t gsm = sizeof(TC) * (size_t)kOT * (ngp * (info.dim * info.dim + 1) | 1);
   bool per_element = false;
   if constexpr (info.nen * info.dim <= 24) {
     if (gsm <= 100 * 1024) {

@@ -107,7 +107,6 @@ struct LpState {
   float* pr = nullptr;       // [npairs][n]
   float* pe = nullptr;       // [npairs][n]
   int* err = nullptr;        // set by a tensor-core layer whose MMA wait timed out
-  int mm_grid = 0;           // CTAs of the tensor-core layers (resident CTAs per SM x SMs)
   bool ready = false;        // diag / graph set up for the current matrix
   bool coarse = false;       // with the two-level coarse correction (gf_lp_set_coarse)
   int loss = GF_LP_LOSS_ERROR;
@@ -225,16 +224,44 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-#pragma unroll 8
-  for (int q = tid; q < P * NOP * KDP; q += kMmThreads) {   // unrolled: the loads overlap
-    const int p = q / (NOP * KDP), rem = q % (NOP * KDP);
-    const int n = rem / KDP, k = rem % KDP;
-    float v = 0.f;
-    if (n < NO && k < KD) {
-      const __nv_bfloat16* W = p == 0 ? W1 : W2;
-      v = __bfloat162float(WT ? W[(int64_t)k * NO + n] : W[(int64_t)n * KD + k]);
+  if constexpr (!WT && KD % 4 == 0) {
+    // four consecutive k of one output channel per 8-byte load, all loads in flight at once
+    constexpr int NQ = P * NOP * KDP / 4;
+    constexpr int PER = (NQ + kMmThreads - 1) / kMmThreads;
+    uint2 wv[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int q = tid + u * kMmThreads;
+      const int p = q / (NOP * KDP / 4), rem = q % (NOP * KDP / 4);
+      const int n = rem / (KDP / 4), k = (rem % (KDP / 4)) * 4;
+      wv[u] = make_uint2(0u, 0u);
+      if (q < NQ && n < NO && k < KD)
+        wv[u] = __ldg(reinterpret_cast<const uint2*>((p == 0 ? W1 : W2) + (int64_t)n * KD + k));
     }
-    wt[p * NOP * KDP + (k >> 2) * NOP * 4 + n * 4 + (k & 3)] = v;
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int q = tid + u * kMmThreads;
+      if (q < NQ) {
+        const int p = q / (NOP * KDP / 4), rem = q % (NOP * KDP / 4);
+        const int n = rem / (KDP / 4), k = (rem % (KDP / 4)) * 4;
+        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&wv[u].x));
+        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&wv[u].y));
+        *reinterpret_cast<float4*>(wt + p * NOP * KDP + (k >> 2) * NOP * 4 + n * 4) =
+            make_float4(lo.x, lo.y, hi.x, hi.y);
+      }
+    }
+  } else {
+#pragma unroll 8
+    for (int q = tid; q < P * NOP * KDP; q += kMmThreads) {   // unrolled: the loads overlap
+      const int p = q / (NOP * KDP), rem = q % (NOP * KDP);
+      const int n = rem / KDP, k = rem % KDP;
+      float v = 0.f;
+      if (n < NO && k < KD) {
+        const __nv_bfloat16* W = p == 0 ? W1 : W2;
+        v = __bfloat162float(WT ? W[(int64_t)k * NO + n] : W[(int64_t)n * KD + k]);
+      }
+      wt[p * NOP * KDP + (k >> 2) * NOP * 4 + n * 4 + (k & 3)] = v;
+    }
   }
   for (int q = tid; q < NOP; q += kMmThreads)
     sb[q] = (bias && q < NO) ? __bfloat162float(bias[q]) : 0.f;
@@ -248,89 +275,92 @@ k_lp_mm_tc(int N, const float* __restrict__ X1, const float* __restrict__ X2,
   uint32_t phase = 0;
   bool ok = true;
   const int ntiles = (N + 127) / 128;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int a0 = tile * 128;
-    for (int p = 0; p < P && ok; ++p) {
-      const float* X = p == 0 ? X1 : X2;
-      // every thread issues all its loads of the tile before using any (NCH 16-byte
-      // chunks per row, 128 * NCH / 128 = NCH per thread), so the tile arrives in one
-      // round of memory latency
-      float4 xv[NCH];
+  // steps = (tile, part) pairs of this CTA; the X loads of the next step are issued right
+  // after the current step's MMAs, so they are in flight during the MMA wait and the
+  // epilogue
+  const int mytiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int nsteps = mytiles * P;
+  float4 xv[NCH];
+  auto chunk_of = [&](int q, int& r, int& c) {
+    // a warp takes 8 rows x 4 chunks (when NCH >= 4): 64 contiguous bytes of each of 8
+    // rows in global memory, a 4-way bank conflict at most in shared memory
+    if constexpr (NCH % 4 == 0) {
+      const int ln = q & 31, wq = q >> 5;
+      r = (wq & 15) * 8 + (ln & 7);
+      c = (wq >> 4) * 4 + (ln >> 3);
+    } else {
+      r = q & 127;
+      c = q >> 7;
+    }
+  };
+  auto load_step = [&](int st) {
+    // every thread issues all its loads of the tile part before using any (NCH 16-byte
+    // chunks per row, 128 * NCH / 128 = NCH per thread): one round of memory latency
+    const int a0s = (blockIdx.x + (st / P) * gridDim.x) * 128;
+    const float* X = st % P == 0 ? X1 : X2;
 #pragma unroll
-      for (int u = 0; u < NCH; ++u) {
-        const int q = tid + u * kMmThreads;
-        // a warp takes 8 rows x 4 chunks (when NCH >= 4): 64 contiguous bytes of each of 8
-        // rows in global memory, a 4-way bank conflict at most in shared memory
-        int r, c;
-        if constexpr (NCH % 4 == 0) {
-          const int ln = q & 31, wq = q >> 5;
-          r = (wq & 15) * 8 + (ln & 7);
-          c = (wq >> 4) * 4 + (ln >> 3);
-        } else {
-          r = q & 127;
-          c = q >> 7;
-        }
-        const int a = a0 + r;
-        if constexpr (KD % 4 == 0) {
-          xv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (a < N && 4 * c < KD)
-            xv[u] = __ldg(reinterpret_cast<const float4*>(X + (int64_t)a * KD) + c);
-        } else {
-          float* v = &xv[u].x;
-#pragma unroll
-          for (int w = 0; w < 4; ++w) {
-            const int k = 4 * c + w;
-            v[w] = (a < N && k < KD) ? __ldg(X + (int64_t)a * KD + k) : 0.f;
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < NCH; ++u) {
-        const int q = tid + u * kMmThreads;
-        int r, c;
-        if constexpr (NCH % 4 == 0) {
-          const int ln = q & 31, wq = q >> 5;
-          r = (wq & 15) * 8 + (ln & 7);
-          c = (wq >> 4) * 4 + (ln >> 3);
-        } else {
-          r = q & 127;
-          c = q >> 7;
-        }
-        const float* v = &xv[u].x;
-        float4 h, l;
-        float* hp = &h.x;
-        float* lp = &l.x;
+    for (int u = 0; u < NCH; ++u) {
+      int r, c;
+      chunk_of(tid + u * kMmThreads, r, c);
+      const int a = a0s + r;
+      if constexpr (KD % 4 == 0) {
+        xv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a < N && 4 * c < KD)
+          xv[u] = __ldg(reinterpret_cast<const float4*>(X + (int64_t)a * KD) + c);
+      } else {
+        float* v = &xv[u].x;
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
-          const uint32_t hb = tc_tf32_round(v[w]);
-          hp[w] = __uint_as_float(hb);
-          lp[w] = __uint_as_float(tc_tf32_round(v[w] - __uint_as_float(hb)));
+          const int k = 4 * c + w;
+          v[w] = (a < N && k < KD) ? __ldg(X + (int64_t)a * KD + k) : 0.f;
         }
-        *reinterpret_cast<float4*>(xh + c * 512 + r * 4) = h;
-        *reinterpret_cast<float4*>(xl + c * 512 + r * 4) = l;
       }
-      tc_fence_async_smem();
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
-      if (tid == 0) {
-        const uint32_t ah = tc_smem_u32(xh), al = tc_smem_u32(xl);
-        const uint32_t bw = tc_smem_u32(wt + p * NOP * KDP);
-        for (int ks = 0; ks < KDP / 8; ++ks) {
-          const uint64_t db = tc_desc(bw + ks * 2 * NOP * 16, NOP * 16, 128);
-          tc_mma_tf32(tmem, tc_desc(al + ks * 2 * 128 * 16, 128 * 16, 128), db, idesc,
-                      (p > 0 || ks > 0) ? 1u : 0u);
-          tc_mma_tf32(tmem, tc_desc(ah + ks * 2 * 128 * 16, 128 * 16, 128), db, idesc, 1u);
-        }
-        tc_commit(mbar);
-      }
-      // the X tiles are rewritten by the next part or tile only after these MMAs finished
-      const bool done = tc_mbar_wait(mbar, phase, kMmWaitIters);
-      phase ^= 1u;
-      if (!done && lane == 0) atomicExch(err, 1);
-      ok = __syncthreads_and(done);
-      tc_fence_after();
     }
+  };
+  if (nsteps > 0) load_step(0);
+  for (int st = 0; st < nsteps && ok; ++st) {
+    const int p = st % P;
+    const int a0 = (blockIdx.x + (st / P) * gridDim.x) * 128;
+#pragma unroll
+    for (int u = 0; u < NCH; ++u) {
+      int r, c;
+      chunk_of(tid + u * kMmThreads, r, c);
+      const float* v = &xv[u].x;
+      float4 h, l;
+      float* hp = &h.x;
+      float* lp = &l.x;
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        const uint32_t hb = tc_tf32_round(v[w]);
+        hp[w] = __uint_as_float(hb);
+        lp[w] = __uint_as_float(tc_tf32_round(v[w] - __uint_as_float(hb)));
+      }
+      *reinterpret_cast<float4*>(xh + c * 512 + r * 4) = h;
+      *reinterpret_cast<float4*>(xl + c * 512 + r * 4) = l;
+    }
+    tc_fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+      const uint32_t ah = tc_smem_u32(xh), al = tc_smem_u32(xl);
+      const uint32_t bw = tc_smem_u32(wt + p * NOP * KDP);
+      for (int ks = 0; ks < KDP / 8; ++ks) {
+        const uint64_t db = tc_desc(bw + ks * 2 * NOP * 16, NOP * 16, 128);
+        tc_mma_tf32(tmem, tc_desc(al + ks * 2 * 128 * 16, 128 * 16, 128), db, idesc,
+                    (p > 0 || ks > 0) ? 1u : 0u);
+        tc_mma_tf32(tmem, tc_desc(ah + ks * 2 * 128 * 16, 128 * 16, 128), db, idesc, 1u);
+      }
+      tc_commit(mbar);
+    }
+    if (st + 1 < nsteps) load_step(st + 1);
+    // the X tiles are rewritten by the next step (or the staging) only after these MMAs
+    const bool done = tc_mbar_wait(mbar, phase, kMmWaitIters);
+    phase ^= 1u;
+    if (!done && lane == 0) atomicExch(err, 1);
+    ok = __syncthreads_and(done);
+    tc_fence_after();
+    if (p < P - 1) continue;
     if (!ok) break;
     // epilogue: a thread per node (TMEM lane), its NO output channels
     const int a = a0 + warp * 32 + lane;
@@ -760,48 +790,55 @@ static void lp_aggregate(gf_ctx* ctx, const float* h, float* out, int backward) 
   ctx->launches++;
 }
 
-// Tensor-core dense layer on the context stream (see k_lp_mm_tc).
+// Resident CTAs per SM of one tensor-core layer kernel (set by lp_mm_attr).
+template <int KD, int NO, bool TWO, bool WT>
+static int& lp_mm_per_sm() {
+  static int v = 1;
+  return v;
+}
+
+// Tensor-core dense layer on the context stream (see k_lp_mm_tc): a persistent grid of
+// the kernel's own resident CTAs per SM on every SM.
 template <int KD, int NO, bool TWO, bool WT>
 static void lp_mm(gf_ctx* ctx, const float* X1, const float* X2, const __nv_bfloat16* W1,
                   const __nv_bfloat16* W2, const __nv_bfloat16* bias, float* pre, float* out,
                   int relu, int accumulate) {
   LpState* s = ctx->lp;
   const int ntiles = (s->N + 127) / 128;
-  const int grid = std::max(1, std::min(ntiles, s->mm_grid));
+  const int grid =
+      std::max(1, std::min(ntiles, ctx->sm_count * lp_mm_per_sm<KD, NO, TWO, WT>()));
   k_lp_mm_tc<KD, NO, TWO, WT><<<grid, kMmThreads, mm_smem_bytes<KD, NO, TWO>(), ctx->stream>>>(
       s->N, X1, X2, W1, W2, bias, pre, out, relu, accumulate, s->err);
   ctx->launches++;
 }
 
 template <int KD, int NO, bool TWO, bool WT>
-static gf_status lp_mm_attr(gf_ctx* ctx, int* per_sm) {
+static gf_status lp_mm_attr(gf_ctx* ctx) {
   auto k = k_lp_mm_tc<KD, NO, TWO, WT>;
   const int sm = (int)mm_smem_bytes<KD, NO, TWO>();
   GF_CUDA(ctx, gf_smem_attr(k, sm));
   GF_CUDA(ctx, gf_func_attr(reinterpret_cast<const void*>(k),
                             cudaFuncAttributePreferredSharedMemoryCarveout,
                             (int)cudaSharedmemCarveoutMaxShared));
-  *per_sm = std::min(*per_sm, tc_ctas_per_sm(k, kMmThreads, (size_t)sm, (int)mm_tmem_cols(mm_pad16(NO))));
+  lp_mm_per_sm<KD, NO, TWO, WT>() =
+      tc_ctas_per_sm(k, kMmThreads, (size_t)sm, (int)mm_tmem_cols(mm_pad16(NO)));
   return GF_OK;
 }
 
 // One-time set-up of the tensor-core layers of a dim-dimensional network.
 static gf_status lp_mm_setup(gf_ctx* ctx, int dim) {
-  LpState* s = ctx->lp;
-  int per_sm = 512 / 64;   // TMEM: 64 columns per CTA
   gf_status st;
   if (dim == 2) {
-    if ((st = lp_mm_attr<8, H, false, false>(ctx, &per_sm)) != GF_OK) return st;
-    if ((st = lp_mm_attr<H, 2, false, false>(ctx, &per_sm)) != GF_OK) return st;
-    if ((st = lp_mm_attr<2, H, false, true>(ctx, &per_sm)) != GF_OK) return st;
+    if ((st = lp_mm_attr<8, H, false, false>(ctx)) != GF_OK) return st;
+    if ((st = lp_mm_attr<H, 2, false, false>(ctx)) != GF_OK) return st;
+    if ((st = lp_mm_attr<2, H, false, true>(ctx)) != GF_OK) return st;
   } else {
-    if ((st = lp_mm_attr<12, H, false, false>(ctx, &per_sm)) != GF_OK) return st;
-    if ((st = lp_mm_attr<H, 3, false, false>(ctx, &per_sm)) != GF_OK) return st;
-    if ((st = lp_mm_attr<3, H, false, true>(ctx, &per_sm)) != GF_OK) return st;
+    if ((st = lp_mm_attr<12, H, false, false>(ctx)) != GF_OK) return st;
+    if ((st = lp_mm_attr<H, 3, false, false>(ctx)) != GF_OK) return st;
+    if ((st = lp_mm_attr<3, H, false, true>(ctx)) != GF_OK) return st;
   }
-  if ((st = lp_mm_attr<H, H, true, false>(ctx, &per_sm)) != GF_OK) return st;
-  if ((st = lp_mm_attr<H, H, false, true>(ctx, &per_sm)) != GF_OK) return st;
-  s->mm_grid = ctx->sm_count * per_sm;
+  if ((st = lp_mm_attr<H, H, true, false>(ctx)) != GF_OK) return st;
+  if ((st = lp_mm_attr<H, H, false, true>(ctx)) != GF_OK) return st;
   return GF_OK;
 }
 

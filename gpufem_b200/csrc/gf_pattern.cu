@@ -121,61 +121,81 @@ __global__ void k_node_adjacency(int nnodes, int nen, const int32_t* __restrict_
   }
 }
 
-// Warp per node, for meshes whose nodes all see at most 32 element-node slots (every
-// 2-D mesh with at most 32 / nen elements per node): one pass gives the node's incident
-// elements in ascending order (written back to inc), its local index in each, the rank
-// of every element node among the node's distinct neighbours (= the neighbour's slot in
-// the sorted adjacency list, inc_slot), the node's own slot (diagpos), the neighbour
-// count and the sorted list itself, at adj_tmp[inc_off[node] * nen + rank] (a node's list
-// has at most as many entries as it has element-node slots).  The same quantities as
-// k_node_adjacency + k_incidence_finish + k_diagpos, without their searches.
-__global__ void k_node_pattern(int nnodes, int nen, const int32_t* __restrict__ conn,
-                               const int32_t* __restrict__ inc_off, int32_t* __restrict__ inc,
-                               int32_t* __restrict__ nadj, int32_t* __restrict__ adj_tmp,
-                               uint8_t* __restrict__ inc_loc, uint16_t* __restrict__ inc_slot,
-                               int32_t* __restrict__ diagpos) {
-  constexpr unsigned kFull = 0xffffffffu;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int node = blockIdx.x * kWarpsPerBlock + warp;
-  if (node >= nnodes) return;   // whole warp
+// Ascending bitonic sorting network over N register values (N a power of two; every
+// index is a compile-time constant once unrolled, so the array stays in registers).
+template <int N>
+__device__ __forceinline__ void sort_net(int (&a)[N]) {
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const int x = a[i], y = a[l];
+          const bool up = (i & k) == 0;
+          a[i] = up ? min(x, y) : max(x, y);
+          a[l] = up ? max(x, y) : min(x, y);
+        }
+      }
+}
+
+// Thread per node, for meshes whose nodes all see at most 32 element-node slots (every
+// 2-D mesh with at most 32 / nen elements per node) and fewer than 2^26 nodes: one pass
+// gives the node's incident elements in ascending order (written back to inc), its local
+// index in each, the slot of every element node in the node's sorted neighbour list
+// (inc_slot), the node's own slot (diagpos), the neighbour count and the sorted list itself,
+// at adj_tmp[inc_off[node] * nen + rank] (a node's list has at most as many entries as it
+// has element-node slots).  The element-node slots are sorted as keys node id * 32 + slot
+// in registers, so equal neighbours are adjacent and each slot's rank falls out of one
+// pass.  The same quantities as k_node_adjacency + k_incidence_finish + k_diagpos,
+// without their searches.
+template <int NEN>
+__global__ void __launch_bounds__(256)
+k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __restrict__ inc_off,
+               int32_t* __restrict__ inc, int32_t* __restrict__ nadj,
+               int32_t* __restrict__ adj_tmp, uint8_t* __restrict__ inc_loc,
+               uint16_t* __restrict__ inc_slot, int32_t* __restrict__ diagpos) {
+  constexpr int MAXD = 32 / NEN;   // incident elements per node (checked by the caller)
+  constexpr int kEmpty = 0x7fffffff;
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= nnodes) return;
   const int e0 = inc_off[node], deg = inc_off[node + 1] - e0;
-  const int C = deg * nen;      // <= 32 (the caller checked max degree * nen)
-  // ascending order of the incident elements (distinct ids): rank by comparison
-  const int el = lane < deg ? inc[e0 + lane] : 0x7fffffff;
-  int er = 0;
-  for (int q = 0; q < deg; ++q) er += __shfl_sync(kFull, el, q) < el ? 1 : 0;
-  // element of candidate slot `lane`: the one of rank lane / nen
-  const int kq = lane / nen, j = lane - kq * nen;
-  int myel = 0;
-  for (int q = 0; q < deg; ++q) {
-    const int rq = __shfl_sync(kFull, er, q);
-    const int eq = __shfl_sync(kFull, el, q);
-    if (rq == kq) myel = eq;
+  int el[MAXD];
+#pragma unroll
+  for (int q = 0; q < MAXD; ++q) el[q] = q < deg ? inc[e0 + q] : kEmpty;
+  sort_net<MAXD>(el);
+  int key[32];
+#pragma unroll
+  for (int q = 0; q < MAXD; ++q) {
+    if (q < deg) inc[e0 + q] = el[q];
+#pragma unroll
+    for (int j = 0; j < NEN; ++j)
+      key[q * NEN + j] = q < deg ? conn[(int64_t)el[q] * NEN + j] * 32 + q * NEN + j : kEmpty;
   }
-  __syncwarp();
-  if (lane < deg) inc[e0 + er] = el;
-  const bool act = lane < C;
-  const int v = act ? conn[(int64_t)myel * nen + j] : 0x7fffffff;
-  const unsigned same = __match_any_sync(kFull, v);
-  const bool first = act && (__ffs(same) - 1) == lane;
-  const unsigned firsts = __ballot_sync(kFull, first);
-  int rank = 0;   // distinct neighbours below v
-  for (int q = 0; q < C; ++q) {
-    const int vq = __shfl_sync(kFull, v, q);
-    rank += ((firsts >> q) & 1u) && vq < v ? 1 : 0;
-  }
-  if (lane == 0) {
-    nadj[node] = __popc(firsts);
-    if (C == 0) diagpos[node] = 0;
-  }
-  if (first) adj_tmp[(int64_t)e0 * nen + rank] = v;
-  if (act) {
-    inc_slot[(int64_t)(e0 + kq) * nen + j] = (uint16_t)rank;
-    if (v == node) {
-      inc_loc[e0 + kq] = (uint8_t)j;
-      diagpos[node] = rank;
+  sort_net<32>(key);
+  int rank = -1, prev = -1;
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const int kk = key[k];
+    if (kk != kEmpty) {
+      const int v = kk >> 5, slot = kk & 31;
+      if (v != prev) {
+        ++rank;
+        adj_tmp[(int64_t)e0 * NEN + rank] = v;
+        prev = v;
+      }
+      const int q = slot / NEN, j = slot - q * NEN;
+      inc_slot[(int64_t)(e0 + q) * NEN + j] = (uint16_t)rank;
+      if (v == node) {
+        inc_loc[e0 + q] = (uint8_t)j;
+        diagpos[node] = rank;
+      }
     }
   }
+  nadj[node] = rank + 1;
+  if (deg == 0) diagpos[node] = 0;
 }
 
 // Thread per row after k_node_pattern: rownnz and the row's columns from the node's sorted
@@ -382,16 +402,18 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   int32_t h_maxval = 0;
   GF_TRYC(cudaMemcpyAsync(&h_maxval, d_max + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_TRYC(cudaStreamSynchronize(s));
-  const bool fused = (int64_t)h_maxval * nen <= 32;
+  const bool fused = (int64_t)h_maxval * nen <= 32 && (nen == 4 || nen == 8) &&
+                     nnodes < (1 << 26);
   const int ablocks = (nnodes + kWarpsPerBlock - 1) / kWarpsPerBlock;
   if (fused) {
     GF_TRY(gf_palloc(ctx, &d_adjtmp, (size_t)total * nen));
     GF_TRY(gf_palloc(ctx, &ctx->d_inc_loc, (size_t)total));
     GF_TRY(gf_palloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
     GF_TRY(gf_palloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
-    k_node_pattern<<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
-        nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, d_adjtmp, ctx->d_inc_loc,
-        ctx->d_inc_slot, ctx->d_diagpos);
+    auto kp = nen == 4 ? k_node_pattern<4> : k_node_pattern<8>;
+    kp<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_conn, d_inc_off, d_inc, d_nadj,
+                                               d_adjtmp, ctx->d_inc_loc, ctx->d_inc_slot,
+                                               ctx->d_diagpos);
   } else {
     k_node_adjacency<0><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
         nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, nullptr, nullptr, d_err);

@@ -68,7 +68,8 @@ typedef enum gf_scatter {
                             of its rows in shared memory and writes every K entry once
                             (no colouring, no global atomics, no zero-fill)            */
   GF_SCATTER_AUTO = 3    /* the fastest of the above for the element type, as measured
-                            on B200: OWNER for Q4, Q8 and Brick8, ATOMIC for Brick20  */
+                            on B200: OWNER for Q4 and Q8, ATOMIC for Brick8 and Brick20
+                            (OWNER with GF_ENGINE_TF32_MMA)                           */
 } gf_scatter;
 
 /* Element-integration engine of gf_assemble (FP32 only; FP64 always uses CUDA cores). */
