@@ -170,9 +170,17 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
 #pragma unroll
   for (int q = 0; q < MAXD; ++q) {
     if (q < deg) inc[e0 + q] = el[q];
+    // the element's nodes as 16-byte loads (a row of conn is NEN * 4 = 16 or 32 bytes)
+    int4 nd[NEN / 4];
 #pragma unroll
-    for (int j = 0; j < NEN; ++j)
-      key[q * NEN + j] = q < deg ? conn[(int64_t)el[q] * NEN + j] * 32 + q * NEN + j : kEmpty;
+    for (int h = 0; h < NEN / 4; ++h)
+      nd[h] = q < deg ? __ldg(reinterpret_cast<const int4*>(conn + (int64_t)el[q] * NEN) + h)
+                      : make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int j = 0; j < NEN; ++j) {
+      const int* v = &nd[j / 4].x;
+      key[q * NEN + j] = q < deg ? v[j % 4] * 32 + q * NEN + j : kEmpty;
+    }
   }
   sort_net<32>(key);
   int rank = -1, prev = -1;
@@ -212,6 +220,7 @@ __global__ void k_rows_from_lists(int n, int W, int nen, const int32_t* __restri
   const int len = nadj[node] * DIM;
   const int32_t* list = adj_tmp + (int64_t)inc_off[node] * nen;
   rownnz[row] = len;
+#pragma unroll 6
   for (int s = 0; s < W; ++s) {
     const int b = s < len ? __ldg(list + s / DIM) : 0;
     colidx[(int64_t)s * n + row] = s < len ? b * DIM + s % DIM : row;

@@ -91,6 +91,50 @@ def test_per_element_modulus_matches_oracle(fem, oracle, et, n, ng):
             assert row_rel_err(A, ell_to_dense(rn, ci, v.astype(np.float64))) <= tol
 
 
+def _fan_mesh(et, k, R=2.5):
+    """k quadrilaterals around one centre node (the centre has k elements; every other
+    node one or two): spoke nodes at radius 1, outer corners at radius R between the
+    spokes, counter-clockwise in the reference's node order; Q8 adds the edge midpoints."""
+    th = 2 * np.pi * np.arange(k) / k
+    xy = [[0.0, 0.0]] + [[np.cos(t), np.sin(t)] for t in th] + \
+         [[R * np.cos(t + np.pi / k), R * np.sin(t + np.pi / k)] for t in th]
+    conn = [[1, 2 + j, 2 + k + j, 2 + (j + 1) % k] for j in range(k)]   # 1-based
+    if et == mg.Q8:
+        mids = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mids:
+                xy.append([(xy[a - 1][0] + xy[b - 1][0]) / 2, (xy[a - 1][1] + xy[b - 1][1]) / 2])
+                mids[key] = len(xy)
+            return mids[key]
+        conn = [c + [mid(c[0], c[1]), mid(c[1], c[2]), mid(c[2], c[3]), mid(c[3], c[0])]
+                for c in conn]
+    return np.array(xy), np.array(conn, np.int32)
+
+
+# (R keeps the elements well enough shaped for the FP32 tolerance: a numpy FP32
+# restatement of Ke gives 2-3e-7 of max|row| on these four, against 1e-5 for a Q8 fan of
+# 5 elements with R = 1.6)
+@pytest.mark.parametrize("et,k,R", [(mg.Q4, 5, 2.5), (mg.Q4, 7, 2.5), (mg.Q8, 3, 1.6),
+                                    (mg.Q8, 5, 2.5)])
+def test_irregular_node_degree_matches_oracle(fem, oracle, et, k, R):
+    """A node shared by k elements: the per-node pattern pass (at most 32 element-node
+    slots per node: Q4 k = 5, 7, Q8 k = 3) or the general one (Q8 k = 5: 40 slots), the
+    degree-sorted owner kernel, and every schedule, FP32 and FP64, against the oracle."""
+    xy, conn = _fan_mesh(et, k, R)
+    ctx = fem(0)
+    ctx.mesh_create(et, xy, conn, 3, 210e3, None, 0.3)
+    ro, co, vo = oracle.assemble(et, 3, xy, conn, 210e3, 0.3)
+    A = ell_to_dense(ro, co, vo)
+    for dtype, tol in ((_lib.GF_F64, TOL64), (_lib.GF_F32, TOL32)):
+        for scatter in SCATTERS:
+            ctx.assemble(dtype, scatter)
+            rn, ci, v = ctx.ell_download(dtype)
+            assert np.array_equal(rn, ro) and np.array_equal(ci, co)
+            assert row_rel_err(A, ell_to_dense(rn, ci, v.astype(np.float64))) <= tol
+
+
 def test_colour_and_atomic_agree_and_parity_colouring(fem):
     m = mg.workload("brick20_64", scale=1 / 8)
     ctx = make_ctx(fem, mesh=m)
