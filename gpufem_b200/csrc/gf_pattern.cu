@@ -141,23 +141,24 @@ __device__ __forceinline__ void sort_net(int (&a)[N]) {
       }
 }
 
-// Thread per node, for meshes whose nodes all see at most 32 element-node slots (every
-// 2-D mesh with at most 32 / nen elements per node) and fewer than 2^26 nodes: one pass
-// gives the node's incident elements in ascending order (written back to inc), its local
-// index in each, the slot of every element node in the node's sorted neighbour list
-// (inc_slot), the node's own slot (diagpos), the neighbour count and the sorted list itself,
-// at adj_tmp[inc_off[node] * nen + rank] (a node's list has at most as many entries as it
-// has element-node slots).  The element-node slots are sorted as keys node id * 32 + slot
-// in registers, so equal neighbours are adjacent and each slot's rank falls out of one
-// pass.  The same quantities as k_node_adjacency + k_incidence_finish + k_diagpos,
-// without their searches.
-template <int NEN>
+// Thread per node, for meshes whose nodes all see at most NK = 32 or 64 element-node slots
+// (2-D meshes with at most 32 / nen elements per node, Brick8 meshes with at most 8) and
+// fewer than 2^31 / NK nodes: one pass gives the node's incident elements in ascending
+// order (written back to inc), its local index in each, the slot of every element node in
+// the node's sorted neighbour list (inc_slot), the node's own slot (diagpos), the
+// neighbour count and the sorted list itself, at adj_tmp[inc_off[node] * nen + rank] (a
+// node's list has at most as many entries as it has element-node slots).  The
+// element-node slots are sorted as keys node id * NK + slot in registers, so equal
+// neighbours are adjacent and each slot's rank falls out of one pass.  The same quantities
+// as k_node_adjacency + k_incidence_finish + k_diagpos, without their searches.
+template <int NEN, int NK>
 __global__ void __launch_bounds__(256)
 k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __restrict__ inc_off,
                int32_t* __restrict__ inc, int32_t* __restrict__ nadj,
                int32_t* __restrict__ adj_tmp, uint8_t* __restrict__ inc_loc,
                uint16_t* __restrict__ inc_slot, int32_t* __restrict__ diagpos) {
-  constexpr int MAXD = 32 / NEN;   // incident elements per node (checked by the caller)
+  constexpr int MAXD = NK / NEN;   // incident elements per node (checked by the caller)
+  constexpr int SH = NK == 32 ? 5 : 6;
   constexpr int kEmpty = 0x7fffffff;
   const int node = blockIdx.x * blockDim.x + threadIdx.x;
   if (node >= nnodes) return;
@@ -166,7 +167,7 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
 #pragma unroll
   for (int q = 0; q < MAXD; ++q) el[q] = q < deg ? inc[e0 + q] : kEmpty;
   sort_net<MAXD>(el);
-  int key[32];
+  int key[NK];
 #pragma unroll
   for (int q = 0; q < MAXD; ++q) {
     if (q < deg) inc[e0 + q] = el[q];
@@ -179,16 +180,16 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
 #pragma unroll
     for (int j = 0; j < NEN; ++j) {
       const int* v = &nd[j / 4].x;
-      key[q * NEN + j] = q < deg ? v[j % 4] * 32 + q * NEN + j : kEmpty;
+      key[q * NEN + j] = q < deg ? (v[j % 4] << SH) + q * NEN + j : kEmpty;
     }
   }
-  sort_net<32>(key);
+  sort_net<NK>(key);
   int rank = -1, prev = -1;
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
+  for (int k = 0; k < NK; ++k) {
     const int kk = key[k];
     if (kk != kEmpty) {
-      const int v = kk >> 5, slot = kk & 31;
+      const int v = kk >> SH, slot = kk & (NK - 1);
       if (v != prev) {
         ++rank;
         adj_tmp[(int64_t)e0 * NEN + rank] = v;
@@ -206,6 +207,91 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
   if (deg == 0) diagpos[node] = 0;
 }
 
+// Warp per node, for meshes whose nodes see at most 32 elements and 256 element-node slots
+// (Brick20: 8 x 20 = 160) and fewer than 2^23 nodes: the same outputs as k_node_pattern.
+// The incident elements are sorted across the lanes by a shuffle bitonic network; the
+// element-node slots, as keys node id * 256 + slot, by a bitonic network in the warp's
+// shared-memory row over the next power of two above their count; each lane then ranks
+// a run of the sorted keys, with the distinct counts of the lanes before it from a
+// shuffle scan.
+constexpr int kWarpKeys = 256;
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+k_node_pattern_warp(int nnodes, int nen, const int32_t* __restrict__ conn,
+                    const int32_t* __restrict__ inc_off, int32_t* __restrict__ inc,
+                    int32_t* __restrict__ nadj, int32_t* __restrict__ adj_tmp,
+                    uint8_t* __restrict__ inc_loc, uint16_t* __restrict__ inc_slot,
+                    int32_t* __restrict__ diagpos) {
+  constexpr unsigned kFull = 0xffffffffu;
+  constexpr int kEmpty = 0x7fffffff;
+  __shared__ int skeys[kWarpsPerBlock][kWarpKeys];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int node = blockIdx.x * kWarpsPerBlock + warp;
+  if (node >= nnodes) return;   // whole warp
+  int* keys = skeys[warp];
+  const int e0 = inc_off[node], deg = inc_off[node + 1] - e0;   // deg <= 32
+  const int C = deg * nen;                                        // <= 256
+  int el = lane < deg ? inc[e0 + lane] : kEmpty;
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const int o = __shfl_xor_sync(kFull, el, j);
+      el = (((lane & j) == 0) == ((lane & k) == 0)) ? min(el, o) : max(el, o);
+    }
+  if (lane < deg) inc[e0 + lane] = el;   // lane q holds the element of rank q
+  int NP = 32;
+  while (NP < C) NP <<= 1;
+  for (int sl = lane; sl < NP; sl += 32) {
+    const int q = min(sl / nen, 31);
+    const int eq = __shfl_sync(kFull, el, q);
+    keys[sl] = sl < C ? (conn[(int64_t)eq * nen + (sl - q * nen)] << 8) | sl : kEmpty;
+  }
+  __syncwarp();
+  for (int k = 2; k <= NP; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int pr = lane; pr < NP / 2; pr += 32) {
+        const int i = 2 * j * (pr / j) + (pr % j), l = i + j;
+        const int x = keys[i], y = keys[l];
+        if ((x > y) == ((i & k) == 0)) {
+          keys[i] = y;
+          keys[l] = x;
+        }
+      }
+      __syncwarp();
+    }
+  const int per = NP / 32, b0 = lane * per;
+  int cnt = 0;
+  for (int m = 0; m < per; ++m) {
+    const int kk = keys[b0 + m];
+    if (kk != kEmpty && (b0 + m == 0 || (keys[b0 + m - 1] >> 8) != (kk >> 8))) ++cnt;
+  }
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  int rank = incl - cnt - 1;
+  for (int m = 0; m < per; ++m) {
+    const int pos = b0 + m, kk = keys[pos];
+    if (kk == kEmpty) break;
+    const int v = kk >> 8, slot = kk & 255;
+    if (pos == 0 || (keys[pos - 1] >> 8) != v) {
+      ++rank;
+      adj_tmp[(int64_t)e0 * nen + rank] = v;
+    }
+    const int q = slot / nen, j = slot - q * nen;
+    inc_slot[(int64_t)(e0 + q) * nen + j] = (uint16_t)rank;
+    if (v == node) {
+      inc_loc[e0 + q] = (uint8_t)j;
+      diagpos[node] = rank;
+    }
+  }
+  if (lane == 31) nadj[node] = incl;
+  if (lane == 0 && C == 0) diagpos[node] = 0;
+}
+
 // Thread per row after k_node_pattern: rownnz and the row's columns from the node's sorted
 // list in adj_tmp (slots past the row's length hold col = row; all threads walk the
 // slots together, so each slot's column of colidx is written by consecutive threads).
@@ -220,10 +306,13 @@ __global__ void k_rows_from_lists(int n, int W, int nen, const int32_t* __restri
   const int len = nadj[node] * DIM;
   const int32_t* list = adj_tmp + (int64_t)inc_off[node] * nen;
   rownnz[row] = len;
-#pragma unroll 6
-  for (int s = 0; s < W; ++s) {
-    const int b = s < len ? __ldg(list + s / DIM) : 0;
-    colidx[(int64_t)s * n + row] = s < len ? b * DIM + s % DIM : row;
+  // a neighbour at a time (W is a multiple of DIM): one list read per DIM slots
+#pragma unroll 2
+  for (int k = 0; k < W / DIM; ++k) {
+    const bool in = k * DIM < len;
+    const int b = in ? __ldg(list + k) * DIM : 0;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) colidx[(int64_t)(k * DIM + c) * n + row] = in ? b + c : row;
   }
 }
 
@@ -245,7 +334,7 @@ __global__ void k_adj_fill(int nnodes, int nen, const int32_t* __restrict__ inc_
     const int mi = __shfl_sync(kFull, m, i);
     const int64_t si = __shfl_sync(kFull, src, i);
     const int di = __shfl_sync(kFull, dst, i);
-    if (lane < mi) adj[di + lane] = __ldg(adj_tmp + si + lane);
+    for (int k = lane; k < mi; k += 32) adj[di + k] = __ldg(adj_tmp + si + k);
   }
 }
 
@@ -273,26 +362,27 @@ __global__ void k_colidx(int n, int W, const int32_t* __restrict__ adj_off,
   }
 }
 
-// thread per (element, local node i); e fastest so slot-map writes coalesce.
+// Thread per (element e, local node i), e fastest so the slot-map writes coalesce: the
+// slots of e's nodes in node i's adjacency list are the ones the pattern pass recorded for
+// that incidence (inc_slot), found by a short scan of node i's sorted incident elements.
 __global__ void k_slotmap(int nelem, int nen, const int32_t* __restrict__ conn,
-                          const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
+                          const int32_t* __restrict__ inc_off, const int32_t* __restrict__ inc,
+                          const uint16_t* __restrict__ inc_slot,
                           uint16_t* __restrict__ slotmap, int32_t* __restrict__ errflag) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= (int64_t)nelem * nen) return;
   const int e = (int)(t % nelem);
   const int i = (int)(t / nelem);
   const int a = conn[(int64_t)e * nen + i];
-  const int lo0 = adj_off[a], hi0 = adj_off[a + 1];
-  for (int j = 0; j < nen; ++j) {
-    const int b = conn[(int64_t)e * nen + j];
-    int lo = lo0, hi = hi0;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (adj[mid] < b) lo = mid + 1; else hi = mid;
-    }
-    if (lo >= hi0 || adj[lo] != b) atomicExch(errflag, 2);
-    slotmap[(int64_t)(i * nen + j) * nelem + e] = (uint16_t)(lo - lo0);
+  const int q1 = inc_off[a + 1];
+  int q = inc_off[a];
+  while (q < q1 && __ldg(inc + q) != e) ++q;
+  if (q >= q1) {
+    atomicExch(errflag, 2);
+    return;
   }
+  const uint16_t* src = inc_slot + (int64_t)q * nen;
+  for (int j = 0; j < nen; ++j) slotmap[(int64_t)(i * nen + j) * nelem + e] = __ldg(src + j);
 }
 
 __global__ void k_diagpos(int nnodes, const int32_t* __restrict__ adj_off,
@@ -411,18 +501,32 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   int32_t h_maxval = 0;
   GF_TRYC(cudaMemcpyAsync(&h_maxval, d_max + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GF_TRYC(cudaStreamSynchronize(s));
-  const bool fused = (int64_t)h_maxval * nen <= 32 && (nen == 4 || nen == 8) &&
-                     nnodes < (1 << 26);
+  // one pass per node: a register sort of its element-node slots (32 or 64 keys, a thread
+  // per node), else a shared-memory sort (up to 256 keys, a warp per node), else the
+  // general count / write / search passes
+  const int64_t slots_max = (int64_t)h_maxval * nen;
+  const int nkeys = slots_max <= 32 ? 32 : slots_max <= 64 ? 64 : 0;
+  const bool thread_pass = nkeys > 0 && (nen == 4 || nen == 8) && nnodes < (1 << 24);
+  const bool warp_pass = !thread_pass && h_maxval <= 32 && slots_max <= kWarpKeys &&
+                         nnodes < (1 << 23);
+  const bool fused = thread_pass || warp_pass;
   const int ablocks = (nnodes + kWarpsPerBlock - 1) / kWarpsPerBlock;
   if (fused) {
     GF_TRY(gf_palloc(ctx, &d_adjtmp, (size_t)total * nen));
     GF_TRY(gf_palloc(ctx, &ctx->d_inc_loc, (size_t)total));
     GF_TRY(gf_palloc(ctx, &ctx->d_inc_slot, (size_t)total * nen));
     GF_TRY(gf_palloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
-    auto kp = nen == 4 ? k_node_pattern<4> : k_node_pattern<8>;
-    kp<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_conn, d_inc_off, d_inc, d_nadj,
-                                               d_adjtmp, ctx->d_inc_loc, ctx->d_inc_slot,
-                                               ctx->d_diagpos);
+    if (thread_pass) {
+      auto kp = nen == 4 ? (nkeys == 32 ? k_node_pattern<4, 32> : k_node_pattern<4, 64>)
+                         : (nkeys == 32 ? k_node_pattern<8, 32> : k_node_pattern<8, 64>);
+      kp<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_conn, d_inc_off, d_inc, d_nadj,
+                                                 d_adjtmp, ctx->d_inc_loc, ctx->d_inc_slot,
+                                                 ctx->d_diagpos);
+    } else {
+      k_node_pattern_warp<<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
+          nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, d_adjtmp, ctx->d_inc_loc,
+          ctx->d_inc_slot, ctx->d_diagpos);
+    }
   } else {
     k_node_adjacency<0><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
         nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, nullptr, nullptr, d_err);
@@ -525,8 +629,9 @@ gf_status gf_slotmap_ensure(gf_ctx* ctx) {
   }
   int32_t h_err = 0;
   cudaMemsetAsync(d_err, 0, sizeof(int32_t), s);
-  k_slotmap<<<gf_blocks(total, 256), 256, 0, s>>>(nelem, nen, ctx->d_conn, ctx->d_adj_off,
-                                                  ctx->d_adj, ctx->d_slotmap, d_err);
+  k_slotmap<<<gf_blocks(total, 256), 256, 0, s>>>(nelem, nen, ctx->d_conn, ctx->d_inc_off,
+                                                  ctx->d_inc, ctx->d_inc_slot, ctx->d_slotmap,
+                                                  d_err);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
