@@ -50,9 +50,13 @@ def test_untrained_network_is_jacobi():
     assert np.allclose(z, r / d, rtol=1e-6, atol=0)
 
 
-@pytest.mark.parametrize("loss", ["error", "residual"])
-def test_forward_and_gradient_match_oracle(loss):
-    m, ctx = brick8_problem()
+# the 4x3x3 cube puts every node next to the boundary; the 16^3 cube (4,913 nodes,
+# 14,739 dofs) is the smallest mesh of the learned-preconditioner workload, where the
+# tensor-core layers run 39 full 128-node tiles and the aggregation walks interior nodes
+@pytest.mark.parametrize("loss,n", [("error", (4, 3, 3)), ("residual", (4, 3, 3)),
+                                    ("error", (16, 16, 16))])
+def test_forward_and_gradient_match_oracle(loss, n):
+    m, ctx = brick8_problem(n=n)
     ctx.lp_init(3, seed=1)
     if loss == "residual":
         ctx.lp_set_loss(_lib.GF_LP_LOSS_RESIDUAL)
