@@ -793,6 +793,7 @@ static gf_status owner_geo_buffer(gf_ctx* ctx, size_t bytes) {
 // memory, four CTAs per SM; trimmed to fit five, the kernel measured 4% slower: the
 // larger shared carve-out leaves less L1 for the geometry loads).
 constexpr int kOwnerNodeNB = 128;
+constexpr size_t kOwnerNodeSmemLimit = 112 * 1024;   // two CTAs per SM
 
 template <int ET>
 gf_status launch_owner_node(gf_ctx* ctx, float* K, const AsmTables* d_tab) {
@@ -815,7 +816,7 @@ gf_status launch_owner_node(gf_ctx* ctx, float* K, const AsmTables* d_tab) {
   auto kern = ctx->ngauss == 2 ? k_assemble_owner_node<ET, 2, NB> : k_assemble_owner_node<ET, 3, NB>;
   const size_t sm = ctx->ngauss == 2 ? owner_node_smem_bytes<ET, 2, NB>(W)
                                      : owner_node_smem_bytes<ET, 3, NB>(W);
-  if (sm > 200 * 1024)
+  if (sm > kOwnerNodeSmemLimit)
     return gf_fail(ctx, GF_ERR_UNSUPPORTED, "owner scatter: a row block does not fit");
   GF_CUDA(ctx, gf_smem_attr(kern, (int)sm));
   kern<<<(ctx->nnodes + NB - 1) / NB, NB, sm, ctx->stream>>>(
@@ -828,7 +829,14 @@ gf_status launch_owner_node(gf_ctx* ctx, float* K, const AsmTables* d_tab) {
 template <int ET, typename TC>
 gf_status launch_owner(gf_ctx* ctx, TC* K, const AsmTables* d_tab) {
   constexpr ElemInfo info = gf_elem_info(ET);
-  if constexpr (info.dim == 2 && sizeof(TC) == 4) return launch_owner_node<ET>(ctx, K, d_tab);
+  // 2-D FP32: the thread-per-node kernel, while its row tile keeps two CTAs per SM (a node
+  // with very many neighbours, e.g. the centre of a fan of 30 elements, makes W large);
+  // wider rows take the task kernel below, which shrinks its node block to fit
+  if constexpr (info.dim == 2 && sizeof(TC) == 4) {
+    const size_t node_sm = ctx->ngauss == 2 ? owner_node_smem_bytes<ET, 2, kOwnerNodeNB>(ctx->W)
+                                            : owner_node_smem_bytes<ET, 3, kOwnerNodeNB>(ctx->W);
+    if (node_sm <= kOwnerNodeSmemLimit) return launch_owner_node<ET>(ctx, K, d_tab);
+  }
   const int W = ctx->W, ngp = ctx->ngp;
   const int PER = ngp * (info.dim * info.dim + 1);
   gf_status st = owner_geo_buffer(ctx, (size_t)ctx->nelem * PER * sizeof(TC));

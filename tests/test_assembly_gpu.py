@@ -118,14 +118,16 @@ def _fan_mesh(et, k, R=2.5):
 # elements with R = 1.6)
 @pytest.mark.parametrize("et,k,R,fp32", [(mg.Q4, 5, 2.5, True), (mg.Q4, 7, 2.5, True),
                                          (mg.Q8, 3, 1.6, True), (mg.Q8, 5, 2.5, True),
-                                         (mg.Q8, 9, 3.0, True), (mg.Q4, 34, 2.0, False)])
+                                         (mg.Q8, 9, 3.0, True), (mg.Q8, 11, 3.0, True),
+                                         (mg.Q4, 34, 2.0, False)])
 def test_irregular_node_degree_matches_oracle(fem, oracle, et, k, R, fp32):
     """A node shared by k elements, through each per-node pattern pass: 32 register keys
     (at most 32 element-node slots per node: Q4 k = 5, 7, Q8 k = 3), 64 (Q8 k = 5: 40
     slots), the warp's shared-memory sort (Q8 k = 9: 72 slots) and the general passes
     (Q4 k = 34: more than 32 elements at a node; FP64 only, its 34 slivers are beyond the
-    FP32 tolerance); then the degree-sorted owner kernel and every schedule against the
-    oracle."""
+    FP32 tolerance); then the owner kernels (Q8 k = 11: rows of 112 slots, too wide for the
+    thread-per-node row tile, take the task kernel in FP32 too) and every schedule against
+    the oracle."""
     xy, conn = _fan_mesh(et, k, R)
     ctx = fem(0)
     ctx.mesh_create(et, xy, conn, 3, 210e3, None, 0.3)
