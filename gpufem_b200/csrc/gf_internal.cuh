@@ -256,6 +256,9 @@ struct gf_ctx {
   size_t work_bytes = 0;
   SolveScalars* d_scal = nullptr;
   void* h_pinned = nullptr;  // pinned scalars readback
+  int32_t* h_adj_stage = nullptr;   // pinned node adjacency for gf_ell_download
+  size_t h_adj_stage_n = 0;
+  cudaEvent_t ev_dl = nullptr;      // adjacency copied (gf_ell_download)
   double* d_red = nullptr;   // reduction scratch
   void* d_fcg = nullptr;     // flexible-CG scalars
 

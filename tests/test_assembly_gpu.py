@@ -141,6 +141,36 @@ def test_irregular_node_degree_matches_oracle(fem, oracle, et, k, R, fp32):
             assert row_rel_err(A, ell_to_dense(rn, ci, v.astype(np.float64))) <= tol
 
 
+class _I32View:
+    """A device int32 buffer as __cuda_array_interface__ (zero-copy)."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<i4",
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None, "stream": None}
+
+
+@pytest.mark.parametrize("name,scale", [("q8_512", 1.0), ("brick8_128", 0.25),
+                                        ("brick20_64", 0.25)])
+def test_download_expands_pattern_exactly(fem, name, scale):
+    """gf_ell_download sends a mesh-built pattern as its node adjacency and expands rownnz
+    and colidx on host threads: bit-equal to the device arrays (read through gf_ell_view)."""
+    import ctypes as C
+    import torch
+    m = mg.workload(name, scale=scale)
+    ctx = make_ctx(fem, mesh=m)
+    ctx.assemble(_lib.GF_F32)
+    rn, ci, v = ctx.ell_download(_lib.GF_F32)
+    n, W = C.c_int32(), C.c_int32()
+    drn, dci, dv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _lib.check(_lib.lib.gf_ell_view(ctx.h, _lib.GF_F32, C.byref(n), C.byref(W), C.byref(drn),
+                                    C.byref(dci), C.byref(dv)), ctx.h)
+    rn_dev = torch.as_tensor(_I32View(drn.value, n.value), device="cuda").cpu().numpy()
+    ci_dev = torch.as_tensor(_I32View(dci.value, n.value * W.value), device="cuda").cpu().numpy()
+    assert np.array_equal(rn, rn_dev)
+    assert np.array_equal(ci.ravel(), ci_dev)
+
+
 def test_colour_and_atomic_agree_and_parity_colouring(fem):
     m = mg.workload("brick20_64", scale=1 / 8)
     ctx = make_ctx(fem, mesh=m)
