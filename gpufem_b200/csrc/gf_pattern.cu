@@ -151,8 +151,18 @@ __device__ __forceinline__ void sort_net(int (&a)[N]) {
 // element-node slots are sorted as keys node id * NK + slot in registers, so equal
 // neighbours are adjacent and each slot's rank falls out of one pass.  The same quantities
 // as k_node_adjacency + k_incidence_finish + k_diagpos, without their searches.
+// Threads per block of k_node_pattern (64 keys: more registers per thread) and the
+// shared staging per warp (the warp's incidence slots and candidate lists, stored to HBM
+// as one contiguous run each instead of scattered 2- and 4-byte stores).
+template <int NK>
+constexpr int node_pattern_threads() { return NK == 32 ? 256 : 128; }
 template <int NEN, int NK>
-__global__ void __launch_bounds__(256)
+constexpr size_t node_pattern_smem() {
+  return (size_t)(node_pattern_threads<NK>() / 32) * 32 * NK * (sizeof(uint16_t) + sizeof(int32_t));
+}
+
+template <int NEN, int NK>
+__global__ void __launch_bounds__(node_pattern_threads<NK>())
 k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __restrict__ inc_off,
                int32_t* __restrict__ inc, int32_t* __restrict__ nadj,
                int32_t* __restrict__ adj_tmp, uint8_t* __restrict__ inc_loc,
@@ -160,9 +170,19 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
   constexpr int MAXD = NK / NEN;   // incident elements per node (checked by the caller)
   constexpr int SH = NK == 32 ? 5 : 6;
   constexpr int kEmpty = 0x7fffffff;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node >= nnodes) return;
-  const int e0 = inc_off[node], deg = inc_off[node + 1] - e0;
+  const int wnode0 = node - lane;
+  if (wnode0 >= nnodes) return;   // whole warp
+  const bool valid = node < nnodes;
+  int32_t* sadj = reinterpret_cast<int32_t*>(smem_raw) + (size_t)wib * 32 * NK;
+  uint16_t* sslot = reinterpret_cast<uint16_t*>(reinterpret_cast<int32_t*>(smem_raw) +
+                                                (size_t)(blockDim.x / 32) * 32 * NK) +
+                    (size_t)wib * 32 * NK;
+  const int E0 = inc_off[wnode0], E1 = inc_off[min(wnode0 + 32, nnodes)];
+  const int e0 = valid ? inc_off[node] : E1;
+  const int deg = valid ? inc_off[node + 1] - e0 : 0;
   int el[MAXD];
 #pragma unroll
   for (int q = 0; q < MAXD; ++q) el[q] = q < deg ? inc[e0 + q] : kEmpty;
@@ -185,6 +205,7 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
   }
   sort_net<NK>(key);
   int rank = -1, prev = -1;
+  const int l0 = (e0 - E0) * NEN;   // this node's place in the warp's staging
 #pragma unroll
   for (int k = 0; k < NK; ++k) {
     const int kk = key[k];
@@ -192,19 +213,36 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
       const int v = kk >> SH, slot = kk & (NK - 1);
       if (v != prev) {
         ++rank;
-        adj_tmp[(int64_t)e0 * NEN + rank] = v;
+        sadj[l0 + rank] = v;
         prev = v;
       }
-      const int q = slot / NEN, j = slot - q * NEN;
-      inc_slot[(int64_t)(e0 + q) * NEN + j] = (uint16_t)rank;
+      sslot[l0 + slot] = (uint16_t)rank;   // slot = q * NEN + j
       if (v == node) {
-        inc_loc[e0 + q] = (uint8_t)j;
+        inc_loc[e0 + slot / NEN] = (uint8_t)(slot % NEN);
         diagpos[node] = rank;
       }
     }
   }
-  nadj[node] = rank + 1;
-  if (deg == 0) diagpos[node] = 0;
+  if (valid) {
+    nadj[node] = rank + 1;
+    if (deg == 0) diagpos[node] = 0;
+  }
+  __syncwarp();
+  // the warp's runs, 16 bytes per store: NEN slots of an incidence are 16 (NEN = 8) or 8
+  // bytes, its NEN list entries 32 or 16 bytes, and E0 * NEN keeps both aligned
+  const int R = (E1 - E0) * NEN;
+  if constexpr (NEN == 8) {
+    const uint4* src = reinterpret_cast<const uint4*>(sslot);
+    uint4* dst = reinterpret_cast<uint4*>(inc_slot + (int64_t)E0 * NEN);
+    for (int i = lane; i < R / 8; i += 32) dst[i] = src[i];
+  } else {
+    const uint2* src = reinterpret_cast<const uint2*>(sslot);
+    uint2* dst = reinterpret_cast<uint2*>(inc_slot + (int64_t)E0 * NEN);
+    for (int i = lane; i < R / 4; i += 32) dst[i] = src[i];
+  }
+  const int4* asrc = reinterpret_cast<const int4*>(sadj);
+  int4* adst = reinterpret_cast<int4*>(adj_tmp + (int64_t)E0 * NEN);
+  for (int i = lane; i < R / 4; i += 32) adst[i] = asrc[i];
 }
 
 // Warp per node, for meshes whose nodes see at most 32 elements and 256 element-node slots
@@ -306,8 +344,9 @@ __global__ void k_rows_from_lists(int n, int W, int nen, const int32_t* __restri
   const int len = nadj[node] * DIM;
   const int32_t* list = adj_tmp + (int64_t)inc_off[node] * nen;
   rownnz[row] = len;
-  // a neighbour at a time (W is a multiple of DIM): one list read per DIM slots
-#pragma unroll 2
+  // a neighbour at a time (W is a multiple of DIM): one list read per DIM slots, several
+  // reads in flight
+#pragma unroll 8
   for (int k = 0; k < W / DIM; ++k) {
     const bool in = k * DIM < len;
     const int b = in ? __ldg(list + k) * DIM : 0;
@@ -519,9 +558,15 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
     if (thread_pass) {
       auto kp = nen == 4 ? (nkeys == 32 ? k_node_pattern<4, 32> : k_node_pattern<4, 64>)
                          : (nkeys == 32 ? k_node_pattern<8, 32> : k_node_pattern<8, 64>);
-      kp<<<gf_blocks(nnodes, 256), 256, 0, s>>>(nnodes, ctx->d_conn, d_inc_off, d_inc, d_nadj,
-                                                 d_adjtmp, ctx->d_inc_loc, ctx->d_inc_slot,
-                                                 ctx->d_diagpos);
+      const int nt = nkeys == 32 ? node_pattern_threads<32>() : node_pattern_threads<64>();
+      const size_t sm = nen == 4 ? (nkeys == 32 ? node_pattern_smem<4, 32>()
+                                                : node_pattern_smem<4, 64>())
+                                 : (nkeys == 32 ? node_pattern_smem<8, 32>()
+                                                : node_pattern_smem<8, 64>());
+      GF_TRYC(gf_smem_attr(kp, sm));
+      kp<<<gf_blocks(nnodes, nt), nt, sm, s>>>(nnodes, ctx->d_conn, d_inc_off, d_inc, d_nadj,
+                                               d_adjtmp, ctx->d_inc_loc, ctx->d_inc_slot,
+                                               ctx->d_diagpos);
     } else {
       k_node_pattern_warp<<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
           nnodes, nen, ctx->d_conn, d_inc_off, d_inc, d_nadj, d_adjtmp, ctx->d_inc_loc,
