@@ -330,50 +330,68 @@ k_node_pattern_warp(int nnodes, int nen, const int32_t* __restrict__ conn,
   if (lane == 0 && C == 0) diagpos[node] = 0;
 }
 
-// Thread per row after k_node_pattern: rownnz and the row's columns from the node's sorted
-// list in adj_tmp (slots past the row's length hold col = row; all threads walk the
-// slots together, so each slot's column of colidx is written by consecutive threads).
-template <int DIM>
-__global__ void k_rows_from_lists(int n, int W, int nen, const int32_t* __restrict__ inc_off,
-                                  const int32_t* __restrict__ nadj,
-                                  const int32_t* __restrict__ adj_tmp,
-                                  int32_t* __restrict__ rownnz, int32_t* __restrict__ colidx) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n) return;
-  const int node = row / DIM;
-  const int len = nadj[node] * DIM;
-  const int32_t* list = adj_tmp + (int64_t)inc_off[node] * nen;
-  rownnz[row] = len;
-  // a neighbour at a time (W is a multiple of DIM): one list read per DIM slots, several
-  // reads in flight
-#pragma unroll 8
-  for (int k = 0; k < W / DIM; ++k) {
-    const bool in = k * DIM < len;
-    const int b = in ? __ldg(list + k) * DIM : 0;
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) colidx[(int64_t)(k * DIM + c) * n + row] = in ? b + c : row;
-  }
-}
+// Block per NB consecutive nodes after the pattern pass: their sorted lists lie in one
+// contiguous run of adj_tmp (each node's at its incidence offset x nen), which the block
+// stages in shared memory with 16-byte loads and writes out three ways: the compact
+// adjacency (flat over the block's output range, so every store coalesces), rownnz, and
+// the column-major colidx rows (a thread per row; all threads walk the slots together, so
+// each slot's column of colidx is written by consecutive threads; slots past the row's
+// length hold col = row).  One read of the lists instead of one per output.
+constexpr int kListsThreadsMax = 512;
 
-// Warp per 32 consecutive nodes: their sorted lists from adj_tmp into adj, one node at a
-// time (lane k copies entry k), so the stores into each list coalesce.
-__global__ void k_adj_fill(int nnodes, int nen, const int32_t* __restrict__ inc_off,
-                           const int32_t* __restrict__ nadj, const int32_t* __restrict__ adj_off,
-                           const int32_t* __restrict__ adj_tmp, int32_t* __restrict__ adj) {
-  constexpr unsigned kFull = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
-  if (base >= nnodes) return;   // whole warp
-  const int mine = base + lane;
-  const int m = mine < nnodes ? nadj[mine] : 0;
-  const int64_t src = mine < nnodes ? (int64_t)inc_off[mine] * nen : 0;
-  const int dst = mine < nnodes ? adj_off[mine] : 0;
+__host__ __device__ constexpr int lists_table_ints(int NB) { return (2 * (NB + 1) + 3) & ~3; }
+
+template <int DIM>
+__global__ void __launch_bounds__(kListsThreadsMax)
+k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict__ inc_off,
+            const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj_tmp,
+            int32_t* __restrict__ adj, int32_t* __restrict__ rownnz,
+            int32_t* __restrict__ colidx) {
+  extern __shared__ __align__(16) int32_t lsm[];
+  int32_t* sbase = lsm;             // NB + 1: each node's list start in the staging run
+  int32_t* soff = lsm + NB + 1;     // NB + 1: adj_off of the block's nodes
+  int32_t* stage = lsm + lists_table_ints(NB);
+  const int n0 = blockIdx.x * NB;
+  const int nb = min(NB, nnodes - n0);
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const int I0 = __ldg(inc_off + n0);
+  for (int j = tid; j <= nb; j += bd) {
+    sbase[j] = (__ldg(inc_off + n0 + j) - I0) * nen;
+    soff[j] = __ldg(adj_off + n0 + j);
+  }
+  const int64_t S0 = (int64_t)I0 * nen;
+  const int cnt = (__ldg(inc_off + n0 + nb) - I0) * nen;
+  if ((nen & 3) == 0) {   // S0 and cnt are multiples of 4: the run is 16-byte aligned
+    const int4* src = reinterpret_cast<const int4*>(adj_tmp + S0);
+    int4* dst = reinterpret_cast<int4*>(stage);
+    for (int i = tid; i < cnt / 4; i += bd) dst[i] = __ldg(src + i);
+  } else {
+    for (int i = tid; i < cnt; i += bd) stage[i] = __ldg(adj_tmp + S0 + i);
+  }
+  __syncthreads();
+  // compact adjacency: output word p of the block belongs to the last node j with
+  // soff[j] <= soff[0] + p
+  const int A0 = soff[0], A = soff[nb] - A0;
+  for (int p = tid; p < A; p += bd) {
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (soff[mid] - A0 <= p) lo = mid; else hi = mid - 1;
+    }
+    adj[A0 + p] = stage[sbase[lo] + (A0 + p - soff[lo])];
+  }
+  for (int r = tid; r < nb * DIM; r += bd) {
+    const int j = r / DIM, row = n0 * DIM + r;
+    const int m = soff[j + 1] - soff[j];
+    const int32_t* list = stage + sbase[j];
+    rownnz[row] = m * DIM;
 #pragma unroll 4
-  for (int i = 0; i < 32; ++i) {
-    const int mi = __shfl_sync(kFull, m, i);
-    const int64_t si = __shfl_sync(kFull, src, i);
-    const int di = __shfl_sync(kFull, dst, i);
-    for (int k = lane; k < mi; k += 32) adj[di + k] = __ldg(adj_tmp + si + k);
+    for (int k = 0; k < W / DIM; ++k) {
+      const bool in = k < m;
+      const int b = in ? list[k] * DIM : 0;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) colidx[(int64_t)(k * DIM + c) * n + row] = in ? b + c : row;
+    }
   }
 }
 
@@ -604,15 +622,19 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   GF_TRY(gf_palloc(ctx, &ctx->d_rownnz, (size_t)n));
   GF_TRY(gf_palloc(ctx, &ctx->d_colidx, (size_t)slots));
   if (fused) {
-    k_adj_fill<<<gf_blocks((nnodes + 31) / 32, 8), 256, 0, s>>>(
-        nnodes, nen, d_inc_off, d_nadj, ctx->d_adj_off, d_adjtmp, ctx->d_adj);
-    if (dim == 2)
-      k_rows_from_lists<2><<<gf_blocks(n, 256), 256, 0, s>>>(
-          n, ctx->W, nen, d_inc_off, d_nadj, d_adjtmp, ctx->d_rownnz, ctx->d_colidx);
-    else
-      k_rows_from_lists<3><<<gf_blocks(n, 256), 256, 0, s>>>(
-          n, ctx->W, nen, d_inc_off, d_nadj, d_adjtmp, ctx->d_rownnz, ctx->d_colidx);
-    ctx->launches += 2;
+    // nodes per block: the staged lists (at most maxval * nen words per node) within 48 KB
+    const int per_node = h_maxval * nen;
+    int NB = 128;
+    while (NB > 32 && (size_t)NB * per_node * sizeof(int32_t) > 48 * 1024) NB >>= 1;
+    const size_t lsm = sizeof(int32_t) * ((size_t)lists_table_ints(NB) + (size_t)NB * per_node);
+    const int nt = std::min(kListsThreadsMax, (NB * dim + 31) / 32 * 32);
+    const int nblk = (nnodes + NB - 1) / NB;
+    auto kl = dim == 2 ? k_lists_out<2> : k_lists_out<3>;
+    GF_TRYC(gf_smem_attr(kl, lsm));
+    if (nblk > 0)
+      kl<<<nblk, nt, lsm, s>>>(nnodes, NB, n, ctx->W, nen, d_inc_off, ctx->d_adj_off, d_adjtmp,
+                               ctx->d_adj, ctx->d_rownnz, ctx->d_colidx);
+    ctx->launches++;
   } else {
     GF_TRY(gf_palloc(ctx, &ctx->d_diagpos, (size_t)nnodes));
     k_node_adjacency<1><<<ablocks, 32 * kWarpsPerBlock, 0, s>>>(
