@@ -245,14 +245,114 @@ k_node_pattern(int nnodes, const int32_t* __restrict__ conn, const int32_t* __re
   for (int i = lane; i < R / 4; i += 32) adst[i] = asrc[i];
 }
 
+// Ascending bitonic sort of 32 K keys held by a warp in blocked order (key[r] of lane l is
+// element l K + r): stages with a stride below K swap inside a lane, wider stages exchange
+// with lane l ^ (stride / K) by shuffles.  Every loop is unrolled, so the keys stay in
+// registers.
+template <int K>
+__device__ __forceinline__ void warp_sort(int (&key)[K], int lane) {
+  constexpr unsigned kFull = 0xffffffffu;
+#pragma unroll
+  for (int k = 2; k <= 32 * K; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= K) {
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+          const int i = lane * K + r;
+          const int o = __shfl_xor_sync(kFull, key[r], j / K);
+          key[r] = (((i & j) == 0) == ((i & k) == 0)) ? min(key[r], o) : max(key[r], o);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+          if ((r & j) == 0) {
+            const bool up = ((lane * K + r) & k) == 0;
+            const int x = key[r], y = key[r + j];
+            key[r] = up ? min(x, y) : max(x, y);
+            key[r + j] = up ? max(x, y) : min(x, y);
+          }
+      }
+    }
+}
+
 // Warp per node, for meshes whose nodes see at most 32 elements and 256 element-node slots
 // (Brick20: 8 x 20 = 160) and fewer than 2^23 nodes: the same outputs as k_node_pattern.
 // The incident elements are sorted across the lanes by a shuffle bitonic network; the
-// element-node slots, as keys node id * 256 + slot, by a bitonic network in the warp's
-// shared-memory row over the next power of two above their count; each lane then ranks
-// a run of the sorted keys, with the distinct counts of the lanes before it from a
-// shuffle scan.
+// element-node slots, as keys node id * 256 + slot, by a register bitonic network over the
+// warp (K = 2, 4 or 8 keys per lane: the next power of two above the node's slot count);
+// each lane then ranks its run of sorted keys, with the distinct counts of the lanes before
+// it from a shuffle scan.  The sorted list and the slots' ranks are staged in shared memory
+// and stored as contiguous runs.
 constexpr int kWarpKeys = 256;
+
+template <int K>
+__device__ __forceinline__ void warp_node_keys(int node, int nen, int C, int el, int lane,
+                                               int e0, const int32_t* __restrict__ conn,
+                                               int32_t* sadj, uint16_t* sslot,
+                                               int32_t* __restrict__ nadj,
+                                               int32_t* __restrict__ adj_tmp,
+                                               uint8_t* __restrict__ inc_loc,
+                                               uint16_t* __restrict__ inc_slot,
+                                               int32_t* __restrict__ diagpos) {
+  constexpr unsigned kFull = 0xffffffffu;
+  constexpr int kEmpty = 0x7fffffff;
+  int key[K];
+  // slot lane K + r is local node j of incident element q (q, j stepped, not divided)
+  int q = (lane * K) / nen, j = lane * K - q * nen;
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    const int sl = lane * K + r;
+    const int eq = __shfl_sync(kFull, el, min(q, 31));
+    key[r] = sl < C ? (__ldg(conn + (int64_t)eq * nen + j) << 8) | sl : kEmpty;
+    if (++j == nen) { j = 0; ++q; }
+  }
+  warp_sort<K>(key, lane);
+  const int last = __shfl_up_sync(kFull, key[K - 1], 1);
+  const int pv0 = lane == 0 ? -1 : last >> 8;
+  int cnt = 0, pv = pv0;
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    const int kk = key[r];
+    if (kk != kEmpty && (kk >> 8) != pv) ++cnt;
+    pv = kk >> 8;
+  }
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  int rank = incl - cnt - 1;
+  pv = pv0;
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    const int kk = key[r];
+    if (kk != kEmpty) {
+      const int v = kk >> 8, slot = kk & 255;
+      if (v != pv) {
+        ++rank;
+        sadj[rank] = v;
+      }
+      sslot[slot] = (uint16_t)rank;
+      if (v == node) {
+        const int qq = slot / nen;
+        inc_loc[e0 + qq] = (uint8_t)(slot - qq * nen);
+        diagpos[node] = rank;
+      }
+    }
+    pv = kk >> 8;
+  }
+  const int D = __shfl_sync(kFull, incl, 31);
+  if (lane == 0) {
+    nadj[node] = D;
+    if (C == 0) diagpos[node] = 0;
+  }
+  __syncwarp();
+  const int64_t o0 = (int64_t)e0 * nen;
+  for (int i = lane; i < D; i += 32) adj_tmp[o0 + i] = sadj[i];
+  for (int i = lane; i < C; i += 32) inc_slot[o0 + i] = sslot[i];
+}
 
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
 k_node_pattern_warp(int nnodes, int nen, const int32_t* __restrict__ conn,
@@ -262,11 +362,11 @@ k_node_pattern_warp(int nnodes, int nen, const int32_t* __restrict__ conn,
                     int32_t* __restrict__ diagpos) {
   constexpr unsigned kFull = 0xffffffffu;
   constexpr int kEmpty = 0x7fffffff;
-  __shared__ int skeys[kWarpsPerBlock][kWarpKeys];
+  __shared__ int32_t sadj[kWarpsPerBlock][kWarpKeys];
+  __shared__ uint16_t sslot[kWarpsPerBlock][kWarpKeys];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int node = blockIdx.x * kWarpsPerBlock + warp;
   if (node >= nnodes) return;   // whole warp
-  int* keys = skeys[warp];
   const int e0 = inc_off[node], deg = inc_off[node + 1] - e0;   // deg <= 32
   const int C = deg * nen;                                        // <= 256
   int el = lane < deg ? inc[e0 + lane] : kEmpty;
@@ -278,65 +378,25 @@ k_node_pattern_warp(int nnodes, int nen, const int32_t* __restrict__ conn,
       el = (((lane & j) == 0) == ((lane & k) == 0)) ? min(el, o) : max(el, o);
     }
   if (lane < deg) inc[e0 + lane] = el;   // lane q holds the element of rank q
-  int NP = 32;
-  while (NP < C) NP <<= 1;
-  for (int sl = lane; sl < NP; sl += 32) {
-    const int q = min(sl / nen, 31);
-    const int eq = __shfl_sync(kFull, el, q);
-    keys[sl] = sl < C ? (conn[(int64_t)eq * nen + (sl - q * nen)] << 8) | sl : kEmpty;
-  }
-  __syncwarp();
-  for (int k = 2; k <= NP; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int pr = lane; pr < NP / 2; pr += 32) {
-        const int i = 2 * j * (pr / j) + (pr % j), l = i + j;
-        const int x = keys[i], y = keys[l];
-        if ((x > y) == ((i & k) == 0)) {
-          keys[i] = y;
-          keys[l] = x;
-        }
-      }
-      __syncwarp();
-    }
-  const int per = NP / 32, b0 = lane * per;
-  int cnt = 0;
-  for (int m = 0; m < per; ++m) {
-    const int kk = keys[b0 + m];
-    if (kk != kEmpty && (b0 + m == 0 || (keys[b0 + m - 1] >> 8) != (kk >> 8))) ++cnt;
-  }
-  int incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += t;
-  }
-  int rank = incl - cnt - 1;
-  for (int m = 0; m < per; ++m) {
-    const int pos = b0 + m, kk = keys[pos];
-    if (kk == kEmpty) break;
-    const int v = kk >> 8, slot = kk & 255;
-    if (pos == 0 || (keys[pos - 1] >> 8) != v) {
-      ++rank;
-      adj_tmp[(int64_t)e0 * nen + rank] = v;
-    }
-    const int q = slot / nen, j = slot - q * nen;
-    inc_slot[(int64_t)(e0 + q) * nen + j] = (uint16_t)rank;
-    if (v == node) {
-      inc_loc[e0 + q] = (uint8_t)j;
-      diagpos[node] = rank;
-    }
-  }
-  if (lane == 31) nadj[node] = incl;
-  if (lane == 0 && C == 0) diagpos[node] = 0;
+  // warp-uniform choice of the key count
+  if (C <= 64)
+    warp_node_keys<2>(node, nen, C, el, lane, e0, conn, sadj[warp], sslot[warp], nadj, adj_tmp,
+                      inc_loc, inc_slot, diagpos);
+  else if (C <= 128)
+    warp_node_keys<4>(node, nen, C, el, lane, e0, conn, sadj[warp], sslot[warp], nadj, adj_tmp,
+                      inc_loc, inc_slot, diagpos);
+  else
+    warp_node_keys<8>(node, nen, C, el, lane, e0, conn, sadj[warp], sslot[warp], nadj, adj_tmp,
+                      inc_loc, inc_slot, diagpos);
 }
 
-// Block per NB consecutive nodes after the pattern pass: their sorted lists lie in one
-// contiguous run of adj_tmp (each node's at its incidence offset x nen), which the block
-// stages in shared memory with 16-byte loads and writes out three ways: the compact
-// adjacency (flat over the block's output range, so every store coalesces), rownnz, and
-// the column-major colidx rows (a thread per row; all threads walk the slots together, so
-// each slot's column of colidx is written by consecutive threads; slots past the row's
-// length hold col = row).  One read of the lists instead of one per output.
+// Block per NB consecutive nodes after the pattern pass: the block's part of the compact
+// adjacency (adj_off[n0] .. adj_off[n0 + NB]) is gathered from the nodes' sorted lists in
+// adj_tmp (each node's at its incidence offset x nen) by a flat loop over the output range,
+// so every store coalesces, and kept in shared memory; rownnz and the column-major colidx
+// rows (a thread per row; all threads walk the slots together, so each slot's column of
+// colidx is written by consecutive threads; slots past the row's length hold col = row)
+// are then written from there.  One read of the lists instead of one per output.
 constexpr int kListsThreadsMax = 512;
 
 __host__ __device__ constexpr int lists_table_ints(int NB) { return (2 * (NB + 1) + 3) & ~3; }
@@ -348,9 +408,9 @@ k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict
             int32_t* __restrict__ adj, int32_t* __restrict__ rownnz,
             int32_t* __restrict__ colidx) {
   extern __shared__ __align__(16) int32_t lsm[];
-  int32_t* sbase = lsm;             // NB + 1: each node's list start in the staging run
+  int32_t* sbase = lsm;             // NB + 1: each node's list start in adj_tmp, from S0
   int32_t* soff = lsm + NB + 1;     // NB + 1: adj_off of the block's nodes
-  int32_t* stage = lsm + lists_table_ints(NB);
+  int32_t* stage = lsm + lists_table_ints(NB);   // the block's compact adjacency
   const int n0 = blockIdx.x * NB;
   const int nb = min(NB, nnodes - n0);
   const int tid = threadIdx.x, bd = blockDim.x;
@@ -359,18 +419,9 @@ k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict
     sbase[j] = (__ldg(inc_off + n0 + j) - I0) * nen;
     soff[j] = __ldg(adj_off + n0 + j);
   }
-  const int64_t S0 = (int64_t)I0 * nen;
-  const int cnt = (__ldg(inc_off + n0 + nb) - I0) * nen;
-  if ((nen & 3) == 0) {   // S0 and cnt are multiples of 4: the run is 16-byte aligned
-    const int4* src = reinterpret_cast<const int4*>(adj_tmp + S0);
-    int4* dst = reinterpret_cast<int4*>(stage);
-    for (int i = tid; i < cnt / 4; i += bd) dst[i] = __ldg(src + i);
-  } else {
-    for (int i = tid; i < cnt; i += bd) stage[i] = __ldg(adj_tmp + S0 + i);
-  }
   __syncthreads();
-  // compact adjacency: output word p of the block belongs to the last node j with
-  // soff[j] <= soff[0] + p
+  const int32_t* src = adj_tmp + (int64_t)I0 * nen;
+  // output word p of the block belongs to the last node j with soff[j] <= soff[0] + p
   const int A0 = soff[0], A = soff[nb] - A0;
   for (int p = tid; p < A; p += bd) {
     int lo = 0, hi = nb - 1;
@@ -378,12 +429,15 @@ k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict
       const int mid = (lo + hi + 1) >> 1;
       if (soff[mid] - A0 <= p) lo = mid; else hi = mid - 1;
     }
-    adj[A0 + p] = stage[sbase[lo] + (A0 + p - soff[lo])];
+    const int v = __ldg(src + sbase[lo] + (A0 + p - soff[lo]));
+    adj[A0 + p] = v;
+    stage[p] = v;
   }
+  __syncthreads();
   for (int r = tid; r < nb * DIM; r += bd) {
     const int j = r / DIM, row = n0 * DIM + r;
     const int m = soff[j + 1] - soff[j];
-    const int32_t* list = stage + sbase[j];
+    const int32_t* list = stage + (soff[j] - A0);
     rownnz[row] = m * DIM;
 #pragma unroll 4
     for (int k = 0; k < W / DIM; ++k) {
@@ -622,8 +676,8 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   GF_TRY(gf_palloc(ctx, &ctx->d_rownnz, (size_t)n));
   GF_TRY(gf_palloc(ctx, &ctx->d_colidx, (size_t)slots));
   if (fused) {
-    // nodes per block: the staged lists (at most maxval * nen words per node) within 48 KB
-    const int per_node = h_maxval * nen;
+    // nodes per block: the staged lists (at most h_max words per node) within 48 KB
+    const int per_node = h_max;
     int NB = 128;
     while (NB > 32 && (size_t)NB * per_node * sizeof(int32_t) > 48 * 1024) NB >>= 1;
     const size_t lsm = sizeof(int32_t) * ((size_t)lists_table_ints(NB) + (size_t)NB * per_node);
