@@ -114,25 +114,34 @@ __global__ void k_bsell_col(int n, int nnodes, int dim, int nslots, const int64_
         p < nadj ? colidx[(int64_t)(p * dim) * n + (int64_t)node * dim] / dim : node;
 }
 
-// thread per (component c, node slot): c = t / nslots, so the node slots of one c coalesce
-template <typename TI, typename TO>
-__global__ void k_bsell_val(int n, int nnodes, int dim, int nslots, const int64_t* __restrict__ off,
+// Thread per node slot: per neighbour p and column component c2, the node's DIM rows of
+// that ELL column are DIM consecutive entries (one or two sectors, read once), and each of
+// the DIM x DIM values goes to its slice word, so a warp's stores coalesce.  Slots of one
+// block are one degree-sorting window (256 consecutive nodes), so the sectors that several
+// nodes of the window share are read from L1.
+template <typename TI, typename TO, int DIM>
+__global__ void k_bsell_val(int n, int nnodes, int nslots, const int64_t* __restrict__ off,
                             const int32_t* __restrict__ width, const int32_t* __restrict__ rownnz,
                             const int32_t* __restrict__ perm, const TI* __restrict__ K,
                             TO* __restrict__ val) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= (int64_t)nslots * dim) return;
-  const int c = (int)(t / nslots), a = (int)(t % nslots);
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= nslots) return;
   const int k = a >> 5, l = a & 31;
   const int w = width[k];
   const int node = a < nnodes ? perm[a] : 0;
-  const int nadj = a < nnodes ? rownnz[(int64_t)node * dim] / dim : 0;
-  const int64_t base = off[k] * dim * dim + (int64_t)c * dim * 32 + l;
-  const int64_t row = (int64_t)node * dim + c;
-  for (int p = 0; p < w; ++p)
-    for (int c2 = 0; c2 < dim; ++c2)
-      val[base + (int64_t)(p * dim * dim + c2) * 32] =
-          p < nadj ? (TO)K[(int64_t)(p * dim + c2) * n + row] : (TO)0;
+  const int nadj = a < nnodes ? rownnz[(int64_t)node * DIM] / DIM : 0;
+  TO* dst = val + off[k] * DIM * DIM + l;
+  const int64_t row = (int64_t)node * DIM;
+  for (int p = 0; p < w; ++p) {
+    const bool in = p < nadj;
+#pragma unroll
+    for (int c2 = 0; c2 < DIM; ++c2) {
+      const TI* src = K + (int64_t)(p * DIM + c2) * n + row;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+        dst[(int64_t)((p * DIM + c) * DIM + c2) * 32] = in ? (TO)__ldg(src + c) : (TO)0;
+    }
+  }
 }
 
 }  // namespace
@@ -223,9 +232,10 @@ gf_status gf_sell_prepare(gf_ctx* ctx, int dtype) {
   if (dtype == GF_F64 && ctx->sell_ver64 != ctx->kver64) {
     if (!ctx->d_sell_v64 && (st = gf_alloc(ctx, &ctx->d_sell_v64, total)) != GF_OK) return st;
     if (bdim)
-      k_bsell_val<double, double><<<gf_blocks((int64_t)nslots * bdim, 256), 256, 0, s>>>(
-          n, ctx->nnodes, bdim, nslots, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz,
-          ctx->d_sell_perm, ctx->d_K64, ctx->d_sell_v64);
+      (bdim == 2 ? k_bsell_val<double, double, 2> : k_bsell_val<double, double, 3>)
+          <<<gf_blocks(nslots, kWin), kWin, 0, s>>>(n, ctx->nnodes, nslots, ctx->d_sell_off,
+                                                   ctx->d_sell_w, ctx->d_rownnz,
+                                                   ctx->d_sell_perm, ctx->d_K64, ctx->d_sell_v64);
     else
       k_sell_fill<double, double><<<gf_blocks(nslots, 256), 256, 0, s>>>(
           n, nslots, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz, ctx->d_K64,
@@ -236,9 +246,10 @@ gf_status gf_sell_prepare(gf_ctx* ctx, int dtype) {
   if (dtype == GF_F32 && ctx->sell_ver32 != ctx->kver32) {
     if (!ctx->d_sell_v32 && (st = gf_alloc(ctx, &ctx->d_sell_v32, total)) != GF_OK) return st;
     if (bdim)
-      k_bsell_val<float, float><<<gf_blocks((int64_t)nslots * bdim, 256), 256, 0, s>>>(
-          n, ctx->nnodes, bdim, nslots, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz,
-          ctx->d_sell_perm, ctx->d_K32, ctx->d_sell_v32);
+      (bdim == 2 ? k_bsell_val<float, float, 2> : k_bsell_val<float, float, 3>)
+          <<<gf_blocks(nslots, kWin), kWin, 0, s>>>(n, ctx->nnodes, nslots, ctx->d_sell_off,
+                                                   ctx->d_sell_w, ctx->d_rownnz,
+                                                   ctx->d_sell_perm, ctx->d_K32, ctx->d_sell_v32);
     else
       k_sell_fill<float, float><<<gf_blocks(nslots, 256), 256, 0, s>>>(
           n, nslots, ctx->d_sell_off, ctx->d_sell_w, ctx->d_rownnz, ctx->d_K32,

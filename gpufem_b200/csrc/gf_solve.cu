@@ -485,17 +485,23 @@ __global__ void k_penalty(int nblocks, const double* __restrict__ blockmax, int 
   }
 }
 
-template <typename T>
-__global__ void k_eliminate(int n, int W, const int32_t* __restrict__ rownnz,
+// Elimination of constrained dofs on both value arrays at once (either may be null): a
+// thread per row walks its slots, so each slot's column words and values are read by
+// consecutive threads; rows of fixed dofs become unit rows, columns of fixed dofs zero.
+__global__ void k_eliminate(int n, const int32_t* __restrict__ rownnz,
                             const int32_t* __restrict__ col, const uint8_t* __restrict__ fixed,
-                            T* __restrict__ K) {
-  const int64_t total = (int64_t)n * W;
-  for (int64_t i = blockIdx.x * (int64_t)kT + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * kT) {
-    const int row = (int)(i % n), slot = (int)(i / n);
-    if (slot >= rownnz[row]) continue;
-    const int c = col[i];
-    if (fixed[row] || fixed[c]) K[i] = (c == row) ? T(1) : T(0);
+                            double* __restrict__ K64, float* __restrict__ K32) {
+  for (int row = blockIdx.x * kT + threadIdx.x; row < n; row += gridDim.x * kT) {
+    const int nz = rownnz[row];
+    const bool frow = fixed[row];
+    for (int s = 0; s < nz; ++s) {
+      const int64_t i = (int64_t)s * n + row;
+      const int c = col[i];
+      if (frow || fixed[c]) {
+        if (K64) K64[i] = c == row ? 1.0 : 0.0;
+        if (K32) K32[i] = c == row ? 1.f : 0.f;
+      }
+    }
   }
 }
 
@@ -607,17 +613,10 @@ gf_status gf_constraints_apply(gf_ctx* ctx, int mode) {
     cudaFree(d_bmax);
     if (e != cudaSuccess) return gf_cuda_fail(ctx, e, "penalty");
   } else {
-    const int nb = ctx->sm_count * 8;
-    if (ctx->has64) {
-      k_eliminate<double><<<nb, kT, 0, ctx->stream>>>(n, ctx->W, ctx->d_rownnz, ctx->d_colidx,
-                                                      ctx->d_fixed, ctx->d_K64);
-      ctx->launches++;
-    }
-    if (ctx->has32) {
-      k_eliminate<float><<<nb, kT, 0, ctx->stream>>>(n, ctx->W, ctx->d_rownnz, ctx->d_colidx,
-                                                     ctx->d_fixed, ctx->d_K32);
-      ctx->launches++;
-    }
+    k_eliminate<<<gf_blocks(n, kT), kT, 0, ctx->stream>>>(
+        n, ctx->d_rownnz, ctx->d_colidx, ctx->d_fixed, ctx->has64 ? ctx->d_K64 : nullptr,
+        ctx->has32 ? ctx->d_K32 : nullptr);
+    ctx->launches++;
     k_zero_fixed<<<gf_blocks(n, kT), kT, 0, ctx->stream>>>(n, ctx->d_fixed, ctx->d_f);
     ctx->launches++;
     GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

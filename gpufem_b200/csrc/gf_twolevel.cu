@@ -312,6 +312,174 @@ k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
   }
 }
 
+// The same sums with a warp per node (mesh-built patterns, whose ELL slot p of node a's
+// rows is entry p of a's sorted adjacency list): the lanes take a's neighbours 32 at a
+// time, so the list reads coalesce and every lane has its own K loads in flight.  Lane
+// sums S_b = K_ab P_b for B = A accumulate over the node's neighbours and are reduced once
+// per node; other aggregates (nodes near box faces) are reduced per distinct B among the
+// lanes.  Lane 0 forms P_a^T S and adds it to its warp's (A, A) partial or to the block's
+// table.  Each block takes kCW * per consecutive nodes of A's list, warps interleaved.
+constexpr int kCW = 4;  // warps per block
+
+// Entry (c, m) of the P row of a dof with scaled offset d (the entries of p_row one at a
+// time; with c and m compile-time constants it folds to 0, 1 or +-d).
+template <int DIM>
+__device__ __forceinline__ double p_entry(int c, int m, const double* d) {
+  if (m < DIM) return m == c ? 1.0 : 0.0;
+  if (DIM == 2) return c == 0 ? -d[1] : d[0];
+  if (m == 3) return c == 1 ? -d[2] : c == 2 ? d[1] : 0.0;
+  if (m == 4) return c == 0 ? d[2] : c == 2 ? -d[0] : 0.0;
+  return c == 0 ? -d[1] : c == 1 ? d[0] : 0.0;
+}
+
+template <int DIM, int NM>
+__device__ __forceinline__ void warp_sum_rows(double (&v)[DIM][NM]) {
+#pragma unroll
+  for (int c = 0; c < DIM; ++c)
+#pragma unroll
+    for (int m = 0; m < NM; ++m)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[c][m] += __shfl_down_sync(0xffffffffu, v[c][m], o);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(32 * kCW)
+k_coarse_rows_warp(int n, const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
+                   const double* __restrict__ K, const uint8_t* __restrict__ fixed,
+                   const int32_t* __restrict__ agg, const int32_t* __restrict__ off,
+                   const int32_t* __restrict__ nodes, const double* __restrict__ x,
+                   const double* __restrict__ cen, double sinv, int nc, int per,
+                   double* __restrict__ Ac) {
+  constexpr unsigned kFull = 0xffffffffu;
+  constexpr int NM = DIM == 2 ? 3 : 6;
+  constexpr int NMM = NM * NM;
+  __shared__ int ids[kTab];
+  __shared__ double tab[kTab][NMM];
+  __shared__ double wacc[kCW][NMM];
+  __shared__ double sbuf[kCW][DIM * NM][32];   // lane sums of other aggregates
+  const int A = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qend = off[A + 1];
+  const int qb = off[A] + blockIdx.y * kCW * per;
+  if (qb >= qend) return;  // block-uniform: this aggregate has fewer chunks
+  for (int i = threadIdx.x; i < kTab; i += blockDim.x) ids[i] = -1;
+  for (int i = threadIdx.x; i < kTab * NMM; i += blockDim.x) (&tab[0][0])[i] = 0.0;
+  for (int i = threadIdx.x; i < kCW * NMM; i += blockDim.x) (&wacc[0][0])[i] = 0.0;
+  __syncthreads();
+  double cA[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) cA[c] = cen[(int64_t)A * DIM + c];
+  // lane 0: T = P_a^T S added to the warp's (A, A) partial or to the table entry of B
+  auto add_block = [&](const double (&S)[DIM][NM], const double (&da)[DIM], int ra, int B) {
+    bool fa[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) fa[c] = fixed[ra + c] != 0;
+    const int sl = B == A ? -1 : tab_slot(ids, B);
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      double pm[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) pm[c] = fa[c] ? 0.0 : p_entry<DIM>(c, m, da);
+#pragma unroll
+      for (int m2 = 0; m2 < NM; ++m2) {
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) v += pm[c] * S[c][m2];
+        if (B == A) wacc[warp][m * NM + m2] += v;
+        else if (v != 0.0) {
+          if (sl >= 0) atomicAdd(&tab[sl][m * NM + m2], v);
+          else atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
+        }
+      }
+    }
+  };
+  for (int t = 0; t < per; ++t) {
+    const int q = qb + t * kCW + warp;
+    if (q >= qend) break;  // warp-uniform
+    const int a = nodes[q];
+    const int ra = a * DIM;
+    double da[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) da[c] = (x[(int64_t)ra + c] - cA[c]) * sinv;
+    const int p0 = adj_off[a], np = adj_off[a + 1] - p0;
+    double Sacc[DIM][NM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c)
+#pragma unroll
+      for (int m = 0; m < NM; ++m) Sacc[c][m] = 0.0;
+    for (int pb = 0; pb < np; pb += 32) {  // warp-uniform trip count
+      const int p = pb + lane;
+      const bool valid = p < np;
+      int B = -1;
+      if (valid) {
+        const int b = adj[p0 + p];
+        B = agg[b];
+        double db[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+          db[c] = (x[(int64_t)b * DIM + c] - cen[(int64_t)B * DIM + c]) * sinv;
+        double Sb[DIM][NM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+          for (int m = 0; m < NM; ++m) Sb[c][m] = 0.0;
+#pragma unroll
+        for (int c2 = 0; c2 < DIM; ++c2) {
+          if (fixed[b * DIM + c2]) continue;
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) {
+            const double kv = __ldg(K + (int64_t)(p * DIM + c2) * n + ra + c);
+#pragma unroll
+            for (int m = 0; m < NM; ++m) Sb[c][m] += kv * p_entry<DIM>(c2, m, db);
+          }
+        }
+        if (B == A) {
+#pragma unroll
+          for (int c = 0; c < DIM; ++c)
+#pragma unroll
+            for (int m = 0; m < NM; ++m) Sacc[c][m] += Sb[c][m];
+        } else {
+#pragma unroll
+          for (int c = 0; c < DIM; ++c)
+#pragma unroll
+            for (int m = 0; m < NM; ++m) sbuf[warp][c * NM + m][lane] = Sb[c][m];
+        }
+      }
+      // neighbours in other aggregates: one warp sum per distinct B among the lanes
+      unsigned rem = __ballot_sync(kFull, valid && B != A);
+      __syncwarp();
+      while (rem) {
+        const int Bl = __shfl_sync(kFull, B, __ffs(rem) - 1);
+        const bool sel = valid && B == Bl;
+        rem &= ~__ballot_sync(kFull, sel);
+        double v[DIM][NM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+          for (int m = 0; m < NM; ++m) v[c][m] = sel ? sbuf[warp][c * NM + m][lane] : 0.0;
+        warp_sum_rows<DIM, NM>(v);
+        if (lane == 0) add_block(v, da, ra, Bl);
+      }
+      __syncwarp();
+    }
+    warp_sum_rows<DIM, NM>(Sacc);
+    if (lane == 0) add_block(Sacc, da, ra, A);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < NMM; e += blockDim.x) {
+    double v = 0.0;
+    for (int w = 0; w < kCW; ++w) v += wacc[w][e];
+    atomicAdd(&Ac[(int64_t)(A * NM + e / NM) * nc + A * NM + e % NM], v);
+  }
+  for (int e = threadIdx.x; e < kTab * NMM; e += blockDim.x) {
+    const int sl = e / NMM, B = ids[sl];
+    if (B < 0) continue;
+    const int m = (e % NMM) / NM, m2 = e % NM;
+    const double v = tab[sl][e % NMM];
+    if (v != 0.0) atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
+  }
+}
+
 __global__ void k_diag_max(int nc, const double* __restrict__ Ac, double* __restrict__ out) {
   __shared__ double sh[kCT];
   double m = 0.0;
@@ -911,14 +1079,28 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   for (int A = 0; A < na; ++A) maxcnt = std::max(maxcnt, hoff[A + 1] - hoff[A]);
   const int per = (int)((maxcnt + (int64_t)kCMT * 65535 - 1) / ((int64_t)kCMT * 65535));
   const dim3 gcm(na, (maxcnt + kCMT * per - 1) / (kCMT * per));
-  if (dim == 2)
+  if (ctx->d_adj && ctx->d_adj_off) {
+    // mesh-built pattern: a warp per node over the node's adjacency list
+    const int pw = (int)((maxcnt + (int64_t)kCW * 65535 - 1) / ((int64_t)kCW * 65535));
+    const int perw = std::max(pw, 8);
+    const dim3 gw(na, (maxcnt + kCW * perw - 1) / (kCW * perw));
+    if (dim == 2)
+      k_coarse_rows_warp<2><<<gw, 32 * kCW, 0, s>>>(
+          n, ctx->d_adj_off, ctx->d_adj, ctx->d_K64, ctx->d_fixed, C->node_agg, C->agg_off,
+          C->agg_nodes, ctx->d_coords64, C->cen, sinv, nc, perw, d_Ac);
+    else
+      k_coarse_rows_warp<3><<<gw, 32 * kCW, 0, s>>>(
+          n, ctx->d_adj_off, ctx->d_adj, ctx->d_K64, ctx->d_fixed, C->node_agg, C->agg_off,
+          C->agg_nodes, ctx->d_coords64, C->cen, sinv, nc, perw, d_Ac);
+  } else if (dim == 2) {
     k_coarse_rows<2><<<gcm, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
                                           ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
                                           ctx->d_coords64, C->cen, sinv, nc, per, d_Ac);
-  else
+  } else {
     k_coarse_rows<3><<<gcm, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
                                           ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
                                           ctx->d_coords64, C->cen, sinv, nc, per, d_Ac);
+  }
   k_diag_max<<<1, kCT, 0, s>>>(nc, d_Ac, d_dmax);
   k_regularise<<<gf_blocks(nc, kCT), kCT, 0, s>>>(nc, d_dmax, 1e-10, d_Ac);
   ctx->launches += 8;
