@@ -312,17 +312,44 @@ k_coarse_rows(int n, const int32_t* __restrict__ rownnz, const int32_t* __restri
   }
 }
 
-// The same sums with a warp per node (mesh-built patterns, whose ELL slot p of node a's
-// rows is entry p of a's sorted adjacency list): the lanes take a's neighbours 32 at a
-// time, so the list reads coalesce and every lane has its own K loads in flight.  Lane
-// sums S_b = K_ab P_b for B = A accumulate over the node's neighbours and are reduced once
-// per node; other aggregates (nodes near box faces) are reduced per distinct B among the
-// lanes.  Lane 0 forms P_a^T S and adds it to its warp's (A, A) partial or to the block's
-// table.  Each block takes kCW * per consecutive nodes of A's list, warps interleaved.
-constexpr int kCW = 4;  // warps per block
+// The same sums over the solver's node-block slices (mesh-built patterns): a thread per
+// node slot walks its slice row like the SpMV, so the neighbour ids and the dim x dim value
+// blocks are read coalesced.  What a neighbour b contributes besides its K block comes from
+// one 32-byte record per node (k_node_records: scaled offset from its aggregate's centroid,
+// aggregate id and fixed-dof bits).  S_b = K_ab P_b accumulates in registers for b in the
+// node's own aggregate A; for other aggregates (nodes near box faces, at most a few) in
+// kSellSlots per-thread shared-memory sums keyed by B, flushed as P_a^T S to Ac at the end
+// (or when a further aggregate needs the slot).  The (A, A) blocks P_a^T S_A are summed over
+// the warp's lanes of equal A by shuffles, one atomic per entry.
+constexpr int kSellThreads = 128;
+constexpr int kSellSlots = 3;
+
+// rec[a] = {d_0, d_1, d_2 (scaled offset from the centroid of a's aggregate; 2-D: d_2 = 0),
+//           agg[a] + 2^24 * (bit c: dof c of a fixed)}
+__global__ void k_node_records(int nnodes, int dim, const double* __restrict__ x,
+                               const int32_t* __restrict__ agg, const double* __restrict__ cen,
+                               const uint8_t* __restrict__ fixed, double sinv,
+                               double4* __restrict__ rec) {
+  const int a = blockIdx.x * kCT + threadIdx.x;
+  if (a >= nnodes) return;
+  const int A = agg[a];
+  double d[3] = {0.0, 0.0, 0.0};
+  int fm = 0;
+  for (int c = 0; c < dim; ++c) {
+    d[c] = (x[(int64_t)a * dim + c] - cen[(int64_t)A * dim + c]) * sinv;
+    if (fixed[(int64_t)a * dim + c]) fm |= 1 << c;
+  }
+  rec[a] = make_double4(d[0], d[1], d[2], (double)(A + (fm << 24)));
+}
+
+__device__ __forceinline__ double4 load_rec(const double4* __restrict__ rec, int b) {
+  const double2* r = reinterpret_cast<const double2*>(rec + b);
+  const double2 lo = __ldg(r), hi = __ldg(r + 1);
+  return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
 
 // Entry (c, m) of the P row of a dof with scaled offset d (the entries of p_row one at a
-// time; with c and m compile-time constants it folds to 0, 1 or +-d).
+// time).
 template <int DIM>
 __device__ __forceinline__ double p_entry(int c, int m, const double* d) {
   if (m < DIM) return m == c ? 1.0 : 0.0;
@@ -332,151 +359,137 @@ __device__ __forceinline__ double p_entry(int c, int m, const double* d) {
   return c == 0 ? -d[1] : c == 1 ? d[0] : 0.0;
 }
 
-template <int DIM, int NM>
-__device__ __forceinline__ void warp_sum_rows(double (&v)[DIM][NM]) {
-#pragma unroll
-  for (int c = 0; c < DIM; ++c)
-#pragma unroll
-    for (int m = 0; m < NM; ++m)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v[c][m] += __shfl_down_sync(0xffffffffu, v[c][m], o);
+template <int DIM>
+constexpr size_t sell_coarse_smem() {
+  return (size_t)kSellSlots * DIM * (DIM == 2 ? 3 : 6) * kSellThreads * sizeof(double);
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(32 * kCW)
-k_coarse_rows_warp(int n, const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj,
-                   const double* __restrict__ K, const uint8_t* __restrict__ fixed,
-                   const int32_t* __restrict__ agg, const int32_t* __restrict__ off,
-                   const int32_t* __restrict__ nodes, const double* __restrict__ x,
-                   const double* __restrict__ cen, double sinv, int nc, int per,
+__global__ void __launch_bounds__(kSellThreads)
+k_coarse_rows_sell(int nnodes, const int64_t* __restrict__ off, const int32_t* __restrict__ width,
+                   const int32_t* __restrict__ bcol, const int32_t* __restrict__ perm,
+                   const double* __restrict__ val, const double4* __restrict__ rec, int nc,
                    double* __restrict__ Ac) {
   constexpr unsigned kFull = 0xffffffffu;
   constexpr int NM = DIM == 2 ? 3 : 6;
   constexpr int NMM = NM * NM;
-  __shared__ int ids[kTab];
-  __shared__ double tab[kTab][NMM];
-  __shared__ double wacc[kCW][NMM];
-  __shared__ double sbuf[kCW][DIM * NM][32];   // lane sums of other aggregates
-  const int A = blockIdx.x;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int qend = off[A + 1];
-  const int qb = off[A] + blockIdx.y * kCW * per;
-  if (qb >= qend) return;  // block-uniform: this aggregate has fewer chunks
-  for (int i = threadIdx.x; i < kTab; i += blockDim.x) ids[i] = -1;
-  for (int i = threadIdx.x; i < kTab * NMM; i += blockDim.x) (&tab[0][0])[i] = 0.0;
-  for (int i = threadIdx.x; i < kCW * NMM; i += blockDim.x) (&wacc[0][0])[i] = 0.0;
-  __syncthreads();
-  double cA[DIM];
+  constexpr int NS = DIM * NM;   // entries of a sum S (row c, mode m at c * NM + m)
+  extern __shared__ __align__(16) double csm[];   // [kSellSlots][NS][kSellThreads]
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int t = blockIdx.x * kSellThreads + tid;   // node slot
+  const bool live = t < nnodes;
+  const int a = live ? perm[t] : 0;
+  const double4 ra = load_rec(rec, a);
+  const int A = ((int)ra.w) & 0xffffff, fa = ((int)ra.w) >> 24;
+  double da[DIM];
+  da[0] = ra.x;
+  da[1] = ra.y;
+  if constexpr (DIM == 3) da[DIM - 1] = ra.z;
+  auto slot = [&](int sl, int k) -> double& { return csm[((size_t)sl * NS + k) * kSellThreads + tid]; };
+  int key[kSellSlots];
 #pragma unroll
-  for (int c = 0; c < DIM; ++c) cA[c] = cen[(int64_t)A * DIM + c];
-  // lane 0: T = P_a^T S added to the warp's (A, A) partial or to the table entry of B
-  auto add_block = [&](const double (&S)[DIM][NM], const double (&da)[DIM], int ra, int B) {
-    bool fa[DIM];
+  for (int i = 0; i < kSellSlots; ++i) key[i] = -1;
+  // P_a^T S of slot sl added to block (A, B) of Ac
+  auto flush = [&](int sl, int B) {
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) fa[c] = fixed[ra + c] != 0;
-    const int sl = B == A ? -1 : tab_slot(ids, B);
-#pragma unroll
-    for (int m = 0; m < NM; ++m) {
-      double pm[DIM];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) pm[c] = fa[c] ? 0.0 : p_entry<DIM>(c, m, da);
+    for (int m = 0; m < NM; ++m)
 #pragma unroll
       for (int m2 = 0; m2 < NM; ++m2) {
         double v = 0.0;
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) v += pm[c] * S[c][m2];
-        if (B == A) wacc[warp][m * NM + m2] += v;
-        else if (v != 0.0) {
-          if (sl >= 0) atomicAdd(&tab[sl][m * NM + m2], v);
-          else atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
-        }
+        for (int c = 0; c < DIM; ++c)
+          if (!((fa >> c) & 1)) v += p_entry<DIM>(c, m, da) * slot(sl, c * NM + m2);
+        if (v != 0.0) atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
       }
-    }
   };
-  for (int t = 0; t < per; ++t) {
-    const int q = qb + t * kCW + warp;
-    if (q >= qend) break;  // warp-uniform
-    const int a = nodes[q];
-    const int ra = a * DIM;
-    double da[DIM];
+  double Sacc[NS];
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) da[c] = (x[(int64_t)ra + c] - cA[c]) * sinv;
-    const int p0 = adj_off[a], np = adj_off[a + 1] - p0;
-    double Sacc[DIM][NM];
+  for (int k = 0; k < NS; ++k) Sacc[k] = 0.0;
+  if (live) {
+    const int k = t >> 5;
+    const int64_t o = off[k];
+    const int w = width[k];
+    const int32_t* bc = bcol + o + lane;
+    const double* vb = val + o * DIM * DIM + lane;
+    for (int p = 0; p < w; ++p) {
+      const int b = __ldg(bc + 32 * p);
+      double kv[DIM][DIM];
 #pragma unroll
-    for (int c = 0; c < DIM; ++c)
+      for (int c = 0; c < DIM; ++c)
 #pragma unroll
-      for (int m = 0; m < NM; ++m) Sacc[c][m] = 0.0;
-    for (int pb = 0; pb < np; pb += 32) {  // warp-uniform trip count
-      const int p = pb + lane;
-      const bool valid = p < np;
-      int B = -1;
-      if (valid) {
-        const int b = adj[p0 + p];
-        B = agg[b];
-        double db[DIM];
-#pragma unroll
-        for (int c = 0; c < DIM; ++c)
-          db[c] = (x[(int64_t)b * DIM + c] - cen[(int64_t)B * DIM + c]) * sinv;
-        double Sb[DIM][NM];
-#pragma unroll
-        for (int c = 0; c < DIM; ++c)
-#pragma unroll
-          for (int m = 0; m < NM; ++m) Sb[c][m] = 0.0;
+        for (int c2 = 0; c2 < DIM; ++c2)
+          kv[c][c2] = __ldg(vb + (int64_t)((p * DIM + c) * DIM + c2) * 32);
+      const double4 rb = load_rec(rec, b);
+      const int wb = (int)rb.w;
+      const int B = wb & 0xffffff, fb = wb >> 24;
+      double db[DIM];
+      db[0] = rb.x;
+      db[1] = rb.y;
+      if constexpr (DIM == 3) db[DIM - 1] = rb.z;
+      if (B == A) {
 #pragma unroll
         for (int c2 = 0; c2 < DIM; ++c2) {
-          if (fixed[b * DIM + c2]) continue;
+          if ((fb >> c2) & 1) continue;
 #pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            const double kv = __ldg(K + (int64_t)(p * DIM + c2) * n + ra + c);
+          for (int c = 0; c < DIM; ++c)
 #pragma unroll
-            for (int m = 0; m < NM; ++m) Sb[c][m] += kv * p_entry<DIM>(c2, m, db);
+            for (int m = 0; m < NM; ++m) Sacc[c * NM + m] += kv[c][c2] * p_entry<DIM>(c2, m, db);
+        }
+      } else {
+        // the slot of B: an existing one, a free one, or slot 0 after flushing it
+        int sl = -1;
+#pragma unroll
+        for (int i = 0; i < kSellSlots; ++i)
+          if (sl < 0 && key[i] == B) sl = i;
+        if (sl < 0) {
+#pragma unroll
+          for (int i = 0; i < kSellSlots; ++i)
+            if (sl < 0 && key[i] < 0) sl = i;
+          if (sl < 0) {
+            flush(0, key[0]);
+            sl = 0;
           }
+          key[sl] = B;
+#pragma unroll
+          for (int q = 0; q < NS; ++q) slot(sl, q) = 0.0;
         }
-        if (B == A) {
-#pragma unroll
-          for (int c = 0; c < DIM; ++c)
-#pragma unroll
-            for (int m = 0; m < NM; ++m) Sacc[c][m] += Sb[c][m];
-        } else {
-#pragma unroll
-          for (int c = 0; c < DIM; ++c)
-#pragma unroll
-            for (int m = 0; m < NM; ++m) sbuf[warp][c * NM + m][lane] = Sb[c][m];
-        }
-      }
-      // neighbours in other aggregates: one warp sum per distinct B among the lanes
-      unsigned rem = __ballot_sync(kFull, valid && B != A);
-      __syncwarp();
-      while (rem) {
-        const int Bl = __shfl_sync(kFull, B, __ffs(rem) - 1);
-        const bool sel = valid && B == Bl;
-        rem &= ~__ballot_sync(kFull, sel);
-        double v[DIM][NM];
 #pragma unroll
         for (int c = 0; c < DIM; ++c)
 #pragma unroll
-          for (int m = 0; m < NM; ++m) v[c][m] = sel ? sbuf[warp][c * NM + m][lane] : 0.0;
-        warp_sum_rows<DIM, NM>(v);
-        if (lane == 0) add_block(v, da, ra, Bl);
+          for (int m = 0; m < NM; ++m) {
+            double v = 0.0;
+#pragma unroll
+            for (int c2 = 0; c2 < DIM; ++c2)
+              if (!((fb >> c2) & 1)) v += kv[c][c2] * p_entry<DIM>(c2, m, db);
+            slot(sl, c * NM + m) += v;
+          }
       }
-      __syncwarp();
     }
-    warp_sum_rows<DIM, NM>(Sacc);
-    if (lane == 0) add_block(Sacc, da, ra, A);
+#pragma unroll
+    for (int i = 0; i < kSellSlots; ++i)
+      if (key[i] >= 0) flush(i, key[i]);
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < NMM; e += blockDim.x) {
-    double v = 0.0;
-    for (int w = 0; w < kCW; ++w) v += wacc[w][e];
-    atomicAdd(&Ac[(int64_t)(A * NM + e / NM) * nc + A * NM + e % NM], v);
-  }
-  for (int e = threadIdx.x; e < kTab * NMM; e += blockDim.x) {
-    const int sl = e / NMM, B = ids[sl];
-    if (B < 0) continue;
-    const int m = (e % NMM) / NM, m2 = e % NM;
-    const double v = tab[sl][e % NMM];
-    if (v != 0.0) atomicAdd(&Ac[(int64_t)(A * NM + m) * nc + B * NM + m2], v);
+  // (A, A): P_a^T S_A summed over the lanes of equal A
+  unsigned pending = __ballot_sync(kFull, live);
+  while (pending) {
+    const int src = __ffs(pending) - 1;
+    const int Al = __shfl_sync(kFull, A, src);
+    const bool sel = live && A == Al;
+    pending &= ~__ballot_sync(kFull, sel);
+#pragma unroll
+    for (int m = 0; m < NM; ++m)
+#pragma unroll
+      for (int m2 = 0; m2 < NM; ++m2) {
+        double v = 0.0;
+        if (sel) {
+#pragma unroll
+          for (int c = 0; c < DIM; ++c)
+            if (!((fa >> c) & 1)) v += p_entry<DIM>(c, m, da) * Sacc[c * NM + m2];
+        }
+#pragma unroll
+        for (int o2 = 16; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(kFull, v, o2);
+        if (lane == src) atomicAdd(&Ac[(int64_t)(Al * NM + m) * nc + Al * NM + m2], v);
+      }
   }
 }
 
@@ -507,93 +520,47 @@ __global__ void k_regularise(int nc, const double* __restrict__ dmax, double eps
 //   A_PP <- A_PP^-1,  A_PR <- A_PP^-1 A_PR,  A_RP <- -A_RP A_PP^-1,
 //   A_RR <- A_RR - A_RP A_PP^-1 A_PR
 // After a sweep over every block A holds its inverse.  Three kernels per block:
-// the pivot block's inverse (one CTA), the two panels, and the rank-kGJ update.
-constexpr int kGJ = 32;
+// the pivot block's inverse (one CTA), the two panels, and the rank-kGJ update; the
+// panels and the update are 64 x 64 output tiles of 64-deep products (4 x 4 outputs per
+// thread from shared-memory operands), so every pass over A does 64 FMAs per entry.
+constexpr int kGJ = 64;
+constexpr int kGT = 64;                 // output tile side
+constexpr int kGJRows = 16;             // pivot CTA: kGJ x kGJRows threads, 4 rows each
+constexpr size_t kGJSmem = sizeof(double) * ((size_t)kGT * (kGJ + 1) + (size_t)kGJ * kGT);
 
-// Pi = A_PP^-1 by scalar sweeps in shared memory (bs <= 32; one thread per entry)
-__global__ void __launch_bounds__(kGJ * kGJ)
+// Pi = A_PP^-1 by scalar sweeps in shared memory (bs <= kGJ)
+__global__ void __launch_bounds__(kGJ * kGJRows)
 k_gj_pivot(int nc, int kb, int bs, const double* __restrict__ A, double* __restrict__ Pi) {
   __shared__ double M[kGJ][kGJ + 1];
-  __shared__ double row[kGJ], col[kGJ];
-  const int i = threadIdx.y, j = threadIdx.x;
-  if (i < bs && j < bs) M[i][j] = A[(int64_t)(kb + i) * nc + kb + j];
+  __shared__ double row[kGJ], col[kGJ], piv;
+  const int j = threadIdx.x, i0 = threadIdx.y;
+  for (int i = i0; i < kGJ; i += kGJRows)
+    M[i][j] = (i < bs && j < bs) ? A[(int64_t)(kb + i) * nc + kb + j] : 0.0;
   __syncthreads();
   for (int k = 0; k < bs; ++k) {
-    if (i == 0 && j < bs) row[j] = M[k][j];
-    if (j == 0 && i < bs) col[i] = M[i][k];
+    if (i0 == 0) row[j] = M[k][j];
+    if (i0 == 1) col[j] = M[j][k];
+    if (i0 == 2 && j == 0) piv = 1.0 / M[k][k];   // one division per step
     __syncthreads();
-    if (i < bs && j < bs) {
-      const double p = 1.0 / row[k];
-      double v;
-      if (i == k && j == k) v = p;
-      else if (i == k) v = row[j] * p;
-      else if (j == k) v = -col[i] * p;
-      else v = M[i][j] - col[i] * row[j] * p;
-      M[i][j] = v;
-    }
+    const double p = piv;
+    if (j < bs)
+      for (int i = i0; i < bs; i += kGJRows) {
+        double v;
+        if (i == k && j == k) v = p;
+        else if (i == k) v = row[j] * p;
+        else if (j == k) v = -col[i] * p;
+        else v = M[i][j] - col[i] * row[j] * p;
+        M[i][j] = v;
+      }
     __syncthreads();
   }
-  if (i < bs && j < bs) Pi[i * kGJ + j] = M[i][j];
+  for (int i = i0; i < kGJ; i += kGJRows) Pi[i * kGJ + j] = M[i][j];
 }
 
-// Rw[t][j] = sum_u Pi[t][u] A[kb+u][j]   (row panel, every column j)
-// Cold[i][t] = A[i][kb+t]; Cn[i][t] = -sum_u A[i][kb+u] Pi[u][t]   (column panel)
-__global__ void __launch_bounds__(128)
-k_gj_panels(int nc, int kb, int bs, const double* __restrict__ A, const double* __restrict__ Pi,
-            double* __restrict__ Rw, double* __restrict__ Cold, double* __restrict__ Cn) {
-  __shared__ double sP[kGJ][kGJ];
-  for (int e = threadIdx.x; e < kGJ * kGJ; e += 128) sP[e / kGJ][e % kGJ] = Pi[e];
-  __syncthreads();
-  const int t = blockIdx.x * 128 + threadIdx.x;
-  if (t >= nc) return;
-  if (blockIdx.y == 0) {
-    const int j = t;
-    double a[kGJ];
-#pragma unroll
-    for (int u = 0; u < kGJ; ++u) a[u] = u < bs ? A[(int64_t)(kb + u) * nc + j] : 0.0;
-#pragma unroll
-    for (int r = 0; r < kGJ; ++r) {
-      if (r >= bs) break;
-      double v = 0.0;
-#pragma unroll
-      for (int u = 0; u < kGJ; ++u) v += sP[r][u] * a[u];
-      Rw[(int64_t)r * nc + j] = v;
-    }
-  } else {
-    const int i = t;
-    double a[kGJ];
-#pragma unroll
-    for (int u = 0; u < kGJ; ++u) a[u] = u < bs ? A[(int64_t)i * nc + kb + u] : 0.0;
-#pragma unroll
-    for (int r = 0; r < kGJ; ++r) {
-      if (r >= bs) break;
-      double v = 0.0;
-#pragma unroll
-      for (int u = 0; u < kGJ; ++u) v += a[u] * sP[u][r];
-      Cold[(int64_t)i * kGJ + r] = a[r];
-      Cn[(int64_t)i * kGJ + r] = -v;
-    }
-  }
-}
-
-// Every entry (i, j): 64 x 64 tile per CTA, 4 x 4 per thread.
-constexpr int kGT = 64;
-__global__ void __launch_bounds__(256)
-k_gj_update(int nc, int kb, int bs, double* __restrict__ A, const double* __restrict__ Pi,
-            const double* __restrict__ Rw, const double* __restrict__ Cold,
-            const double* __restrict__ Cn) {
-  __shared__ double sC[kGT][kGJ + 1];  // Cold rows of this tile
-  __shared__ double sR[kGJ][kGT];      // Rw columns of this tile
-  const int i0 = blockIdx.y * kGT, j0 = blockIdx.x * kGT;
-  for (int e = threadIdx.x; e < kGT * kGJ; e += 256) {
-    const int r = e / kGJ, u = e % kGJ;
-    sC[r][u] = (i0 + r < nc && u < bs) ? Cold[(int64_t)(i0 + r) * kGJ + u] : 0.0;
-    const int u2 = e / kGT, c2 = e % kGT;
-    sR[u2][c2] = (j0 + c2 < nc && u2 < bs) ? Rw[(int64_t)u2 * nc + j0 + c2] : 0.0;
-  }
-  __syncthreads();
+// acc[a][b] = sum_u X[ty + 16a][u] Y[u][tx + 16b] over u < kGJ (X rows padded to kGJ + 1)
+__device__ __forceinline__ void gj_tile_product(const double (*X)[kGJ + 1],
+                                                const double (*Y)[kGT], double (&acc)[4][4]) {
   const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-  double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -602,14 +569,74 @@ k_gj_update(int nc, int kb, int bs, double* __restrict__ A, const double* __rest
   for (int u = 0; u < kGJ; ++u) {
     double cv[4], rv[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) cv[a] = sC[ty + 16 * a][u];
+    for (int a = 0; a < 4; ++a) cv[a] = X[ty + 16 * a][u];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) rv[b] = sR[u][tx + 16 * b];
+    for (int b = 0; b < 4; ++b) rv[b] = Y[u][tx + 16 * b];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] += cv[a] * rv[b];
   }
+}
+
+// blockIdx.y = 0: row panel Rw[r][j] = sum_u Pi[r][u] A[kb+u][j] for the 64 columns j0..
+// blockIdx.y = 1: column panel Cold[i][t] = A[i][kb+t], Cn[i][t] = -sum_u A[i][kb+u] Pi[u][t]
+__global__ void __launch_bounds__(256)
+k_gj_panels(int nc, int kb, int bs, const double* __restrict__ A, const double* __restrict__ Pi,
+            double* __restrict__ Rw, double* __restrict__ Cold, double* __restrict__ Cn) {
+  extern __shared__ __align__(16) double gsm[];
+  double (*X)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(gsm);
+  double (*Y)[kGT] = reinterpret_cast<double (*)[kGT]>(gsm + kGT * (kGJ + 1));
+  const int t0 = blockIdx.x * kGT;
+  const bool rowp = blockIdx.y == 0;
+  for (int e = threadIdx.x; e < kGT * kGJ; e += 256) {
+    const int r = e / kGJ, u = e % kGJ;      // X[r][u]
+    const int u2 = e / kGT, c2 = e % kGT;    // Y[u2][c2]
+    if (rowp) {
+      X[r][u] = Pi[r * kGJ + u];
+      Y[u2][c2] = (u2 < bs && t0 + c2 < nc) ? A[(int64_t)(kb + u2) * nc + t0 + c2] : 0.0;
+    } else {
+      X[r][u] = (u < bs && t0 + r < nc) ? A[(int64_t)(t0 + r) * nc + kb + u] : 0.0;
+      Y[u2][c2] = Pi[u2 * kGJ + c2];
+    }
+  }
+  __syncthreads();
+  double acc[4][4];
+  gj_tile_product(X, Y, acc);
+  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = ty + 16 * a, c = tx + 16 * b;
+      if (rowp) {
+        if (r < bs && t0 + c < nc) Rw[(int64_t)r * nc + t0 + c] = acc[a][b];
+      } else if (t0 + r < nc && c < bs) {
+        Cold[(int64_t)(t0 + r) * kGJ + c] = X[r][c];
+        Cn[(int64_t)(t0 + r) * kGJ + c] = -acc[a][b];
+      }
+    }
+}
+
+// Every entry (i, j): 64 x 64 tile per CTA, 4 x 4 per thread.
+__global__ void __launch_bounds__(256)
+k_gj_update(int nc, int kb, int bs, double* __restrict__ A, const double* __restrict__ Pi,
+            const double* __restrict__ Rw, const double* __restrict__ Cold,
+            const double* __restrict__ Cn) {
+  extern __shared__ __align__(16) double gsm[];
+  double (*sC)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(gsm);   // Cold rows
+  double (*sR)[kGT] = reinterpret_cast<double (*)[kGT]>(gsm + kGT * (kGJ + 1));  // Rw cols
+  const int i0 = blockIdx.y * kGT, j0 = blockIdx.x * kGT;
+  for (int e = threadIdx.x; e < kGT * kGJ; e += 256) {
+    const int r = e / kGJ, u = e % kGJ;
+    sC[r][u] = (i0 + r < nc && u < bs) ? Cold[(int64_t)(i0 + r) * kGJ + u] : 0.0;
+    const int u2 = e / kGT, c2 = e % kGT;
+    sR[u2][c2] = (j0 + c2 < nc && u2 < bs) ? Rw[(int64_t)u2 * nc + j0 + c2] : 0.0;
+  }
+  __syncthreads();
+  double acc[4][4];
+  gj_tile_product(sC, sR, acc);
+  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const int i = i0 + ty + 16 * a;
@@ -1011,10 +1038,11 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   double* d_Ac = nullptr;
   double *d_pi = nullptr, *d_rw = nullptr, *d_cold = nullptr, *d_cn = nullptr,
          *d_dmax = nullptr;
+  double4* d_rec = nullptr;   // per-node records of the slice coarse kernel
   auto cleanup2 = [&]() {
     cleanup();
     gf_pfree(ctx, d_Ac); gf_pfree(ctx, d_pi); gf_pfree(ctx, d_rw); gf_pfree(ctx, d_cold); gf_pfree(ctx, d_cn);
-    gf_pfree(ctx, d_dmax);
+    gf_pfree(ctx, d_dmax); gf_pfree(ctx, d_rec);
   };
   if ((st = gf_palloc(ctx, &C->node_agg, (size_t)nnodes)) != GF_OK ||
       (st = gf_palloc(ctx, &d_cnt, (size_t)na + 1)) != GF_OK ||
@@ -1079,19 +1107,24 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   for (int A = 0; A < na; ++A) maxcnt = std::max(maxcnt, hoff[A + 1] - hoff[A]);
   const int per = (int)((maxcnt + (int64_t)kCMT * 65535 - 1) / ((int64_t)kCMT * 65535));
   const dim3 gcm(na, (maxcnt + kCMT * per - 1) / (kCMT * per));
-  if (ctx->d_adj && ctx->d_adj_off) {
-    // mesh-built pattern: a warp per node over the node's adjacency list
-    const int pw = (int)((maxcnt + (int64_t)kCW * 65535 - 1) / ((int64_t)kCW * 65535));
-    const int perw = std::max(pw, 8);
-    const dim3 gw(na, (maxcnt + kCW * perw - 1) / (kCW * perw));
-    if (dim == 2)
-      k_coarse_rows_warp<2><<<gw, 32 * kCW, 0, s>>>(
-          n, ctx->d_adj_off, ctx->d_adj, ctx->d_K64, ctx->d_fixed, C->node_agg, C->agg_off,
-          C->agg_nodes, ctx->d_coords64, C->cen, sinv, nc, perw, d_Ac);
-    else
-      k_coarse_rows_warp<3><<<gw, 32 * kCW, 0, s>>>(
-          n, ctx->d_adj_off, ctx->d_adj, ctx->d_K64, ctx->d_fixed, C->node_agg, C->agg_off,
-          C->agg_nodes, ctx->d_coords64, C->cen, sinv, nc, perw, d_Ac);
+  if (ctx->d_adj && ctx->d_adj_off && na < (1 << 24) && gf_sell_prepare(ctx, GF_F64) == GF_OK &&
+      ctx->sell_bdim == dim && gf_palloc(ctx, &d_rec, (size_t)nnodes) == GF_OK) {
+    // node-block slices of the FP64 matrix: a thread per node slot, read like the SpMV
+    k_node_records<<<gf_blocks(nnodes, kCT), kCT, 0, s>>>(nnodes, dim, ctx->d_coords64,
+                                                          C->node_agg, C->cen, ctx->d_fixed,
+                                                          sinv, d_rec);
+    const int gsl = (nnodes + kSellThreads - 1) / kSellThreads;
+    if (dim == 2) {
+      GF_CUDA(ctx, gf_smem_attr(k_coarse_rows_sell<2>, sell_coarse_smem<2>()));
+      k_coarse_rows_sell<2><<<gsl, kSellThreads, sell_coarse_smem<2>(), s>>>(
+          nnodes, ctx->d_sell_off, ctx->d_sell_w, ctx->d_sell_col, ctx->d_sell_perm,
+          ctx->d_sell_v64, d_rec, nc, d_Ac);
+    } else {
+      GF_CUDA(ctx, gf_smem_attr(k_coarse_rows_sell<3>, sell_coarse_smem<3>()));
+      k_coarse_rows_sell<3><<<gsl, kSellThreads, sell_coarse_smem<3>(), s>>>(
+          nnodes, ctx->d_sell_off, ctx->d_sell_w, ctx->d_sell_col, ctx->d_sell_perm,
+          ctx->d_sell_v64, d_rec, nc, d_Ac);
+    }
   } else if (dim == 2) {
     k_coarse_rows<2><<<gcm, kCMT, 0, s>>>(n, ctx->d_rownnz, ctx->d_colidx, ctx->d_K64,
                                           ctx->d_fixed, C->node_agg, C->agg_off, C->agg_nodes,
@@ -1105,12 +1138,14 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   k_regularise<<<gf_blocks(nc, kCT), kCT, 0, s>>>(nc, d_dmax, 1e-10, d_Ac);
   ctx->launches += 8;
   // blocked Gauss-Jordan inverse
-  const dim3 gp((nc + 127) / 128, 2), gu((nc + kGT - 1) / kGT, (nc + kGT - 1) / kGT);
+  const dim3 gp((nc + kGT - 1) / kGT, 2), gu((nc + kGT - 1) / kGT, (nc + kGT - 1) / kGT);
+  GF_CUDA(ctx, gf_smem_attr(k_gj_panels, kGJSmem));
+  GF_CUDA(ctx, gf_smem_attr(k_gj_update, kGJSmem));
   for (int kb = 0; kb < nc; kb += kGJ) {
     const int bs = std::min(kGJ, nc - kb);
-    k_gj_pivot<<<1, dim3(kGJ, kGJ), 0, s>>>(nc, kb, bs, d_Ac, d_pi);
-    k_gj_panels<<<gp, 128, 0, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
-    k_gj_update<<<gu, 256, 0, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
+    k_gj_pivot<<<1, dim3(kGJ, kGJRows), 0, s>>>(nc, kb, bs, d_Ac, d_pi);
+    k_gj_panels<<<gp, 256, kGJSmem, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
+    k_gj_update<<<gu, 256, kGJSmem, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
     ctx->launches += 3;
   }
   std::vector<int2> hij;
