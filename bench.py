@@ -32,7 +32,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "elems/s assembled"
-SOLVERS = ["pcg_fp64", "mixed_pcg", "mixed_pcg32", "twolevel_pcg", "twolevel_pcg_k32", "learned"]
+SOLVERS = ["pcg_fp64", "mixed_pcg", "mixed_pcg32", "twolevel_pcg", "twolevel_pcg_k32",
+           "twolevel_pcg32", "learned"]
 UNIT = "elements/s"
 WORKLOADS = {
     # name: (description, dtype of the timed assembly)
@@ -280,6 +281,9 @@ SOLVER_TABLE = {
                      "FP64 PCG, M = Jacobi + rigid-body modes of box aggregates"),
     "twolevel_pcg_k32": ("GF_SOLVER_TWOLEVEL_PCG", "GF_F32", True,
                          "two-level PCG with K32 SpMVs, FP64 vectors, reliable updates on K64"),
+    "twolevel_pcg32": ("GF_SOLVER_TWOLEVEL_PCG32", "GF_F32", True,
+                       "two-level PCG with K32 SpMVs and FP32 vectors, FP64 dot products, "
+                       "reliable updates on K64"),
 }
 
 

@@ -24,7 +24,7 @@ GF_SCATTER_COLOR, GF_SCATTER_ATOMIC, GF_SCATTER_OWNER, GF_SCATTER_AUTO = 0, 1, 2
 GF_ENGINE_CUDA_CORE, GF_ENGINE_TF32_MMA = 0, 1
 GF_BC_PENALTY, GF_BC_ELIMINATION = 0, 1
 GF_SOLVER_CG, GF_SOLVER_PCG, GF_SOLVER_MIXED_PCG, GF_SOLVER_LEARNED_FCG, GF_SOLVER_MIXED_PCG32 = 0, 1, 2, 3, 4
-GF_SOLVER_TWOLEVEL_PCG = 5
+GF_SOLVER_TWOLEVEL_PCG, GF_SOLVER_TWOLEVEL_PCG32 = 5, 6
 GF_LP_LOSS_ERROR, GF_LP_LOSS_RESIDUAL = 0, 1
 
 

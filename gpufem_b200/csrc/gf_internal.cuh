@@ -408,6 +408,12 @@ void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q
 void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
                  double* x, double* r, double* p, const double* dinv, SolveScalars* sc,
                  float* p32 = nullptr);
+// The same two steps on FP32 vectors (r from the FP64 b; the scalars in FP64): the
+// direction itself is the FP32 operand of the SpMV on K32.
+void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
+                 float* x, float* r, float* p, const float* dinv, SolveScalars* sc);
+void gf_tl_iterate(gf_ctx* ctx, float* x, float* r, float* p, const float* q,
+                   const float* dinv, SolveScalars* sc);
 void gf_lp_mesh_changed(gf_ctx* ctx);
 gf_status gf_lp_prepare(gf_ctx* ctx);
 bool gf_lp_ready(const gf_ctx* ctx);

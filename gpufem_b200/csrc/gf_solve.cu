@@ -822,8 +822,10 @@ __global__ void k_mixed_scalars(SolveScalars* sc, double tol2) {
   sc->done = sc->iter >= sc->maxit ? 3 : 0;
 }
 
-// twolevel (V = double only): the two-level preconditioner (gf_twolevel.cu) in place of
-// Jacobi, in the recursion and at every reliable update.
+// twolevel: the two-level preconditioner (gf_twolevel.cu) in place of Jacobi, in the
+// recursion and at every reliable update.  V = double: FP64 vectors with an FP32 copy of
+// the direction for the K32 SpMV; V = float: FP32 vectors throughout the recursion (the
+// direction is the SpMV operand itself), with the dot products and scalars in FP64.
 template <typename V>
 gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
                     std::chrono::steady_clock::time_point t0, gf_solve_info* info,
@@ -845,8 +847,6 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
   if ((st = solver_matrix(ctx, GF_F32, &L32, &v32)) != GF_OK) return st;
   if ((st = solver_matrix(ctx, GF_F64, &L64, &v64)) != GF_OK) return st;
   const float* val32 = (const float*)v32;
-  if (twolevel && sizeof(V) != sizeof(double))
-    return gf_fail(ctx, GF_ERR_INVALID_ARG, "two-level mixed solve runs on FP64 vectors");
   if (twolevel && (st = gf_coarse_prepare(ctx, 0)) != GF_OK) return st;
   // FP32 copy of the FP64 direction for the K32 SpMV: the two-level recursion never
   // stores z, so its room holds it; Jacobi uses the work area past dinv (10 n doubles)
@@ -864,8 +864,10 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     double sigma = std::sqrt(ff);
     GF_CUDA(ctx, cudaMemsetAsync(sc, 0, sizeof(SolveScalars), s));
     if (twolevel) {
-      gf_tl_reset(ctx, r64, 1.0 / sigma, true, 1.0, (double*)x, (double*)r, (double*)p,
-                  (const double*)dinv, sc, p32);
+      if constexpr (sizeof(V) == sizeof(double))
+        gf_tl_reset(ctx, r64, 1.0 / sigma, true, 1.0, x, r, p, dinv, sc, p32);
+      else
+        gf_tl_reset(ctx, r64, 1.0 / sigma, true, 1.0, x, r, p, dinv, sc);
       GF_LAUNCH_CHECK(ctx, "gf_tl_reset");
     } else {
       k_scale_to<V><<<nb, kT, 0, s>>>(n, r64, 1.0 / sigma, q);  // q: scratch until K1
@@ -885,10 +887,13 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
     const int64_t l0 = ctx->launches;
     for (int k = 0; k < check; ++k) {
       if (twolevel) {
-        k_cg_spmv_dot_x32<<<mat_grid(ctx, L32), L32.threads, 0, s>>>(
-            L32, val32, p32, (const double*)p, (double*)q, sc);
-        gf_tl_iterate(ctx, (double*)x, (double*)r, (double*)p, (const double*)q,
-                      (const double*)dinv, sc, p32);
+        if constexpr (sizeof(V) == sizeof(double)) {
+          k_cg_spmv_dot_x32<<<mat_grid(ctx, L32), L32.threads, 0, s>>>(L32, val32, p32, p, q, sc);
+          gf_tl_iterate(ctx, x, r, p, q, dinv, sc, p32);
+        } else {
+          k_cg_spmv_dot<float, V><<<mat_grid(ctx, L32), L32.threads, 0, s>>>(L32, val32, p, q, sc);
+          gf_tl_iterate(ctx, x, r, p, q, dinv, sc);
+        }
       } else {
         if (p32)
           k_cg_spmv_dot_x32<<<mat_grid(ctx, L32), L32.threads, 0, s>>>(
@@ -956,10 +961,13 @@ gf_status run_mixed(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check,
       if (ce != cudaSuccess) { st = gf_cuda_fail(ctx, ce, "reset"); break; }
       // done flag and pq first: the two-level kernels skip their work while done != 0
       k_mixed_scalars<<<1, 1, 0, s>>>(sc, tol * tol * ff / rr64);
-      if (twolevel)
-        gf_tl_reset(ctx, r64, 1.0 / sigma_new, restart, sigma / sigma_new, (double*)x,
-                    (double*)r, (double*)p, (const double*)dinv, sc, p32);
-      else
+      if (twolevel) {
+        if constexpr (sizeof(V) == sizeof(double))
+          gf_tl_reset(ctx, r64, 1.0 / sigma_new, restart, sigma / sigma_new, x, r, p, dinv, sc,
+                      p32);
+        else
+          gf_tl_reset(ctx, r64, 1.0 / sigma_new, restart, sigma / sigma_new, x, r, p, dinv, sc);
+      } else
         k_mixed_reset<V><<<red_grid(ctx, n), kT, 0, s>>>(n, r64, 1.0 / sigma_new,
                                                          (V)(sigma / sigma_new), restart ? 1 : 0,
                                                          dinv, r, z, p, sc, p32);
@@ -1422,7 +1430,7 @@ gf_status run_twolevel(gf_ctx* ctx, const gf_solve_opts* o, int maxit, int check
 gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info) {
   *info = gf_solve_info{};
   const int solver = o->solver;
-  if (solver < GF_SOLVER_CG || solver > GF_SOLVER_TWOLEVEL_PCG)
+  if (solver < GF_SOLVER_CG || solver > GF_SOLVER_TWOLEVEL_PCG32)
     return gf_fail(ctx, GF_ERR_INVALID_ARG, "unknown solver %d", solver);
   if (!(o->tol > 0.0)) return gf_fail(ctx, GF_ERR_INVALID_ARG, "tol must be > 0");
   const int maxit = o->max_iter > 0 ? o->max_iter : 10000;
@@ -1440,6 +1448,11 @@ gf_status gf_solve_run(gf_ctx* ctx, const gf_solve_opts* o, gf_solve_info* info)
     return run_fcg(ctx, o, maxit, check, t0, info);
   }
 
+  if (solver == GF_SOLVER_TWOLEVEL_PCG32) {
+    if (!ctx->has64 || !ctx->has32)
+      return gf_fail(ctx, GF_ERR_STATE, "two-level PCG32 needs both FP64 and FP32 matrices");
+    return run_mixed<float>(ctx, o, maxit, check, t0, info, true);
+  }
   if (solver == GF_SOLVER_TWOLEVEL_PCG && o->matrix == GF_F32) {
     if (!ctx->has64 || !ctx->has32)
       return gf_fail(ctx, GF_ERR_STATE, "two-level PCG on K32 needs both FP64 and FP32 matrices");

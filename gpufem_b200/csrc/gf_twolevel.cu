@@ -672,11 +672,11 @@ __global__ void k_pack_tiles(int nc, const int2* __restrict__ ij, const double* 
 
 // rc = P^T r (and zc = 0 for the coarse product): block per aggregate over its node list
 constexpr int kRT = 256;
-template <int DIM>
+template <int DIM, typename V>
 __global__ void __launch_bounds__(kRT)
 k_restrict(const int32_t* __restrict__ off, const int32_t* __restrict__ nodes,
            const double* __restrict__ x, const double* __restrict__ cen, double sinv,
-           const uint8_t* __restrict__ fixed, const double* __restrict__ r,
+           const uint8_t* __restrict__ fixed, const V* __restrict__ r,
            double* __restrict__ rc, double* __restrict__ zc, const int* __restrict__ done) {
   constexpr int NM = DIM == 2 ? 3 : 6;
   __shared__ double ws[kRT / 32][NM];
@@ -696,7 +696,7 @@ k_restrict(const int32_t* __restrict__ off, const int32_t* __restrict__ nodes,
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
       if (fixed[a * DIM + c]) continue;
-      const double rv = r[a * DIM + c];
+      const double rv = (double)r[a * DIM + c];
       double pr[NM];
       p_row<DIM>(c, d, pr);
 #pragma unroll
@@ -853,13 +853,13 @@ k_prolong(int n, const int32_t* __restrict__ agg, const double* __restrict__ x,
 // atomics per aggregate, measured slower than the block-per-aggregate kernel: the
 // shuffles cost more than the second read of r.)
 
-// INIT: x = 0, r = scale * b (bq = b).  Else: alpha = rz / p.q, x += alpha p,
-// r -= alpha q (bq = q).  Accumulates rr = r.r and rzn += r.D^-1 r.
-template <bool INIT>
+// INIT: x = 0, r = scale * b.  Else: alpha = rz / p.q, x += alpha p, r -= alpha q.
+// Accumulates rr = r.r and rzn += r.D^-1 r (in FP64 whatever the vector type V).
+template <bool INIT, typename V>
 __global__ void __launch_bounds__(kCT)
-k_tl_update(int n, const double* __restrict__ bq, double scale, double* __restrict__ x,
-            double* __restrict__ r, const double* __restrict__ p, const double* __restrict__ dinv,
-            SolveScalars* sc) {
+k_tl_update(int n, const double* __restrict__ b, const V* __restrict__ q, double scale,
+            V* __restrict__ x, V* __restrict__ r, const V* __restrict__ p,
+            const V* __restrict__ dinv, SolveScalars* sc) {
   __shared__ double sh[32];
   double alpha = 0.0;
   if (!INIT) {
@@ -873,17 +873,18 @@ k_tl_update(int n, const double* __restrict__ bq, double scale, double* __restri
   }
   double rr = 0.0, rdr = 0.0;
   for (int i = blockIdx.x * kCT + threadIdx.x; i < n; i += gridDim.x * kCT) {
-    double ri;
+    V ri;
     if (INIT) {
-      ri = bq[i] * scale;
-      x[i] = 0.0;
+      ri = (V)(b[i] * scale);
+      x[i] = V(0);
     } else {
-      x[i] += alpha * p[i];
-      ri = r[i] - alpha * bq[i];
+      x[i] += (V)alpha * p[i];
+      ri = r[i] - (V)alpha * q[i];
     }
     r[i] = ri;
-    rr += ri * ri;
-    rdr += ri * ri * dinv[i];
+    const double rd = (double)ri;
+    rr += rd * rd;
+    rdr += rd * rd * (double)dinv[i];
   }
   const double s1 = cg_block_sum(rr, sh);
   if (threadIdx.x == 0) atomicAdd(&sc->rr, s1);
@@ -896,18 +897,18 @@ k_tl_update(int n, const double* __restrict__ bq, double scale, double* __restri
 // beta = rzn / rz, then the iteration count and the convergence test.  p32 (or null)
 // receives an FP32 copy of p for SpMVs on the FP32 matrix.
 constexpr int kTlFirst = 0, kTlKeep = 1, kTlStep = 2;
-template <int DIM, int MODE>
+template <int DIM, int MODE, typename V>
 __global__ void __launch_bounds__(kCT)
-k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ dinv,
+k_tl_direction(int n, const V* __restrict__ r, const V* __restrict__ dinv,
                const uint8_t* __restrict__ fixed, const int32_t* __restrict__ agg,
                const double* __restrict__ xc, const double* __restrict__ cen, double sinv,
-               const double* __restrict__ zc, double* __restrict__ p, float* __restrict__ p32,
+               const double* __restrict__ zc, V* __restrict__ p, float* __restrict__ p32,
                double pscale, SolveScalars* sc) {
   constexpr int NM = DIM == 2 ? 3 : 6;
   if (sc->done) return;
   if (MODE == kTlKeep) {
     for (int64_t t = (int64_t)blockIdx.x * kCT + threadIdx.x; t < n; t += (int64_t)gridDim.x * kCT) {
-      const double pn = p[t] * pscale;
+      const V pn = (V)((double)p[t] * pscale);
       p[t] = pn;
       if (p32) p32[t] = (float)pn;
     }
@@ -917,7 +918,7 @@ k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ d
   const int64_t stride = (int64_t)gridDim.x * kCT;
   for (int64_t t = (int64_t)blockIdx.x * kCT + threadIdx.x; t < n; t += stride) {
     const int i = (int)t;
-    double zi = dinv[i] * r[i];
+    double zi = (double)dinv[i] * (double)r[i];
     if (!fixed[i]) {
       const int a = i / DIM, c = i - a * DIM;
       const int A = agg[a];
@@ -930,7 +931,7 @@ k_tl_direction(int n, const double* __restrict__ r, const double* __restrict__ d
 #pragma unroll
       for (int m = 0; m < NM; ++m) zi += pr[m] * zc[A * NM + m];
     }
-    const double pn = MODE == kTlFirst ? zi : zi + beta * p[i];
+    const V pn = (V)(MODE == kTlFirst ? zi : zi + beta * (double)p[i]);
     p[i] = pn;
     if (p32) p32[i] = (float)pn;
   }
@@ -1205,14 +1206,14 @@ static void coarse_apply_impl(gf_ctx* ctx, const double* r, const double* dinv, 
   const double sinv = 1.0 / c->s;
   const int pb = std::min(gf_blocks(ctx->n, kCT), ctx->sm_count * 8);
   if (c->dim == 2) {
-    k_restrict<2><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
+    k_restrict<2, double><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
                                         ctx->d_fixed, r, c->rc, c->zc, done);
     k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, nullptr,
                                             nullptr, done);
     k_prolong<2><<<pb, kCT, 0, s>>>(ctx->n, c->node_agg, ctx->d_coords64, c->cen, sinv,
                                     ctx->d_fixed, dinv, r, c->zc, z, rz_acc, done, add);
   } else {
-    k_restrict<3><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
+    k_restrict<3, double><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
                                         ctx->d_fixed, r, c->rc, c->zc, done);
     k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, nullptr,
                                             nullptr, done);
@@ -1231,58 +1232,83 @@ void gf_coarse_add(gf_ctx* ctx, const double* r, double* z) {
   coarse_apply_impl(ctx, r, nullptr, z, nullptr, nullptr, 1);
 }
 
-template <int DIM>
-static void tl_launch(gf_ctx* ctx, int mode, const double* bq, double scale, double pscale,
-                      double* x, double* r, double* p, const double* dinv, SolveScalars* sc,
+template <int DIM, typename V>
+static void tl_launch(gf_ctx* ctx, int mode, const double* b, const V* q, double scale,
+                      double pscale, V* x, V* r, V* p, const V* dinv, SolveScalars* sc,
                       float* p32) {
   Coarse* c = static_cast<Coarse*>(ctx->coarse);
   cudaStream_t s = ctx->stream;
   const int n = ctx->n;
   const double sinv = 1.0 / c->s;
   const int grid = std::min(gf_blocks(n, kCT), ctx->sm_count * 8);
-  if (mode == kTlStep) k_tl_update<false><<<grid, kCT, 0, s>>>(n, bq, 1.0, x, r, p, dinv, sc);
-  else k_tl_update<true><<<grid, kCT, 0, s>>>(n, bq, scale, x, r, nullptr, dinv, sc);
-  k_restrict<DIM><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen, sinv,
-                                        ctx->d_fixed, r, c->rc, c->zc, &sc->done);
+  if (mode == kTlStep)
+    k_tl_update<false, V><<<grid, kCT, 0, s>>>(n, nullptr, q, 1.0, x, r, p, dinv, sc);
+  else
+    k_tl_update<true, V><<<grid, kCT, 0, s>>>(n, b, nullptr, scale, x, r, nullptr, dinv, sc);
+  k_restrict<DIM, V><<<c->na, kRT, 0, s>>>(c->agg_off, c->agg_nodes, ctx->d_coords64, c->cen,
+                                           sinv, ctx->d_fixed, r, c->rc, c->zc, &sc->done);
   k_coarse_symv<<<c->ntiles, 256, 0, s>>>(c->nc, c->tile_ij, c->ainv, c->rc, c->zc, c->counter,
                                           sc, &sc->done);
   const uint8_t* fx = ctx->d_fixed;
   if (mode == kTlFirst)
-    k_tl_direction<DIM, kTlFirst><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
-                                                       ctx->d_coords64, c->cen, sinv, c->zc, p,
-                                                       p32, 1.0, sc);
+    k_tl_direction<DIM, kTlFirst, V><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
+                                                          ctx->d_coords64, c->cen, sinv, c->zc,
+                                                          p, p32, 1.0, sc);
   else if (mode == kTlKeep)
-    k_tl_direction<DIM, kTlKeep><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
-                                                      ctx->d_coords64, c->cen, sinv, c->zc, p,
-                                                      p32, pscale, sc);
+    k_tl_direction<DIM, kTlKeep, V><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
+                                                         ctx->d_coords64, c->cen, sinv, c->zc,
+                                                         p, p32, pscale, sc);
   else
-    k_tl_direction<DIM, kTlStep><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
-                                                      ctx->d_coords64, c->cen, sinv, c->zc, p,
-                                                      p32, 1.0, sc);
+    k_tl_direction<DIM, kTlStep, V><<<grid, kCT, 0, s>>>(n, r, dinv, fx, c->node_agg,
+                                                         ctx->d_coords64, c->cen, sinv, c->zc,
+                                                         p, p32, 1.0, sc);
   ctx->launches += 4;
+}
+
+template <typename V>
+static void tl_reset_impl(gf_ctx* ctx, const double* b, double scale, bool restart,
+                          double pscale, V* x, V* r, V* p, const V* dinv, SolveScalars* sc,
+                          float* p32) {
+  const int mode = restart ? kTlFirst : kTlKeep;
+  if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
+    tl_launch<2, V>(ctx, mode, b, nullptr, scale, pscale, x, r, p, dinv, sc, p32);
+  else
+    tl_launch<3, V>(ctx, mode, b, nullptr, scale, pscale, x, r, p, dinv, sc, p32);
+}
+
+template <typename V>
+static void tl_iterate_impl(gf_ctx* ctx, V* x, V* r, V* p, const V* q, const V* dinv,
+                            SolveScalars* sc, float* p32) {
+  if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
+    tl_launch<2, V>(ctx, kTlStep, nullptr, q, 1.0, 1.0, x, r, p, dinv, sc, p32);
+  else
+    tl_launch<3, V>(ctx, kTlStep, nullptr, q, 1.0, 1.0, x, r, p, dinv, sc, p32);
 }
 
 void gf_tl_begin(gf_ctx* ctx, const double* b, double* x, double* r, double* p,
                  const double* dinv, SolveScalars* sc, float* p32) {
-  gf_tl_reset(ctx, b, 1.0, true, 1.0, x, r, p, dinv, sc, p32);
+  tl_reset_impl<double>(ctx, b, 1.0, true, 1.0, x, r, p, dinv, sc, p32);
 }
 
 void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
                  double* x, double* r, double* p, const double* dinv, SolveScalars* sc,
                  float* p32) {
-  const int mode = restart ? kTlFirst : kTlKeep;
-  if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
-    tl_launch<2>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc, p32);
-  else
-    tl_launch<3>(ctx, mode, b, scale, pscale, x, r, p, dinv, sc, p32);
+  tl_reset_impl<double>(ctx, b, scale, restart, pscale, x, r, p, dinv, sc, p32);
+}
+
+void gf_tl_reset(gf_ctx* ctx, const double* b, double scale, bool restart, double pscale,
+                 float* x, float* r, float* p, const float* dinv, SolveScalars* sc) {
+  tl_reset_impl<float>(ctx, b, scale, restart, pscale, x, r, p, dinv, sc, nullptr);
 }
 
 void gf_tl_iterate(gf_ctx* ctx, double* x, double* r, double* p, const double* q,
                    const double* dinv, SolveScalars* sc, float* p32) {
-  if (static_cast<Coarse*>(ctx->coarse)->dim == 2)
-    tl_launch<2>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc, p32);
-  else
-    tl_launch<3>(ctx, kTlStep, q, 1.0, 1.0, x, r, p, dinv, sc, p32);
+  tl_iterate_impl<double>(ctx, x, r, p, q, dinv, sc, p32);
+}
+
+void gf_tl_iterate(gf_ctx* ctx, float* x, float* r, float* p, const float* q,
+                   const float* dinv, SolveScalars* sc) {
+  tl_iterate_impl<float>(ctx, x, r, p, q, dinv, sc, nullptr);
 }
 
 extern "C" GF_API gf_status gf_twolevel_setup(gf_ctx* ctx, int32_t target_coarse,

@@ -101,10 +101,13 @@ typedef enum gf_solver {
                                 down or stalls. Needs K64 and gf_lp_init.                 */
   GF_SOLVER_MIXED_PCG32 = 4, /* as MIXED_PCG with FP32 vectors as well (half the vector
                                 traffic; for moderately conditioned systems)              */
-  GF_SOLVER_TWOLEVEL_PCG = 5 /* PCG with the two-level preconditioner (gf_twolevel_setup);
+  GF_SOLVER_TWOLEVEL_PCG = 5, /* PCG with the two-level preconditioner (gf_twolevel_setup);
                                 needs a mesh-built pattern.  matrix = GF_F64: FP64 PCG on
                                 K64; GF_F32: SpMVs on K32 with FP64 vectors and reliable
                                 updates on K64 as in MIXED_PCG (needs K64 and K32)       */
+  GF_SOLVER_TWOLEVEL_PCG32 = 6 /* two-level PCG with the recursion in FP32 (K32 SpMVs, FP32
+                                vectors, FP64 dot products and scalars) and FP64 reliable
+                                updates r = f - K64 u; needs K64 and K32 (matrix ignored) */
 } gf_solver;
 
 typedef struct gf_solve_opts {

@@ -92,6 +92,32 @@ def test_twolevel_on_fp32_matrix_with_reliable_updates(oracle, name, scale):
     assert info.iterations <= 2 * info64.iterations + 10, (info.iterations, info64.iterations)
 
 
+@pytest.mark.parametrize("name,scale", CASES)
+def test_twolevel_fp32_recursion_with_reliable_updates(oracle, name, scale):
+    """GF_SOLVER_TWOLEVEL_PCG32: K32 SpMVs and FP32 vectors in the recursion, FP64 dot
+    products, residual replaced from K64: converges to the FP64 oracle solution."""
+    m = mg.workload(name, scale=scale)
+    ctx = _ctx(m)
+    ctx.convert_f64_to_f32()
+    rn, ci, v = oracle.assemble(m.elem_type, m.ngauss, m.coords, m.conn, m.E0, m.nu, E_elem=m.E)
+    v, f = oracle.eliminate(rn, ci, v, _fixed(m), m.f)
+    ustar, _ = oracle.cg(rn, ci, v, f, maxit=200000, eps=1e-13, precond=True)
+    info = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG32, _lib.GF_F32, tol=1e-10, max_iter=200000)
+    assert info.status == _lib.GF_OK and info.rel_residual <= 1e-10 and info.outer >= 2
+    u = ctx.solution()
+    assert np.linalg.norm(u - ustar) <= 1e-7 * np.linalg.norm(ustar)
+    info64 = ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG, _lib.GF_F64, tol=1e-10, max_iter=200000)
+    assert info.iterations <= 2 * info64.iterations + 10, (info.iterations, info64.iterations)
+
+
+def test_twolevel_fp32_recursion_needs_both_matrices():
+    m = mg.workload("brick8_128", scale=1 / 16)
+    ctx = _ctx(m)   # K64 only
+    with pytest.raises(_lib.GpufemError) as ei:
+        ctx.solve(_lib.GF_SOLVER_TWOLEVEL_PCG32, _lib.GF_F32, tol=1e-8)
+    assert ei.value.status == _lib.GF_ERR_STATE
+
+
 @pytest.mark.parametrize("name", ["ref_Q8", "ref_brick8", "ref_2bricks20", "ref_placa16_Q4"])
 def test_penalty_twolevel_matches_reference(name):
     """FEM::ApplyConstraint(PEN), then two-level PCG, against the reference's CG
