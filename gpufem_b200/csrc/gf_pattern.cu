@@ -390,18 +390,19 @@ k_node_pattern_warp(int nnodes, int nen, const int32_t* __restrict__ conn,
                       inc_loc, inc_slot, diagpos);
 }
 
-// Block per NB consecutive nodes after the pattern pass: the block's part of the compact
-// adjacency (adj_off[n0] .. adj_off[n0 + NB]) is gathered from the nodes' sorted lists in
-// adj_tmp (each node's at its incidence offset x nen) by a flat loop over the output range,
-// so every store coalesces, and kept in shared memory; rownnz and the column-major colidx
+// Block per NB consecutive nodes after the pattern pass: rownnz, the column-major colidx
 // rows (a thread per row; all threads walk the slots together, so each slot's column of
-// colidx is written by consecutive threads; slots past the row's length hold col = row)
-// are then written from there.  One read of the lists instead of one per output.
+// colidx is written by consecutive threads; slots past the row's length hold col = row) and
+// the block's part of the compact adjacency (adj_off[n0] .. adj_off[n0 + NB], a flat loop
+// over the output range, so every store coalesces), all from the nodes' sorted lists in
+// adj_tmp (each node's at its incidence offset x nen), staged in shared memory once.
+// FULL: the block's whole scratch run is staged with 16-byte loads (few slots per node:
+// 2-D meshes); else only the compact adjacency is gathered (many unused slots: Brick20).
 constexpr int kListsThreadsMax = 512;
 
 __host__ __device__ constexpr int lists_table_ints(int NB) { return (2 * (NB + 1) + 3) & ~3; }
 
-template <int DIM>
+template <int DIM, bool FULL>
 __global__ void __launch_bounds__(kListsThreadsMax)
 k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict__ inc_off,
             const int32_t* __restrict__ adj_off, const int32_t* __restrict__ adj_tmp,
@@ -410,7 +411,7 @@ k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict
   extern __shared__ __align__(16) int32_t lsm[];
   int32_t* sbase = lsm;             // NB + 1: each node's list start in adj_tmp, from S0
   int32_t* soff = lsm + NB + 1;     // NB + 1: adj_off of the block's nodes
-  int32_t* stage = lsm + lists_table_ints(NB);   // the block's compact adjacency
+  int32_t* stage = lsm + lists_table_ints(NB);
   const int n0 = blockIdx.x * NB;
   const int nb = min(NB, nnodes - n0);
   const int tid = threadIdx.x, bd = blockDim.x;
@@ -419,8 +420,19 @@ k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict
     sbase[j] = (__ldg(inc_off + n0 + j) - I0) * nen;
     soff[j] = __ldg(adj_off + n0 + j);
   }
-  __syncthreads();
   const int32_t* src = adj_tmp + (int64_t)I0 * nen;
+  if constexpr (FULL) {
+    // the run [I0 nen, inc_off[n0 + nb] nen) is 16-byte aligned when nen % 4 == 0
+    const int cnt = (__ldg(inc_off + n0 + nb) - I0) * nen;
+    if ((nen & 3) == 0) {
+      const int4* s4 = reinterpret_cast<const int4*>(src);
+      int4* d4 = reinterpret_cast<int4*>(stage);
+      for (int i = tid; i < cnt / 4; i += bd) d4[i] = __ldg(s4 + i);
+    } else {
+      for (int i = tid; i < cnt; i += bd) stage[i] = __ldg(src + i);
+    }
+  }
+  __syncthreads();
   // output word p of the block belongs to the last node j with soff[j] <= soff[0] + p
   const int A0 = soff[0], A = soff[nb] - A0;
   for (int p = tid; p < A; p += bd) {
@@ -429,15 +441,20 @@ k_lists_out(int nnodes, int NB, int n, int W, int nen, const int32_t* __restrict
       const int mid = (lo + hi + 1) >> 1;
       if (soff[mid] - A0 <= p) lo = mid; else hi = mid - 1;
     }
-    const int v = __ldg(src + sbase[lo] + (A0 + p - soff[lo]));
-    adj[A0 + p] = v;
-    stage[p] = v;
+    const int k = A0 + p - soff[lo];
+    if constexpr (FULL) {
+      adj[A0 + p] = stage[sbase[lo] + k];
+    } else {
+      const int v = __ldg(src + sbase[lo] + k);
+      adj[A0 + p] = v;
+      stage[p] = v;
+    }
   }
-  __syncthreads();
+  if constexpr (!FULL) __syncthreads();
   for (int r = tid; r < nb * DIM; r += bd) {
     const int j = r / DIM, row = n0 * DIM + r;
     const int m = soff[j + 1] - soff[j];
-    const int32_t* list = stage + (soff[j] - A0);
+    const int32_t* list = FULL ? stage + sbase[j] : stage + (soff[j] - A0);
     rownnz[row] = m * DIM;
 #pragma unroll 4
     for (int k = 0; k < W / DIM; ++k) {
@@ -676,14 +693,18 @@ gf_status gf_pattern_build(gf_ctx* ctx) {
   GF_TRY(gf_palloc(ctx, &ctx->d_rownnz, (size_t)n));
   GF_TRY(gf_palloc(ctx, &ctx->d_colidx, (size_t)slots));
   if (fused) {
-    // nodes per block: the staged lists (at most h_max words per node) within 48 KB
-    const int per_node = h_max;
+    // whole scratch runs staged when nodes have at most 32 element-node slots (measured on
+    // Q8 512: 85 against 97 us for the compact gather), else the compact lists (Brick20
+    // 64: 0.96 against 1.25 ms); nodes per block: the staged words within 48 KB
+    const bool full = (int64_t)h_maxval * nen <= 32;
+    const int per_node = full ? h_maxval * nen : h_max;
     int NB = 128;
     while (NB > 32 && (size_t)NB * per_node * sizeof(int32_t) > 48 * 1024) NB >>= 1;
     const size_t lsm = sizeof(int32_t) * ((size_t)lists_table_ints(NB) + (size_t)NB * per_node);
     const int nt = std::min(kListsThreadsMax, (NB * dim + 31) / 32 * 32);
     const int nblk = (nnodes + NB - 1) / NB;
-    auto kl = dim == 2 ? k_lists_out<2> : k_lists_out<3>;
+    auto kl = dim == 2 ? (full ? k_lists_out<2, true> : k_lists_out<2, false>)
+                       : (full ? k_lists_out<3, true> : k_lists_out<3, false>);
     GF_TRYC(gf_smem_attr(kl, lsm));
     if (nblk > 0)
       kl<<<nblk, nt, lsm, s>>>(nnodes, NB, n, ctx->W, nen, d_inc_off, ctx->d_adj_off, d_adjtmp,
