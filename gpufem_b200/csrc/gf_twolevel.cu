@@ -618,41 +618,111 @@ k_gj_panels(int nc, int kb, int bs, const double* __restrict__ A, const double* 
     }
 }
 
-// Every entry (i, j): 64 x 64 tile per CTA, 4 x 4 per thread.
-__global__ void __launch_bounds__(256)
+// Every entry (i, j): a 64 x 64 tile per CTA of four warps, each warp a 32 x 32 quarter
+// as 4 x 4 fragments of the FP64 tensor-core product mma.m8n8k4 (per lane: one A value
+// A[g][t], one B value B[t][g], two accumulators D[g][2t], D[g][2t + 1] with g = lane / 4,
+// t = lane % 4).  The Cold rows and Rw columns of the tile sit in shared memory with rows
+// of kGJ + 4 doubles (the fragment loads of a warp fall on distinct bank pairs).
+constexpr int kGU = kGJ + 4;   // shared row length (doubles) of the update's operand tiles
+constexpr size_t kGJUpdateSmem = sizeof(double) * 2 * (size_t)kGT * kGU;
+
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128)
 k_gj_update(int nc, int kb, int bs, double* __restrict__ A, const double* __restrict__ Pi,
             const double* __restrict__ Rw, const double* __restrict__ Cold,
             const double* __restrict__ Cn) {
   extern __shared__ __align__(16) double gsm[];
-  double (*sC)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(gsm);   // Cold rows
-  double (*sR)[kGT] = reinterpret_cast<double (*)[kGT]>(gsm + kGT * (kGJ + 1));  // Rw cols
+  double (*sC)[kGU] = reinterpret_cast<double (*)[kGU]>(gsm);               // [row][u]
+  double (*sR)[kGU] = reinterpret_cast<double (*)[kGU]>(gsm + kGT * kGU);   // [u][col]
   const int i0 = blockIdx.y * kGT, j0 = blockIdx.x * kGT;
-  for (int e = threadIdx.x; e < kGT * kGJ; e += 256) {
-    const int r = e / kGJ, u = e % kGJ;
-    sC[r][u] = (i0 + r < nc && u < bs) ? Cold[(int64_t)(i0 + r) * kGJ + u] : 0.0;
-    const int u2 = e / kGT, c2 = e % kGT;
-    sR[u2][c2] = (j0 + c2 < nc && u2 < bs) ? Rw[(int64_t)u2 * nc + j0 + c2] : 0.0;
+  const int tid = threadIdx.x;
+  if (bs == kGJ && i0 + kGT <= nc && j0 + kGT <= nc && (nc & 1) == 0) {
+    // full interior tile, rows of Rw 16-byte aligned: 16-byte loads, all in flight at once
+    constexpr int P = kGT * kGJ / 2 / 128;   // double pairs per thread and operand
+    double2 c[P], r[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      const int e = tid + 128 * k;            // pair index: row e / 32, pair e % 32
+      c[k] = __ldcg(reinterpret_cast<const double2*>(Cold + (int64_t)(i0 + e / 32) * kGJ) + e % 32);
+      r[k] = __ldcg(reinterpret_cast<const double2*>(Rw + (int64_t)(e / 32) * nc + j0) + e % 32);
+    }
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      const int e = tid + 128 * k;
+      sC[e / 32][2 * (e % 32)] = c[k].x;
+      sC[e / 32][2 * (e % 32) + 1] = c[k].y;
+      sR[e / 32][2 * (e % 32)] = r[k].x;
+      sR[e / 32][2 * (e % 32) + 1] = r[k].y;
+    }
+  } else {
+    for (int e = tid; e < kGT * kGJ; e += 128) {
+      const int r = e / kGJ, u = e % kGJ;
+      sC[r][u] = (i0 + r < nc && u < bs) ? Cold[(int64_t)(i0 + r) * kGJ + u] : 0.0;
+      const int u2 = e / kGT, c2 = e % kGT;
+      sR[u2][c2] = (j0 + c2 < nc && u2 < bs) ? Rw[(int64_t)u2 * nc + j0 + c2] : 0.0;
+    }
   }
   __syncthreads();
-  double acc[4][4];
-  gj_tile_product(sC, sR, acc);
-  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  double acc[4][4][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int i = i0 + ty + 16 * a;
+  for (int fm = 0; fm < 4; ++fm)
+#pragma unroll
+    for (int fn = 0; fn < 4; ++fn) acc[fm][fn][0] = acc[fm][fn][1] = 0.0;
+#pragma unroll 4
+  for (int k0 = 0; k0 < kGJ; k0 += 4) {
+    double a[4], b[4];
+#pragma unroll
+    for (int fm = 0; fm < 4; ++fm) a[fm] = sC[wr + fm * 8 + g][k0 + t4];
+#pragma unroll
+    for (int fn = 0; fn < 4; ++fn) b[fn] = sR[k0 + t4][wc + fn * 8 + g];
+#pragma unroll
+    for (int fm = 0; fm < 4; ++fm)
+#pragma unroll
+      for (int fn = 0; fn < 4; ++fn) dmma_m8n8k4(acc[fm][fn][0], acc[fm][fn][1], a[fm], b[fn]);
+  }
+  const bool plain = i0 + kGT <= nc && j0 + kGT <= nc && (nc & 1) == 0 &&
+                     (kb + bs <= i0 || kb >= i0 + kGT) && (kb + bs <= j0 || kb >= j0 + kGT);
+  if (plain) {
+    // no pivot row or column in the tile: 16-byte read-modify-writes of the entry pairs
+#pragma unroll
+    for (int fm = 0; fm < 4; ++fm) {
+      double2* row = reinterpret_cast<double2*>(A + (int64_t)(i0 + wr + fm * 8 + g) * nc + j0 + wc);
+#pragma unroll
+      for (int fn = 0; fn < 4; ++fn) {
+        double2 v = row[fn * 4 + t4];
+        v.x -= acc[fm][fn][0];
+        v.y -= acc[fm][fn][1];
+        row[fn * 4 + t4] = v;
+      }
+    }
+    return;
+  }
+#pragma unroll
+  for (int fm = 0; fm < 4; ++fm) {
+    const int i = i0 + wr + fm * 8 + g;
     if (i >= nc) continue;
     const bool ip = i >= kb && i < kb + bs;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int j = j0 + tx + 16 * b;
-      if (j >= nc) continue;
-      const bool jp = j >= kb && j < kb + bs;
-      double* dst = A + (int64_t)i * nc + j;
-      if (ip && jp) *dst = Pi[(i - kb) * kGJ + (j - kb)];
-      else if (ip) *dst = Rw[(int64_t)(i - kb) * nc + j];
-      else if (jp) *dst = Cn[(int64_t)i * kGJ + (j - kb)];
-      else *dst -= acc[a][b];
-    }
+    for (int fn = 0; fn < 4; ++fn)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = j0 + wc + fn * 8 + 2 * t4 + h;
+        if (j >= nc) continue;
+        const bool jp = j >= kb && j < kb + bs;
+        double* dst = A + (int64_t)i * nc + j;
+        if (ip && jp) *dst = Pi[(i - kb) * kGJ + (j - kb)];
+        else if (ip) *dst = Rw[(int64_t)(i - kb) * nc + j];
+        else if (jp) *dst = Cn[(int64_t)i * kGJ + (j - kb)];
+        else *dst -= acc[fm][fn][h];
+      }
   }
 }
 
@@ -1141,12 +1211,12 @@ gf_status build(gf_ctx* ctx, Coarse* C, int target) {
   // blocked Gauss-Jordan inverse
   const dim3 gp((nc + kGT - 1) / kGT, 2), gu((nc + kGT - 1) / kGT, (nc + kGT - 1) / kGT);
   GF_CUDA(ctx, gf_smem_attr(k_gj_panels, kGJSmem));
-  GF_CUDA(ctx, gf_smem_attr(k_gj_update, kGJSmem));
+  GF_CUDA(ctx, gf_smem_attr(k_gj_update, kGJUpdateSmem));
   for (int kb = 0; kb < nc; kb += kGJ) {
     const int bs = std::min(kGJ, nc - kb);
     k_gj_pivot<<<1, dim3(kGJ, kGJRows), 0, s>>>(nc, kb, bs, d_Ac, d_pi);
     k_gj_panels<<<gp, 256, kGJSmem, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
-    k_gj_update<<<gu, 256, kGJSmem, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
+    k_gj_update<<<gu, 128, kGJUpdateSmem, s>>>(nc, kb, bs, d_Ac, d_pi, d_rw, d_cold, d_cn);
     ctx->launches += 3;
   }
   std::vector<int2> hij;
