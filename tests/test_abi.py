@@ -81,3 +81,15 @@ def test_noalloc_maximum_matches_header():
     hdr = (ROOT / "include" / "gpufem_b200.h").read_text()
     m = re.search(r"#define\s+GF_PCG_NOALLOC_MAX_N\s+(\d+)", hdr)
     assert m and int(m.group(1)) == _lib.GF_PCG_NOALLOC_MAX_N
+
+
+def test_enum_values_match_header():
+    """Every GF_SOLVER_* / GF_SCATTER_* / GF_ENGINE_* / GF_BC_* / GF_LP_LOSS_* constant of
+    the Python binding equals the header's enumerator of the same name."""
+    from gpufem_b200 import _lib
+    hdr = (ROOT / "include" / "gpufem_b200.h").read_text()
+    found = dict((k, int(v)) for k, v in re.findall(
+        r"\b(GF_(?:SOLVER|SCATTER|ENGINE|BC|LP_LOSS)_[A-Z0-9_]+)\s*=\s*(\d+)", hdr))
+    assert "GF_SOLVER_TWOLEVEL_PCG32" in found
+    for name, value in found.items():
+        assert getattr(_lib, name) == value, name
