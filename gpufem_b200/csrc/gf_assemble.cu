@@ -36,15 +36,37 @@ namespace {
 
 constexpr int kThreads = 256;
 
-template <int ET, typename TC, bool ATOMIC>
+template <int ET, typename TC>
+constexpr size_t smem_bytes(int TE, int ngp) {
+  constexpr ElemInfo info = gf_elem_info(ET);
+  const size_t nTC = (size_t)ngp * info.dim * info.nen + ngp + (size_t)TE * info.nen * info.dim +
+                     (size_t)ngp * info.nen * info.dim * TE + (size_t)ngp * TE;
+  return nTC * sizeof(TC) + sizeof(int) * ((size_t)TE * info.nen + 2 * TE) +
+         sizeof(uint16_t) * (size_t)(info.nen * (info.nen + 1) / 2) + 16;
+}
+
+template <int ET, typename TC>
+constexpr int pick_tile(int ngp) {
+  // largest power of two <= 128 whose working set fits ~100 KB (2 CTAs per SM)
+  int TE = 128;
+  while (TE > 4 && smem_bytes<ET, TC>(TE, ngp) > 100 * 1024) TE >>= 1;
+  return TE;
+}
+
+// The Gauss-point count (NG1 per axis) and the tile of TE elements are compile-time, so the
+// Gauss loops unroll and every shared-memory offset is an immediate; the node pair of a
+// task comes from a table in shared memory.
+template <int ET, typename TC, bool ATOMIC, int NG1>
 __global__ void __launch_bounds__(kThreads)
-k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
-           const int32_t* __restrict__ conn, const double* __restrict__ coords,
-           const TC* __restrict__ Eel, const uint16_t* __restrict__ slotmap, int nelem, int n,
+k_assemble(const int32_t* __restrict__ elems, int count, const int32_t* __restrict__ conn,
+           const double* __restrict__ coords, const TC* __restrict__ Eel,
+           const uint16_t* __restrict__ slotmap, int nelem, int n,
            const AsmTables* __restrict__ tab, TC lam1, TC mu1, TC* __restrict__ K) {
   constexpr ElemInfo info = gf_elem_info(ET);
   constexpr int NEN = info.nen, DIM = info.dim;
   constexpr int NPAIR = NEN * (NEN + 1) / 2;
+  constexpr int ngp = DIM == 2 ? NG1 * NG1 : NG1 * NG1 * NG1;
+  constexpr int TE = pick_tile<ET, TC>(ngp);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TC* sdN = reinterpret_cast<TC*>(smem_raw);                 // ngp*DIM*NEN
   TC* sw = sdN + ngp * DIM * NEN;                            // ngp
@@ -54,6 +76,7 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   int* sconn = reinterpret_cast<int*>(swd + ngp * TE);       // TE*NEN
   int* sel = sconn + TE * NEN;                               // TE
   int* sflag = sel + TE;                                     // TE
+  uint16_t* spair = reinterpret_cast<uint16_t*>(sflag + TE); // NPAIR: i * 256 + j, i <= j
 
   const int tile0 = blockIdx.x * TE;
   const int nt = min(TE, count - tile0);
@@ -65,6 +88,12 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   for (int e = threadIdx.x; e < TE; e += kThreads) {
     sel[e] = e < nt ? elems[tile0 + e] : -1;
     sflag[e] = 0;
+  }
+  // pair index -> (i, j), i <= j, row-major upper triangle
+  for (int p = threadIdx.x; p < NPAIR; p += kThreads) {
+    int i = 0, q = p;
+    while (q >= NEN - i) { q -= NEN - i; ++i; }
+    spair[p] = (uint16_t)(i * 256 + i + q);
   }
   __syncthreads();
   // Element-local coordinates x_i - x_0, formed in FP64 before rounding: J depends
@@ -95,6 +124,7 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
     __syncthreads();
     for (int e = threadIdx.x; e < nt; e += kThreads) {
       float dmin = 3.4e38f, dmax = 0.f;
+#pragma unroll
       for (int g = 0; g < ngp; ++g) {
         dmin = fminf(dmin, float(swd[g * TE + e]));
         dmax = fmaxf(dmax, float(swd[g * TE + e]));
@@ -119,23 +149,23 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   for (int t = threadIdx.x; t < TE * NPAIR; t += kThreads) {
     const int e = t % TE;
     if (e >= nt) continue;
-    int p = t / TE;
-    // pair index -> (i, j), i <= j, row-major upper triangle
-    int i = 0;
-    while (p >= NEN - i) { p -= NEN - i; ++i; }
-    const int j = i + p;
+    const int ij = spair[t / TE];
+    const int i = ij >> 8, j = ij & 255;
     TC H[DIM][DIM];
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
 #pragma unroll
       for (int b = 0; b < DIM; ++b) H[a][b] = TC(0);
+    const TC* gI = sG + (i * DIM) * TE + e;
+    const TC* gJ = sG + (j * DIM) * TE + e;
+#pragma unroll
     for (int g = 0; g < ngp; ++g) {
       const TC w = swd[g * TE + e];
       TC gi[DIM], gj[DIM];
 #pragma unroll
       for (int c = 0; c < DIM; ++c) {
-        gi[c] = sG[((g * NEN + i) * DIM + c) * TE + e] * w;
-        gj[c] = sG[((g * NEN + j) * DIM + c) * TE + e];
+        gi[c] = gI[(g * NEN * DIM + c) * TE] * w;
+        gj[c] = gJ[(g * NEN * DIM + c) * TE];
       }
 #pragma unroll
       for (int a = 0; a < DIM; ++a)
@@ -174,49 +204,41 @@ k_assemble(const int32_t* __restrict__ elems, int count, int TE, int ngp,
   }
 }
 
-template <int ET, typename TC>
-size_t smem_bytes(int TE, int ngp) {
-  constexpr ElemInfo info = gf_elem_info(ET);
-  size_t nTC = (size_t)ngp * info.dim * info.nen + ngp + (size_t)TE * info.nen * info.dim +
-               (size_t)ngp * info.nen * info.dim * TE + (size_t)ngp * TE;
-  return nTC * sizeof(TC) + sizeof(int) * ((size_t)TE * info.nen + 2 * TE) + 16;
-}
-
-template <int ET, typename TC>
-int pick_tile(int ngp) {
-  // largest power of two <= 128 whose working set fits ~100 KB (2 CTAs per SM)
-  int TE = 128;
-  while (TE > 4 && smem_bytes<ET, TC>(TE, ngp) > 100 * 1024) TE >>= 1;
-  return TE;
-}
-
-template <int ET, typename TC>
-gf_status launch_et(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* K) {
-  const int TE = pick_tile<ET, TC>(ctx->ngp);
-  const size_t sm = smem_bytes<ET, TC>(TE, ctx->ngp);
+template <int ET, typename TC, int NG1>
+gf_status launch_et_ng(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* K) {
+  constexpr int DIM = gf_elem_info(ET).dim;
+  constexpr int ngp = DIM == 2 ? NG1 * NG1 : NG1 * NG1 * NG1;
+  constexpr int TE = pick_tile<ET, TC>(ngp);
+  constexpr size_t sm = smem_bytes<ET, TC>(TE, ngp);
   const double* coords = ctx->d_coords64;
   const TC* Eel = sizeof(TC) == 8 ? (const TC*)ctx->d_Eel : (const TC*)ctx->d_Eel32;
-  auto kc = k_assemble<ET, TC, false>;
-  auto ka = k_assemble<ET, TC, true>;
+  auto kc = k_assemble<ET, TC, false, NG1>;
+  auto ka = k_assemble<ET, TC, true, NG1>;
   GF_CUDA(ctx, gf_smem_attr(kc, (int)sm));
   GF_CUDA(ctx, gf_smem_attr(ka, (int)sm));
   if (scatter == GF_SCATTER_ATOMIC) {
     const int count = ctx->nelem;
     ka<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
-        ctx->d_allperm, count, TE, ctx->ngp, ctx->d_conn, coords, Eel, ctx->d_slotmap,
-        ctx->nelem, ctx->n, d_tab, TC(ctx->lam1), TC(ctx->mu1), K);
+        ctx->d_allperm, count, ctx->d_conn, coords, Eel, ctx->d_slotmap, ctx->nelem, ctx->n,
+        d_tab, TC(ctx->lam1), TC(ctx->mu1), K);
     GF_LAUNCH_CHECK(ctx, "k_assemble(atomic)");
   } else {
     for (int c = 0; c < ctx->ncolors; ++c) {
       const int c0 = ctx->color_off[c], count = ctx->color_off[c + 1] - c0;
       if (count == 0) continue;
       kc<<<(count + TE - 1) / TE, kThreads, sm, ctx->stream>>>(
-          ctx->d_perm + c0, count, TE, ctx->ngp, ctx->d_conn, coords, Eel, ctx->d_slotmap,
-          ctx->nelem, ctx->n, d_tab, TC(ctx->lam1), TC(ctx->mu1), K);
+          ctx->d_perm + c0, count, ctx->d_conn, coords, Eel, ctx->d_slotmap, ctx->nelem,
+          ctx->n, d_tab, TC(ctx->lam1), TC(ctx->mu1), K);
       GF_LAUNCH_CHECK(ctx, "k_assemble(colour)");
     }
   }
   return GF_OK;
+}
+
+template <int ET, typename TC>
+gf_status launch_et(gf_ctx* ctx, int scatter, const AsmTables* d_tab, TC* K) {
+  return ctx->ngauss == 2 ? launch_et_ng<ET, TC, 2>(ctx, scatter, d_tab, K)
+                          : launch_et_ng<ET, TC, 3>(ctx, scatter, d_tab, K);
 }
 
 template <typename TC>
