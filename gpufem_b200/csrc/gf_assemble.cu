@@ -152,25 +152,58 @@ k_assemble(const int32_t* __restrict__ elems, int count, const int32_t* __restri
     const int ij = spair[t / TE];
     const int i = ij >> 8, j = ij & 255;
     TC H[DIM][DIM];
-#pragma unroll
-    for (int a = 0; a < DIM; ++a)
-#pragma unroll
-      for (int b = 0; b < DIM; ++b) H[a][b] = TC(0);
     const TC* gI = sG + (i * DIM) * TE + e;
     const TC* gJ = sG + (j * DIM) * TE + e;
+    if constexpr (sizeof(TC) == 4) {
+      // FP32: columns 0 and 1 of each row of H two at a time (packed FMA)
+      float2 h01[DIM];
+      float h2[DIM];
 #pragma unroll
-    for (int g = 0; g < ngp; ++g) {
-      const TC w = swd[g * TE + e];
-      TC gi[DIM], gj[DIM];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        gi[c] = gI[(g * NEN * DIM + c) * TE] * w;
-        gj[c] = gJ[(g * NEN * DIM + c) * TE];
+      for (int a = 0; a < DIM; ++a) {
+        h01[a] = make_float2(0.f, 0.f);
+        h2[a] = 0.f;
       }
+#pragma unroll
+      for (int g = 0; g < ngp; ++g) {
+        const float w = swd[g * TE + e];
+        float gi[DIM], gj[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          gi[c] = gI[(g * NEN * DIM + c) * TE] * w;
+          gj[c] = gJ[(g * NEN * DIM + c) * TE];
+        }
+        const float2 gj01 = make_float2(gj[0], gj[1]);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          h01[a] = fma2(make_float2(gi[a], gi[a]), gj01, h01[a]);
+          if constexpr (DIM == 3) h2[a] = fmaf(gi[a], gj[2], h2[a]);
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        H[a][0] = h01[a].x;
+        H[a][1] = h01[a].y;
+        if constexpr (DIM == 3) H[a][DIM - 1] = h2[a];
+      }
+    } else {
 #pragma unroll
       for (int a = 0; a < DIM; ++a)
 #pragma unroll
-        for (int b = 0; b < DIM; ++b) H[a][b] += gi[a] * gj[b];
+        for (int b = 0; b < DIM; ++b) H[a][b] = TC(0);
+#pragma unroll
+      for (int g = 0; g < ngp; ++g) {
+        const TC w = swd[g * TE + e];
+        TC gi[DIM], gj[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          gi[c] = gI[(g * NEN * DIM + c) * TE] * w;
+          gj[c] = gJ[(g * NEN * DIM + c) * TE];
+        }
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) H[a][b] += gi[a] * gj[b];
+      }
     }
     TC tr = TC(0);
 #pragma unroll

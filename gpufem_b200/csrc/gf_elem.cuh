@@ -19,6 +19,18 @@ struct AsmTables {
 // red.global.add.v2.f32 for a 2-D node (its two rows start 8-byte aligned because n
 // is even), a v2 plus a scalar reduction for a 3-D node; FP64 and the colour schedule
 // (plain read-modify-write) go per value.
+// d = a * b + c on two FP32 lanes at once (packed single-precision FMA: two IEEE FMAs,
+// round to nearest, in one instruction)
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
 __device__ inline void red_v2_f32(float* p, float a, float b) {
   asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
 }
