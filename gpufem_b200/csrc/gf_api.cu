@@ -6,6 +6,9 @@
 #include <cstring>
 #include <algorithm>
 #include <thread>
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 #include "gf_internal.cuh"
 
@@ -564,6 +567,18 @@ GF_API gf_status gf_ell_view(gf_ctx* ctx, int32_t dtype, int32_t* n, int32_t* wi
 
 extern "C++" {
 namespace {
+// Column words go to the caller's buffer with non-temporal stores where the host has them
+// (x86-64 movnti): the buffer is written once and not read back here, and plain stores
+// would first read every line they fill (write-allocate), doubling the host memory
+// traffic of the expansion.
+#if defined(__x86_64__) && !defined(__CUDA_ARCH__)
+inline void put_word(int32_t* p, int32_t v) { _mm_stream_si32(reinterpret_cast<int*>(p), v); }
+inline void put_fence() { _mm_sfence(); }
+#else
+inline void put_word(int32_t* p, int32_t v) { *p = v; }
+inline void put_fence() {}
+#endif
+
 // Row lengths and column indices of a mesh-built ELL pattern from its node adjacency: the
 // rows of node a (components c) hold the dofs of a's sorted neighbour list, dim per
 // neighbour, then col = row in the padding slots.  Nodes [a0, a1) in chunks whose lists
@@ -587,14 +602,15 @@ void expand_pattern_dim(int n, int W, const int32_t* off, const int32_t* adj, in
         if (k < off[a + 1] - off[a]) {
           const int v = adj[off[a] + k] * DIM;
           for (int c = 0; c < DIM; ++c)
-            for (int r = 0; r < DIM; ++r) out[c][row + r] = v + c;
+            for (int r = 0; r < DIM; ++r) put_word(out[c] + row + r, v + c);
         } else {
           for (int c = 0; c < DIM; ++c)
-            for (int r = 0; r < DIM; ++r) out[c][row + r] = row + r;
+            for (int r = 0; r < DIM; ++r) put_word(out[c] + row + r, row + r);
         }
       }
     }
   }
+  put_fence();   // the stores are visible before the caller's join
 }
 
 void expand_pattern(int n, int W, int dim, const int32_t* off, const int32_t* adj, int a0,
