@@ -373,8 +373,8 @@ def solve_study(ctx, target, solvers, asm_seconds):
     return out
 
 
-def north_star_study(args, flush):
-    """Brick20 64^3 (the north-star workload): FP32 and FP64 assembly in every schedule,
+def brick20_study(args, flush):
+    """Brick20 64^3 (the solve-time target workload): FP32 and FP64 assembly in every schedule,
     then every solver to FP64-oracle relative error 1e-6 with totals against FP64
     Jacobi-PCG."""
     import torch
@@ -893,11 +893,11 @@ def run_gpu_arm(args):
     if not args.no_solve and rank == 0 and "learned" in solvers:
         learned = learned_comparison()
 
-    north_star = None
-    if (not args.no_solve and not args.no_north_star and rank == 0 and world == 1
+    brick20 = None
+    if (not args.no_solve and not args.no_brick20 and rank == 0 and world == 1
             and cfg == "q8_512"):
         ctx.close()                  # free the Q8 matrices before the Brick20 64^3 study
-        north_star = north_star_study(args, flush)
+        brick20 = brick20_study(args, flush)
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -938,7 +938,7 @@ def run_gpu_arm(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "solve": solve,
-            "north_star": north_star,
+            "brick20_64": brick20,
             "learned": learned,
             "cpu_baseline": cpu_baseline,
         }
@@ -970,7 +970,7 @@ def main():
     ap.add_argument("--learned-application", action="store_true",
                     help="time only one learned-preconditioner application against one FP64 "
                          "SpMV on the Brick8 48^3 mesh (untrained network) and print it")
-    ap.add_argument("--no-north-star", action="store_true",
+    ap.add_argument("--no-brick20", action="store_true",
                     help="skip the Brick20 64^3 assembly + solve study of the default run")
     ap.add_argument("--scatter", default="auto", choices=["owner", "colour", "atomic", "auto"])
     args = ap.parse_args()
