@@ -420,7 +420,7 @@ GF_API gf_status gf_mesh_create(gf_ctx* ctx, int32_t elem_type, int32_t nnodes,
   ctx->d_Eel32 = Eel32;
   ctx->d_f = f;
   ctx->d_fixed = fixed;
-  ctx->h_f.assign(n, 0.0);
+  ctx->h_f.clear();   // f = 0 (an empty host copy stands for zeros)
   ctx->has_mesh = true;
   return GF_OK;
 }
@@ -782,7 +782,7 @@ GF_API gf_status gf_ell_upload(gf_ctx* ctx, int32_t n, int32_t width, const int3
   if ((st = gf_palloc(ctx, &ctx->d_K32, total)) != GF_OK) return st;
   if ((st = gf_palloc(ctx, &ctx->d_f, (size_t)n)) != GF_OK) return st;
   if ((st = gf_palloc(ctx, &ctx->d_fixed, (size_t)n)) != GF_OK) return st;
-  ctx->h_f.assign(n, 0.0);
+  ctx->h_f.clear();   // f = 0 (an empty host copy stands for zeros)
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_f, 0, sizeof(double) * n, ctx->stream));
   GF_CUDA(ctx, cudaMemsetAsync(ctx->d_fixed, 0, n, ctx->stream));
   GF_CUDA(ctx, cudaMemcpyAsync(ctx->d_rownnz, rownnz, sizeof(int32_t) * n,

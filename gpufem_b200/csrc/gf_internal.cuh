@@ -244,7 +244,7 @@ struct gf_ctx {
 
   // loads / constraints
   double* d_f = nullptr;
-  std::vector<double> h_f;
+  std::vector<double> h_f;   // host copy of the force set by the caller; empty: f = 0
   std::vector<int32_t> h_supports;  // nsup*(dim+1)
   int nsup = 0;
   uint8_t* d_fixed = nullptr;       // per dof
